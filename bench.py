@@ -1,0 +1,420 @@
+#!/usr/bin/env python
+"""Benchmark of the interval sweep: intervals swept per second on B200.
+
+Default workload ("plain"): the GPU-scale plain configuration — 24 chromosomes with lengths
+uniform in [50M, 250M] bp, a database of 1,000 files with rank-Zipf(1.1) sizes clamped to
+[1e3, 1e7] intervals summing to 2e9 (log-normal lengths, median 500 bp, sigma 1, clipped to
+[20, 100k], plus 5% log-uniform [10k, 1M] broad intervals), u32 start/end/file-id resident in HBM
+(~24 GB), and one query file of 1e5 intervals per step (a different seeded file every step).
+A step is one pass of the hot path: sort the query file, partition the candidate ranges, sweep and
+tally the 1 x 1000 count vector and overlap base pairs.
+
+"intervals swept" = query intervals + database intervals in the union of the reference's candidate
+ranges [q.start - layer_max_K, q.end) over all (shard, layer) (computed by the pipeline itself).
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl riggle|reference]
+       [--workload plain|config1]
+For N > 1 launch with torch.distributed.run: every rank holds a replica of the index and sweeps its
+own query files (weak scaling, no data-path collective); timing is the max over ranks.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "intervals swept/s (plain one-query-file-per-launch form, counts exact)"
+UNIT = "intervals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["riggle", "reference"], default="riggle")
+    ap.add_argument("--workload", choices=["plain", "config1"], default="plain")
+    ap.add_argument("--query-size", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--chunk", type=int, default=0)
+    ap.add_argument("--ctas-per-sm", type=int, default=0)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------------------------
+# workload definitions
+# ---------------------------------------------------------------------------------------------
+def workload_spec(name):
+    import riggle_b200 as rg
+
+    cl = rg.synth_chrom_lengths(1, 24)
+    if name == "plain":
+        sizes = rg.synth_zipf_sizes(1000, 1.1, 1000, 10_000_000, 2_000_000_000)
+        db = rg.SynthSpec(2, cl, sizes, broad_fraction=0.05)
+        qsize = 100_000
+        desc = {"workload": "plain GPU-scale sweep: 1,000-file Zipf(1.1) database, 2e9 intervals "
+                            "(5% broad 10k-1M bp), one 1e5-interval query file per launch",
+                "db_files": 1000, "db_intervals": int(sizes.sum()), "query_intervals_per_step": qsize,
+                "chromosomes": 24, "bin_size": 100, "layer_config": "min_size 128, growth_factor 4"}
+    else:
+        sizes = np.full(64, 50_000, np.uint64)
+        db = rg.SynthSpec(2, cl, sizes)
+        qsize = 10_000
+        desc = {"workload": "plain CPU-runnable sweep: 64-file database x 50k intervals, one 1e4-interval "
+                            "query file per launch",
+                "db_files": 64, "db_intervals": int(sizes.sum()), "query_intervals_per_step": qsize,
+                "chromosomes": 24, "bin_size": 100, "layer_config": "min_size 128, growth_factor 4"}
+    return cl, db, qsize, desc
+
+
+def query_file(cl, seed, qsize):
+    """One seeded query file as AoS (start, end, row=0) grouped by chromosome + shard offsets."""
+    import riggle_b200 as rg
+
+    q = rg.SynthSpec(seed, cl, [qsize])
+    blocks = [q.block(0, c) for c in range(len(cl))]
+    offs = np.zeros(len(cl) + 1, np.uint64)
+    for c, b in enumerate(blocks):
+        offs[c + 1] = offs[c] + len(b)
+    ivs = np.concatenate(blocks).astype(np.uint32)
+    ivs[:, 2] = 0
+    return np.ascontiguousarray(ivs), offs, blocks
+
+
+# ---------------------------------------------------------------------------------------------
+# clocks sampled during the timed region
+# ---------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per sweep launch from the committed ncu summary, when one exists."""
+    p = os.path.join(ROOT, "profiles", "k_sweep_plain.md")
+    try:
+        for ln in open(p):
+            if ln.startswith("traffic_bytes_per_launch:"):
+                return float(ln.split(":", 1)[1].strip().split()[0])
+    except Exception:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------------------------
+# CPU side: the oracle's restatement of the reference's query path on a bounded sample
+# ---------------------------------------------------------------------------------------------
+def sample_layers(db, chroms):
+    """Host-generated layers (and their jump tables) of the sampled chromosomes."""
+    import oracle as O
+
+    out = {}
+    for c in chroms:
+        layers = db.chrom_layers(c)
+        out[c] = (layers, O.jump_tables(layers))
+    return out
+
+
+def cpu_sample(db, layers_by_chrom, qblocks, threads, mode):
+    import oracle as O
+
+    swept = nq = 0
+    t = 0.0
+    for c, (layers, jumps) in layers_by_chrom.items():
+        q = qblocks[c]
+        t0 = time.perf_counter()
+        _, _, _, st = O.query_database(layers, {c: q}, 1, db.num_files, threads=threads, mode=mode, jumps=jumps)
+        t += time.perf_counter() - t0
+        swept += st["db_swept"]
+        nq += st["query_intervals"]
+    return swept + nq, t
+
+
+def pick_sample(cl, workload):
+    # the shortest chromosomes keep the CPU sample to tens of seconds
+    order = np.argsort(cl)
+    return [int(order[0])] if workload == "plain" else [int(x) for x in order[:6]]
+
+
+# ---------------------------------------------------------------------------------------------
+def run_reference(args, rank, world):
+    """The reference's CPU algorithm (the oracle's restatement; the Rust crate cannot be built on
+    this image) on the host cores, on a bounded sample of the same workload."""
+    if rank != 0:
+        return
+    cl, db, qsize, desc = workload_spec(args.workload)
+    qsize = args.query_size or qsize
+    cores = os.cpu_count() or 1
+    chroms = pick_sample(cl, args.workload)
+    sl = sample_layers(db, chroms)
+    vals = []
+    for step in range(args.warmup + args.steps):
+        _, _, blocks = query_file(cl, 1000 + step, qsize)
+        n, t = cpu_sample(db, sl, blocks, cores, 1)
+        if step >= args.warmup:
+            vals.append(n / t)
+    v = float(np.mean(vals))
+    sample = (f"chromosome(s) {[f'chr{c + 1}' for c in chroms]} of each step's query file against all "
+              f"database files, query-block parallel restatement of src/sweep/query.rs on {cores} threads")
+    out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)", "config": desc,
+           "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port", "sample": sample},
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def run_riggle(args, rank, world, local_rank, dist):
+    import torch
+
+    import riggle_b200 as rg
+    from riggle_b200 import _lib
+
+    lib = rg.load()
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    cl, db, qsize, desc = workload_spec(args.workload)
+    qsize = args.query_size or qsize
+    t0 = time.time()
+    idx = rg.Index.synth(db, device=dev)
+    build_s = time.time() - t0
+    ctx = rg.Context(idx)
+    D = idx.num_sources
+    nfiles = args.warmup + args.steps
+    files = [query_file(cl, 1000 + 7919 * rank + i, qsize) for i in range(nfiles)]
+    maxn = max(len(f[0]) for f in files)
+    ctx.reserve(maxn, 1)
+
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    shard_ids = np.arange(len(cl), dtype=np.uint32)
+    opts = _lib.QueryOpts(args.chunk, args.ctas_per_sm, 0, 0)
+    d_files = [torch.from_numpy(f[0].view(np.int32)).to(f"cuda:{dev}") for f in files]
+    d_counts = torch.zeros((1, D), dtype=torch.int32, device=f"cuda:{dev}")
+    d_bp = torch.zeros((1, D), dtype=torch.int64, device=f"cuda:{dev}")
+    torch.cuda.synchronize()
+
+    def dev_step(i, stats=None):
+        f = files[i]
+        _lib.check(lib.rgl_query_counts_device(ctx._h, 1, len(cl), C.c_void_p(shard_ids.ctypes.data),
+                                               C.c_void_p(f[1].ctypes.data), C.c_void_p(d_files[i].data_ptr()),
+                                               C.byref(opts), C.c_void_p(d_counts.data_ptr()),
+                                               C.c_void_p(d_bp.data_ptr()), C.byref(stats) if stats else None))
+
+    # per-file work (intervals swept) from one untimed pass with stats
+    swept = []
+    for i in range(nfiles):
+        st = _lib.QueryStats()
+        dev_step(i, st)
+        swept.append(st.db_swept + st.query_intervals)
+        if i == 0:
+            first_stats = st.as_dict()
+    work = np.array(swept, np.float64)
+
+    # ---- device-resident timing (value) ----
+    for i in range(args.warmup):
+        dev_step(i)
+    _lib.check(lib.rgl_context_check(ctx._h))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(dev)
+    clocks.start()
+    lib.rgl_context_set_timing(ctx._h, 1)
+    e0.record(stream)
+    for i in range(args.warmup, nfiles):
+        dev_step(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    sweep_ms = C.c_float()
+    launches = C.c_uint32()
+    _lib.check(lib.rgl_context_sweep_times(ctx._h, C.byref(sweep_ms), C.byref(launches)))
+    lib.rgl_context_set_timing(ctx._h, 0)
+    clk = clocks.stop()
+    _lib.check(lib.rgl_context_check(ctx._h))
+    ms = e0.elapsed_time(e1)
+    units = float(work[args.warmup:].sum())
+    if dist:
+        t = torch.tensor([ms, units], dtype=torch.float64, device=f"cuda:{dev}")
+        tmax = t.clone()
+        torch.distributed.all_reduce(tmax[:1], op=torch.distributed.ReduceOp.MAX)
+        tsum = t.clone()
+        torch.distributed.all_reduce(tsum[1:], op=torch.distributed.ReduceOp.SUM)
+        ms, units = float(tmax[0]), float(tsum[1])
+    value = units / (ms / 1e3)
+
+    # ---- end to end through the host C ABI with pinned buffers (e2e) ----
+    pin_q = []
+    for f in files:
+        p = C.c_void_p()
+        _lib.check(lib.rgl_host_alloc(f[0].nbytes, C.byref(p)))
+        C.memmove(p, f[0].ctypes.data, f[0].nbytes)
+        pin_q.append(p)
+    pc, pb = C.c_void_p(), C.c_void_p()
+    _lib.check(lib.rgl_host_alloc(D * 4, C.byref(pc)))
+    _lib.check(lib.rgl_host_alloc(D * 8, C.byref(pb)))
+
+    def host_step(i):
+        f = files[i]
+        sh = (_lib.QueryShard * len(cl))()
+        for c in range(len(cl)):
+            n = int(f[1][c + 1] - f[1][c])
+            sh[c] = _lib.QueryShard(None, c, n, C.c_void_p(pin_q[i].value + int(f[1][c]) * 12) if n else None)
+        batch = _lib.QueryBatch(1, len(cl), sh)
+        _lib.check(lib.rgl_query_counts(ctx._h, C.byref(batch), C.byref(opts), pc, pb, None))
+
+    for i in range(args.warmup):
+        host_step(i)
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for i in range(args.warmup, nfiles):
+        host_step(i)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ems = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ems], dtype=torch.float64, device=f"cuda:{dev}")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ems = float(t[0])
+    e2e = units / (ems / 1e3)
+    h2d = float(np.mean([f[0].nbytes for f in files[args.warmup:]]))
+
+    # ---- roofline of the sweep kernel ----
+    per_launch_ms = sweep_ms.value / max(1, launches.value)
+    # algorithmic bytes: 12 per swept DB interval (pos 8 + sid 4), 12 per query interval, 12 per output cell
+    qn = np.array([len(f[0]) for f in files[args.warmup:]], np.float64)
+    dbs = work[args.warmup:] - qn
+    alg_bytes = float(np.mean(12 * dbs + 12 * qn + 12 * D))
+    achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": profiled_traffic(), "kernel": "k_sweep", "peak_source": peak_kind,
+                "sweep_ms_per_launch": per_launch_ms, "algorithmic_bytes_per_launch": alg_bytes}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle  # noqa: F401  (builds the oracle if needed)
+
+        chroms = pick_sample(cl, args.workload)
+        n, t = cpu_sample(db, sample_layers(db, chroms), files[args.warmup][2], 1, 0)
+        cpu = {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{[f'chr{c + 1}' for c in chroms]} of one query file against all database files; "
+                         "restatement of query_database/query_sweep_windowed with the reference's parallel "
+                         "structure (one query file = one 64-row window = one thread)"}
+
+    own_launches = first_stats["kernel_launches"]
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+               "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+               "config": dict(desc, l2="database (24 GB) and per-step swept set exceed L2; a different query "
+                                        "file each step", parallelism=f"replicas x{world}" if world > 1 else "1 GPU",
+                              chunk=first_stats["chunk"], ctas_per_sm=first_stats["ctas_per_sm"]),
+               "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": D * 12,
+                       "ms_per_step": ems / args.steps},
+               "roofline": roofline, "cpu_baseline": cpu, "clocks": clk,
+               "gpu_launches": own_launches * args.steps,
+               "extra": {"index_build_s": build_s, "db_swept_first": first_stats["db_swept"],
+                         "ranges_first": first_stats["ranges"], "device_ms_first": first_stats["device_ms"],
+                         "sweep_ms_first": first_stats["sweep_ms"], "own_kernels_per_step": own_launches}}
+        print(json.dumps(out), flush=True)
+    for p in pin_q:
+        lib.rgl_host_free(p)
+    lib.rgl_host_free(pc)
+    lib.rgl_host_free(pb)
+    ctx.close()
+    idx.close()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+    dist = False
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = True
+    try:
+        run_riggle(args, rank, world, local_rank, dist)
+    finally:
+        if dist:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,264 @@
+/*
+ * riggle.h — C ABI of riggle_b200, a B200 (sm_100a) implementation of the file-to-file
+ * interval-sweep hot path of the `chuckle` crate (simondoesstuff/riggle).
+ *
+ * The ABI takes plain pointers and sizes only.  Each entry point names the reference interface it
+ * replaces (file:line inside the reference crate).  Host buffers are owned by the caller; device
+ * memory is owned by the handle that allocated it.  Every function returns an rgl_status; the
+ * detail of the last failure on the calling thread is available from rgl_last_error().
+ *
+ * Semantics kept from the reference:
+ *   - a query interval q and a database interval d overlap when
+ *       q.start - layer_max_size(K) (saturating) <= d.start < q.end  and  d.end > q.start
+ *     (src/sweep/query.rs:141-152, half-open intervals: touching ends do not overlap);
+ *   - counts are u32 per (query row, database source) and wrap modulo 2^32 as the reference's
+ *     release build does (src/matrix/dense.rs:42-45);
+ *   - the reference's f32 "overlap bins" (src/sweep/query.rs:154-156) are returned as exact u64
+ *     base pairs; bins = bp / bin_size.
+ */
+#ifndef RIGGLE_B200_H
+#define RIGGLE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------------------------ */
+/* Status codes.  Mirrors QueryError (src/tasks/query/mod.rs:26-38), LayerError                 */
+/* (src/io/layer.rs:11-23), MetaError (src/io/meta.rs:9-15), BedParseError                      */
+/* (src/io/parse.rs:22-38) and AddError (src/tasks/build.rs:18-32), plus device conditions.     */
+/* ------------------------------------------------------------------------------------------ */
+typedef enum rgl_status {
+    RGL_OK = 0,
+    RGL_ERR_INVALID_ARGUMENT = 1,
+    RGL_ERR_IO = 2,                          /* QueryError::Io, LayerError::Io, MetaError::Io */
+    RGL_ERR_BED_INVALID_FORMAT = 3,          /* BedParseError::InvalidFormat */
+    RGL_ERR_BED_INVALID_START = 4,           /* BedParseError::InvalidStart */
+    RGL_ERR_BED_INVALID_END = 5,             /* BedParseError::InvalidEnd */
+    RGL_ERR_BED_INVALID_RANGE = 6,           /* BedParseError::InvalidRange (start >= end) */
+    RGL_ERR_META_JSON = 7,                   /* MetaError::Json */
+    RGL_ERR_LAYER_INVALID_POSITION_SIZE = 8, /* LayerError::InvalidPositionSize */
+    RGL_ERR_LAYER_INVALID_SID_SIZE = 9,      /* LayerError::InvalidSidSize */
+    RGL_ERR_LAYER_SID_SIZE_MISMATCH = 10,    /* LayerError::SidSizeMismatch */
+    RGL_ERR_LAYER_INVALID_INDEX_SIZE = 11,   /* LayerError::InvalidIndexSize */
+    RGL_ERR_DATABASE_NOT_FOUND = 12,         /* QueryError::DatabaseNotFound */
+    RGL_ERR_INPUT_NOT_FOUND = 13,            /* AddError::InputNotFound */
+    RGL_ERR_NO_BED_FILES = 14,               /* AddError::NoBedFiles */
+    RGL_ERR_OOM = 15,                        /* device allocation failed / admission refused */
+    RGL_ERR_TIMEOUT = 16,                    /* a bounded device wait gave up */
+    RGL_ERR_DEVICE = 17,                     /* CUDA runtime error */
+    RGL_ERR_INDEX_INVARIANT = 18,            /* layer unsorted, or a source id >= num_sources */
+    RGL_ERR_NO_DEVICE = 19,                  /* no CUDA device visible */
+    RGL_ERR_UNSUPPORTED = 20
+} rgl_status;
+
+const char* rgl_status_str(int status);
+/* Detail of the last failure on this thread ("" when none). */
+const char* rgl_last_error(void);
+/* ABI version: major*10000 + minor*100 + patch. */
+int rgl_version(void);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Layer configuration — LayerConfig (src/io/meta.rs:23-90).  Pure host functions.             */
+/* ------------------------------------------------------------------------------------------ */
+/* LayerConfig::layer_for_size (src/io/meta.rs:33-58) */
+uint32_t rgl_layer_for_size(uint32_t min_size, uint32_t growth_factor, uint32_t size);
+/* LayerConfig::layer_max_size (src/io/meta.rs:64-73) */
+uint32_t rgl_layer_max_size(uint32_t min_size, uint32_t growth_factor, uint32_t layer);
+/* LayerConfig::tile_size (src/io/meta.rs:79-81) */
+uint32_t rgl_tile_size(uint32_t min_size, uint32_t growth_factor, uint32_t layer);
+
+/* Interval (src/core/mod.rs:11-17): 12-byte repr(C) {start, end, sid}. */
+typedef struct rgl_interval {
+    uint32_t start;
+    uint32_t end;
+    uint32_t sid;
+} rgl_interval;
+
+/* ------------------------------------------------------------------------------------------ */
+/* Device-resident database index.                                                              */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct rgl_index rgl_index;
+
+/* One (shard, layer) in the reference's on-disk layout (src/io/layer.rs:31-47):
+ * pos = layer_K.pos, `count` (start, end) u32 pairs sorted by start; sid = layer_K.sid. */
+typedef struct rgl_layer_desc {
+    uint32_t shard;
+    uint32_t layer;
+    uint64_t count;
+    const uint32_t* pos;
+    const uint32_t* sid;
+} rgl_layer_desc;
+
+typedef struct rgl_index_desc {
+    uint32_t min_size;      /* LayerConfig.min_size (default 128) */
+    uint32_t growth_factor; /* LayerConfig.growth_factor (default 4) */
+    uint32_t num_sources;   /* Meta::num_sources (src/io/meta.rs:142-144) = matrix columns */
+    uint32_t num_shards;
+    const char* const* shard_names; /* may be NULL: shards named by their index */
+    const char* const* source_names; /* may be NULL */
+    uint32_t num_layers;            /* number of entries in `layers` */
+    const rgl_layer_desc* layers;
+} rgl_index_desc;
+
+typedef struct rgl_index_info {
+    uint32_t num_sources;
+    uint32_t num_shards;
+    uint32_t num_layer_slots; /* highest layer index + 1 */
+    uint32_t num_layers;      /* non-empty (shard, layer) pairs */
+    uint64_t num_intervals;
+    uint64_t device_bytes;
+    int device;
+} rgl_index_info;
+
+/* Opens `db_dir` written by the reference's `add` (src/tasks/build.rs:86-128): meta.json
+ * (src/io/meta.rs:124-127) and shards/<shard>/layer_K.{pos,sid,idx} (src/io/layer.rs:51-78,
+ * src/io/jump.rs:225-237), with the reference's size checks, and uploads the layers to HBM.
+ * Replaces Meta::load + MappedLayer::open + MappedJumpTable::open in query_database
+ * (src/tasks/query/mod.rs:124-129, 205-233). */
+int rgl_index_open(const char* db_dir, int device, rgl_index** out);
+/* Same from caller-owned host arrays (copied to HBM). */
+int rgl_index_open_mem(const rgl_index_desc* desc, int device, rgl_index** out);
+int rgl_index_close(rgl_index* index);
+int rgl_index_get_info(const rgl_index* index, rgl_index_info* out);
+/* Shard id for a name (RGL_ERR_INVALID_ARGUMENT when absent, as the reference skips shards not in
+ * meta.shards: src/tasks/query/mod.rs:194-196). */
+int rgl_index_shard_id(const rgl_index* index, const char* name, uint32_t* out_id);
+const char* rgl_index_shard_name(const rgl_index* index, uint32_t shard);
+const char* rgl_index_source_name(const rgl_index* index, uint32_t sid);
+/* Number of intervals of (shard, layer) (0 when absent). */
+uint64_t rgl_index_layer_count(const rgl_index* index, uint32_t shard, uint32_t layer);
+/* Copies one (shard, layer) back to host arrays of its count (2*count pos words, count sids). */
+int rgl_index_export_layer(const rgl_index* index, uint32_t shard, uint32_t layer, uint32_t* pos, uint32_t* sid);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Query contexts and the sweep.                                                                 */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct rgl_context rgl_context;
+
+/* A context binds one index to one CUDA stream and owns a reusable device workspace (grown on
+ * demand, never shrunk).  `stream` is a cudaStream_t or NULL (the context creates its own). */
+int rgl_context_create(rgl_index* index, void* stream, rgl_context** out);
+int rgl_context_destroy(rgl_context* ctx);
+/* Pre-sizes the workspace for batches of up to max_intervals query intervals and max_rows rows,
+ * so later calls allocate nothing. */
+int rgl_context_reserve(rgl_context* ctx, uint64_t max_intervals, uint32_t max_rows);
+void* rgl_context_stream(rgl_context* ctx);
+
+/* Queries of one shard: the reference's `shard_intervals[shard]` after parsing
+ * (src/tasks/query/files.rs:40-111); `sid` of each interval is its query row (Q_SID).
+ * `shard_name` selects the shard by name; when NULL, `shard_id` is used. */
+typedef struct rgl_query_shard {
+    const char* shard_name;
+    uint32_t shard_id;
+    uint64_t count;
+    const rgl_interval* intervals;
+} rgl_query_shard;
+
+typedef struct rgl_query_batch {
+    uint32_t num_rows; /* batch_len: query rows (src/tasks/query/mod.rs:184) */
+    uint32_t num_shards;
+    const rgl_query_shard* shards;
+} rgl_query_batch;
+
+/* Launch shape.  0 = default / autotuned. */
+typedef struct rgl_query_opts {
+    uint32_t chunk;       /* DB positions per work item */
+    uint32_t ctas_per_sm; /* persistent CTAs per SM */
+    uint32_t block;       /* threads per CTA */
+    uint32_t flags;       /* RGL_QF_* */
+} rgl_query_opts;
+
+#define RGL_QF_NO_OVERLAP 1u /* skip base-pair accumulation (counts only) */
+
+typedef struct rgl_query_stats {
+    uint64_t query_intervals;  /* intervals in the batch (on shards present in the index) */
+    uint64_t db_swept;         /* DB intervals in the union of candidate ranges, all (shard, layer) */
+    uint64_t ranges;           /* merged candidate ranges */
+    uint64_t work_items;       /* work items pulled by the sweep kernel */
+    float sweep_ms;            /* sweep kernel time (CUDA events on the context stream) */
+    float device_ms;           /* whole device pipeline incl. sort/partition (CUDA events) */
+    uint32_t chunk, ctas_per_sm, block, kernel_launches;
+} rgl_query_stats;
+
+/* Replaces the counting path of query_database (src/tasks/query/mod.rs:182-307): the per-shard,
+ * per-64-row-window, per-layer calls to query_sweep_windowed (src/sweep/query.rs:127-160) and the
+ * window merge (add_submatrix_rows, src/matrix/dense.rs:75-86).  Host buffers: the batch is copied
+ * to HBM, `counts` (num_rows x num_sources u32, row-major) and `overlap_bp` (same shape, u64; may
+ * be NULL) are written on return.  Query intervals need start < end (the parser guarantees it,
+ * src/io/parse.rs:94-100) and sid < num_rows. */
+int rgl_query_counts(rgl_context* ctx, const rgl_query_batch* batch, const rgl_query_opts* opts, uint32_t* counts,
+                     uint64_t* overlap_bp, rgl_query_stats* stats);
+
+/* Device-resident variant: `d_intervals` (device, AoS) holds the shards back to back;
+ * shard_offsets (host, num_shards+1) delimit them; shard_ids (host) name each block's shard.
+ * d_counts / d_overlap_bp are device buffers.  Runs asynchronously on the context stream unless
+ * stats is non-NULL (stats need one synchronisation). */
+int rgl_query_counts_device(rgl_context* ctx, uint32_t num_rows, uint32_t num_shards, const uint32_t* shard_ids,
+                            const uint64_t* shard_offsets, const rgl_interval* d_intervals,
+                            const rgl_query_opts* opts, uint32_t* d_counts, uint64_t* d_overlap_bp,
+                            rgl_query_stats* stats);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Seeded synthetic workloads (no counterpart in the reference; used by tests and benchmarks).  */
+/* SplitMix64 counter streams (Steele, Lea & Flood 2014) drive identical host and device        */
+/* generators; lengths come from a host-built 65537-point quantile table.                       */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct rgl_synth_spec {
+    uint64_t seed;          /* per-dataset seed (files use seed + file index) */
+    uint32_t num_chroms;    /* chromosome count (names chr1..chr22, chrX, chrY for 24) */
+    const uint32_t* chrom_len;
+    uint32_t num_files;
+    const uint64_t* file_sizes; /* intervals per file */
+    double broad_fraction;      /* share of intervals with log-uniform[10k,1M] lengths */
+    double hotspot_fraction;    /* share placed in 1 Mbp hot spots */
+    uint32_t num_hotspots;      /* hot spots per file */
+    uint32_t sid_base;          /* sid of file 0 */
+} rgl_synth_spec;
+
+/* Chromosome lengths uniform in [50M, 250M] from `seed`. */
+int rgl_synth_chrom_lengths(uint64_t seed, uint32_t num_chroms, uint32_t* out);
+/* Rank-size Zipf file sizes clamp(round(C r^-s), lo, hi) with C chosen so the sum is ~target. */
+int rgl_synth_zipf_sizes(uint32_t num_files, double s, uint64_t lo, uint64_t hi, uint64_t target, uint64_t* out);
+/* Log-uniform file sizes in [lo, hi]. */
+int rgl_synth_loguniform_sizes(uint64_t seed, uint32_t num_files, uint64_t lo, uint64_t hi, uint64_t* out);
+/* Intervals of file f split over chromosomes (proportional split, largest remainder). */
+int rgl_synth_file_chrom_counts(const rgl_synth_spec* spec, uint32_t file, uint64_t* out_per_chrom);
+/* Host generation of one (file, chrom) block, sorted by (start, end); sid = sid_base + file. */
+int rgl_synth_block_host(const rgl_synth_spec* spec, uint32_t file, uint32_t chrom, rgl_interval* out,
+                         uint64_t capacity, uint64_t* out_count);
+/* Host generation of every file's intervals on one chromosome, bucketed into layers like the
+ * reference's add (src/tasks/build.rs:190-211): pos/sid are sorted by (layer, start) and
+ * layer_counts[K] (K < max_layers) gives each layer's length.  Call with pos = sid = NULL to get
+ * *out_total first. */
+int rgl_synth_chrom_layers_host(const rgl_synth_spec* spec, uint32_t chrom, uint32_t min_size, uint32_t growth_factor,
+                                uint64_t* layer_counts, uint32_t max_layers, uint32_t* pos, uint32_t* sid,
+                                uint64_t capacity, uint64_t* out_total);
+/* Builds an index in HBM directly from a spec (generation, bucketing by (shard, layer) and sort by
+ * start all on the device).  Same content as bucketing the host blocks. */
+int rgl_index_synth(const rgl_synth_spec* spec, uint32_t min_size, uint32_t growth_factor, int device,
+                    rgl_index** out);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Stream helpers, timing and pinned host memory (no counterpart in the reference).              */
+/* ------------------------------------------------------------------------------------------ */
+int rgl_context_sync(rgl_context* ctx);
+/* Synchronises the context stream and reports a query error raised by the last asynchronous
+ * rgl_query_counts_device call (invalid query intervals). */
+int rgl_context_check(rgl_context* ctx);
+/* When on, every sweep launch is bracketed by CUDA events on the context stream. */
+int rgl_context_set_timing(rgl_context* ctx, int on);
+/* Synchronises, returns the summed sweep-kernel time and launch count since the last call. */
+int rgl_context_sweep_times(rgl_context* ctx, float* total_ms, uint32_t* launches);
+/* Page-locked host buffers for fast host<->device copies. */
+int rgl_host_alloc(uint64_t bytes, void** out);
+int rgl_host_free(void* ptr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RIGGLE_B200_H */

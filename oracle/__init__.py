@@ -1,0 +1,317 @@
+"""ctypes binding of the CPU oracle (oracle/oracle.cpp) — test infrastructure only.
+
+Used by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg, never by the product.
+Builds oracle/_build/liboracle.so with make when it is missing.  Every function here forwards to a
+restatement of the reference's Rust code; see the header of oracle/oracle.cpp.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ORACLE_DIR = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(ORACLE_DIR, "_build", "liboracle.so")
+
+_P = C.c_void_p
+
+
+class OrcLayer(C.Structure):
+    _fields_ = [("shard", C.c_uint32), ("layer", C.c_uint32), ("count", C.c_uint64), ("pos", _P), ("sid", _P),
+                ("jump", _P), ("jump_len", C.c_uint64)]
+
+
+class OrcQShard(C.Structure):
+    _fields_ = [("shard", C.c_uint32), ("count", C.c_uint64), ("ivs", _P)]
+
+
+_SIGS = {
+    "orc_layer_for_size": (C.c_uint32, [C.c_uint32] * 3),
+    "orc_layer_max_size": (C.c_uint32, [C.c_uint32] * 3),
+    "orc_tile_size": (C.c_uint32, [C.c_uint32] * 3),
+    "orc_build_jump_table": (C.c_uint64, [_P, C.c_uint64, C.c_uint32, _P, C.c_uint64]),
+    "orc_extend_jump_table": (C.c_uint64, [_P, C.c_uint64, _P, C.c_uint64, C.c_uint32, _P, C.c_uint64]),
+    "orc_jump_lookup": (C.c_uint64, [_P, C.c_uint64, C.c_uint32, C.c_uint32]),
+    "orc_extend_layer": (None, [_P, _P, C.c_uint64, _P, C.c_uint64, _P, _P]),
+    "orc_query_sweep_windowed": (None, [_P, _P, C.c_uint64, C.c_uint32, _P, C.c_uint64, C.c_uint32, _P, C.c_uint64,
+                                        C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]),
+    "orc_query_database": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P,
+                                     C.c_uint32, C.c_int, C.c_int, _P, _P, _P, _P]),
+    "orc_bruteforce_counts": (None, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
+                                     _P, _P]),
+    "orc_simd_cumsum_f32": (None, [_P, C.c_uint64]),
+    "orc_build_depth_signal": (None, [_P, _P, C.c_uint64, C.c_uint64, C.c_uint32, _P]),
+    "orc_compact_index": (C.c_uint64, [C.c_uint64]),
+    "orc_moment_grid": (C.c_uint64, [C.c_uint64, _P, C.c_uint64]),
+    "orc_autocorr_fft": (None, [_P, C.c_uint64, _P]),
+    "orc_prefix_sum_f32_to_f64": (None, [_P, C.c_uint64, _P]),
+    "orc_d2_prefix_sum": (None, [_P, C.c_uint64, _P]),
+    "orc_window_moments_from_dstar": (None, [_P, C.c_uint64, C.c_uint64, C.POINTER(C.c_double),
+                                             C.POINTER(C.c_double)]),
+    "orc_moments_from_signal": (C.c_uint64, [_P, C.c_uint64, _P, _P, _P]),
+    "orc_moments_exact": (None, [_P, C.c_uint64, _P, C.c_uint64, _P, _P, C.c_int]),
+    "orc_erfc": (C.c_double, [C.c_double]),
+    "orc_nb_llr": (C.c_int, [C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+    "orc_poisson_llr": (C.c_int, [C.c_double, C.c_double, C.POINTER(C.c_double)]),
+    "orc_query_groups": (C.c_uint64, [_P, _P, C.c_uint64, C.c_uint32, _P, _P, _P, _P]),
+    "orc_analytic_stats": (C.c_int, [C.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_double,
+                                     C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
+    "orc_log_p": (C.c_double, [C.c_double, C.c_int, C.c_double, C.c_double]),
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        src = os.path.join(ORACLE_DIR, "oracle.cpp")
+        if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(src):
+            subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
+        L = C.CDLL(ORACLE_LIB)
+        for k, (r, a) in _SIGS.items():
+            f = getattr(L, k)
+            f.restype = r
+            f.argtypes = a
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return C.c_void_p(a.ctypes.data) if a is not None and a.size else None
+
+
+def build_jump_table(starts, tile):
+    starts = np.ascontiguousarray(starts, np.uint32)
+    n = lib().orc_build_jump_table(_p(starts), len(starts), tile, None, 0)
+    out = np.empty(n, np.uint64)
+    lib().orc_build_jump_table(_p(starts), len(starts), tile, _p(out), n)
+    return out
+
+
+def extend_jump_table(old, new_starts, tile):
+    old = np.ascontiguousarray(old, np.uint64)
+    new_starts = np.ascontiguousarray(new_starts, np.uint32)
+    n = lib().orc_extend_jump_table(_p(old), len(old), _p(new_starts), len(new_starts), tile, None, 0)
+    out = np.empty(n, np.uint64)
+    lib().orc_extend_jump_table(_p(old), len(old), _p(new_starts), len(new_starts), tile, _p(out), n)
+    return out
+
+
+def jump_lookup(table, tile, target):
+    table = np.ascontiguousarray(table, np.uint64)
+    return lib().orc_jump_lookup(_p(table), len(table), tile, target)
+
+
+def extend_layer(old_pos, old_sid, new_ivs):
+    old_pos = np.ascontiguousarray(old_pos, np.uint32).reshape(-1, 2)
+    old_sid = np.ascontiguousarray(old_sid, np.uint32)
+    new_ivs = np.ascontiguousarray(new_ivs, np.uint32).reshape(-1, 3)
+    tot = len(old_sid) + len(new_ivs)
+    pos = np.empty((tot, 2), np.uint32)
+    sid = np.empty(tot, np.uint32)
+    lib().orc_extend_layer(_p(old_pos), _p(old_sid), len(old_sid), _p(new_ivs), len(new_ivs), _p(pos), _p(sid))
+    return pos, sid
+
+
+def query_sweep(db, layer_max, queries, nrows, ncols, bin_size=100):
+    """Reference unit-test helper `sweep` (src/sweep/query.rs:187-200): db/queries are (start,end,sid)."""
+    db = np.asarray(db, np.uint32).reshape(-1, 3)
+    q = np.ascontiguousarray(np.asarray(queries, np.uint32).reshape(-1, 3))
+    tile = max(layer_max // 2, 1)
+    jt = build_jump_table(db[:, 0], tile) if len(db) else np.zeros(1, np.uint64)
+    pos = np.ascontiguousarray(db[:, :2])
+    sid = np.ascontiguousarray(db[:, 2])
+    counts = np.zeros((nrows, ncols), np.uint32)
+    overlap = np.zeros((nrows, ncols), np.float32)
+    lib().orc_query_sweep_windowed(_p(pos), _p(sid), len(db), layer_max, _p(jt), len(jt), tile, _p(q), len(q), 0,
+                                   ncols, bin_size, _p(counts), _p(overlap))
+    return counts, overlap
+
+
+def _layer_structs(layers, jumps=None):
+    """layers: {(shard, layer): (pos[n,2], sid[n])}; jumps: optional {(shard, layer): u64 table}"""
+    keep = []
+    arr = (OrcLayer * max(1, len(layers)))()
+    for i, ((sh, k), (pos, sid)) in enumerate(sorted(layers.items())):
+        pos = np.ascontiguousarray(pos, np.uint32).reshape(-1, 2)
+        sid = np.ascontiguousarray(sid, np.uint32)
+        keep += [pos, sid]
+        jt = None
+        if jumps is not None and (sh, k) in jumps:
+            jt = np.ascontiguousarray(jumps[(sh, k)], np.uint64)
+            keep.append(jt)
+        arr[i] = OrcLayer(sh, k, len(sid), _p(pos), _p(sid), _p(jt), len(jt) if jt is not None else 0)
+    return arr, keep
+
+
+def jump_tables(layers, min_size=128, growth_factor=4):
+    """The `.idx` table a freshly written layer carries (build_jump_table, tile = max_K / 2)."""
+    return {key: build_jump_table(pos[:, 0], lib().orc_tile_size(min_size, growth_factor, key[1]))
+            for key, (pos, sid) in layers.items()}
+
+
+def _qshard_structs(qshards):
+    keep = []
+    arr = (OrcQShard * max(1, len(qshards)))()
+    for i, (sh, ivs) in enumerate(sorted(qshards.items())):
+        ivs = np.ascontiguousarray(ivs, np.uint32).reshape(-1, 3)
+        keep.append(ivs)
+        arr[i] = OrcQShard(sh, len(ivs), _p(ivs))
+    return arr, keep
+
+
+def query_database(layers, qshards, rows, num_sources, min_size=128, growth_factor=4, bin_size=100, threads=1,
+                   mode=0, jumps=None):
+    """Restated counting path of query_database.  Returns counts, overlap_f32, overlap_bp, stats."""
+    la, k1 = _layer_structs(layers, jumps)
+    qa, k2 = _qshard_structs(qshards)
+    counts = np.zeros((rows, num_sources), np.uint32)
+    of32 = np.zeros((rows, num_sources), np.float32)
+    bp = np.zeros((rows, num_sources), np.uint64)
+    st = np.zeros(4, np.uint64)
+    lib().orc_query_database(min_size, growth_factor, num_sources, bin_size, len(layers), la, len(qshards), qa, rows,
+                             threads, mode, _p(counts), _p(of32), _p(bp), _p(st))
+    stats = dict(candidates=int(st[0]), hits=int(st[1]), db_swept=int(st[2]), query_intervals=int(st[3]))
+    return counts, of32, bp, stats
+
+
+def bruteforce(layers, qshards, rows, num_sources, min_size=128, growth_factor=4):
+    la, k1 = _layer_structs(layers)
+    qa, k2 = _qshard_structs(qshards)
+    counts = np.zeros((rows, num_sources), np.uint32)
+    bp = np.zeros((rows, num_sources), np.uint64)
+    lib().orc_bruteforce_counts(min_size, growth_factor, num_sources, len(layers), la, len(qshards), qa, rows,
+                                _p(counts), _p(bp))
+    return counts, bp
+
+
+def depth_signal(starts, ends, n_bins, bin_size=100):
+    starts = np.ascontiguousarray(starts, np.uint32)
+    ends = np.ascontiguousarray(ends, np.uint32)
+    g = np.empty(n_bins, np.float32)
+    lib().orc_build_depth_signal(_p(starts), _p(ends), len(starts), n_bins, bin_size, _p(g))
+    return g
+
+
+def cumsum_f32(x):
+    g = np.ascontiguousarray(x, np.float32).copy()
+    lib().orc_simd_cumsum_f32(_p(g), len(g))
+    return g
+
+
+def moment_grid(n_bins):
+    n = lib().orc_moment_grid(n_bins, None, 0)
+    out = np.empty(n, np.uint64)
+    lib().orc_moment_grid(n_bins, _p(out), n)
+    return out
+
+
+def moments_from_signal(g):
+    g = np.ascontiguousarray(g, np.float32)
+    n = len(moment_grid(len(g)))
+    mv = np.empty(2 * n, np.float32)
+    m = np.empty(n, np.float64)
+    v = np.empty(n, np.float64)
+    lib().orc_moments_from_signal(_p(g), len(g), _p(mv), _p(m), _p(v))
+    return mv.reshape(-1, 2), m, v
+
+
+def moments_exact(g, ls, threads=4):
+    g = np.ascontiguousarray(g, np.float32)
+    ls = np.ascontiguousarray(ls, np.uint64)
+    m = np.empty(len(ls), np.float64)
+    v = np.empty(len(ls), np.float64)
+    lib().orc_moments_exact(_p(g), len(g), _p(ls), len(ls), _p(m), _p(v), threads)
+    return m, v
+
+
+def autocorr(x):
+    x = np.ascontiguousarray(x, np.float64)
+    r = np.empty(len(x), np.float64)
+    lib().orc_autocorr_fft(_p(x), len(x), _p(r))
+    return r
+
+
+def window_moments_from_g(g, l):
+    """Test hook for src/fourier/moments.rs:511-562: d* by plain f64 prefix of g."""
+    g = np.asarray(g, np.float32)
+    ds = np.zeros(len(g) + 1, np.float64)
+    for j in range(1, len(g) + 1):
+        ds[j] = ds[j - 1] + float(g[j - 1])
+    m, v = C.c_double(), C.c_double()
+    lib().orc_window_moments_from_dstar(_p(ds), len(g), l, C.byref(m), C.byref(v))
+    return m.value, v.value
+
+
+def d2_prefix_sum(x):
+    x = np.ascontiguousarray(x, np.float64)
+    out = np.empty(len(x) + 1, np.float64)
+    lib().orc_d2_prefix_sum(_p(x), len(x), _p(out))
+    return out
+
+
+def nb_llr(mu, var, obs):
+    out = C.c_double()
+    ok = lib().orc_nb_llr(mu, var, obs, C.byref(out))
+    return out.value if ok else None
+
+
+def poisson_llr(mu, obs):
+    out = C.c_double()
+    ok = lib().orc_poisson_llr(mu, obs, C.byref(out))
+    return out.value if ok else None
+
+
+def erfc(x):
+    return lib().orc_erfc(x)
+
+
+def compact_index(l):
+    return lib().orc_compact_index(l)
+
+
+def query_groups(starts, ends, bin_size=100):
+    starts = np.ascontiguousarray(starts, np.uint32)
+    ends = np.ascontiguousarray(ends, np.uint32)
+    n = len(starts)
+    li = np.empty(max(n, 1), np.uint64)
+    ss = np.empty(max(n, 1), np.float64)
+    ss2 = np.empty(max(n, 1), np.float64)
+    cnt = np.empty(max(n, 1), np.uint64)
+    g = lib().orc_query_groups(_p(starts), _p(ends), n, bin_size, _p(li), _p(ss), _p(ss2), _p(cnt))
+    return li[:g], ss[:g], ss2[:g], cnt[:g]
+
+
+def analytic_stats(q_chroms, db, observed):
+    """q_chroms: list of (chrom_id, (l_int, ss, ss2, count)); db: {chrom_id: (n_bins, mv float32[n,2])}.
+
+    Returns None (no shared chromosome) or (p, llr or None)."""
+    nq = len(q_chroms)
+    qc = np.array([c for c, _ in q_chroms], np.uint32)
+    goff = np.zeros(nq + 1, np.uint64)
+    parts = [g for _, g in q_chroms]
+    for i, g in enumerate(parts):
+        goff[i + 1] = goff[i] + len(g[0])
+    cat = lambda j, dt: np.ascontiguousarray(np.concatenate([g[j] for g in parts]) if parts else np.zeros(0), dt)
+    gl, gs, gs2, gc = cat(0, np.uint64), cat(1, np.float64), cat(2, np.float64), cat(3, np.uint64)
+    ncid = max([c for c, _ in q_chroms] + list(db.keys()) + [0]) + 1
+    nb = np.zeros(ncid, np.uint64)
+    off = np.zeros(ncid, np.uint64)
+    ln = np.zeros(ncid, np.uint64)
+    mvs = []
+    acc = 0
+    for c, (n_bins, mv) in sorted(db.items()):
+        mv = np.asarray(mv, np.float32).reshape(-1, 2)
+        nb[c] = n_bins
+        off[c] = acc
+        ln[c] = len(mv)
+        acc += len(mv)
+        mvs.append(mv)
+    mvall = np.ascontiguousarray(np.concatenate(mvs) if mvs else np.zeros((1, 2), np.float32), np.float32)
+    p, llr, has = C.c_double(), C.c_double(), C.c_int()
+    ok = lib().orc_analytic_stats(nq, _p(qc), _p(goff), _p(gl), _p(gs), _p(gs2), _p(gc), _p(nb), _p(off), _p(ln),
+                                  _p(mvall), observed, C.byref(p), C.byref(llr), C.byref(has))
+    if not ok:
+        return None
+    return p.value, (llr.value if has.value else None)

@@ -1,0 +1,286 @@
+"""Python face of the C ABI, named after the reference crate's types and functions.
+
+`LayerConfig` mirrors src/io/meta.rs:23-90; `Index` is the device-resident form of the database a
+query opens (src/tasks/query/mod.rs:124-233); `Context.query_counts` replaces the counting sweep of
+query_database (src/tasks/query/mod.rs:182-307) and returns the dense count matrix together with
+exact overlap base pairs.  All compute happens in libriggle_b200.so on the GPU.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, load
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None and a.size else None
+
+
+class LayerConfig:
+    """LayerConfig (src/io/meta.rs:23-90)."""
+
+    def __init__(self, min_size=128, growth_factor=4):
+        self.min_size = int(min_size)
+        self.growth_factor = int(growth_factor)
+
+    @classmethod
+    def default_genomic(cls):
+        return cls(128, 4)
+
+    def layer_for_size(self, size):
+        return load().rgl_layer_for_size(self.min_size, self.growth_factor, int(size))
+
+    def layer_max_size(self, layer):
+        return load().rgl_layer_max_size(self.min_size, self.growth_factor, int(layer))
+
+    def tile_size(self, layer):
+        return load().rgl_tile_size(self.min_size, self.growth_factor, int(layer))
+
+
+class Index:
+    """A database index resident in HBM (the handle owns the device memory)."""
+
+    def __init__(self, handle):
+        self._h = C.c_void_p(handle) if not isinstance(handle, C.c_void_p) else handle
+        info = _lib.IndexInfo()
+        check(load().rgl_index_get_info(self._h, C.byref(info)))
+        self.num_sources = info.num_sources
+        self.num_shards = info.num_shards
+        self.num_layer_slots = info.num_layer_slots
+        self.num_layers = info.num_layers
+        self.num_intervals = info.num_intervals
+        self.device_bytes = info.device_bytes
+        self.device = info.device
+
+    @classmethod
+    def open(cls, db_dir, device=0):
+        """Opens a database directory written by the reference's `add`."""
+        h = C.c_void_p()
+        check(load().rgl_index_open(str(db_dir).encode(), device, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def from_layers(cls, layers, num_sources, shard_names, min_size=128, growth_factor=4, source_names=None,
+                    device=0):
+        """layers: {(shard_id, layer): (pos uint32[n,2] sorted by start, sid uint32[n])}."""
+        keep = []
+        descs = (_lib.LayerDesc * max(1, len(layers)))()
+        for i, ((sh, k), (pos, sid)) in enumerate(sorted(layers.items())):
+            pos = np.ascontiguousarray(pos, dtype=np.uint32).reshape(-1, 2)
+            sid = np.ascontiguousarray(sid, dtype=np.uint32).reshape(-1)
+            keep += [pos, sid]
+            descs[i] = _lib.LayerDesc(int(sh), int(k), len(sid), _ptr(pos), _ptr(sid))
+        names = (C.c_char_p * max(1, len(shard_names)))(*[s.encode() for s in shard_names])
+        srcs = None
+        if source_names is not None:
+            srcs = (C.c_char_p * max(1, len(source_names)))(*[s.encode() for s in source_names])
+        d = _lib.IndexDesc(min_size, growth_factor, num_sources, len(shard_names), names, srcs, len(layers), descs)
+        h = C.c_void_p()
+        check(load().rgl_index_open_mem(C.byref(d), device, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def synth(cls, spec, min_size=128, growth_factor=4, device=0):
+        """Builds a seeded synthetic database directly in HBM (see SynthSpec)."""
+        h = C.c_void_p()
+        check(load().rgl_index_synth(C.byref(spec.c), min_size, growth_factor, device, C.byref(h)))
+        return cls(h)
+
+    def shard_id(self, name):
+        out = C.c_uint32()
+        check(load().rgl_index_shard_id(self._h, name.encode(), C.byref(out)))
+        return out.value
+
+    def shard_name(self, shard):
+        r = load().rgl_index_shard_name(self._h, shard)
+        return r.decode() if r else None
+
+    def source_name(self, sid):
+        r = load().rgl_index_source_name(self._h, sid)
+        return r.decode() if r else None
+
+    def layer_count(self, shard, layer):
+        return load().rgl_index_layer_count(self._h, shard, layer)
+
+    def export_layer(self, shard, layer):
+        n = self.layer_count(shard, layer)
+        pos = np.empty((n, 2), np.uint32)
+        sid = np.empty(n, np.uint32)
+        if n:
+            check(load().rgl_index_export_layer(self._h, shard, layer, _ptr(pos), _ptr(sid)))
+        return pos, sid
+
+    def close(self):
+        if self._h:
+            load().rgl_index_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Context:
+    """One CUDA stream + reusable device workspace bound to an Index."""
+
+    def __init__(self, index, stream=None):
+        self.index = index
+        h = C.c_void_p()
+        check(load().rgl_context_create(index._h, C.c_void_p(stream) if stream else None, C.byref(h)))
+        self._h = h
+
+    @property
+    def stream(self):
+        return load().rgl_context_stream(self._h)
+
+    def reserve(self, max_intervals, max_rows):
+        check(load().rgl_context_reserve(self._h, int(max_intervals), int(max_rows)))
+
+    def sync(self):
+        check(load().rgl_context_sync(self._h))
+
+    @staticmethod
+    def _opts(chunk=0, ctas_per_sm=0, counts_only=False):
+        return _lib.QueryOpts(chunk, ctas_per_sm, 0, 1 if counts_only else 0)
+
+    def query_counts(self, shards, num_rows, with_overlap=True, chunk=0, ctas_per_sm=0, out=None):
+        """shards: {shard name (str) or id (int): uint32[n,3] (start, end, row)}.
+
+        Returns (counts uint32[num_rows, D], overlap_bp uint64[num_rows, D] or None, stats dict).
+        """
+        keep = []
+        arr = (_lib.QueryShard * max(1, len(shards)))()
+        for i, (k, ivs) in enumerate(shards.items()):
+            ivs = np.ascontiguousarray(ivs, dtype=np.uint32).reshape(-1, 3)
+            keep.append(ivs)
+            if isinstance(k, str):
+                arr[i] = _lib.QueryShard(k.encode(), 0, len(ivs), _ptr(ivs))
+            else:
+                arr[i] = _lib.QueryShard(None, int(k), len(ivs), _ptr(ivs))
+        batch = _lib.QueryBatch(int(num_rows), len(shards), arr)
+        D = self.index.num_sources
+        if out is None:
+            counts = np.empty((num_rows, D), np.uint32)
+            bp = np.empty((num_rows, D), np.uint64) if with_overlap else None
+        else:
+            counts, bp = out
+        st = _lib.QueryStats()
+        opts = self._opts(chunk, ctas_per_sm, not with_overlap)
+        check(load().rgl_query_counts(self._h, C.byref(batch), C.byref(opts), _ptr(counts), _ptr(bp), C.byref(st)))
+        return counts, bp, st.as_dict()
+
+    def close(self):
+        if self._h:
+            load().rgl_context_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class SynthSpec:
+    """Seeded synthetic dataset description (rgl_synth_spec)."""
+
+    def __init__(self, seed, chrom_len, file_sizes, broad_fraction=0.0, hotspot_fraction=0.0, num_hotspots=0,
+                 sid_base=0):
+        self.chrom_len = np.ascontiguousarray(chrom_len, dtype=np.uint32)
+        self.file_sizes = np.ascontiguousarray(file_sizes, dtype=np.uint64)
+        self.c = _lib.SynthSpec(int(seed), len(self.chrom_len),
+                                self.chrom_len.ctypes.data_as(C.POINTER(C.c_uint32)), len(self.file_sizes),
+                                self.file_sizes.ctypes.data_as(C.POINTER(C.c_uint64)), float(broad_fraction),
+                                float(hotspot_fraction), int(num_hotspots), int(sid_base))
+
+    @property
+    def num_files(self):
+        return len(self.file_sizes)
+
+    @property
+    def num_chroms(self):
+        return len(self.chrom_len)
+
+    def chrom_counts(self, file):
+        out = np.empty(self.num_chroms, np.uint64)
+        check(load().rgl_synth_file_chrom_counts(C.byref(self.c), file, _ptr(out)))
+        return out
+
+    def block(self, file, chrom):
+        """Intervals of (file, chrom) sorted by (start, end) as uint32[n,3] (start, end, sid)."""
+        n = C.c_uint64()
+        check(load().rgl_synth_block_host(C.byref(self.c), file, chrom, None, 0, C.byref(n)))
+        out = np.empty((n.value, 3), np.uint32)
+        check(load().rgl_synth_block_host(C.byref(self.c), file, chrom, _ptr(out), n.value, C.byref(n)))
+        return out
+
+    def chrom_layers(self, chrom, min_size=128, growth_factor=4):
+        """Host-generated layers of one chromosome: {(chrom, K): (pos uint32[n,2], sid uint32[n])}."""
+        tot = C.c_uint64()
+        cnt = np.zeros(64, np.uint64)
+        check(load().rgl_synth_chrom_layers_host(C.byref(self.c), chrom, min_size, growth_factor, _ptr(cnt), 64,
+                                                 None, None, 0, C.byref(tot)))
+        pos = np.empty((tot.value, 2), np.uint32)
+        sid = np.empty(tot.value, np.uint32)
+        check(load().rgl_synth_chrom_layers_host(C.byref(self.c), chrom, min_size, growth_factor, _ptr(cnt), 64,
+                                                 _ptr(pos), _ptr(sid), tot.value, C.byref(tot)))
+        out, acc = {}, 0
+        for k in range(64):
+            n = int(cnt[k])
+            if n:
+                out[(chrom, k)] = (pos[acc:acc + n], sid[acc:acc + n])
+                acc += n
+        return out
+
+    def file(self, file):
+        """All intervals of a file: {chrom index: uint32[n,3]}."""
+        return {c: self.block(file, c) for c in range(self.num_chroms)}
+
+
+CHROM_NAMES_24 = [f"chr{i}" for i in range(1, 23)] + ["chrX", "chrY"]
+
+
+def synth_chrom_lengths(seed=1, num_chroms=24):
+    out = np.empty(num_chroms, np.uint32)
+    check(load().rgl_synth_chrom_lengths(seed, num_chroms, _ptr(out)))
+    return out
+
+
+def synth_zipf_sizes(num_files, s=1.1, lo=1000, hi=10_000_000, target=2_000_000_000):
+    out = np.empty(num_files, np.uint64)
+    check(load().rgl_synth_zipf_sizes(num_files, s, lo, hi, target, _ptr(out)))
+    return out
+
+
+def synth_loguniform_sizes(seed, num_files, lo, hi):
+    out = np.empty(num_files, np.uint64)
+    check(load().rgl_synth_loguniform_sizes(seed, num_files, lo, hi, _ptr(out)))
+    return out
+
+
+def bucket_layers(blocks, config=None):
+    """Host bucketing of interval blocks into the reference's (shard, layer) layers, sorted by start
+    (src/tasks/build.rs:190-211).  blocks: iterable of (shard_id, uint32[n,3]).  Returns
+    {(shard, layer): (pos uint32[n,2], sid uint32[n])}.  Ties in start keep input order."""
+    config = config or LayerConfig()
+    per = {}
+    for sh, ivs in blocks:
+        ivs = np.asarray(ivs, np.uint32).reshape(-1, 3)
+        if not len(ivs):
+            continue
+        sizes = ivs[:, 1] - ivs[:, 0]
+        ks = np.array([config.layer_for_size(int(x)) for x in np.unique(sizes)], np.uint32)
+        lut = dict(zip(np.unique(sizes).tolist(), ks.tolist()))
+        kk = np.vectorize(lut.__getitem__, otypes=[np.uint32])(sizes)
+        for k in np.unique(kk):
+            per.setdefault((int(sh), int(k)), []).append(ivs[kk == k])
+    out = {}
+    for key, parts in per.items():
+        a = np.concatenate(parts)
+        o = np.argsort(a[:, 0], kind="stable")
+        a = a[o]
+        out[key] = (np.ascontiguousarray(a[:, :2]), np.ascontiguousarray(a[:, 2]))
+    return out

@@ -1,0 +1,398 @@
+// Device-resident database index: the reference's per-(shard, layer) `.pos` / `.sid` arrays
+// (src/io/layer.rs:31-105) copied into two index-wide HBM arrays, plus a layer table.
+//
+// HBM layout: d_pos is uint2[(start, end)] exactly as layer_K.pos stores it, d_sid is u32 as in
+// layer_K.sid; layer l occupies elements [off_l, off_l + n_l) of both, with off_l a multiple of 4
+// (16-byte aligned sid blocks, 32-byte aligned pos blocks).  The reference's `.idx` jump table
+// (src/io/jump.rs) is size-checked at open for error parity but not uploaded: the device computes
+// exact partition points by binary search, which is what the reference's conservative lookup plus
+// partition_point yields (src/sweep/query.rs:141-143).
+#include <algorithm>
+#include <cstring>
+
+#include "internal.h"
+
+namespace rgl {
+
+int DevBuf::ensure(size_t bytes) {
+    if (bytes <= cap) return RGL_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = bytes + bytes / 4 + 256;
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+        p = nullptr;
+        return fail(RGL_ERR_OOM, std::string("cudaMalloc(") + std::to_string(want) + "): " + cudaGetErrorString(e));
+    }
+    cap = want;
+    return RGL_OK;
+}
+
+void DevBuf::release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+}
+
+__global__ void k_validate_layer(const uint2* __restrict__ pos, const uint32_t* __restrict__ sid, uint64_t n,
+                                 uint32_t max_size, uint32_t num_sources, uint32_t* __restrict__ flags) {
+    uint32_t f = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        uint2 p = pos[i];
+        if (p.x >= p.y) f |= LF_EMPTY_IV;
+        else if (p.y - p.x >= max_size) f |= LF_OVERSIZE;
+        if (i > 0 && pos[i - 1].x > p.x) f |= LF_UNSORTED;
+        if (sid[i] >= num_sources) f |= LF_BAD_SID;
+    }
+    f = __reduce_or_sync(0xffffffffu, f);
+    if (f && (threadIdx.x & 31) == 0) atomicOr(flags, f);
+}
+
+int index_alloc(rgl_index* idx) {
+    uint64_t off = 0;
+    for (auto& l : idx->layers)
+        if (l.n >= 0xFFFFFFFFull)
+            return fail(RGL_ERR_UNSUPPORTED, "a layer holds 2^32-1 or more intervals (layer indices are 32-bit)");
+    for (auto& l : idx->layers) {
+        l.off = off;
+        off += (l.n + 3) & ~uint64_t(3);
+    }
+    idx->cap_elems = off < 4 ? 4 : off;
+    RGL_CUDA(cudaSetDevice(idx->device));
+    RGL_CUDA(cudaMalloc(&idx->d_pos, idx->cap_elems * sizeof(uint2)));
+    RGL_CUDA(cudaMalloc(&idx->d_sid, idx->cap_elems * sizeof(uint32_t)));
+    idx->device_bytes = idx->cap_elems * 12;
+    return RGL_OK;
+}
+
+int index_finalize(rgl_index* idx) {
+    RGL_CUDA(cudaSetDevice(idx->device));
+    size_t nl = idx->layers.size() ? idx->layers.size() : 1;
+    RGL_CUDA(cudaMalloc(&idx->d_layers, nl * sizeof(LayerDev)));
+    size_t ns = idx->slot.size() ? idx->slot.size() : 1;
+    RGL_CUDA(cudaMalloc(&idx->d_slot, ns * sizeof(int32_t)));
+    idx->device_bytes += nl * sizeof(LayerDev) + ns * sizeof(int32_t);
+    uint32_t* d_flags = nullptr;
+    RGL_CUDA(cudaMalloc(&d_flags, nl * sizeof(uint32_t)));
+    RGL_CUDA(cudaMemset(d_flags, 0, nl * sizeof(uint32_t)));
+    for (size_t i = 0; i < idx->layers.size(); i++) {
+        const LayerDev& l = idx->layers[i];
+        uint64_t blocks = (l.n + 255) / 256;
+        if (blocks > 148 * 16) blocks = 148 * 16;
+        if (blocks == 0) blocks = 1;
+        k_validate_layer<<<(unsigned)blocks, 256>>>(idx->d_pos + l.off, idx->d_sid + l.off, l.n, l.max_size,
+                                                     idx->num_sources, d_flags + i);
+    }
+    RGL_CUDA(cudaGetLastError());
+    std::vector<uint32_t> flags(nl, 0);
+    RGL_CUDA(cudaMemcpy(flags.data(), d_flags, nl * sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    cudaFree(d_flags);
+    for (size_t i = 0; i < idx->layers.size(); i++) {
+        LayerDev& l = idx->layers[i];
+        l.flags = flags[i];
+        std::string where = "shard '" + idx->shard_names[l.shard] + "' layer " + std::to_string(l.layer);
+        if (l.flags & LF_UNSORTED)
+            return fail(RGL_ERR_INDEX_INVARIANT, where + ": positions are not sorted by start");
+        if (l.flags & LF_BAD_SID)
+            return fail(RGL_ERR_INDEX_INVARIANT,
+                        where + ": a source id is >= num_sources (" + std::to_string(idx->num_sources) + ")");
+        if (l.flags & (LF_EMPTY_IV | LF_OVERSIZE))
+            return fail(RGL_ERR_INDEX_INVARIANT,
+                        where + ": an interval has start >= end or a size outside its layer's class "
+                                "(the reference's add never writes one)");
+    }
+    if (!idx->layers.empty())
+        RGL_CUDA(cudaMemcpy(idx->d_layers, idx->layers.data(), idx->layers.size() * sizeof(LayerDev),
+                            cudaMemcpyHostToDevice));
+    if (!idx->slot.empty())
+        RGL_CUDA(cudaMemcpy(idx->d_slot, idx->slot.data(), idx->slot.size() * sizeof(int32_t), cudaMemcpyHostToDevice));
+    return RGL_OK;
+}
+
+void index_free(rgl_index* idx) {
+    if (!idx) return;
+    cudaSetDevice(idx->device);
+    if (idx->d_pos) cudaFree(idx->d_pos);
+    if (idx->d_sid) cudaFree(idx->d_sid);
+    if (idx->d_layers) cudaFree(idx->d_layers);
+    if (idx->d_slot) cudaFree(idx->d_slot);
+    idx->d_pos = nullptr;
+    idx->d_sid = nullptr;
+    idx->d_layers = nullptr;
+    idx->d_slot = nullptr;
+}
+
+static int check_layer_config(uint32_t min_size, uint32_t gf) {
+    if (min_size == 0 || gf < 2)
+        return fail(RGL_ERR_INVALID_ARGUMENT, "layer_config needs min_size >= 1 and growth_factor >= 2 (min_size=" +
+                                                  std::to_string(min_size) + ", growth_factor=" + std::to_string(gf) + ")");
+    return RGL_OK;
+}
+
+static int device_check(int device) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) return fail(RGL_ERR_NO_DEVICE, "no CUDA device visible");
+    if (device < 0 || device >= n) return fail(RGL_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    return RGL_OK;
+}
+
+}  // namespace rgl
+
+using namespace rgl;
+
+// Builds the shard/slot tables of an index from its (shard, layer, n) triples.
+static void build_slots(rgl_index* idx) {
+    uint32_t maxk = 0;
+    for (auto& l : idx->layers) maxk = std::max(maxk, l.layer + 1);
+    idx->num_slots = maxk;
+    idx->slot.assign((size_t)idx->num_shards * maxk, -1);
+    for (size_t i = 0; i < idx->layers.size(); i++)
+        idx->slot[(size_t)idx->layers[i].shard * maxk + idx->layers[i].layer] = (int32_t)i;
+}
+
+extern "C" {
+
+int rgl_index_open_mem(const rgl_index_desc* desc, int device, rgl_index** out) {
+    clear_error();
+    if (!desc || !out) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    RGL_TRY(check_layer_config(desc->min_size, desc->growth_factor));
+    RGL_TRY(device_check(device));
+    auto* idx = new rgl_index();
+    idx->device = device;
+    idx->min_size = desc->min_size;
+    idx->gf = desc->growth_factor;
+    idx->num_sources = desc->num_sources;
+    idx->num_shards = desc->num_shards;
+    for (uint32_t s = 0; s < desc->num_shards; s++) {
+        std::string nm = desc->shard_names && desc->shard_names[s] ? desc->shard_names[s] : std::to_string(s);
+        idx->shard_names.push_back(nm);
+        idx->shard_ids[nm] = s;
+    }
+    for (uint32_t d = 0; d < desc->num_sources; d++)
+        idx->source_names.push_back(desc->source_names && desc->source_names[d] ? desc->source_names[d]
+                                                                               : "source_" + std::to_string(d));
+    for (uint32_t i = 0; i < desc->num_layers; i++) {
+        const rgl_layer_desc& ld = desc->layers[i];
+        if (ld.shard >= desc->num_shards) {
+            delete idx;
+            return fail(RGL_ERR_INVALID_ARGUMENT, "layer descriptor names shard " + std::to_string(ld.shard));
+        }
+        if (ld.count == 0) continue;
+        if (!ld.pos || !ld.sid) {
+            delete idx;
+            return fail(RGL_ERR_INVALID_ARGUMENT, "layer descriptor without pos/sid arrays");
+        }
+        for (auto& l : idx->layers)
+            if (l.shard == ld.shard && l.layer == ld.layer) {
+                delete idx;
+                return fail(RGL_ERR_INVALID_ARGUMENT, "duplicate (shard, layer) descriptor");
+            }
+        LayerDev l{};
+        l.n = ld.count;
+        l.shard = ld.shard;
+        l.layer = ld.layer;
+        l.max_size = layer_max_size(desc->min_size, desc->growth_factor, ld.layer);
+        idx->layers.push_back(l);
+        idx->total += ld.count;
+    }
+    build_slots(idx);
+    int s = index_alloc(idx);
+    if (s == RGL_OK) {
+        size_t li = 0;
+        for (uint32_t i = 0; i < desc->num_layers && s == RGL_OK; i++) {
+            const rgl_layer_desc& ld = desc->layers[i];
+            if (ld.count == 0) continue;
+            const LayerDev& l = idx->layers[li++];
+            cudaError_t e1 = cudaMemcpy(idx->d_pos + l.off, ld.pos, l.n * 8, cudaMemcpyHostToDevice);
+            cudaError_t e2 = cudaMemcpy(idx->d_sid + l.off, ld.sid, l.n * 4, cudaMemcpyHostToDevice);
+            if (e1 != cudaSuccess || e2 != cudaSuccess)
+                s = fail(RGL_ERR_DEVICE, std::string("layer upload: ") + cudaGetErrorString(e1 != cudaSuccess ? e1 : e2));
+        }
+    }
+    if (s == RGL_OK) s = index_finalize(idx);
+    if (s != RGL_OK) {
+        index_free(idx);
+        delete idx;
+        return s;
+    }
+    *out = idx;
+    return RGL_OK;
+}
+
+int rgl_index_open(const char* db_dir, int device, rgl_index** out) {
+    clear_error();
+    if (!db_dir || !out) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    std::string dir(db_dir);
+    // query_database returns DatabaseNotFound when meta.json is absent (src/tasks/query/mod.rs:124-127).
+    if (!file_exists(dir + "/meta.json")) return fail(RGL_ERR_DATABASE_NOT_FOUND, "Database not found at " + dir);
+    MetaInfo meta;
+    RGL_TRY(meta_load(dir, &meta));
+    RGL_TRY(check_layer_config(meta.min_size, meta.growth_factor));
+    RGL_TRY(device_check(device));
+
+    auto* idx = new rgl_index();
+    idx->device = device;
+    idx->min_size = meta.min_size;
+    idx->gf = meta.growth_factor;
+    idx->num_sources = (uint32_t)meta.sid_map.size();  // Meta::num_sources (src/io/meta.rs:142-144)
+    idx->num_shards = (uint32_t)meta.shards.size();
+    for (uint32_t s = 0; s < idx->num_shards; s++) {
+        idx->shard_names.push_back(meta.shards[s]);
+        idx->shard_ids[meta.shards[s]] = s;
+    }
+    for (uint32_t d = 0; d < idx->num_sources; d++) {
+        auto it = meta.sid_map.find(d);
+        idx->source_names.push_back(it != meta.sid_map.end() ? it->second : "source_" + std::to_string(d));
+    }
+    struct Pending {
+        std::string pos, sid;
+    };
+    std::vector<Pending> files;
+    int s = RGL_OK;
+    // Same file checks and order as query_database's layer loading (src/tasks/query/mod.rs:205-233)
+    // and MappedLayer::open / MappedJumpTable::open (src/io/layer.rs:51-78, src/io/jump.rs:225-237).
+    for (uint32_t sh = 0; sh < idx->num_shards && s == RGL_OK; sh++) {
+        for (uint64_t k = 0; k < meta.num_layers && s == RGL_OK; k++) {
+            std::string base = dir + "/shards/" + meta.shards[sh] + "/layer_" + std::to_string(k);
+            if (!file_exists(base + ".pos")) continue;
+            FILE* fp = std::fopen((base + ".pos").c_str(), "rb");
+            FILE* fs = std::fopen((base + ".sid").c_str(), "rb");
+            if (!fp || !fs) {
+                if (fp) std::fclose(fp);
+                if (fs) std::fclose(fs);
+                s = fail(RGL_ERR_IO, "cannot open " + base + (fp ? ".sid" : ".pos"));
+                break;
+            }
+            std::fseek(fp, 0, SEEK_END);
+            std::fseek(fs, 0, SEEK_END);
+            uint64_t psz = (uint64_t)std::ftell(fp), ssz = (uint64_t)std::ftell(fs);
+            std::fclose(fp);
+            std::fclose(fs);
+            if (psz % 8) { s = fail(RGL_ERR_LAYER_INVALID_POSITION_SIZE, "Position file has invalid size: " + std::to_string(psz) + " bytes"); break; }
+            if (ssz % 4) { s = fail(RGL_ERR_LAYER_INVALID_SID_SIZE, "Sid file has invalid size: " + std::to_string(ssz) + " bytes"); break; }
+            if (psz / 8 != ssz / 4) {
+                s = fail(RGL_ERR_LAYER_SID_SIZE_MISMATCH, "Position count " + std::to_string(psz / 8) +
+                                                              " does not match sid count " + std::to_string(ssz / 4));
+                break;
+            }
+            if (psz == 0) continue;  // empty layers are skipped before the jump table is opened
+            FILE* fi = std::fopen((base + ".idx").c_str(), "rb");
+            if (!fi) { s = fail(RGL_ERR_IO, "cannot open " + base + ".idx"); break; }
+            std::fseek(fi, 0, SEEK_END);
+            uint64_t isz = (uint64_t)std::ftell(fi);
+            std::fclose(fi);
+            if (isz % 8) { s = fail(RGL_ERR_LAYER_INVALID_INDEX_SIZE, "Index file has invalid size: " + std::to_string(isz) + " bytes (not a multiple of 4)"); break; }
+            LayerDev l{};
+            l.n = psz / 8;
+            l.shard = sh;
+            l.layer = (uint32_t)k;
+            l.max_size = layer_max_size(meta.min_size, meta.growth_factor, (uint32_t)k);
+            idx->layers.push_back(l);
+            idx->total += l.n;
+            files.push_back({base + ".pos", base + ".sid"});
+        }
+    }
+    if (s == RGL_OK) {
+        build_slots(idx);
+        s = index_alloc(idx);
+    }
+    // Stream the files through a pinned staging buffer.
+    if (s == RGL_OK && !files.empty()) {
+        const size_t CH = 64u << 20;
+        void* stage = nullptr;
+        if (cudaMallocHost(&stage, CH) != cudaSuccess) s = fail(RGL_ERR_OOM, "pinned staging buffer");
+        for (size_t i = 0; i < files.size() && s == RGL_OK; i++) {
+            const LayerDev& l = idx->layers[i];
+            for (int which = 0; which < 2 && s == RGL_OK; which++) {
+                const std::string& path = which == 0 ? files[i].pos : files[i].sid;
+                uint8_t* dst = which == 0 ? reinterpret_cast<uint8_t*>(idx->d_pos + l.off)
+                                          : reinterpret_cast<uint8_t*>(idx->d_sid + l.off);
+                uint64_t bytes = l.n * (which == 0 ? 8 : 4);
+                FILE* f = std::fopen(path.c_str(), "rb");
+                if (!f) { s = fail(RGL_ERR_IO, "cannot open " + path); break; }
+                uint64_t done = 0;
+                while (done < bytes) {
+                    size_t want = (size_t)std::min<uint64_t>(CH, bytes - done);
+                    size_t got = std::fread(stage, 1, want, f);
+                    if (got != want) { s = fail(RGL_ERR_IO, "short read of " + path); break; }
+                    if (cudaMemcpy(dst + done, stage, got, cudaMemcpyHostToDevice) != cudaSuccess) {
+                        s = fail(RGL_ERR_DEVICE, "layer upload failed");
+                        break;
+                    }
+                    done += got;
+                }
+                std::fclose(f);
+            }
+        }
+        if (stage) cudaFreeHost(stage);
+    }
+    if (s == RGL_OK) s = index_finalize(idx);
+    if (s != RGL_OK) {
+        index_free(idx);
+        delete idx;
+        return s;
+    }
+    *out = idx;
+    return RGL_OK;
+}
+
+int rgl_index_close(rgl_index* index) {
+    if (!index) return RGL_OK;
+    index_free(index);
+    delete index;
+    return RGL_OK;
+}
+
+int rgl_index_get_info(const rgl_index* index, rgl_index_info* out) {
+    if (!index || !out) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    out->num_sources = index->num_sources;
+    out->num_shards = index->num_shards;
+    out->num_layer_slots = index->num_slots;
+    out->num_layers = (uint32_t)index->layers.size();
+    out->num_intervals = index->total;
+    out->device_bytes = index->device_bytes;
+    out->device = index->device;
+    return RGL_OK;
+}
+
+int rgl_index_shard_id(const rgl_index* index, const char* name, uint32_t* out_id) {
+    if (!index || !name || !out_id) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    auto it = index->shard_ids.find(name);
+    if (it == index->shard_ids.end()) return fail(RGL_ERR_INVALID_ARGUMENT, std::string("shard not in index: ") + name);
+    *out_id = it->second;
+    return RGL_OK;
+}
+
+const char* rgl_index_shard_name(const rgl_index* index, uint32_t shard) {
+    if (!index || shard >= index->num_shards) return nullptr;
+    return index->shard_names[shard].c_str();
+}
+
+const char* rgl_index_source_name(const rgl_index* index, uint32_t sid) {
+    if (!index || sid >= index->num_sources) return nullptr;
+    return index->source_names[sid].c_str();
+}
+
+uint64_t rgl_index_layer_count(const rgl_index* index, uint32_t shard, uint32_t layer) {
+    if (!index || shard >= index->num_shards || layer >= index->num_slots) return 0;
+    int32_t li = index->slot[(size_t)shard * index->num_slots + layer];
+    return li < 0 ? 0 : index->layers[li].n;
+}
+
+int rgl_index_export_layer(const rgl_index* index, uint32_t shard, uint32_t layer, uint32_t* pos, uint32_t* sid) {
+    if (!index) return fail(RGL_ERR_INVALID_ARGUMENT, "null index");
+    if (shard >= index->num_shards || layer >= index->num_slots) return RGL_OK;
+    int32_t li = index->slot[(size_t)shard * index->num_slots + layer];
+    if (li < 0) return RGL_OK;
+    const LayerDev& l = index->layers[li];
+    RGL_CUDA(cudaSetDevice(index->device));
+    if (pos) RGL_CUDA(cudaMemcpy(pos, index->d_pos + l.off, l.n * 8, cudaMemcpyDeviceToHost));
+    if (sid) RGL_CUDA(cudaMemcpy(sid, index->d_sid + l.off, l.n * 4, cudaMemcpyDeviceToHost));
+    return RGL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,113 @@
+// Internal declarations shared by the host and device translation units of libriggle_b200.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/riggle.h"
+
+namespace rgl {
+
+// ---- errors ------------------------------------------------------------------------------------
+// Sets the thread-local detail string and returns `code`.
+int fail(int code, const std::string& msg);
+void clear_error();
+
+#define RGL_CUDA(call)                                                                              \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return ::rgl::fail(e_ == cudaErrorMemoryAllocation ? RGL_ERR_OOM : RGL_ERR_DEVICE,      \
+                               std::string(#call) + ": " + cudaGetErrorString(e_));                 \
+    } while (0)
+
+#define RGL_TRY(expr)                     \
+    do {                                  \
+        int s_ = (expr);                  \
+        if (s_ != RGL_OK) return s_;      \
+    } while (0)
+
+// ---- layer configuration (src/io/meta.rs:33-81) ---------------------------------------------
+uint32_t layer_for_size(uint32_t min_size, uint32_t gf, uint32_t size);
+uint32_t layer_max_size(uint32_t min_size, uint32_t gf, uint32_t layer);
+uint32_t tile_size(uint32_t min_size, uint32_t gf, uint32_t layer);
+
+// ---- device index ------------------------------------------------------------------------------
+// One non-empty (shard, layer).  `off` is the element offset of the layer in the index-wide pos
+// (uint2) and sid (u32) arrays; offsets are multiples of 4 so every layer starts 16-byte aligned.
+struct LayerDev {
+    uint64_t off;
+    uint64_t n;
+    uint32_t max_size;  // layer_max_size(K): the look-back of the sweep
+    uint32_t shard;
+    uint32_t layer;
+    uint32_t flags;  // LF_* bits from validation
+};
+enum : uint32_t { LF_UNSORTED = 1u, LF_BAD_SID = 2u, LF_EMPTY_IV = 4u, LF_OVERSIZE = 8u };
+
+// A device allocation that grows on demand (never shrinks).
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    int ensure(size_t bytes);  // cudaMalloc (after cudaFree) when bytes > cap
+    void release();
+    template <class T>
+    T* as() const {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
+}  // namespace rgl
+
+struct rgl_index {
+    int device = 0;
+    uint32_t min_size = 128, gf = 4, num_sources = 0, num_shards = 0, num_slots = 0;
+    std::vector<std::string> shard_names;
+    std::unordered_map<std::string, uint32_t> shard_ids;
+    std::vector<std::string> source_names;
+    std::vector<rgl::LayerDev> layers;  // host copy of the layer table
+    std::vector<int32_t> slot;          // [shard * num_slots + K] -> layer index or -1
+    uint64_t total = 0;                 // intervals
+    uint64_t cap_elems = 0;             // allocated elements (with alignment padding)
+    uint2* d_pos = nullptr;
+    uint32_t* d_sid = nullptr;
+    rgl::LayerDev* d_layers = nullptr;
+    int32_t* d_slot = nullptr;
+    uint64_t device_bytes = 0;
+};
+
+namespace rgl {
+
+// Allocates the device arrays of an index whose host-side layer table is filled (layers, slot,
+// total computed from counts); assigns aligned offsets.
+int index_alloc(rgl_index* idx);
+// Uploads the layer tables and validates every layer on the device (sortedness, source ids,
+// non-empty intervals, size class).  Fails with RGL_ERR_INDEX_INVARIANT on an unsorted layer or a
+// source id >= num_sources.
+int index_finalize(rgl_index* idx);
+void index_free(rgl_index* idx);
+
+// ---- host IO (src/io) -------------------------------------------------------------------------
+struct MetaInfo {
+    std::unordered_map<uint32_t, std::string> sid_map;
+    uint32_t min_size = 128, growth_factor = 4;
+    std::vector<std::string> shards;
+    uint64_t num_layers = 0;
+};
+int meta_load(const std::string& db_dir, MetaInfo* out);
+int read_file(const std::string& path, std::vector<uint8_t>* out);
+bool file_exists(const std::string& path);
+
+// ---- synthetic generator (shared host/device arithmetic) ---------------------------------------
+struct SynthTables {
+    std::vector<uint32_t> lognormal;  // 65537 quantiles of the clipped log-normal length
+    std::vector<uint32_t> loguniform; // 65537 quantiles of log-uniform [10k, 1M]
+};
+const SynthTables& synth_tables();
+
+}  // namespace rgl

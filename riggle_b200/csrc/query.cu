@@ -1,0 +1,790 @@
+// The sweep: query_database's counting path (src/tasks/query/mod.rs:182-307) and
+// query_sweep_windowed (src/sweep/query.rs:127-160) as one device pipeline.
+//
+// Per batch (all on the context stream, no host synchronisation, graph-capturable once the
+// workspace is reserved):
+//   1. k_expand_keys: each query interval becomes key (segment << 32 | start), value end, and a
+//      second key (segment << 32 | end); segment = shard * rows + Q_SID.  Invalid intervals
+//      (start >= end, sid >= rows) raise an error bit.
+//   2. radix sort both key sets (the reference sorts by (sid, start), mod.rs:202; ends are sorted
+//      too, which the rank formulation below needs).
+//   3. exclusive u64 prefix sums of the sorted starts and sorted ends (PS, PE).
+//   4. K1 partition: for every (layer slot K, query i) the candidate range of the reference's scan,
+//      [pp(start - max_K), pp(end)) with pp = partition point of the layer's starts
+//      (src/sweep/query.rs:141-148); a segmented max-scan merges them into disjoint ranges per
+//      (K, segment); an exclusive scan of the range lengths lays all ranges end to end.
+//   5. K2 sweep (k_sweep): a persistent kernel pulls fixed-size chunks of that concatenated range
+//      space from a device counter.  Each thread takes one DB interval d and computes, against the
+//      segment's sorted query starts S and ends E,
+//          count(d) = #{q : q.start < d.end} - #{q : q.end <= d.start}
+//          bp(d)    = Cov(d.end) - Cov(d.start),  Cov(x) = x (S<x - E<=x) - PS(S<x) + PE(E<=x)
+//      which equal the number of overlapping query intervals and their summed intersection length
+//      whenever every DB interval of layer K is non-empty and shorter than max_K — the size-class
+//      invariant the reference's add establishes (src/io/meta.rs:33-58) and index validation checks.
+//      Under that invariant the look-back bound q.start - max_K <= d.start of the reference's scan
+//      never excludes an overlapping pair, so the counts are the reference's, bit for bit.  All
+//      ranks lie inside the window of queries that produced d's range, so the searches are short.
+//      Counts and base pairs are tallied per (row, source) in shared memory when a chunk belongs to
+//      one row, else with global atomics.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cstring>
+
+#include "internal.h"
+
+namespace rgl {
+
+struct RangeDesc {
+    uint32_t db_lo, db_hi;      // DB index range within the layer
+    uint32_t i_first, i_last;   // query window (positions in the sorted arrays)
+    uint32_t layer_idx;         // index into the layer table
+    uint32_t qrow;              // query row (Q_SID)
+};
+
+struct MaxOp {
+    __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
+};
+
+enum : uint32_t { ERR_BAD_INTERVAL = 1u, ERR_BAD_ROW = 2u };
+
+// ---- small device helpers ----------------------------------------------------------------------
+__device__ __forceinline__ uint32_t lb_u32(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi, uint32_t x) {
+    // first index in [lo, hi) with a[i] >= x
+    while (lo < hi) {
+        uint32_t m = lo + ((hi - lo) >> 1);
+        if (__ldg(a + m) < x) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+__device__ __forceinline__ uint32_t ub_u32(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi, uint32_t x) {
+    // first index in [lo, hi) with a[i] > x
+    while (lo < hi) {
+        uint32_t m = lo + ((hi - lo) >> 1);
+        if (__ldg(a + m) <= x) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+__device__ __forceinline__ uint32_t pp_layer(const uint2* __restrict__ pos, uint32_t n, uint32_t x) {
+    // partition point of (start < x) over a layer sorted by start
+    uint32_t lo = 0, hi = n;
+    while (lo < hi) {
+        uint32_t m = lo + ((hi - lo) >> 1);
+        if (__ldg(&pos[m].x) < x) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+
+// ---- 1. keys ------------------------------------------------------------------------------------
+__global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, const uint64_t* __restrict__ blk_off,
+                              const uint32_t* __restrict__ blk_shard, uint32_t nblk, uint32_t rows,
+                              uint64_t* __restrict__ key, uint32_t* __restrict__ val, uint64_t* __restrict__ ekey,
+                              uint32_t* __restrict__ err) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t lo = 0, hi = nblk;  // block b with blk_off[b] <= i < blk_off[b+1]
+    while (hi - lo > 1) {
+        uint32_t m = (lo + hi) >> 1;
+        if (blk_off[m] <= i) lo = m; else hi = m;
+    }
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(iv) + 3ull * i;
+    uint32_t s = w[0], e = w[1], q = w[2];
+    uint32_t bad = 0;
+    if (s >= e) bad |= ERR_BAD_INTERVAL;
+    if (q >= rows) { bad |= ERR_BAD_ROW; q = 0; }
+    if (bad) atomicOr(err, bad);
+    uint64_t seg = (uint64_t)blk_shard[lo] * rows + q;
+    key[i] = (seg << 32) | s;
+    val[i] = e;
+    ekey[i] = (seg << 32) | e;
+}
+
+// ---- 2/3. unpack sorted keys ---------------------------------------------------------------------
+__global__ void k_unpack(uint32_t n, const uint64_t* __restrict__ key, const uint64_t* __restrict__ ekey,
+                         uint32_t* __restrict__ starts, uint32_t* __restrict__ ends_s, uint32_t* __restrict__ seg,
+                         uint32_t* __restrict__ segflag, uint64_t* __restrict__ ps_in, uint64_t* __restrict__ pe_in) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    if (i == n) {
+        ps_in[n] = 0;
+        pe_in[n] = 0;
+        return;
+    }
+    uint64_t k = key[i], ek = ekey[i];
+    uint32_t s = (uint32_t)k, e = (uint32_t)ek;
+    uint32_t sg = (uint32_t)(k >> 32);
+    starts[i] = s;
+    ends_s[i] = e;
+    seg[i] = sg;
+    segflag[i] = (i == 0 || (uint32_t)(key[i - 1] >> 32) != sg) ? 1u : 0u;
+    ps_in[i] = s;
+    pe_in[i] = e;
+}
+
+// ---- 4. K1 partition -----------------------------------------------------------------------------
+// lo/hi of the reference's candidate scan for (slot K, query i), layer-major arrays [K][n].
+__global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ starts,
+                       const uint32_t* __restrict__ qend, const uint32_t* __restrict__ seg,
+                       const int32_t* __restrict__ slot, const LayerDev* __restrict__ layers,
+                       const uint2* __restrict__ pos, uint32_t* __restrict__ lo_out, uint32_t* __restrict__ hi_out) {
+    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)n * nslots) return;
+    uint32_t K = (uint32_t)(t / n), i = (uint32_t)(t % n);
+    uint32_t shard = seg[i] / rows;
+    int32_t li = slot[(uint64_t)shard * nslots + K];
+    uint32_t lo = 0, hi = 0;
+    if (li >= 0) {
+        LayerDev L = layers[li];
+        const uint2* p = pos + L.off;
+        uint32_t s = starts[i];
+        uint32_t back = s >= L.max_size ? s - L.max_size : 0u;  // saturating_sub, query.rs:141
+        lo = pp_layer(p, (uint32_t)L.n, back);
+        hi = pp_layer(p, (uint32_t)L.n, qend[i]);
+        if (hi < lo) hi = lo;
+    }
+    lo_out[t] = lo;
+    hi_out[t] = hi;
+}
+
+// Range starts: first query of a segment, or a query whose lo is past every earlier hi.
+__global__ void k_range_flags(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ seg,
+                              const uint32_t* __restrict__ segflag, const int32_t* __restrict__ slot,
+                              const uint32_t* __restrict__ lo, const uint32_t* __restrict__ maxhi,
+                              uint32_t* __restrict__ rflag) {
+    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t total = (uint64_t)n * nslots;
+    if (t > total) return;
+    if (t == total) {
+        rflag[t] = 0;
+        return;
+    }
+    uint32_t K = (uint32_t)(t / n), i = (uint32_t)(t % n);
+    uint32_t shard = seg[i] / rows;
+    int32_t li = slot[(uint64_t)shard * nslots + K];
+    uint32_t f = 0;
+    if (li >= 0) f = (segflag[i] || lo[t] >= maxhi[t - 1]) ? 1u : 0u;
+    rflag[t] = f;
+}
+
+__global__ void k_range_emit(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ seg,
+                             const uint32_t* __restrict__ segflag, const int32_t* __restrict__ slot,
+                             const uint32_t* __restrict__ lo, const uint32_t* __restrict__ maxhi,
+                             const uint32_t* __restrict__ rflag, const uint32_t* __restrict__ ridx,
+                             RangeDesc* __restrict__ ranges) {
+    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t total = (uint64_t)n * nslots;
+    if (t >= total) return;
+    uint32_t K = (uint32_t)(t / n), i = (uint32_t)(t % n);
+    uint32_t sg = seg[i];
+    int32_t li = slot[(uint64_t)(sg / rows) * nslots + K];
+    if (li < 0) return;
+    uint32_t f = rflag[t];
+    if (!f && ridx[t] == 0) return;  // unreachable: every valid (K, segment) row starts with a flag
+    uint32_t r = ridx[t] + f - 1;  // inclusive range index of this element
+    if (f) {
+        ranges[r].db_lo = lo[t];
+        ranges[r].i_first = i;
+        ranges[r].layer_idx = (uint32_t)li;
+        ranges[r].qrow = sg % rows;
+    }
+    bool last = (i + 1 == n) || segflag[i + 1] || rflag[t + 1];
+    if (last) {
+        ranges[r].i_last = i;
+        ranges[r].db_hi = maxhi[t];
+    }
+}
+
+__global__ void k_range_len(uint64_t cap, const uint32_t* __restrict__ ridx_total_ptr,
+                            const RangeDesc* __restrict__ ranges, uint64_t* __restrict__ rlen) {
+    uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (r > cap) return;
+    uint32_t R = *ridx_total_ptr;
+    rlen[r] = (r < R) ? (uint64_t)(ranges[r].db_hi - ranges[r].db_lo) : 0ull;
+}
+
+// ---- 5. K2 sweep -----------------------------------------------------------------------------------
+struct SweepParams {
+    const uint64_t* rpos;   // exclusive scan of range lengths, cap+1 entries; rpos[cap] = total
+    uint64_t rcap;          // range capacity (entries of rpos minus one)
+    const RangeDesc* ranges;
+    const LayerDev* layers;
+    const uint2* pos;
+    const uint32_t* sid;
+    const uint32_t* starts;  // sorted (segment, start)
+    const uint32_t* ends;    // sorted (segment, end)
+    const uint64_t* ps;      // exclusive prefix sums of starts
+    const uint64_t* pe;      // exclusive prefix sums of ends
+    uint32_t* counts;        // rows x D
+    unsigned long long* bp;  // rows x D (may be null)
+    uint32_t* queue;         // work counter
+    uint32_t rows, D, chunk;
+    int smem_tally;          // 1: one row, shared-memory histograms
+};
+
+template <bool WITH_BP>
+__global__ void __launch_bounds__(256) k_sweep(SweepParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
+    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
+    __shared__ uint32_t s_item;
+    __shared__ uint32_t s_r0, s_r1;
+
+    const uint64_t total = P.rpos[P.rcap];
+    if (P.smem_tally) {
+        for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
+            s_cnt[k] = 0;
+            if (WITH_BP) s_bp[k] = 0;
+        }
+    }
+    __syncthreads();
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(P.queue, 1u);
+        __syncthreads();
+        const uint64_t p0 = (uint64_t)s_item * P.chunk;
+        if (p0 >= total) break;
+        const uint64_t p1 = min(p0 + P.chunk, total);
+        if (threadIdx.x == 0) {
+            // last range r with rpos[r] <= p0, and last with rpos[r] <= p1 - 1
+            uint64_t lo = 0, hi = P.rcap;
+            while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (P.rpos[m] <= p0) lo = m; else hi = m - 1; }
+            s_r0 = (uint32_t)lo;
+            uint64_t lo2 = lo;
+            hi = P.rcap;
+            while (lo2 < hi) { uint64_t m = (lo2 + hi + 1) >> 1; if (P.rpos[m] <= p1 - 1) lo2 = m; else hi = m - 1; }
+            s_r1 = (uint32_t)lo2;
+        }
+        __syncthreads();
+        const uint32_t r0 = s_r0, r1 = s_r1;
+        uint32_t r = r0;
+        for (uint64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+            // advance to the range holding p (positions are visited in increasing order)
+            {
+                uint32_t lo = r, hi = r1;
+                while (lo < hi) {
+                    uint32_t m = (lo + hi + 1) >> 1;
+                    if (__ldg(P.rpos + m) <= p) lo = m; else hi = m - 1;
+                }
+                r = lo;
+            }
+            const RangeDesc rd = P.ranges[r];
+            const LayerDev L = P.layers[rd.layer_idx];
+            const uint64_t di = L.off + rd.db_lo + (p - P.rpos[r]);
+            const uint2 d = P.pos[di];
+            const uint32_t wlo = rd.i_first, whi = rd.i_last + 1;
+            const uint32_t sl_s = lb_u32(P.starts, wlo, whi, d.x);
+            const uint32_t el_s = ub_u32(P.ends, wlo, whi, d.x);
+            const uint32_t sl_e = lb_u32(P.starts, sl_s, whi, d.y);
+            const uint32_t cnt = sl_e - el_s;
+            if (cnt) {
+                const uint32_t sid = __ldg(P.sid + di);
+                unsigned long long bpv = 0;
+                if (WITH_BP) {
+                    const uint32_t el_e = ub_u32(P.ends, el_s, whi, d.y);
+                    const unsigned long long ce = (unsigned long long)d.y * (unsigned long long)(sl_e - el_e) -
+                                                  P.ps[sl_e] + P.pe[el_e];
+                    const unsigned long long cs = (unsigned long long)d.x * (unsigned long long)(sl_s - el_s) -
+                                                  P.ps[sl_s] + P.pe[el_s];
+                    bpv = ce - cs;
+                }
+                if (P.smem_tally) {
+                    atomicAdd(&s_cnt[sid], cnt);
+                    if (WITH_BP) atomicAdd(&s_bp[sid], bpv);
+                } else {
+                    const uint64_t cell = (uint64_t)rd.qrow * P.D + sid;
+                    atomicAdd(&P.counts[cell], cnt);
+                    if (WITH_BP) atomicAdd(&P.bp[cell], bpv);
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (P.smem_tally) {
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
+            if (s_cnt[k]) atomicAdd(&P.counts[k], s_cnt[k]);
+            if (WITH_BP && s_bp[k]) atomicAdd(&P.bp[k], s_bp[k]);
+        }
+    }
+}
+
+}  // namespace rgl
+
+using namespace rgl;
+
+// ================================================================================================
+// Context
+// ================================================================================================
+struct rgl_context {
+    rgl_index* idx = nullptr;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int num_sms = 148;
+    DevBuf iv, blk_off, blk_shard, key_a, key_b, val_a, val_b, ekey_a, ekey_b;
+    DevBuf starts, ends, seg, segflag, segnum, seg_begin, ps_in, pe_in, ps, pe;
+    DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp;
+    uint32_t* h_small = nullptr;  // pinned mirror of `small`
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    uint64_t res_n = 0;
+    uint32_t res_rows = 0;
+    // sweep-kernel timing on the launch stream (rgl_context_set_timing)
+    bool timing = false;
+    std::vector<cudaEvent_t> tev;  // pairs (start, end)
+    size_t tev_used = 0;
+    // state of the last launch, for stats
+    uint64_t last_tot = 0;
+    uint32_t last_launches = 0;
+    uint32_t last_n = 0;
+};
+
+namespace {
+
+int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
+    rgl_index* idx = c->idx;
+    const uint64_t ns = std::max<uint32_t>(idx->num_slots, 1);
+    const uint64_t tot = n * ns;
+    RGL_TRY(c->iv.ensure(n * sizeof(rgl_interval) + 16));
+    RGL_TRY(c->blk_off.ensure((nblk + 1) * 8ull));
+    RGL_TRY(c->blk_shard.ensure((nblk + 1) * 4ull));
+    RGL_TRY(c->key_a.ensure(n * 8 + 8));
+    RGL_TRY(c->key_b.ensure(n * 8 + 8));
+    RGL_TRY(c->val_a.ensure(n * 4 + 4));
+    RGL_TRY(c->val_b.ensure(n * 4 + 4));
+    RGL_TRY(c->ekey_a.ensure(n * 8 + 8));
+    RGL_TRY(c->ekey_b.ensure(n * 8 + 8));
+    RGL_TRY(c->starts.ensure(n * 4 + 4));
+    RGL_TRY(c->ends.ensure(n * 4 + 4));
+    RGL_TRY(c->seg.ensure(n * 4 + 4));
+    RGL_TRY(c->segflag.ensure(n * 4 + 4));
+    RGL_TRY(c->segnum.ensure(n * 4 + 4));
+    RGL_TRY(c->seg_begin.ensure(n * 4 + 4));
+    RGL_TRY(c->ps_in.ensure(n * 8 + 16));
+    RGL_TRY(c->pe_in.ensure(n * 8 + 16));
+    RGL_TRY(c->ps.ensure(n * 8 + 16));
+    RGL_TRY(c->pe.ensure(n * 8 + 16));
+    RGL_TRY(c->lo.ensure(tot * 4 + 4));
+    RGL_TRY(c->hi.ensure(tot * 4 + 4));
+    RGL_TRY(c->maxhi.ensure(tot * 4 + 4));
+    RGL_TRY(c->rflag.ensure(tot * 4 + 8));
+    RGL_TRY(c->ridx.ensure(tot * 4 + 8));
+    RGL_TRY(c->ranges.ensure(tot * sizeof(RangeDesc) + sizeof(RangeDesc)));
+    RGL_TRY(c->rlen.ensure(tot * 8 + 16));
+    RGL_TRY(c->rpos.ensure(tot * 8 + 16));
+    RGL_TRY(c->small.ensure(256));
+    // CUB temporary storage: the maximum over every primitive used, at these sizes.
+    size_t need = 0, b = 0;
+    int nn = (int)std::max<uint64_t>(n, 1);
+    int nt = (int)std::max<uint64_t>(tot + 1, 1);
+    cub::DeviceRadixSort::SortPairs(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, (uint32_t*)nullptr,
+                                    (uint32_t*)nullptr, nn, 0, 64, c->stream);
+    need = std::max(need, b);
+    cub::DeviceRadixSort::SortKeys(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nn, 0, 64, c->stream);
+    need = std::max(need, b);
+    cub::DeviceScan::InclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, nn, c->stream);
+    need = std::max(need, b);
+    cub::DeviceScan::ExclusiveSum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nn + 1, c->stream);
+    need = std::max(need, b);
+    cub::DeviceScan::InclusiveScanByKey(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, (uint32_t*)nullptr,
+                                        MaxOp(), nn, cub::Equality(), c->stream);
+    need = std::max(need, b);
+    cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, nt, c->stream);
+    need = std::max(need, b);
+    cub::DeviceScan::ExclusiveSum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nt, c->stream);
+    need = std::max(need, b);
+    RGL_TRY(c->cub_tmp.ensure(need + 256));
+    if (rows) {
+        RGL_TRY(c->out_counts.ensure((uint64_t)rows * idx->num_sources * 4 + 16));
+        RGL_TRY(c->out_bp.ensure((uint64_t)rows * idx->num_sources * 8 + 16));
+    }
+    c->res_n = std::max(c->res_n, n);
+    c->res_rows = std::max(c->res_rows, rows);
+    return RGL_OK;
+}
+
+inline unsigned grid_for(uint64_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
+
+struct Launch {
+    uint32_t chunk, ctas_per_sm, block;
+};
+
+Launch pick_launch(const rgl_query_opts* o) {
+    Launch l{4096, 4, 256};
+    if (o) {
+        if (o->chunk) l.chunk = o->chunk;
+        if (o->ctas_per_sm) l.ctas_per_sm = o->ctas_per_sm;
+        if (o->block) l.block = 256;  // the kernel is compiled for 256 threads
+    }
+    if (l.chunk < 256) l.chunk = 256;
+    if (l.ctas_per_sm < 1) l.ctas_per_sm = 1;
+    if (l.ctas_per_sm > 8) l.ctas_per_sm = 8;
+    return l;
+}
+
+int timing_record(rgl_context* c, bool start) {
+    if (start) {
+        while (c->tev.size() < 2 * (c->tev_used + 1)) {
+            cudaEvent_t e;
+            RGL_CUDA(cudaEventCreate(&e));
+            c->tev.push_back(e);
+        }
+        RGL_CUDA(cudaEventRecord(c->tev[2 * c->tev_used], c->stream));
+    } else {
+        RGL_CUDA(cudaEventRecord(c->tev[2 * c->tev_used + 1], c->stream));
+        c->tev_used++;
+    }
+    return RGL_OK;
+}
+
+// After the stream has been synchronised: error bits and stats of the last launch.
+int finish(rgl_context* c, const Launch& L, rgl_query_stats* stats) {
+    if (stats) {
+        float t_sweep = 0, t_all = 0;
+        cudaEventElapsedTime(&t_sweep, c->ev[1], c->ev[2]);
+        cudaEventElapsedTime(&t_all, c->ev[0], c->ev[2]);
+        stats->query_intervals = c->last_n;
+        stats->ranges = c->last_n ? c->h_small[2] : 0;
+        uint64_t T = 0;
+        if (c->last_n) std::memcpy(&T, c->h_small + 4, 8);
+        stats->db_swept = T;
+        stats->work_items = (T + L.chunk - 1) / L.chunk;
+        stats->sweep_ms = c->last_n ? t_sweep : 0.f;
+        stats->device_ms = c->last_n ? t_all : 0.f;
+        stats->chunk = L.chunk;
+        stats->ctas_per_sm = L.ctas_per_sm;
+        stats->block = L.block;
+        stats->kernel_launches = c->last_launches;
+    }
+    if (c->h_small[0] & ERR_BAD_INTERVAL) return fail(RGL_ERR_INVALID_ARGUMENT, "a query interval has start >= end");
+    if (c->h_small[0] & ERR_BAD_ROW) return fail(RGL_ERR_INVALID_ARGUMENT, "a query interval's sid >= num_rows");
+    return RGL_OK;
+}
+
+// Runs steps 1-5 for n intervals already in c->iv with block table in c->blk_off/c->blk_shard.
+int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, const rgl_query_opts* opts,
+                 uint32_t* d_counts, unsigned long long* d_bp, rgl_query_stats* stats) {
+    rgl_index* idx = c->idx;
+    cudaStream_t st = c->stream;
+    const uint32_t D = idx->num_sources;
+    const uint32_t ns = idx->num_slots;
+    const uint32_t n = (uint32_t)n64;
+    Launch L = pick_launch(opts);
+    const bool with_bp = d_bp != nullptr && !(opts && (opts->flags & RGL_QF_NO_OVERLAP));
+
+    uint32_t* d_small = c->small.as<uint32_t>();  // [0] error bits, [1] queue, [2..] scratch
+    RGL_CUDA(cudaMemsetAsync(d_small, 0, 64, st));
+    if (d_counts) RGL_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)rows * D * 4, st));
+    if (d_bp) RGL_CUDA(cudaMemsetAsync(d_bp, 0, (size_t)rows * D * 8, st));
+    if (n == 0 || ns == 0) {
+        c->last_n = 0;
+        c->last_tot = 0;
+        c->last_launches = 0;
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
+        return RGL_OK;
+    }
+    // key width: segment = shard * rows + row
+    uint64_t nseg = (uint64_t)idx->num_shards * rows;
+    int segbits = 1;
+    while (segbits < 32 && (1ull << segbits) < nseg) segbits++;
+    if (nseg >= (1ull << 32)) return fail(RGL_ERR_INVALID_ARGUMENT, "num_shards * num_rows must be < 2^32");
+
+    if (stats) RGL_CUDA(cudaEventRecord(c->ev[0], st));
+    uint32_t launches = 0;
+    k_expand_keys<<<grid_for(n, 256), 256, 0, st>>>(n, c->iv.as<rgl_interval>(), c->blk_off.as<uint64_t>(),
+                                                    c->blk_shard.as<uint32_t>(), nblk, rows, c->key_a.as<uint64_t>(),
+                                                    c->val_a.as<uint32_t>(), c->ekey_a.as<uint64_t>(), d_small);
+    launches++;
+    size_t tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tb, c->key_a.as<uint64_t>(), c->key_b.as<uint64_t>(),
+                                             c->val_a.as<uint32_t>(), c->val_b.as<uint32_t>(), (int)n, 0,
+                                             32 + segbits, st));
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceRadixSort::SortKeys(c->cub_tmp.p, tb, c->ekey_a.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
+                                            (int)n, 0, 32 + segbits, st));
+    k_unpack<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->key_b.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
+                                                   c->starts.as<uint32_t>(), c->ends.as<uint32_t>(),
+                                                   c->seg.as<uint32_t>(), c->segflag.as<uint32_t>(),
+                                                   c->ps_in.as<uint64_t>(), c->pe_in.as<uint64_t>());
+    launches++;
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tb, c->segflag.as<uint32_t>(), c->segnum.as<uint32_t>(),
+                                           (int)n, st));
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->ps_in.as<uint64_t>(), c->ps.as<uint64_t>(),
+                                           (int)n + 1, st));
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->pe_in.as<uint64_t>(), c->pe.as<uint64_t>(),
+                                           (int)n + 1, st));
+    const uint64_t tot = (uint64_t)n * ns;
+    k_lohi<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, rows, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
+                                                c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, idx->d_pos,
+                                                c->lo.as<uint32_t>(), c->hi.as<uint32_t>());
+    launches++;
+    for (uint32_t K = 0; K < ns; K++) {
+        tb = c->cub_tmp.cap;
+        RGL_CUDA(cub::DeviceScan::InclusiveScanByKey(c->cub_tmp.p, tb, c->segnum.as<uint32_t>(),
+                                                     c->hi.as<uint32_t>() + (uint64_t)K * n,
+                                                     c->maxhi.as<uint32_t>() + (uint64_t)K * n, MaxOp(), (int)n,
+                                                     cub::Equality(), st));
+    }
+    k_range_flags<<<grid_for(tot + 1, 256), 256, 0, st>>>(n, ns, rows, c->seg.as<uint32_t>(),
+                                                          c->segflag.as<uint32_t>(), idx->d_slot,
+                                                          c->lo.as<uint32_t>(), c->maxhi.as<uint32_t>(),
+                                                          c->rflag.as<uint32_t>());
+    launches++;
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
+                                           (int)(tot + 1), st));
+    k_range_emit<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, rows, c->seg.as<uint32_t>(), c->segflag.as<uint32_t>(),
+                                                     idx->d_slot, c->lo.as<uint32_t>(), c->maxhi.as<uint32_t>(),
+                                                     c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
+                                                     c->ranges.as<RangeDesc>());
+    launches++;
+    k_range_len<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, c->ridx.as<uint32_t>() + tot, c->ranges.as<RangeDesc>(),
+                                                        c->rlen.as<uint64_t>());
+    launches++;
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(),
+                                           (int)(tot + 1), st));
+
+    SweepParams P;
+    P.rpos = c->rpos.as<uint64_t>();
+    P.rcap = tot;
+    P.ranges = c->ranges.as<RangeDesc>();
+    P.layers = idx->d_layers;
+    P.pos = idx->d_pos;
+    P.sid = idx->d_sid;
+    P.starts = c->starts.as<uint32_t>();
+    P.ends = c->ends.as<uint32_t>();
+    P.ps = c->ps.as<uint64_t>();
+    P.pe = c->pe.as<uint64_t>();
+    P.counts = d_counts;
+    P.bp = with_bp ? d_bp : nullptr;
+    P.queue = d_small + 1;
+    P.rows = rows;
+    P.D = D;
+    P.chunk = L.chunk;
+    size_t smem = (size_t)D * (with_bp ? 12 : 4);
+    P.smem_tally = (rows == 1 && smem <= 160 * 1024) ? 1 : 0;
+    if (!P.smem_tally) smem = 0;
+    unsigned grid = (unsigned)(c->num_sms * L.ctas_per_sm);
+    if (stats) RGL_CUDA(cudaEventRecord(c->ev[1], st));
+    if (c->timing) RGL_TRY(timing_record(c, true));
+    if (with_bp) {
+        if (smem > 48 * 1024)
+            RGL_CUDA(cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_sweep<true><<<grid, 256, smem, st>>>(P);
+    } else {
+        if (smem > 48 * 1024)
+            RGL_CUDA(cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_sweep<false><<<grid, 256, smem, st>>>(P);
+    }
+    launches++;
+    RGL_CUDA(cudaGetLastError());
+    if (c->timing) RGL_TRY(timing_record(c, false));
+    c->last_tot = tot;
+    c->last_launches = launches;
+    c->last_n = n;
+    if (stats) {
+        RGL_CUDA(cudaEventRecord(c->ev[2], st));
+        RGL_CUDA(cudaMemcpyAsync(c->h_small + 2, c->ridx.as<uint32_t>() + tot, 4, cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaMemcpyAsync(c->h_small + 4, c->rpos.as<uint64_t>() + tot, 8, cudaMemcpyDeviceToHost, st));
+    }
+    RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
+    return RGL_OK;
+}
+
+// Maps a batch's shards to index shard ids; shards absent from the index are skipped, as the
+// reference skips shards not in meta.shards (src/tasks/query/mod.rs:194-196).
+int resolve_blocks(rgl_context* c, const rgl_query_batch* b, std::vector<uint32_t>* shard_ids,
+                   std::vector<const rgl_query_shard*>* blocks) {
+    for (uint32_t i = 0; i < b->num_shards; i++) {
+        const rgl_query_shard& s = b->shards[i];
+        uint32_t id;
+        if (s.shard_name) {
+            auto it = c->idx->shard_ids.find(s.shard_name);
+            if (it == c->idx->shard_ids.end()) continue;
+            id = it->second;
+        } else {
+            id = s.shard_id;
+            if (id >= c->idx->num_shards) continue;
+        }
+        if (s.count == 0) continue;
+        if (!s.intervals) return fail(RGL_ERR_INVALID_ARGUMENT, "query shard without intervals");
+        shard_ids->push_back(id);
+        blocks->push_back(&s);
+    }
+    return RGL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
+    clear_error();
+    if (!index || !out) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    auto* c = new rgl_context();
+    c->idx = index;
+    int s = RGL_OK;
+    if (cudaSetDevice(index->device) != cudaSuccess) s = fail(RGL_ERR_DEVICE, "cudaSetDevice");
+    if (s == RGL_OK) {
+        if (stream) c->stream = reinterpret_cast<cudaStream_t>(stream);
+        else if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess)
+            s = fail(RGL_ERR_DEVICE, "cudaStreamCreate");
+        else
+            c->own_stream = true;
+    }
+    if (s == RGL_OK) cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, index->device);
+    for (int i = 0; i < 4 && s == RGL_OK; i++)
+        if (cudaEventCreate(&c->ev[i]) != cudaSuccess) s = fail(RGL_ERR_DEVICE, "cudaEventCreate");
+    if (s == RGL_OK && cudaMallocHost(&c->h_small, 256) != cudaSuccess) s = fail(RGL_ERR_OOM, "pinned");
+    if (s == RGL_OK) s = c->small.ensure(256);
+    if (s != RGL_OK) {
+        rgl_context_destroy(c);
+        return s;
+    }
+    *out = c;
+    return RGL_OK;
+}
+
+int rgl_context_destroy(rgl_context* c) {
+    if (!c) return RGL_OK;
+    cudaSetDevice(c->idx->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    DevBuf* bufs[] = {&c->iv, &c->blk_off, &c->blk_shard, &c->key_a, &c->key_b, &c->val_a, &c->val_b,
+                      &c->ekey_a, &c->ekey_b, &c->starts, &c->ends, &c->seg, &c->segflag, &c->segnum,
+                      &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps, &c->pe, &c->lo, &c->hi, &c->maxhi,
+                      &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos, &c->cub_tmp, &c->small,
+                      &c->out_counts, &c->out_bp};
+    for (DevBuf* b : bufs) b->release();
+    for (auto& e : c->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : c->tev) cudaEventDestroy(e);
+    if (c->h_small) cudaFreeHost(c->h_small);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return RGL_OK;
+}
+
+int rgl_context_reserve(rgl_context* c, uint64_t max_intervals, uint32_t max_rows) {
+    clear_error();
+    if (!c) return fail(RGL_ERR_INVALID_ARGUMENT, "null context");
+    RGL_CUDA(cudaSetDevice(c->idx->device));
+    return ensure_workspace(c, max_intervals, max_rows, 4096);
+}
+
+void* rgl_context_stream(rgl_context* c) { return c ? (void*)c->stream : nullptr; }
+
+int rgl_context_sync(rgl_context* c) {
+    if (!c) return fail(RGL_ERR_INVALID_ARGUMENT, "null context");
+    RGL_CUDA(cudaStreamSynchronize(c->stream));
+    return RGL_OK;
+}
+
+int rgl_query_counts_device(rgl_context* c, uint32_t num_rows, uint32_t num_shards, const uint32_t* shard_ids,
+                            const uint64_t* shard_offsets, const rgl_interval* d_intervals,
+                            const rgl_query_opts* opts, uint32_t* d_counts, uint64_t* d_overlap_bp,
+                            rgl_query_stats* stats) {
+    clear_error();
+    if (!c || (num_shards && (!shard_ids || !shard_offsets))) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    if (!d_counts) return fail(RGL_ERR_INVALID_ARGUMENT, "counts buffer is required");
+    RGL_CUDA(cudaSetDevice(c->idx->device));
+    uint64_t n = num_shards ? shard_offsets[num_shards] - shard_offsets[0] : 0;
+    if (n >= (1ull << 31)) return fail(RGL_ERR_INVALID_ARGUMENT, "at most 2^31-1 query intervals per call");
+    for (uint32_t i = 0; i < num_shards; i++)
+        if (shard_ids[i] >= c->idx->num_shards) return fail(RGL_ERR_INVALID_ARGUMENT, "shard id out of range");
+    RGL_TRY(ensure_workspace(c, n, 0, num_shards));
+    std::vector<uint64_t> off(num_shards + 1);
+    for (uint32_t i = 0; i <= num_shards; i++) off[i] = shard_offsets[i] - shard_offsets[0];
+    if (num_shards) {
+        RGL_CUDA(cudaMemcpyAsync(c->blk_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice, c->stream));
+        RGL_CUDA(cudaMemcpyAsync(c->blk_shard.p, shard_ids, num_shards * 4ull, cudaMemcpyHostToDevice, c->stream));
+        RGL_CUDA(cudaMemcpyAsync(c->iv.p, d_intervals + shard_offsets[0], n * sizeof(rgl_interval),
+                                 cudaMemcpyDeviceToDevice, c->stream));
+    }
+    RGL_TRY(run_pipeline(c, n, num_rows, num_shards, opts, d_counts,
+                         reinterpret_cast<unsigned long long*>(d_overlap_bp), stats));
+    if (!stats) return RGL_OK;
+    RGL_CUDA(cudaStreamSynchronize(c->stream));
+    return finish(c, pick_launch(opts), stats);
+}
+
+int rgl_query_counts(rgl_context* c, const rgl_query_batch* b, const rgl_query_opts* opts, uint32_t* counts,
+                     uint64_t* overlap_bp, rgl_query_stats* stats) {
+    clear_error();
+    if (!c || !b || !counts) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    RGL_CUDA(cudaSetDevice(c->idx->device));
+    std::vector<uint32_t> ids;
+    std::vector<const rgl_query_shard*> blocks;
+    RGL_TRY(resolve_blocks(c, b, &ids, &blocks));
+    uint64_t n = 0;
+    std::vector<uint64_t> off(blocks.size() + 1, 0);
+    for (size_t i = 0; i < blocks.size(); i++) {
+        off[i] = n;
+        n += blocks[i]->count;
+    }
+    off[blocks.size()] = n;
+    if (n >= (1ull << 31)) return fail(RGL_ERR_INVALID_ARGUMENT, "at most 2^31-1 query intervals per call");
+    const uint32_t rows = b->num_rows;
+    const uint64_t cells = (uint64_t)rows * c->idx->num_sources;
+    RGL_TRY(ensure_workspace(c, n, rows, (uint32_t)blocks.size()));
+    cudaStream_t st = c->stream;
+    for (size_t i = 0; i < blocks.size(); i++)
+        RGL_CUDA(cudaMemcpyAsync(c->iv.as<rgl_interval>() + off[i], blocks[i]->intervals,
+                                 blocks[i]->count * sizeof(rgl_interval), cudaMemcpyHostToDevice, st));
+    if (!blocks.empty()) {
+        RGL_CUDA(cudaMemcpyAsync(c->blk_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st));
+        RGL_CUDA(cudaMemcpyAsync(c->blk_shard.p, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st));
+    }
+    RGL_TRY(run_pipeline(c, n, rows, (uint32_t)blocks.size(), opts, c->out_counts.as<uint32_t>(),
+                         overlap_bp ? c->out_bp.as<unsigned long long>() : nullptr, stats));
+    if (cells) {
+        RGL_CUDA(cudaMemcpyAsync(counts, c->out_counts.p, cells * 4, cudaMemcpyDeviceToHost, st));
+        if (overlap_bp) RGL_CUDA(cudaMemcpyAsync(overlap_bp, c->out_bp.p, cells * 8, cudaMemcpyDeviceToHost, st));
+    }
+    RGL_CUDA(cudaStreamSynchronize(st));
+    return finish(c, pick_launch(opts), stats);
+}
+
+int rgl_context_check(rgl_context* c) {
+    clear_error();
+    if (!c) return fail(RGL_ERR_INVALID_ARGUMENT, "null context");
+    RGL_CUDA(cudaStreamSynchronize(c->stream));
+    return finish(c, pick_launch(nullptr), nullptr);
+}
+
+int rgl_context_set_timing(rgl_context* c, int on) {
+    if (!c) return fail(RGL_ERR_INVALID_ARGUMENT, "null context");
+    c->timing = on != 0;
+    c->tev_used = 0;
+    return RGL_OK;
+}
+
+int rgl_context_sweep_times(rgl_context* c, float* total_ms, uint32_t* launches) {
+    if (!c || !total_ms || !launches) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    RGL_CUDA(cudaStreamSynchronize(c->stream));
+    float tot = 0;
+    for (size_t i = 0; i < c->tev_used; i++) {
+        float ms = 0;
+        RGL_CUDA(cudaEventElapsedTime(&ms, c->tev[2 * i], c->tev[2 * i + 1]));
+        tot += ms;
+    }
+    *total_ms = tot;
+    *launches = (uint32_t)c->tev_used;
+    c->tev_used = 0;
+    return RGL_OK;
+}
+
+int rgl_host_alloc(uint64_t bytes, void** out) {
+    if (!out) return fail(RGL_ERR_INVALID_ARGUMENT, "null output");
+    *out = nullptr;
+    RGL_CUDA(cudaMallocHost(out, bytes ? bytes : 1));
+    return RGL_OK;
+}
+
+int rgl_host_free(void* p) {
+    if (p) RGL_CUDA(cudaFreeHost(p));
+    return RGL_OK;
+}
+
+}  // extern "C"
