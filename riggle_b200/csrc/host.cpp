@@ -19,7 +19,10 @@ int fail(int code, const std::string& msg) {
     g_last_error = msg;
     return code;
 }
-void clear_error() { g_last_error.clear(); }
+void clear_error() {
+    g_last_error.clear();
+    (void)cudaGetLastError();  // a failed call of an earlier, unrelated operation must not leak into this one
+}
 
 static inline bool is_pow2(uint32_t x) { return x != 0 && (x & (x - 1)) == 0; }
 

@@ -110,6 +110,13 @@ int index_finalize(rgl_index* idx) {
     return RGL_OK;
 }
 
+void index_release(rgl_index* idx) {
+    if (idx && idx->refs.fetch_sub(1) == 1) {
+        index_free(idx);
+        delete idx;
+    }
+}
+
 void index_free(rgl_index* idx) {
     if (!idx) return;
     cudaSetDevice(idx->device);
@@ -341,9 +348,8 @@ int rgl_index_open(const char* db_dir, int device, rgl_index** out) {
 }
 
 int rgl_index_close(rgl_index* index) {
-    if (!index) return RGL_OK;
-    index_free(index);
-    delete index;
+    clear_error();
+    index_release(index);
     return RGL_OK;
 }
 

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 #include <string>
@@ -79,6 +80,9 @@ struct rgl_index {
     rgl::LayerDev* d_layers = nullptr;
     int32_t* d_slot = nullptr;
     uint64_t device_bytes = 0;
+    // one reference for the handle returned to the caller plus one per live context; the device
+    // memory is released when the last reference goes (rgl_index_close may precede the contexts)
+    std::atomic<int> refs{1};
 };
 
 namespace rgl {
@@ -91,6 +95,7 @@ int index_alloc(rgl_index* idx);
 // source id >= num_sources.
 int index_finalize(rgl_index* idx);
 void index_free(rgl_index* idx);
+void index_release(rgl_index* idx);
 
 // ---- host IO (src/io) -------------------------------------------------------------------------
 struct MetaInfo {

@@ -315,7 +315,8 @@ using namespace rgl;
 // Context
 // ================================================================================================
 struct rgl_context {
-    rgl_index* idx = nullptr;
+    rgl_index* idx = nullptr;  // holds one reference of the index
+    int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     int num_sms = 148;
@@ -438,8 +439,10 @@ int timing_record(rgl_context* c, bool start) {
 int finish(rgl_context* c, const Launch& L, rgl_query_stats* stats) {
     if (stats) {
         float t_sweep = 0, t_all = 0;
-        cudaEventElapsedTime(&t_sweep, c->ev[1], c->ev[2]);
-        cudaEventElapsedTime(&t_all, c->ev[0], c->ev[2]);
+        if (c->last_n) {  // the events are recorded only when the pipeline ran
+            RGL_CUDA(cudaEventElapsedTime(&t_sweep, c->ev[1], c->ev[2]));
+            RGL_CUDA(cudaEventElapsedTime(&t_all, c->ev[0], c->ev[2]));
+        }
         stats->query_intervals = c->last_n;
         stats->ranges = c->last_n ? c->h_small[2] : 0;
         uint64_t T = 0;
@@ -625,6 +628,8 @@ int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
     if (!index || !out) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
     auto* c = new rgl_context();
     c->idx = index;
+    c->device = index->device;
+    index->refs.fetch_add(1);
     int s = RGL_OK;
     if (cudaSetDevice(index->device) != cudaSuccess) s = fail(RGL_ERR_DEVICE, "cudaSetDevice");
     if (s == RGL_OK) {
@@ -648,8 +653,9 @@ int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
 }
 
 int rgl_context_destroy(rgl_context* c) {
+    clear_error();
     if (!c) return RGL_OK;
-    cudaSetDevice(c->idx->device);
+    cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->iv, &c->blk_off, &c->blk_shard, &c->key_a, &c->key_b, &c->val_a, &c->val_b,
                       &c->ekey_a, &c->ekey_b, &c->starts, &c->ends, &c->seg, &c->segflag, &c->segnum,
@@ -662,7 +668,9 @@ int rgl_context_destroy(rgl_context* c) {
     for (auto& e : c->tev) cudaEventDestroy(e);
     if (c->h_small) cudaFreeHost(c->h_small);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    index_release(c->idx);
     delete c;
+    (void)cudaGetLastError();
     return RGL_OK;
 }
 

@@ -46,7 +46,13 @@ def test_random_parity_with_oracle(seed):
     c, bp, st = gpu_counts(layers, {f"s{k}": v for k, v in qsh.items()}, rows, D, nsh)
     assert (c == oc).all()
     assert (bp == obp).all()
-    assert st["db_swept"] == ost["db_swept"]
+    # the device sweeps the union of candidate ranges once per (shard, query row)
+    per_row = 0
+    for r in range(rows):
+        sub = {k: v[v[:, 2] == r] for k, v in qsh.items()}
+        sub = {k: np.concatenate([v[:, :2], np.zeros((len(v), 1), np.uint32)], 1) for k, v in sub.items() if len(v)}
+        per_row += O.query_database(layers, sub, 1, D)[3]["db_swept"] if sub else 0
+    assert st["db_swept"] == per_row
 
 
 def test_small_parity_with_bruteforce_u32_extremes():
