@@ -46,32 +46,40 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
+    ap.add_argument("--db-intervals", type=int, default=2_000_000_000,
+                    help="database size of the plain workload (smaller values for profiling captures)")
+    ap.add_argument("--chroms", type=int, default=24,
+                    help="keep only the first N chromosomes, scaling database and query sizes by their share "
+                         "of the genome (same per-bp density; for profiling captures)")
     return ap.parse_args()
 
 
 # ---------------------------------------------------------------------------------------------
 # workload definitions
 # ---------------------------------------------------------------------------------------------
-def workload_spec(name):
+def workload_spec(name, db_intervals=2_000_000_000, chroms=24):
     import riggle_b200 as rg
 
     cl = rg.synth_chrom_lengths(1, 24)
+    share = float(cl[:chroms].sum()) / float(cl.sum())
+    cl = cl[:chroms]
     if name == "plain":
-        sizes = rg.synth_zipf_sizes(1000, 1.1, 1000, 10_000_000, 2_000_000_000)
+        sizes = rg.synth_zipf_sizes(1000, 1.1, max(1, int(1000 * share)), max(1, int(10_000_000 * share)),
+                                    int(db_intervals * share))
         db = rg.SynthSpec(2, cl, sizes, broad_fraction=0.05)
-        qsize = 100_000
-        desc = {"workload": "plain GPU-scale sweep: 1,000-file Zipf(1.1) database, 2e9 intervals "
+        qsize = int(round(100_000 * share))
+        desc = {"workload": f"plain GPU-scale sweep: 1,000-file Zipf(1.1) database, {db_intervals:.3g} intervals "
                             "(5% broad 10k-1M bp), one 1e5-interval query file per launch",
                 "db_files": 1000, "db_intervals": int(sizes.sum()), "query_intervals_per_step": qsize,
-                "chromosomes": 24, "bin_size": 100, "layer_config": "min_size 128, growth_factor 4"}
+                "chromosomes": len(cl), "bin_size": 100, "layer_config": "min_size 128, growth_factor 4"}
     else:
-        sizes = np.full(64, 50_000, np.uint64)
+        sizes = np.full(64, int(round(50_000 * share)), np.uint64)
         db = rg.SynthSpec(2, cl, sizes)
-        qsize = 10_000
+        qsize = int(round(10_000 * share))
         desc = {"workload": "plain CPU-runnable sweep: 64-file database x 50k intervals, one 1e4-interval "
                             "query file per launch",
                 "db_files": 64, "db_intervals": int(sizes.sum()), "query_intervals_per_step": qsize,
-                "chromosomes": 24, "bin_size": 100, "layer_config": "min_size 128, growth_factor 4"}
+                "chromosomes": len(cl), "bin_size": 100, "layer_config": "min_size 128, growth_factor 4"}
     return cl, db, qsize, desc
 
 
@@ -203,7 +211,9 @@ def run_reference(args, rank, world):
     this image) on the host cores, on a bounded sample of the same workload."""
     if rank != 0:
         return
-    cl, db, qsize, desc = workload_spec(args.workload)
+    import riggle_b200 as rg
+
+    cl, db, qsize, desc = workload_spec(args.workload, args.db_intervals, args.chroms)
     qsize = args.query_size or qsize
     cores = os.cpu_count() or 1
     chroms = pick_sample(cl, args.workload)
@@ -215,7 +225,7 @@ def run_reference(args, rank, world):
         if step >= args.warmup:
             vals.append(n / t)
     v = float(np.mean(vals))
-    sample = (f"chromosome(s) {[f'chr{c + 1}' for c in chroms]} of each step's query file against all "
+    sample = (f"chromosome(s) {[rg.CHROM_NAMES_24[c] for c in chroms]} of each step's query file against all "
               f"database files, query-block parallel restatement of src/sweep/query.rs on {cores} threads")
     out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
@@ -234,7 +244,7 @@ def run_riggle(args, rank, world, local_rank, dist):
     lib = rg.load()
     dev = local_rank
     torch.cuda.set_device(dev)
-    cl, db, qsize, desc = workload_spec(args.workload)
+    cl, db, qsize, desc = workload_spec(args.workload, args.db_intervals, args.chroms)
     qsize = args.query_size or qsize
     t0 = time.time()
     idx = rg.Index.synth(db, device=dev)
@@ -362,7 +372,7 @@ def run_riggle(args, rank, world, local_rank, dist):
         chroms = pick_sample(cl, args.workload)
         n, t = cpu_sample(db, sample_layers(db, chroms), files[args.warmup][2], 1, 0)
         cpu = {"value": n / t, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{[f'chr{c + 1}' for c in chroms]} of one query file against all database files; "
+               "sample": f"{[rg.CHROM_NAMES_24[c] for c in chroms]} of one query file against all database files; "
                          "restatement of query_database/query_sweep_windowed with the reference's parallel "
                          "structure (one query file = one 64-row window = one thread)"}
 

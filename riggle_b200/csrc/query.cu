@@ -37,9 +37,21 @@ namespace rgl {
 
 struct RangeDesc {
     uint32_t db_lo, db_hi;      // DB index range within the layer
-    uint32_t i_first, i_last;   // query window (positions in the sorted arrays)
+    uint32_t i_first, i_last;   // queries whose candidate windows formed the range (sorted positions)
     uint32_t layer_idx;         // index into the layer table
     uint32_t qrow;              // query row (Q_SID)
+    uint32_t seg;               // query segment (shard, row)
+    uint32_t pad;
+};
+
+// Rank table of one query segment: bin b (width 2^shift bp) holds, at tab[off + b], the number of
+// the segment's sorted starts (tab_s) or ends (tab_e) below b << shift, as absolute positions in
+// the sorted arrays.  A rank is then one table read plus a search over at most one bin.
+struct SegTab {
+    uint32_t beg, end;  // the segment's positions in the sorted arrays
+    uint32_t shift, nbins;
+    uint32_t off;       // first entry of the segment's tables (nbins + 1 entries each)
+    uint32_t pad;
 };
 
 struct MaxOp {
@@ -121,6 +133,67 @@ __global__ void k_unpack(uint32_t n, const uint64_t* __restrict__ key, const uin
     pe_in[i] = e;
 }
 
+__global__ void k_seg_begin(uint32_t n, const uint32_t* __restrict__ segflag, const uint32_t* __restrict__ segnum,
+                            uint32_t* __restrict__ seg_begin) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (segflag[i]) seg_begin[segnum[i] - 1] = i;
+    if (i == n - 1) seg_begin[segnum[i]] = n;
+}
+
+// Bin width per segment: about four bins per query, at least 64 bp; tab_len = nbins + 1.
+__global__ void k_seg_tabsize(uint32_t n, const uint32_t* __restrict__ segnum, const uint32_t* __restrict__ seg_begin,
+                              const uint32_t* __restrict__ ends_s, SegTab* __restrict__ tabs,
+                              uint32_t* __restrict__ tab_len) {
+    uint32_t sgi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sgi > n) return;
+    const uint32_t nseg = segnum[n - 1];
+    if (sgi >= nseg) {
+        tab_len[sgi] = 0;
+        return;
+    }
+    const uint32_t beg = seg_begin[sgi], end = seg_begin[sgi + 1];
+    const uint64_t extent = (uint64_t)ends_s[end - 1] + 1;  // covers every start and end of the segment
+    const uint64_t want = extent / (4ull * (end - beg));
+    uint32_t shift = want > 1 ? 63u - __clzll(want) : 0u;
+    if (shift < 6) shift = 6;
+    if (shift > 31) shift = 31;
+    const uint32_t nbins = (uint32_t)(extent >> shift) + 1;
+    tabs[sgi] = SegTab{beg, end, shift, nbins, 0, 0};
+    tab_len[sgi] = nbins + 1;
+}
+
+// One thread per table entry (grid-stride over all segments' entries): the entry's segment is found
+// by binary search over the table offsets, then tab_s[b] = #starts < b << shift and
+// tab_e[b] = #ends < b << shift within the segment.
+__global__ void k_seg_tabfill(uint32_t n, const uint32_t* __restrict__ segnum, SegTab* __restrict__ tabs,
+                              const uint32_t* __restrict__ tab_off, const uint32_t* __restrict__ starts,
+                              const uint32_t* __restrict__ ends_s, uint32_t* __restrict__ tab_s,
+                              uint32_t* __restrict__ tab_e) {
+    const uint32_t nseg = segnum[n - 1];
+    const uint32_t total = tab_off[nseg];
+    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+        uint32_t lo = 0, hi = nseg - 1;  // last segment with tab_off <= e
+        while (lo < hi) {
+            uint32_t m = (lo + hi + 1) >> 1;
+            if (__ldg(tab_off + m) <= e) lo = m; else hi = m - 1;
+        }
+        const SegTab t = tabs[lo];
+        const uint32_t b = e - __ldg(tab_off + lo);
+        if (b == 0) tabs[lo].off = e;
+        const uint64_t x = (uint64_t)b << t.shift;
+        uint32_t rs, re;
+        if (x > 0xFFFFFFFFull) {
+            rs = re = t.end;
+        } else {
+            rs = lb_u32(starts, t.beg, t.end, (uint32_t)x);
+            re = lb_u32(ends_s, t.beg, t.end, (uint32_t)x);
+        }
+        tab_s[e] = rs;
+        tab_e[e] = re;
+    }
+}
+
 // ---- 4. K1 partition -----------------------------------------------------------------------------
 // lo/hi of the reference's candidate scan for (slot K, query i), layer-major arrays [K][n].
 __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ starts,
@@ -167,7 +240,8 @@ __global__ void k_range_flags(uint32_t n, uint32_t nslots, uint32_t rows, const 
 }
 
 __global__ void k_range_emit(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ seg,
-                             const uint32_t* __restrict__ segflag, const int32_t* __restrict__ slot,
+                             const uint32_t* __restrict__ segflag, const uint32_t* __restrict__ segnum,
+                             const int32_t* __restrict__ slot,
                              const uint32_t* __restrict__ lo, const uint32_t* __restrict__ maxhi,
                              const uint32_t* __restrict__ rflag, const uint32_t* __restrict__ ridx,
                              RangeDesc* __restrict__ ranges) {
@@ -186,6 +260,7 @@ __global__ void k_range_emit(uint32_t n, uint32_t nslots, uint32_t rows, const u
         ranges[r].i_first = i;
         ranges[r].layer_idx = (uint32_t)li;
         ranges[r].qrow = sg % rows;
+        ranges[r].seg = segnum[i] - 1;
     }
     bool last = (i + 1 == n) || segflag[i + 1] || rflag[t + 1];
     if (last) {
@@ -217,17 +292,164 @@ struct SweepParams {
     uint32_t* counts;        // rows x D
     unsigned long long* bp;  // rows x D (may be null)
     uint32_t* queue;         // work counter
+    const uint32_t* item_r0; // first range of each work item (items < item_cap)
+    const SegTab* segtabs;   // per query segment
+    const uint32_t* tab_s;   // rank tables of sorted starts / ends
+    const uint32_t* tab_e;
+    uint64_t item_cap;
     uint32_t rows, D, chunk;
     int smem_tally;          // 1: one row, shared-memory histograms
 };
 
+// Galloping (exponential) search from a lower bound: first index in [lo, hi) with a[i] >= x
+// (UPPER = false) or a[i] > x (UPPER = true).  Cost ~2 log2(answer - lo), so a rank found from
+// the previous, nearby rank takes one or two probes.
+template <bool UPPER>
+__device__ __forceinline__ uint32_t gallop(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi, uint32_t x) {
+    if (lo >= hi) return lo;
+    uint32_t v = __ldg(a + lo);
+    if (UPPER ? (v > x) : (v >= x)) return lo;
+    uint32_t prev = lo, step = 1, nxt;
+    for (;;) {  // invariant: a[prev] is below the bound
+        if (step >= hi - prev) {
+            nxt = hi;
+            break;
+        }
+        nxt = prev + step;
+        v = __ldg(a + nxt);
+        if (UPPER ? (v > x) : (v >= x)) break;
+        prev = nxt;
+        step <<= 1;
+    }
+    return UPPER ? ub_u32(a, prev + 1, nxt, x) : lb_u32(a, prev + 1, nxt, x);
+}
+
+// Last range r in [r, rmax] with rpos[r] <= p (ranges are visited in increasing p).
+__device__ __forceinline__ uint32_t range_advance(const uint64_t* __restrict__ rpos, uint32_t r, uint32_t rmax,
+                                                  uint64_t p) {
+    if (r >= rmax || __ldg(rpos + r + 1) > p) return r;
+    uint32_t lo = r + 1, step = 1, hi;
+    for (;;) {  // invariant: rpos[lo] <= p
+        if (step > rmax - lo) {
+            hi = rmax;
+            break;
+        }
+        hi = lo + step;
+        if (__ldg(rpos + hi) > p) {
+            hi--;
+            break;
+        }
+        lo = hi;
+        step <<= 1;
+    }
+    while (lo < hi) {  // last m in [lo, hi] with rpos[m] <= p
+        uint32_t m = (lo + hi + 1) >> 1;
+        if (__ldg(rpos + m) <= p) lo = m; else hi = m - 1;
+    }
+    return lo;
+}
+
+// Work-item partition: item i covers positions [i * chunk, (i + 1) * chunk) of the concatenated
+// ranges; item_r0[i] = the range holding its first position (last r with rpos[r] <= i * chunk),
+// found by binary search over the range offsets (grid-stride over items).
+__global__ void k_item_ranges(uint64_t rcap, const uint64_t* __restrict__ rpos, uint32_t chunk, uint64_t item_cap,
+                              uint32_t* __restrict__ item_r0) {
+    const uint64_t total = rpos[rcap];
+    const uint64_t items = min((total + chunk - 1) / chunk, item_cap);
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < items; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t p = i * chunk;
+        uint64_t lo = 0, hi = rcap;
+        while (lo < hi) {
+            uint64_t m = (lo + hi + 1) >> 1;
+            if (__ldg(rpos + m) <= p) lo = m; else hi = m - 1;
+        }
+        item_r0[i] = (uint32_t)lo;
+    }
+}
+
+// A lane's position in the range list, with the range's descriptor cached in registers.
+struct Cursor {
+    uint32_t r;
+    uint64_t rlo, rhi;  // [rpos[r], rpos[r + 1])
+    RangeDesc rd;
+    uint64_t base;      // element offset of the range's first DB interval in the index arrays
+    SegTab tab;         // rank table of the range's query segment
+};
+
+__device__ __forceinline__ void cursor_load(const SweepParams& P, Cursor& c, uint32_t r) {
+    c.r = r;
+    c.rlo = __ldg(P.rpos + r);
+    c.rhi = __ldg(P.rpos + r + 1);
+    c.rd = P.ranges[r];
+    c.base = P.layers[c.rd.layer_idx].off + c.rd.db_lo;
+    c.tab = P.segtabs[c.rd.seg];
+}
+
+// #starts < x and #ends <= x within the cursor's segment, as absolute sorted positions.
+__device__ __forceinline__ uint32_t rank_start(const SweepParams& P, const SegTab& t, uint32_t x) {
+    const uint32_t b = x >> t.shift;
+    if (b >= t.nbins) return t.end;
+    const uint32_t lo = __ldg(P.tab_s + t.off + b), hi = __ldg(P.tab_s + t.off + b + 1);
+    return lo == hi ? lo : lb_u32(P.starts, lo, hi, x);
+}
+__device__ __forceinline__ uint32_t rank_end(const SweepParams& P, const SegTab& t, uint32_t x) {
+    const uint32_t b = x >> t.shift;
+    if (b >= t.nbins) return t.end;
+    const uint32_t lo = __ldg(P.tab_e + t.off + b), hi = __ldg(P.tab_e + t.off + b + 1);
+    return lo == hi ? lo : ub_u32(P.ends, lo, hi, x);
+}
+
+__device__ __forceinline__ void cursor_seek(const SweepParams& P, Cursor& c, uint64_t p) {
+    if (p >= c.rhi) cursor_load(P, c, range_advance(P.rpos, c.r, (uint32_t)P.rcap, p));
+}
+
+// A DB interval with a non-zero count, queued until a full warp of them can finish together.
+struct Hit {
+    uint32_t x, y, sid, cnt, el_s, sl_e, seg, qrow;
+};
+
+// Finishes up to 32 queued hits (one per lane): base pairs and the tally into shared or global memory.
 template <bool WITH_BP>
-__global__ void __launch_bounds__(256) k_sweep(SweepParams P) {
+__device__ __forceinline__ void drain_hits(const SweepParams& P, const Hit* __restrict__ q, uint32_t head,
+                                          uint32_t count, uint32_t lane, uint32_t* s_cnt,
+                                          unsigned long long* s_bp) {
+    if (lane >= count) return;
+    const Hit h = q[(head + lane) & 63u];
+    unsigned long long bpv = 0;
+    if (WITH_BP) {
+        const SegTab t = P.segtabs[h.seg];
+        const uint32_t sl_s = rank_start(P, t, h.x);
+        const uint32_t el_e = rank_end(P, t, h.y);
+        if (h.sl_e == sl_s && el_e == h.el_s) {
+            // no query starts or ends inside d: every overlapping query covers all of d
+            bpv = (unsigned long long)(h.y - h.x) * h.cnt;
+        } else {
+            const unsigned long long ce = (unsigned long long)h.y * (unsigned long long)(h.sl_e - el_e) -
+                                          __ldg(P.ps + h.sl_e) + __ldg(P.pe + el_e);
+            const unsigned long long cs = (unsigned long long)h.x * (unsigned long long)(sl_s - h.el_s) -
+                                          __ldg(P.ps + sl_s) + __ldg(P.pe + h.el_s);
+            bpv = ce - cs;
+        }
+    }
+    if (P.smem_tally) {
+        atomicAdd(&s_cnt[h.sid], h.cnt);
+        if (WITH_BP) atomicAdd(&s_bp[h.sid], bpv);
+    } else {
+        const uint64_t cell = (uint64_t)h.qrow * P.D + h.sid;
+        atomicAdd(&P.counts[cell], h.cnt);
+        if (WITH_BP) atomicAdd(&P.bp[cell], bpv);
+    }
+}
+
+template <bool WITH_BP>
+__global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
-    __shared__ uint32_t s_item;
-    __shared__ uint32_t s_r0, s_r1;
+    __shared__ Hit s_hits[8][64];  // per-warp ring of pending hits
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    Hit* hq = s_hits[warp];
+    uint32_t q_head = 0, q_len = 0;  // warp-uniform
 
     const uint64_t total = P.rpos[P.rcap];
     if (P.smem_tally) {
@@ -237,66 +459,77 @@ __global__ void __launch_bounds__(256) k_sweep(SweepParams P) {
         }
     }
     __syncthreads();
+    // Warps pull work items independently (no block-wide barrier inside the loop).  Within an
+    // item a lane visits positions p0 + lane, p0 + lane + 32, ...; its DB interval for the next
+    // step is loaded before the current one is processed.  The count needs two ranks, each one
+    // rank-table read; intervals with a non-zero count are queued and finished 32 at a time.
     for (;;) {
-        if (threadIdx.x == 0) s_item = atomicAdd(P.queue, 1u);
-        __syncthreads();
-        const uint64_t p0 = (uint64_t)s_item * P.chunk;
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(P.queue, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        const uint64_t p0 = (uint64_t)item * P.chunk;
         if (p0 >= total) break;
         const uint64_t p1 = min(p0 + P.chunk, total);
-        if (threadIdx.x == 0) {
-            // last range r with rpos[r] <= p0, and last with rpos[r] <= p1 - 1
+        uint32_t r0;
+        if (item < P.item_cap) {
+            r0 = __ldg(P.item_r0 + item);
+        } else {
             uint64_t lo = 0, hi = P.rcap;
-            while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (P.rpos[m] <= p0) lo = m; else hi = m - 1; }
-            s_r0 = (uint32_t)lo;
-            uint64_t lo2 = lo;
-            hi = P.rcap;
-            while (lo2 < hi) { uint64_t m = (lo2 + hi + 1) >> 1; if (P.rpos[m] <= p1 - 1) lo2 = m; else hi = m - 1; }
-            s_r1 = (uint32_t)lo2;
+            while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (__ldg(P.rpos + m) <= p0) lo = m; else hi = m - 1; }
+            r0 = (uint32_t)lo;
         }
-        __syncthreads();
-        const uint32_t r0 = s_r0, r1 = s_r1;
-        uint32_t r = r0;
-        for (uint64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
-            // advance to the range holding p (positions are visited in increasing order)
-            {
-                uint32_t lo = r, hi = r1;
-                while (lo < hi) {
-                    uint32_t m = (lo + hi + 1) >> 1;
-                    if (__ldg(P.rpos + m) <= p) lo = m; else hi = m - 1;
-                }
-                r = lo;
+        Cursor c;
+        cursor_load(P, c, r0);
+        uint64_t p = p0 + lane;
+        uint2 dn = make_uint2(0, 0);
+        uint32_t sn = 0;
+        if (p < p1) {
+            cursor_seek(P, c, p);
+            const uint64_t di = c.base + (p - c.rlo);
+            dn = __ldg(P.pos + di);
+            sn = __ldg(P.sid + di);
+        }
+        const uint32_t steps = (uint32_t)((p1 - p0 + 31) >> 5);
+        for (uint32_t k = 0; k < steps; k++, p += 32) {  // warp-uniform trip count
+            const bool valid = p < p1;
+            const uint2 d = dn;
+            const uint32_t sid = sn;
+            const SegTab t = c.tab;
+            const uint32_t qrow = c.rd.qrow, segi = c.rd.seg;
+            const uint64_t pn = p + 32;
+            if (pn < p1) {  // prefetch the next position's DB interval
+                cursor_seek(P, c, pn);
+                const uint64_t di = c.base + (pn - c.rlo);
+                dn = __ldg(P.pos + di);
+                sn = __ldg(P.sid + di);
             }
-            const RangeDesc rd = P.ranges[r];
-            const LayerDev L = P.layers[rd.layer_idx];
-            const uint64_t di = L.off + rd.db_lo + (p - P.rpos[r]);
-            const uint2 d = P.pos[di];
-            const uint32_t wlo = rd.i_first, whi = rd.i_last + 1;
-            const uint32_t sl_s = lb_u32(P.starts, wlo, whi, d.x);
-            const uint32_t el_s = ub_u32(P.ends, wlo, whi, d.x);
-            const uint32_t sl_e = lb_u32(P.starts, sl_s, whi, d.y);
-            const uint32_t cnt = sl_e - el_s;
-            if (cnt) {
-                const uint32_t sid = __ldg(P.sid + di);
-                unsigned long long bpv = 0;
-                if (WITH_BP) {
-                    const uint32_t el_e = ub_u32(P.ends, el_s, whi, d.y);
-                    const unsigned long long ce = (unsigned long long)d.y * (unsigned long long)(sl_e - el_e) -
-                                                  P.ps[sl_e] + P.pe[el_e];
-                    const unsigned long long cs = (unsigned long long)d.x * (unsigned long long)(sl_s - el_s) -
-                                                  P.ps[sl_s] + P.pe[el_s];
-                    bpv = ce - cs;
+            uint32_t cnt = 0, el_s = 0, sl_e = 0;
+            if (valid) {
+                // count(d) = #{q.start < d.end} - #{q.end <= d.start}
+                el_s = rank_end(P, t, d.x);
+                sl_e = rank_start(P, t, d.y);
+                cnt = sl_e - el_s;
+            }
+            const uint32_t m = __ballot_sync(0xffffffffu, cnt != 0);
+            if (m) {
+                if (cnt) {
+                    const uint32_t slot = (q_head + q_len + __popc(m & ((1u << lane) - 1u))) & 63u;
+                    hq[slot] = Hit{d.x, d.y, sid, cnt, el_s, sl_e, segi, qrow};
                 }
-                if (P.smem_tally) {
-                    atomicAdd(&s_cnt[sid], cnt);
-                    if (WITH_BP) atomicAdd(&s_bp[sid], bpv);
-                } else {
-                    const uint64_t cell = (uint64_t)rd.qrow * P.D + sid;
-                    atomicAdd(&P.counts[cell], cnt);
-                    if (WITH_BP) atomicAdd(&P.bp[cell], bpv);
+                q_len += __popc(m);
+                __syncwarp();
+                if (q_len >= 32) {
+                    drain_hits<WITH_BP>(P, hq, q_head, 32, lane, s_cnt, s_bp);
+                    q_head = (q_head + 32) & 63u;
+                    q_len -= 32;
+                    __syncwarp();
                 }
             }
         }
-        __syncthreads();
+    }
+    if (q_len) {
+        drain_hits<WITH_BP>(P, hq, q_head, q_len, lane, s_cnt, s_bp);
+        __syncwarp();
     }
     if (P.smem_tally) {
         __syncthreads();
@@ -322,7 +555,8 @@ struct rgl_context {
     int num_sms = 148;
     DevBuf iv, blk_off, blk_shard, key_a, key_b, val_a, val_b, ekey_a, ekey_b;
     DevBuf starts, ends, seg, segflag, segnum, seg_begin, ps_in, pe_in, ps, pe;
-    DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp;
+    DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp, item_r0;
+    DevBuf segtab, tab_len, tab_off, tab_s, tab_e;
     uint32_t* h_small = nullptr;  // pinned mirror of `small`
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     uint64_t res_n = 0;
@@ -338,6 +572,9 @@ struct rgl_context {
 };
 
 namespace {
+
+// Work items whose first range is precomputed; items beyond it search the range list themselves.
+constexpr uint64_t kItemCap = 1ull << 22;
 
 int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     rgl_index* idx = c->idx;
@@ -371,6 +608,12 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     RGL_TRY(c->rlen.ensure(tot * 8 + 16));
     RGL_TRY(c->rpos.ensure(tot * 8 + 16));
     RGL_TRY(c->small.ensure(256));
+    RGL_TRY(c->item_r0.ensure(kItemCap * 4));
+    RGL_TRY(c->segtab.ensure((n + 1) * sizeof(SegTab)));
+    RGL_TRY(c->tab_len.ensure((n + 2) * 4));
+    RGL_TRY(c->tab_off.ensure((n + 2) * 4));
+    RGL_TRY(c->tab_s.ensure((10 * n + 16) * 4));
+    RGL_TRY(c->tab_e.ensure((10 * n + 16) * 4));
     // CUB temporary storage: the maximum over every primitive used, at these sizes.
     size_t need = 0, b = 0;
     int nn = (int)std::max<uint64_t>(n, 1);
@@ -388,6 +631,8 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
                                         MaxOp(), nn, cub::Equality(), c->stream);
     need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, nt, c->stream);
+    need = std::max(need, b);
+    cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, nn + 1, c->stream);
     need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nt, c->stream);
     need = std::max(need, b);
@@ -408,13 +653,13 @@ struct Launch {
 };
 
 Launch pick_launch(const rgl_query_opts* o) {
-    Launch l{4096, 4, 256};
+    Launch l{512, 4, 256};
     if (o) {
         if (o->chunk) l.chunk = o->chunk;
         if (o->ctas_per_sm) l.ctas_per_sm = o->ctas_per_sm;
         if (o->block) l.block = 256;  // the kernel is compiled for 256 threads
     }
-    if (l.chunk < 256) l.chunk = 256;
+    if (l.chunk < 32) l.chunk = 32;
     if (l.ctas_per_sm < 1) l.ctas_per_sm = 1;
     if (l.ctas_per_sm > 8) l.ctas_per_sm = 8;
     return l;
@@ -517,6 +762,19 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
     tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->pe_in.as<uint64_t>(), c->pe.as<uint64_t>(),
                                            (int)n + 1, st));
+    // rank tables of every query segment
+    k_seg_begin<<<grid_for(n, 256), 256, 0, st>>>(n, c->segflag.as<uint32_t>(), c->segnum.as<uint32_t>(),
+                                                  c->seg_begin.as<uint32_t>());
+    k_seg_tabsize<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->seg_begin.as<uint32_t>(),
+                                                        c->ends.as<uint32_t>(), c->segtab.as<SegTab>(),
+                                                        c->tab_len.as<uint32_t>());
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->tab_len.as<uint32_t>(), c->tab_off.as<uint32_t>(),
+                                           (int)n + 1, st));
+    k_seg_tabfill<<<(unsigned)std::min<uint64_t>((10 * n + 255) / 256, (uint64_t)c->num_sms * 16), 256, 0, st>>>(
+        n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(), c->tab_off.as<uint32_t>(), c->starts.as<uint32_t>(),
+        c->ends.as<uint32_t>(), c->tab_s.as<uint32_t>(), c->tab_e.as<uint32_t>());
+    launches += 3;
     const uint64_t tot = (uint64_t)n * ns;
     k_lohi<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, rows, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
                                                 c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, idx->d_pos,
@@ -538,7 +796,7 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
     RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
                                            (int)(tot + 1), st));
     k_range_emit<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, rows, c->seg.as<uint32_t>(), c->segflag.as<uint32_t>(),
-                                                     idx->d_slot, c->lo.as<uint32_t>(), c->maxhi.as<uint32_t>(),
+                                                     c->segnum.as<uint32_t>(), idx->d_slot, c->lo.as<uint32_t>(), c->maxhi.as<uint32_t>(),
                                                      c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
                                                      c->ranges.as<RangeDesc>());
     launches++;
@@ -549,7 +807,15 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
     RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(),
                                            (int)(tot + 1), st));
 
+    k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(tot, c->rpos.as<uint64_t>(), L.chunk, kItemCap,
+                                                               c->item_r0.as<uint32_t>());
+    launches++;
     SweepParams P;
+    P.item_r0 = c->item_r0.as<uint32_t>();
+    P.segtabs = c->segtab.as<SegTab>();
+    P.tab_s = c->tab_s.as<uint32_t>();
+    P.tab_e = c->tab_e.as<uint32_t>();
+    P.item_cap = kItemCap;
     P.rpos = c->rpos.as<uint64_t>();
     P.rcap = tot;
     P.ranges = c->ranges.as<RangeDesc>();
@@ -661,7 +927,8 @@ int rgl_context_destroy(rgl_context* c) {
                       &c->ekey_a, &c->ekey_b, &c->starts, &c->ends, &c->seg, &c->segflag, &c->segnum,
                       &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps, &c->pe, &c->lo, &c->hi, &c->maxhi,
                       &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos, &c->cub_tmp, &c->small,
-                      &c->out_counts, &c->out_bp};
+                      &c->out_counts, &c->out_bp, &c->item_r0,
+                      &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e};
     for (DevBuf* b : bufs) b->release();
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
