@@ -203,6 +203,59 @@ int rgl_query_counts_device(rgl_context* ctx, uint32_t num_rows, uint32_t num_sh
                             rgl_query_stats* stats);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Sliding-window moment store and analytic p-values.                                           */
+/* ------------------------------------------------------------------------------------------ */
+/* compact_index (src/fourier/moments.rs:58-66): store slot of block size l >= 1. */
+uint64_t rgl_compact_index(uint64_t l);
+/* The L values a chromosome of n_bins bins stores, in store order (src/fourier/moments.rs:215-247);
+ * returns their number, writes min(number, capacity). */
+uint64_t rgl_moment_grid(uint64_t n_bins, uint64_t* out_l, uint64_t capacity);
+/* build_query_chrom_data (src/fourier/moments.rs:138-177) for one query file's intervals on one
+ * chromosome: lengths in bins grouped by l_int = max(ceil(len / bin_size), 1), ascending, with
+ * sum_scale = sum(l / l_int), sum_scale2 = sum((l / l_int)^2) and count. */
+int rgl_query_chrom_groups(const rgl_interval* intervals, uint64_t n, uint32_t bin_size, uint64_t* l_int,
+                           double* sum_scale, double* sum_scale2, uint64_t* count, uint64_t capacity,
+                           uint64_t* out_groups);
+
+/* Device-resident moment store: one (mean, var) f32 table per (source, chromosome), as the
+ * reference's momentmap keeps them (src/io/momentstore.rs:22-34; the rkyv file format itself is
+ * not read).  n_bins[c] = ceil(chromosome size / bin size) fixes each chromosome's L grid. */
+typedef struct rgl_moments rgl_moments;
+int rgl_moments_create(int device, uint32_t num_sources, uint32_t num_chroms, const uint64_t* n_bins,
+                       rgl_moments** out);
+int rgl_moments_destroy(rgl_moments* m);
+/* Entries of a full table for the chromosome (the L grid size). */
+uint64_t rgl_moments_slots(const rgl_moments* m, uint32_t chrom);
+/* MomentStoreBuilder::insert for one (source, chromosome) (src/io/momentstore.rs:134-154):
+ * `entries` (mean, var) f32 pairs in store order; 0 entries = no table. */
+int rgl_moments_set(rgl_moments* m, uint32_t sid, uint32_t chrom, const float* mean_var, uint64_t entries);
+int rgl_moments_get(const rgl_moments* m, uint32_t sid, uint32_t chrom, float* mean_var, uint64_t capacity,
+                    uint64_t* out_entries);
+
+/* Query length groups of a batch: row q owns groups [row_group_offsets[q], row_group_offsets[q+1]),
+ * each on chromosome group_chrom[g] of the moment store. */
+typedef struct rgl_pvalue_batch {
+    uint32_t num_rows;
+    const uint64_t* row_group_offsets;
+    const uint32_t* group_chrom;
+    const uint64_t* group_l_int;
+    const double* group_sum_scale;
+    const double* group_sum_scale2;
+    const uint64_t* group_count;
+} rgl_pvalue_batch;
+
+#define RGL_PV_EMITTED 1u /* count > 0 and a chromosome shared with moments (the reference emits it) */
+#define RGL_PV_HAS_LLR 2u /* the NB / Poisson LLR exists (PValueResult.llr is Some) */
+
+/* compute_analytic_pvalues + compute_analytic_stats (src/tasks/query/pvalues.rs:22-77,
+ * src/fourier/stats.rs:34-126) for every (row, source) cell with a non-zero count, in FP64.
+ * observed = overlap_bp / bin_size (exact; the reference sums f32 bins).  Outputs are dense
+ * num_rows x num_sources host arrays: p, llr, log_p (ln p evaluated without underflow; may be
+ * NULL) and flags (RGL_PV_*).  Cells not emitted hold p = 1, llr = 0, flags = 0. */
+int rgl_query_pvalues(rgl_moments* m, const rgl_pvalue_batch* batch, uint32_t bin_size, const uint32_t* counts,
+                      const uint64_t* overlap_bp, double* p, double* llr, double* log_p, uint8_t* flags);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Seeded synthetic workloads (no counterpart in the reference; used by tests and benchmarks).  */
 /* SplitMix64 counter streams (Steele, Lea & Flood 2014) drive identical host and device        */
 /* generators; lengths come from a host-built 65537-point quantile table.                       */

@@ -83,6 +83,12 @@ class SynthSpec(C.Structure):
                 ("num_hotspots", C.c_uint32), ("sid_base", C.c_uint32)]
 
 
+class PValueBatch(C.Structure):
+    _fields_ = [("num_rows", C.c_uint32), ("row_group_offsets", C.c_void_p), ("group_chrom", C.c_void_p),
+                ("group_l_int", C.c_void_p), ("group_sum_scale", C.c_void_p), ("group_sum_scale2", C.c_void_p),
+                ("group_count", C.c_void_p)]
+
+
 _P = C.c_void_p
 _SIGS = {
     "rgl_status_str": (C.c_char_p, [C.c_int]),
@@ -114,6 +120,16 @@ _SIGS = {
     "rgl_context_sweep_times": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),
     "rgl_host_alloc": (C.c_int, [C.c_uint64, C.POINTER(_P)]),
     "rgl_host_free": (C.c_int, [_P]),
+    "rgl_compact_index": (C.c_uint64, [C.c_uint64]),
+    "rgl_moment_grid": (C.c_uint64, [C.c_uint64, _P, C.c_uint64]),
+    "rgl_query_chrom_groups": (C.c_int, [_P, C.c_uint64, C.c_uint32, _P, _P, _P, _P, C.c_uint64,
+                                         C.POINTER(C.c_uint64)]),
+    "rgl_moments_create": (C.c_int, [C.c_int, C.c_uint32, C.c_uint32, _P, C.POINTER(_P)]),
+    "rgl_moments_destroy": (C.c_int, [_P]),
+    "rgl_moments_slots": (C.c_uint64, [_P, C.c_uint32]),
+    "rgl_moments_set": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, C.c_uint64]),
+    "rgl_moments_get": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
+    "rgl_query_pvalues": (C.c_int, [_P, C.POINTER(PValueBatch), C.c_uint32, _P, _P, _P, _P, _P, _P]),
     "rgl_synth_chrom_lengths": (C.c_int, [C.c_uint64, C.c_uint32, _P]),
     "rgl_synth_zipf_sizes": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, _P]),
     "rgl_synth_loguniform_sizes": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, _P]),

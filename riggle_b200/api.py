@@ -284,3 +284,106 @@ def bucket_layers(blocks, config=None):
         a = a[o]
         out[key] = (np.ascontiguousarray(a[:, :2]), np.ascontiguousarray(a[:, 2]))
     return out
+
+
+# ---------------------------------------------------------------------------------------------
+# sliding-window moments and analytic p-values
+# ---------------------------------------------------------------------------------------------
+HG38_CHROM_SIZES = [  # src/fourier/genome.rs:7-34
+    ("chr1", 248_956_422), ("chr2", 242_193_529), ("chr3", 198_295_559), ("chr4", 190_214_555),
+    ("chr5", 181_538_259), ("chr6", 170_805_979), ("chr7", 159_345_973), ("chr8", 145_138_636),
+    ("chr9", 138_394_717), ("chr10", 133_797_422), ("chr11", 135_086_622), ("chr12", 133_275_309),
+    ("chr13", 114_364_328), ("chr14", 107_043_718), ("chr15", 101_991_189), ("chr16", 90_338_345),
+    ("chr17", 83_257_441), ("chr18", 80_373_285), ("chr19", 58_617_616), ("chr20", 64_444_167),
+    ("chr21", 46_709_983), ("chr22", 50_818_468), ("chrX", 156_040_895), ("chrY", 57_227_415),
+]
+BIN_SIZE = 100  # src/fourier/genome.rs:3
+
+
+def compact_index(l):
+    return load().rgl_compact_index(int(l))
+
+
+def moment_grid(n_bins):
+    n = load().rgl_moment_grid(int(n_bins), None, 0)
+    out = np.empty(n, np.uint64)
+    load().rgl_moment_grid(int(n_bins), _ptr(out), n)
+    return out
+
+
+def query_chrom_groups(intervals, bin_size=BIN_SIZE):
+    """build_query_chrom_data for one chromosome: (l_int, sum_scale, sum_scale2, count)."""
+    iv = np.ascontiguousarray(np.asarray(intervals, np.uint32).reshape(-1, 3))
+    ng = C.c_uint64()
+    check(load().rgl_query_chrom_groups(_ptr(iv), len(iv), bin_size, None, None, None, None, 0, C.byref(ng)))
+    n = ng.value
+    li, ss, ss2, cnt = (np.empty(n, np.uint64), np.empty(n, np.float64), np.empty(n, np.float64),
+                        np.empty(n, np.uint64))
+    check(load().rgl_query_chrom_groups(_ptr(iv), len(iv), bin_size, _ptr(li), _ptr(ss), _ptr(ss2), _ptr(cnt), n,
+                                        C.byref(ng)))
+    return li, ss, ss2, cnt
+
+
+class Moments:
+    """Device moment store: (mean, var) f32 tables per (source, chromosome)."""
+
+    def __init__(self, num_sources, n_bins, device=0):
+        self.n_bins = np.ascontiguousarray(n_bins, np.uint64)
+        self.num_sources = num_sources
+        h = C.c_void_p()
+        check(load().rgl_moments_create(device, num_sources, len(self.n_bins), _ptr(self.n_bins), C.byref(h)))
+        self._h = h
+
+    def slots(self, chrom):
+        return load().rgl_moments_slots(self._h, chrom)
+
+    def set(self, sid, chrom, mean_var):
+        mv = np.ascontiguousarray(np.asarray(mean_var, np.float32).reshape(-1, 2))
+        check(load().rgl_moments_set(self._h, sid, chrom, _ptr(mv), len(mv)))
+
+    def get(self, sid, chrom):
+        n = C.c_uint64()
+        check(load().rgl_moments_get(self._h, sid, chrom, None, 0, C.byref(n)))
+        out = np.empty((n.value, 2), np.float32)
+        check(load().rgl_moments_get(self._h, sid, chrom, _ptr(out), n.value, C.byref(n)))
+        return out
+
+    def pvalues(self, row_groups, counts, overlap_bp, bin_size=BIN_SIZE):
+        """row_groups: per query row a list of (chrom, (l_int, ss, ss2, count)).
+
+        Returns dense (p, llr, log_p, flags) arrays of shape counts.shape."""
+        rows = len(row_groups)
+        offs = np.zeros(rows + 1, np.uint64)
+        parts = []
+        for q, chroms in enumerate(row_groups):
+            n = 0
+            for c, g in chroms:
+                parts.append((c, g))
+                n += len(g[0])
+            offs[q + 1] = offs[q] + n
+        cat = lambda j, dt: np.ascontiguousarray(np.concatenate([g[j] for _, g in parts]) if parts else
+                                                 np.zeros(0), dt)
+        chrom = np.ascontiguousarray(np.concatenate([np.full(len(g[0]), c, np.uint32) for c, g in parts])
+                                     if parts else np.zeros(0, np.uint32))
+        li, ss, ss2, cnt = cat(0, np.uint64), cat(1, np.float64), cat(2, np.float64), cat(3, np.uint64)
+        b = _lib.PValueBatch(rows, _ptr(offs), _ptr(chrom), _ptr(li), _ptr(ss), _ptr(ss2), _ptr(cnt))
+        counts = np.ascontiguousarray(counts, np.uint32)
+        overlap_bp = np.ascontiguousarray(overlap_bp, np.uint64)
+        p = np.empty(counts.shape, np.float64)
+        llr = np.empty(counts.shape, np.float64)
+        lp = np.empty(counts.shape, np.float64)
+        fl = np.empty(counts.shape, np.uint8)
+        check(load().rgl_query_pvalues(self._h, C.byref(b), bin_size, _ptr(counts), _ptr(overlap_bp), _ptr(p),
+                                       _ptr(llr), _ptr(lp), _ptr(fl)))
+        return p, llr, lp, fl
+
+    def close(self):
+        if self._h:
+            load().rgl_moments_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

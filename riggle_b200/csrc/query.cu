@@ -403,53 +403,51 @@ __device__ __forceinline__ void cursor_seek(const SweepParams& P, Cursor& c, uin
     if (p >= c.rhi) cursor_load(P, c, range_advance(P.rpos, c.r, (uint32_t)P.rcap, p));
 }
 
-// A DB interval with a non-zero count, queued until a full warp of them can finish together.
-struct Hit {
-    uint32_t x, y, sid, cnt, el_s, sl_e, seg, qrow;
-};
-
-// Finishes up to 32 queued hits (one per lane): base pairs and the tally into shared or global memory.
+// Base pairs and tally of one DB interval d with a non-zero count (el_s, sl_e already known).
 template <bool WITH_BP>
-__device__ __forceinline__ void drain_hits(const SweepParams& P, const Hit* __restrict__ q, uint32_t head,
-                                          uint32_t count, uint32_t lane, uint32_t* s_cnt,
-                                          unsigned long long* s_bp) {
-    if (lane >= count) return;
-    const Hit h = q[(head + lane) & 63u];
+__device__ __forceinline__ void finish_hit(const SweepParams& P, const SegTab& t, uint32_t qrow, uint2 d,
+                                          uint32_t sid, uint32_t cnt, uint32_t el_s, uint32_t sl_e,
+                                          uint32_t* s_cnt, unsigned long long* s_bp) {
     unsigned long long bpv = 0;
     if (WITH_BP) {
-        const SegTab t = P.segtabs[h.seg];
-        const uint32_t sl_s = rank_start(P, t, h.x);
-        const uint32_t el_e = rank_end(P, t, h.y);
-        if (h.sl_e == sl_s && el_e == h.el_s) {
+        const uint32_t sl_s = rank_start(P, t, d.x);
+        const uint32_t el_e = rank_end(P, t, d.y);
+        if (sl_e == sl_s && el_e == el_s) {
             // no query starts or ends inside d: every overlapping query covers all of d
-            bpv = (unsigned long long)(h.y - h.x) * h.cnt;
+            bpv = (unsigned long long)(d.y - d.x) * cnt;
         } else {
-            const unsigned long long ce = (unsigned long long)h.y * (unsigned long long)(h.sl_e - el_e) -
-                                          __ldg(P.ps + h.sl_e) + __ldg(P.pe + el_e);
-            const unsigned long long cs = (unsigned long long)h.x * (unsigned long long)(sl_s - h.el_s) -
-                                          __ldg(P.ps + sl_s) + __ldg(P.pe + h.el_s);
+            const unsigned long long ce = (unsigned long long)d.y * (unsigned long long)(sl_e - el_e) -
+                                          __ldg(P.ps + sl_e) + __ldg(P.pe + el_e);
+            const unsigned long long cs = (unsigned long long)d.x * (unsigned long long)(sl_s - el_s) -
+                                          __ldg(P.ps + sl_s) + __ldg(P.pe + el_s);
             bpv = ce - cs;
         }
     }
     if (P.smem_tally) {
-        atomicAdd(&s_cnt[h.sid], h.cnt);
-        if (WITH_BP) atomicAdd(&s_bp[h.sid], bpv);
+        atomicAdd(&s_cnt[sid], cnt);
+        if (WITH_BP) atomicAdd(&s_bp[sid], bpv);
     } else {
-        const uint64_t cell = (uint64_t)h.qrow * P.D + h.sid;
-        atomicAdd(&P.counts[cell], h.cnt);
+        const uint64_t cell = (uint64_t)qrow * P.D + sid;
+        atomicAdd(&P.counts[cell], cnt);
         if (WITH_BP) atomicAdd(&P.bp[cell], bpv);
     }
 }
 
+// Two table entries tab[b], tab[b + 1] (b < nbins) for the bin of x, or (end, end) past the table.
+__device__ __forceinline__ uint2 bin_bounds(const uint32_t* __restrict__ tab, const SegTab& t, uint32_t x) {
+    const uint32_t b = x >> t.shift;
+    if (b >= t.nbins) return make_uint2(t.end, t.end);
+    return make_uint2(__ldg(tab + t.off + b), __ldg(tab + t.off + b + 1));
+}
+
+constexpr uint32_t kUnroll = 4;  // DB intervals per lane per step
+
 template <bool WITH_BP>
-__global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
+__global__ void __launch_bounds__(256, 3) k_sweep(SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
-    __shared__ Hit s_hits[8][64];  // per-warp ring of pending hits
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    Hit* hq = s_hits[warp];
-    uint32_t q_head = 0, q_len = 0;  // warp-uniform
+    const uint32_t lane = threadIdx.x & 31u;
 
     const uint64_t total = P.rpos[P.rcap];
     if (P.smem_tally) {
@@ -459,10 +457,12 @@ __global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
         }
     }
     __syncthreads();
-    // Warps pull work items independently (no block-wide barrier inside the loop).  Within an
-    // item a lane visits positions p0 + lane, p0 + lane + 32, ...; its DB interval for the next
-    // step is loaded before the current one is processed.  The count needs two ranks, each one
-    // rank-table read; intervals with a non-zero count are queued and finished 32 at a time.
+    // Warps pull work items independently (no block-wide barrier inside the loop).  A step covers
+    // 32 * kUnroll consecutive positions; lane l takes positions pb + l + 32 j, so every load of the
+    // DB arrays is coalesced, and the kUnroll DB intervals of a lane and their rank-table entries
+    // are all requested before any of them is used.  count(d) = #{q.start < d.end} -
+    // #{q.end <= d.start} needs two ranks, each one rank-table read plus, rarely, a search inside
+    // one bin.
     for (;;) {
         uint32_t item = 0;
         if (lane == 0) item = atomicAdd(P.queue, 1u);
@@ -480,56 +480,53 @@ __global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
         }
         Cursor c;
         cursor_load(P, c, r0);
-        uint64_t p = p0 + lane;
-        uint2 dn = make_uint2(0, 0);
-        uint32_t sn = 0;
-        if (p < p1) {
-            cursor_seek(P, c, p);
-            const uint64_t di = c.base + (p - c.rlo);
-            dn = __ldg(P.pos + di);
-            sn = __ldg(P.sid + di);
-        }
-        const uint32_t steps = (uint32_t)((p1 - p0 + 31) >> 5);
-        for (uint32_t k = 0; k < steps; k++, p += 32) {  // warp-uniform trip count
-            const bool valid = p < p1;
-            const uint2 d = dn;
-            const uint32_t sid = sn;
-            const SegTab t = c.tab;
-            const uint32_t qrow = c.rd.qrow, segi = c.rd.seg;
-            const uint64_t pn = p + 32;
-            if (pn < p1) {  // prefetch the next position's DB interval
-                cursor_seek(P, c, pn);
-                const uint64_t di = c.base + (pn - c.rlo);
-                dn = __ldg(P.pos + di);
-                sn = __ldg(P.sid + di);
-            }
-            uint32_t cnt = 0, el_s = 0, sl_e = 0;
-            if (valid) {
-                // count(d) = #{q.start < d.end} - #{q.end <= d.start}
-                el_s = rank_end(P, t, d.x);
-                sl_e = rank_start(P, t, d.y);
-                cnt = sl_e - el_s;
-            }
-            const uint32_t m = __ballot_sync(0xffffffffu, cnt != 0);
-            if (m) {
-                if (cnt) {
-                    const uint32_t slot = (q_head + q_len + __popc(m & ((1u << lane) - 1u))) & 63u;
-                    hq[slot] = Hit{d.x, d.y, sid, cnt, el_s, sl_e, segi, qrow};
+        for (uint64_t pb = p0 + lane; pb < p1; pb += 32 * kUnroll) {
+            const uint64_t plast = min(pb + 32 * (kUnroll - 1), p1 - 1 - ((p1 - 1 - pb) & 31));
+            cursor_seek(P, c, pb);
+            if (plast < c.rhi) {
+                // all of this lane's positions of the step lie in one range: batch the loads
+                const SegTab t = c.tab;
+                const uint64_t off = c.base - c.rlo;
+                uint2 d[kUnroll];
+                uint32_t sid[kUnroll];
+#pragma unroll
+                for (uint32_t j = 0; j < kUnroll; j++) {
+                    const uint64_t pj = pb + 32 * j;
+                    if (pj < p1) {
+                        d[j] = __ldg(P.pos + off + pj);
+                        sid[j] = __ldg(P.sid + off + pj);
+                    } else {
+                        d[j] = make_uint2(0, 0);
+                        sid[j] = 0;
+                    }
                 }
-                q_len += __popc(m);
-                __syncwarp();
-                if (q_len >= 32) {
-                    drain_hits<WITH_BP>(P, hq, q_head, 32, lane, s_cnt, s_bp);
-                    q_head = (q_head + 32) & 63u;
-                    q_len -= 32;
-                    __syncwarp();
+                uint2 be[kUnroll], bs[kUnroll];
+#pragma unroll
+                for (uint32_t j = 0; j < kUnroll; j++) {
+                    be[j] = bin_bounds(P.tab_e, t, d[j].x);
+                    bs[j] = bin_bounds(P.tab_s, t, d[j].y);
+                }
+#pragma unroll
+                for (uint32_t j = 0; j < kUnroll; j++) {
+                    if (pb + 32 * j >= p1) continue;
+                    const uint32_t el_s = be[j].x == be[j].y ? be[j].x : ub_u32(P.ends, be[j].x, be[j].y, d[j].x);
+                    const uint32_t sl_e = bs[j].x == bs[j].y ? bs[j].x : lb_u32(P.starts, bs[j].x, bs[j].y, d[j].y);
+                    const uint32_t cnt = sl_e - el_s;
+                    if (cnt) finish_hit<WITH_BP>(P, t, c.rd.qrow, d[j], sid[j], cnt, el_s, sl_e, s_cnt, s_bp);
+                }
+            } else {
+                // the step crosses a range boundary: one position at a time
+                for (uint64_t pj = pb; pj < p1 && pj <= pb + 32 * (kUnroll - 1); pj += 32) {
+                    cursor_seek(P, c, pj);
+                    const uint64_t di = c.base + (pj - c.rlo);
+                    const uint2 d = __ldg(P.pos + di);
+                    const uint32_t el_s = rank_end(P, c.tab, d.x);
+                    const uint32_t sl_e = rank_start(P, c.tab, d.y);
+                    const uint32_t cnt = sl_e - el_s;
+                    if (cnt) finish_hit<WITH_BP>(P, c.tab, c.rd.qrow, d, __ldg(P.sid + di), cnt, el_s, sl_e, s_cnt, s_bp);
                 }
             }
         }
-    }
-    if (q_len) {
-        drain_hits<WITH_BP>(P, hq, q_head, q_len, lane, s_cnt, s_bp);
-        __syncwarp();
     }
     if (P.smem_tally) {
         __syncthreads();

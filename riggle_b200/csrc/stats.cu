@@ -1,0 +1,379 @@
+// Analytic p-values (K8): compute_analytic_pvalues (src/tasks/query/pvalues.rs:22-77) and
+// compute_analytic_stats (src/fourier/stats.rs:34-126) in FP64 on the device, plus the host pieces
+// they need: the compact moment-store layout (src/fourier/moments.rs:58-66, 215-247) and the
+// per-chromosome query length groups (build_query_chrom_data, src/fourier/moments.rs:138-177).
+//
+// Moment store in HBM: one float2 (mean, var) table per (source, chromosome), laid out
+// [source][chromosome][slot]; slot = compact_index(L) and the tables hold the reference's L grid in
+// store order, so a lookup is one gather.  Query groups are flattened per query row: every group
+// carries its chromosome, its slot (computed on the host with the same f64 ln as the reference,
+// never on the device) and its FP64 sums.  One warp evaluates one (query row, source) pair:
+// lanes stride over the row's groups, accumulate mu, sigma^2 and mu_raw in FP64, reduce, and lane
+// 0 dispatches NB / Poisson, evaluates the LLR and the A&S 7.1.26 tail exactly as the reference
+// writes it (src/fourier/stats.rs:65-126).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "internal.h"
+
+namespace rgl {
+
+static const uint64_t T_THRESHOLD = 100;  // src/fourier/moments.rs:50
+static const double EPS = 0.01;           // src/fourier/moments.rs:47
+
+uint64_t compact_index(uint64_t l) {
+    // src/fourier/moments.rs:58-66
+    if (l <= T_THRESHOLD) return l - 1;
+    uint64_t k = (uint64_t)(std::log((double)l / (double)T_THRESHOLD) / std::log(1.0 + EPS));
+    return T_THRESHOLD + k - 1;
+}
+
+std::vector<uint64_t> moment_grid(uint64_t n) {
+    // src/fourier/moments.rs:215-247: L = 1..=min(T, N-1), then ceil of repeated *1.01 products,
+    // deduplicated, while L <= N-1.
+    std::vector<uint64_t> ls;
+    if (n <= 1) return ls;
+    const uint64_t max_l = n - 1;
+    for (uint64_t l = 1; l <= std::min(T_THRESHOLD, max_l); l++) ls.push_back(l);
+    double l_f = (double)T_THRESHOLD;
+    uint64_t prev = T_THRESHOLD;
+    for (;;) {
+        l_f *= 1.0 + EPS;
+        const uint64_t l = (uint64_t)std::ceil(l_f);
+        if (l > max_l) break;
+        if (l > prev) {
+            ls.push_back(l);
+            prev = l;
+        }
+    }
+    return ls;
+}
+
+struct QGroupDev {
+    uint32_t chrom, slot;
+    double ss, ss2, l_int, count;
+};
+
+__device__ __forceinline__ double erfc_as(double x) {
+    // A&S 7.1.26 as src/fourier/stats.rs:116-126 writes it (x >= 0 here)
+    const double t = 1.0 / (1.0 + 0.3275911 * x);
+    const double p =
+        t * (0.254829592 + t * (-0.284496736 + t * (1.421413741 + t * (-1.453152027 + t * 1.061405429))));
+    return p * exp(-x * x);
+}
+
+__device__ __forceinline__ double ln_half_erfc_as(double x) {
+    // ln(erfc_as(x) / 2) without underflow: ln(0.5 t poly(t)) - x*x
+    const double t = 1.0 / (1.0 + 0.3275911 * x);
+    const double p =
+        t * (0.254829592 + t * (-0.284496736 + t * (1.421413741 + t * (-1.453152027 + t * 1.061405429))));
+    return log(0.5 * p) + (-x * x);
+}
+
+__global__ void k_pvalues(uint32_t rows, uint32_t D, uint32_t C, const uint32_t* __restrict__ counts,
+                          const unsigned long long* __restrict__ bp, double bin_size,
+                          const uint64_t* __restrict__ g_off, const QGroupDev* __restrict__ groups,
+                          const float2* __restrict__ mv, const uint64_t* __restrict__ chrom_off, uint64_t stride,
+                          const uint32_t* __restrict__ tab_len, double* __restrict__ p_out,
+                          double* __restrict__ llr_out, double* __restrict__ logp_out, uint8_t* __restrict__ flags) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; w < (uint64_t)rows * D; w += nw) {
+        const uint32_t q = (uint32_t)(w / D), d = (uint32_t)(w % D);
+        const uint32_t cnt = counts[w];
+        double p = 1.0, llr = 0.0, lp = 0.0;
+        uint8_t f = 0;
+        if (cnt) {  // zero-count pairs are not emitted (src/tasks/query/pvalues.rs:28-35)
+            double mu = 0.0, var = 0.0, raw = 0.0;
+            uint32_t any = 0;
+            const float2* src = mv + (uint64_t)d * stride;
+            for (uint64_t g = g_off[q] + lane; g < g_off[q + 1]; g += 32) {
+                const QGroupDev G = groups[g];
+                if (G.slot < tab_len[(uint64_t)d * C + G.chrom]) {
+                    const float2 m = src[chrom_off[G.chrom] + G.slot];
+                    const double mean = (double)m.x, v = (double)m.y;
+                    mu += mean * G.ss;
+                    var += v * G.ss2;
+                    raw += mean / G.l_int * G.count;
+                    any = 1;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                mu += __shfl_xor_sync(0xffffffffu, mu, o);
+                var += __shfl_xor_sync(0xffffffffu, var, o);
+                raw += __shfl_xor_sync(0xffffffffu, raw, o);
+                any |= __shfl_xor_sync(0xffffffffu, any, o);
+            }
+            if (any) {
+                f = 1;
+                const double observed = (double)bp[w] / bin_size;
+                bool ok = false;
+                if (var > mu) {
+                    // nb_llr (src/fourier/stats.rs:101-113)
+                    if (mu > 0.0 && var > mu) {
+                        const double r = mu * mu / (var - mu);
+                        const double pp = mu / var;
+                        const double p_o = r / (r + observed);
+                        if (0.0 < pp && pp < 1.0 && 0.0 < p_o && p_o < 1.0) {
+                            const double theta = log((1.0 - p_o) / (1.0 - pp));
+                            llr = observed * theta + r * log(p_o / pp);
+                            ok = true;
+                        }
+                    }
+                } else {
+                    // Poisson on count units (src/fourier/stats.rs:65-74, 93-98)
+                    const double eff = raw > 0.0 ? mu / raw : 1.0;
+                    const double oc = observed / eff;
+                    if (raw > 0.0 && oc > 0.0) {
+                        llr = oc * log(oc / raw) - (oc - raw);
+                        ok = true;
+                    }
+                }
+                if (ok) f |= 2;
+                if (ok && llr > 0.0) {
+                    const double x = sqrt(llr);
+                    const double tail = erfc_as(x) * 0.5;
+                    const double ln_tail = ln_half_erfc_as(x);
+                    if (observed >= mu) {
+                        p = tail;
+                        lp = ln_tail;
+                    } else {
+                        p = 1.0 - tail;
+                        lp = log1p(-exp(ln_tail));
+                    }
+                }
+                if (!ok) llr = 0.0;
+            }
+        }
+        if (lane == 0) {
+            p_out[w] = p;
+            llr_out[w] = llr;
+            if (logp_out) logp_out[w] = lp;
+            flags[w] = f;
+        }
+    }
+}
+
+}  // namespace rgl
+
+using namespace rgl;
+
+struct rgl_moments {
+    int device = 0;
+    uint32_t num_sources = 0, num_chroms = 0;
+    std::vector<uint64_t> n_bins, n_slots, chrom_off;
+    uint64_t stride = 0;
+    float2* d_mv = nullptr;
+    uint32_t* d_len = nullptr;
+    std::vector<uint32_t> len;  // host mirror of the per-(source, chromosome) table lengths
+};
+
+extern "C" {
+
+uint64_t rgl_compact_index(uint64_t l) { return l ? compact_index(l) : 0; }
+
+uint64_t rgl_moment_grid(uint64_t n_bins, uint64_t* out, uint64_t cap) {
+    auto g = moment_grid(n_bins);
+    for (uint64_t i = 0; i < g.size() && i < cap && out; i++) out[i] = g[i];
+    return g.size();
+}
+
+int rgl_query_chrom_groups(const rgl_interval* ivs, uint64_t n, uint32_t bin_size, uint64_t* l_int,
+                           double* sum_scale, double* sum_scale2, uint64_t* count, uint64_t capacity,
+                           uint64_t* out_groups) {
+    // build_query_chrom_data inner loop (src/fourier/moments.rs:148-172): lengths in bins sorted
+    // ascending, grouped by l_int = max(ceil(l), 1), with sums of s = l / l_int and s^2.
+    clear_error();
+    if ((!ivs && n) || !out_groups || bin_size == 0) return fail(RGL_ERR_INVALID_ARGUMENT, "bad arguments");
+    std::vector<double> lengths(n);
+    for (uint64_t i = 0; i < n; i++) {
+        if (ivs[i].end <= ivs[i].start) return fail(RGL_ERR_INVALID_ARGUMENT, "interval with start >= end");
+        lengths[i] = (double)(ivs[i].end - ivs[i].start) / (double)bin_size;
+    }
+    std::sort(lengths.begin(), lengths.end());
+    auto lint_of = [](double l) {
+        uint64_t c = (uint64_t)std::ceil(l);
+        return c < 1 ? (uint64_t)1 : c;
+    };
+    uint64_t ng = 0;
+    for (uint64_t i = 0; i < n;) {
+        const double l = lengths[i];
+        const uint64_t li = lint_of(l);
+        const double s0 = l / (double)li;
+        double ss = s0, ss2 = s0 * s0;
+        uint64_t c = 1;
+        for (i++; i < n && lint_of(lengths[i]) == li; i++) {
+            const double s = lengths[i] / (double)li;
+            ss += s;
+            ss2 += s * s;
+            c++;
+        }
+        if (ng < capacity) {
+            if (l_int) l_int[ng] = li;
+            if (sum_scale) sum_scale[ng] = ss;
+            if (sum_scale2) sum_scale2[ng] = ss2;
+            if (count) count[ng] = c;
+        }
+        ng++;
+    }
+    *out_groups = ng;
+    if (ng > capacity && (l_int || sum_scale || sum_scale2 || count))
+        return fail(RGL_ERR_INVALID_ARGUMENT, "group capacity too small");
+    return RGL_OK;
+}
+
+int rgl_moments_create(int device, uint32_t num_sources, uint32_t num_chroms, const uint64_t* n_bins,
+                       rgl_moments** out) {
+    clear_error();
+    if (!out || !n_bins || !num_chroms) return fail(RGL_ERR_INVALID_ARGUMENT, "bad arguments");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(RGL_ERR_NO_DEVICE, "no CUDA device");
+    auto* m = new rgl_moments();
+    m->device = device;
+    m->num_sources = num_sources;
+    m->num_chroms = num_chroms;
+    uint64_t acc = 0;
+    for (uint32_t c = 0; c < num_chroms; c++) {
+        m->n_bins.push_back(n_bins[c]);
+        const uint64_t ns = moment_grid(n_bins[c]).size();
+        m->n_slots.push_back(ns);
+        m->chrom_off.push_back(acc);
+        acc += ns;
+    }
+    m->stride = acc;
+    m->len.assign((size_t)num_sources * num_chroms, 0);
+    int s = RGL_OK;
+    if (cudaSetDevice(device) != cudaSuccess) s = fail(RGL_ERR_DEVICE, "cudaSetDevice");
+    size_t mv_bytes = std::max<size_t>(1, (size_t)num_sources * acc) * sizeof(float2);
+    size_t len_bytes = std::max<size_t>(1, m->len.size()) * 4;
+    if (s == RGL_OK && cudaMalloc(&m->d_mv, mv_bytes) != cudaSuccess) s = fail(RGL_ERR_OOM, "moment store");
+    if (s == RGL_OK && cudaMalloc(&m->d_len, len_bytes) != cudaSuccess) s = fail(RGL_ERR_OOM, "moment store");
+    if (s == RGL_OK && cudaMemset(m->d_len, 0, len_bytes) != cudaSuccess) s = fail(RGL_ERR_DEVICE, "memset");
+    if (s != RGL_OK) {
+        if (m->d_mv) cudaFree(m->d_mv);
+        if (m->d_len) cudaFree(m->d_len);
+        delete m;
+        return s;
+    }
+    *out = m;
+    return RGL_OK;
+}
+
+int rgl_moments_destroy(rgl_moments* m) {
+    clear_error();
+    if (!m) return RGL_OK;
+    cudaSetDevice(m->device);
+    if (m->d_mv) cudaFree(m->d_mv);
+    if (m->d_len) cudaFree(m->d_len);
+    delete m;
+    return RGL_OK;
+}
+
+uint64_t rgl_moments_slots(const rgl_moments* m, uint32_t chrom) {
+    return (m && chrom < m->num_chroms) ? m->n_slots[chrom] : 0;
+}
+
+int rgl_moments_set(rgl_moments* m, uint32_t sid, uint32_t chrom, const float* mean_var, uint64_t entries) {
+    // MomentStoreBuilder::insert for one (source, chromosome) (src/io/momentstore.rs:134-154)
+    clear_error();
+    if (!m || sid >= m->num_sources || chrom >= m->num_chroms || (entries && !mean_var))
+        return fail(RGL_ERR_INVALID_ARGUMENT, "bad arguments");
+    if (entries > m->n_slots[chrom])
+        return fail(RGL_ERR_INVALID_ARGUMENT, "more entries than the chromosome's L grid");
+    RGL_CUDA(cudaSetDevice(m->device));
+    if (entries)
+        RGL_CUDA(cudaMemcpy(m->d_mv + (uint64_t)sid * m->stride + m->chrom_off[chrom], mean_var, entries * 8,
+                            cudaMemcpyHostToDevice));
+    const uint32_t l = (uint32_t)entries;
+    m->len[(size_t)sid * m->num_chroms + chrom] = l;
+    RGL_CUDA(cudaMemcpy(m->d_len + (size_t)sid * m->num_chroms + chrom, &l, 4, cudaMemcpyHostToDevice));
+    return RGL_OK;
+}
+
+int rgl_moments_get(const rgl_moments* m, uint32_t sid, uint32_t chrom, float* mean_var, uint64_t capacity,
+                    uint64_t* out_entries) {
+    clear_error();
+    if (!m || sid >= m->num_sources || chrom >= m->num_chroms || !out_entries)
+        return fail(RGL_ERR_INVALID_ARGUMENT, "bad arguments");
+    const uint64_t l = m->len[(size_t)sid * m->num_chroms + chrom];
+    *out_entries = l;
+    if (!mean_var || !l) return RGL_OK;
+    if (capacity < l) return fail(RGL_ERR_INVALID_ARGUMENT, "capacity too small");
+    RGL_CUDA(cudaSetDevice(m->device));
+    RGL_CUDA(cudaMemcpy(mean_var, m->d_mv + (uint64_t)sid * m->stride + m->chrom_off[chrom], l * 8,
+                        cudaMemcpyDeviceToHost));
+    return RGL_OK;
+}
+
+int rgl_query_pvalues(rgl_moments* m, const rgl_pvalue_batch* b, uint32_t bin_size, const uint32_t* counts,
+                      const uint64_t* overlap_bp, double* p, double* llr, double* log_p, uint8_t* flags) {
+    clear_error();
+    if (!m || !b || !counts || !overlap_bp || !p || !llr || !flags || bin_size == 0)
+        return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    const uint32_t rows = b->num_rows, D = m->num_sources, C = m->num_chroms;
+    const uint64_t cells = (uint64_t)rows * D;
+    if (!cells) return RGL_OK;
+    // flatten the groups: validity on the host (l_int < n_bins of the chromosome, as the store's
+    // lookup requires, src/io/momentstore.rs:66-79); slot by compact_index
+    std::vector<uint64_t> goff(rows + 1, 0);
+    std::vector<QGroupDev> gs;
+    for (uint32_t q = 0; q < rows; q++) {
+        goff[q] = gs.size();
+        for (uint64_t g = b->row_group_offsets[q]; g < b->row_group_offsets[q + 1]; g++) {
+            const uint32_t c = b->group_chrom[g];
+            if (c >= C) return fail(RGL_ERR_INVALID_ARGUMENT, "group chromosome out of range");
+            const uint64_t l = b->group_l_int[g];
+            if (l == 0 || l >= m->n_bins[c]) continue;
+            const uint64_t slot = compact_index(l);
+            if (slot >= m->n_slots[c]) continue;
+            gs.push_back(QGroupDev{c, (uint32_t)slot, b->group_sum_scale[g], b->group_sum_scale2[g], (double)l,
+                                   (double)b->group_count[g]});
+        }
+    }
+    goff[rows] = gs.size();
+    RGL_CUDA(cudaSetDevice(m->device));
+    DevBuf d_goff, d_g, d_coff, d_cnt, d_bp, d_p, d_llr, d_lp, d_f;
+    int s = RGL_OK;
+    if (s == RGL_OK) s = d_goff.ensure((rows + 1) * 8ull);
+    if (s == RGL_OK) s = d_g.ensure(std::max<size_t>(1, gs.size()) * sizeof(QGroupDev));
+    if (s == RGL_OK) s = d_coff.ensure(C * 8ull);
+    if (s == RGL_OK) s = d_cnt.ensure(cells * 4);
+    if (s == RGL_OK) s = d_bp.ensure(cells * 8);
+    if (s == RGL_OK) s = d_p.ensure(cells * 8);
+    if (s == RGL_OK) s = d_llr.ensure(cells * 8);
+    if (s == RGL_OK) s = d_lp.ensure(cells * 8);
+    if (s == RGL_OK) s = d_f.ensure(cells);
+    auto cp = [&](void* dst, const void* src, size_t n) {
+        if (s == RGL_OK && n && cudaMemcpy(dst, src, n, cudaMemcpyHostToDevice) != cudaSuccess)
+            s = fail(RGL_ERR_DEVICE, "p-value upload");
+    };
+    cp(d_goff.p, goff.data(), goff.size() * 8);
+    cp(d_g.p, gs.data(), gs.size() * sizeof(QGroupDev));
+    cp(d_coff.p, m->chrom_off.data(), C * 8);
+    cp(d_cnt.p, counts, cells * 4);
+    cp(d_bp.p, overlap_bp, cells * 8);
+    if (s == RGL_OK) {
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+        const uint64_t warps = std::min<uint64_t>(cells, (uint64_t)nsm * 64);
+        k_pvalues<<<(unsigned)((warps * 32 + 255) / 256), 256>>>(
+            rows, D, C, d_cnt.as<uint32_t>(), d_bp.as<unsigned long long>(), (double)bin_size, d_goff.as<uint64_t>(),
+            d_g.as<QGroupDev>(), m->d_mv, d_coff.as<uint64_t>(), m->stride, m->d_len, d_p.as<double>(),
+            d_llr.as<double>(), d_lp.as<double>(), d_f.as<uint8_t>());
+        if (cudaGetLastError() != cudaSuccess) s = fail(RGL_ERR_DEVICE, "k_pvalues launch");
+    }
+    auto back = [&](void* dst, const void* src, size_t n) {
+        if (s == RGL_OK && dst && cudaMemcpy(dst, src, n, cudaMemcpyDeviceToHost) != cudaSuccess)
+            s = fail(RGL_ERR_DEVICE, "p-value download");
+    };
+    back(p, d_p.p, cells * 8);
+    back(llr, d_llr.p, cells * 8);
+    back(log_p, d_lp.p, cells * 8);
+    back(flags, d_f.p, cells);
+    for (DevBuf* x : {&d_goff, &d_g, &d_coff, &d_cnt, &d_bp, &d_p, &d_llr, &d_lp, &d_f}) x->release();
+    return s;
+}
+
+}  // extern "C"
