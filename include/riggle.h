@@ -232,6 +232,18 @@ int rgl_moments_set(rgl_moments* m, uint32_t sid, uint32_t chrom, const float* m
 int rgl_moments_get(const rgl_moments* m, uint32_t sid, uint32_t chrom, float* mean_var, uint64_t capacity,
                     uint64_t* out_entries);
 
+/* build_depth_signal (src/fourier/depth.rs:109-204) on the device: the f32 coverage of one source on
+ * one chromosome of n_bins bins, bit for bit the reference's (same impulse and prefix-sum order).
+ * Intervals in the source file's order; g_out holds n_bins floats. */
+int rgl_depth_signal(int device, const rgl_interval* intervals, uint64_t n, uint64_t n_bins, uint32_t bin_size,
+                     float* g_out);
+/* build_chrom_moments (src/fourier/moments.rs:129-132, 192-254) on the device for (sid, chrom) of the
+ * store: depth signal, FP64 Stockham-FFT autocorrelation of the centred signal and double-double
+ * prefix sums, FP64 window mean / variance for the chromosome's L grid, stored as f32.
+ * mean_out / var_out (optional, host, grid length) receive the FP64 values. */
+int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_interval* intervals, uint64_t n,
+                      uint32_t bin_size, double* mean_out, double* var_out);
+
 /* Query length groups of a batch: row q owns groups [row_group_offsets[q], row_group_offsets[q+1]),
  * each on chromosome group_chrom[g] of the moment store. */
 typedef struct rgl_pvalue_batch {

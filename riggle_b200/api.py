@@ -311,6 +311,14 @@ def moment_grid(n_bins):
     return out
 
 
+def depth_signal(intervals, n_bins, bin_size=BIN_SIZE, device=0):
+    """The reference's f32 coverage signal of intervals (file order) on one chromosome (GPU)."""
+    iv = np.ascontiguousarray(np.asarray(intervals, np.uint32).reshape(-1, 3))
+    g = np.empty(int(n_bins), np.float32)
+    check(load().rgl_depth_signal(device, _ptr(iv), len(iv), int(n_bins), bin_size, _ptr(g)))
+    return g
+
+
 def query_chrom_groups(intervals, bin_size=BIN_SIZE):
     """build_query_chrom_data for one chromosome: (l_int, sum_scale, sum_scale2, count)."""
     iv = np.ascontiguousarray(np.asarray(intervals, np.uint32).reshape(-1, 3))
@@ -340,6 +348,15 @@ class Moments:
     def set(self, sid, chrom, mean_var):
         mv = np.ascontiguousarray(np.asarray(mean_var, np.float32).reshape(-1, 2))
         check(load().rgl_moments_set(self._h, sid, chrom, _ptr(mv), len(mv)))
+
+    def build(self, sid, chrom, intervals, bin_size=BIN_SIZE, report=False):
+        """Moments of one source's intervals (file order) on one chromosome, computed on the GPU."""
+        iv = np.ascontiguousarray(np.asarray(intervals, np.uint32).reshape(-1, 3))
+        n = self.slots(chrom)
+        mean = np.empty(n, np.float64) if report else None
+        var = np.empty(n, np.float64) if report else None
+        check(load().rgl_moments_build(self._h, sid, chrom, _ptr(iv), len(iv), bin_size, _ptr(mean), _ptr(var)))
+        return (mean, var) if report else None
 
     def get(self, sid, chrom):
         n = C.c_uint64()

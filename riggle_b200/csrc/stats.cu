@@ -169,6 +169,26 @@ struct rgl_moments {
     std::vector<uint32_t> len;  // host mirror of the per-(source, chromosome) table lengths
 };
 
+namespace rgl {
+// Device pointer of the (sid, chrom) table of a moment store and its full grid length.
+int moments_table_ptr(rgl_moments* m, uint32_t sid, uint32_t chrom, float2** ptr, uint64_t* slots, uint64_t* n_bins,
+                      int* device) {
+    if (!m || sid >= m->num_sources || chrom >= m->num_chroms) return fail(RGL_ERR_INVALID_ARGUMENT, "bad moment table");
+    *ptr = m->d_mv + (uint64_t)sid * m->stride + m->chrom_off[chrom];
+    *slots = m->n_slots[chrom];
+    *n_bins = m->n_bins[chrom];
+    *device = m->device;
+    return RGL_OK;
+}
+// Records that (sid, chrom) now holds `entries` entries.
+int moments_mark(rgl_moments* m, uint32_t sid, uint32_t chrom, uint64_t entries) {
+    const uint32_t l = (uint32_t)entries;
+    m->len[(size_t)sid * m->num_chroms + chrom] = l;
+    RGL_CUDA(cudaMemcpy(m->d_len + (size_t)sid * m->num_chroms + chrom, &l, 4, cudaMemcpyHostToDevice));
+    return RGL_OK;
+}
+}  // namespace rgl
+
 extern "C" {
 
 uint64_t rgl_compact_index(uint64_t l) { return l ? compact_index(l) : 0; }
