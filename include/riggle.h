@@ -237,6 +237,22 @@ int rgl_moments_get(const rgl_moments* m, uint32_t sid, uint32_t chrom, float* m
  * Intervals in the source file's order; g_out holds n_bins floats. */
 int rgl_depth_signal(int device, const rgl_interval* intervals, uint64_t n, uint64_t n_bins, uint32_t bin_size,
                      float* g_out);
+/* Allocation-free depth signal (no counterpart in the reference).  For callers that cannot
+ * allocate device memory during the call: code recording a CUDA graph (cudaMalloc is not a
+ * capturable operation), hosts that route every device allocation through their own arena, and
+ * latency-critical loops that cannot take cudaMalloc's implicit synchronisation.  Same result as
+ * rgl_depth_signal, from device-resident intervals into d_g (n_bins floats, device), enqueued on
+ * `stream` (a cudaStream_t, NULL = legacy default stream) without synchronising.  Its scratch is a
+ * static device array of RGL_NOALLOC_SCRATCH_BYTES (17 MiB) that every GPU loading the library
+ * holds until exit; inputs above RGL_NOALLOC_MAX_INTERVALS intervals or RGL_NOALLOC_MAX_BINS bins
+ * are rejected with RGL_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
+ * device address (make it before any stream capture).  All calls share the array: calls that may
+ * overlap on the GPU (different streams, or threads) race and must be serialised by the caller. */
+#define RGL_NOALLOC_MAX_INTERVALS 65536u
+#define RGL_NOALLOC_MAX_BINS 4194304u
+#define RGL_NOALLOC_SCRATCH_BYTES (17u << 20)
+int rgl_depth_signal_noalloc(int device, const rgl_interval* d_intervals, uint64_t n, uint64_t n_bins,
+                             uint32_t bin_size, float* d_g, void* stream);
 /* build_chrom_moments (src/fourier/moments.rs:129-132, 192-254) on the device for (sid, chrom) of the
  * store: depth signal, FP64 Stockham-FFT autocorrelation of the centred signal and double-double
  * prefix sums, FP64 window mean / variance for the chromosome's L grid, stored as f32.

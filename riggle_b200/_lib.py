@@ -130,6 +130,7 @@ _SIGS = {
     "rgl_moments_set": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, C.c_uint64]),
     "rgl_moments_get": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
     "rgl_depth_signal": (C.c_int, [C.c_int, _P, C.c_uint64, C.c_uint64, C.c_uint32, _P]),
+    "rgl_depth_signal_noalloc": (C.c_int, [C.c_int, _P, C.c_uint64, C.c_uint64, C.c_uint32, _P, _P]),
     "rgl_moments_build": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, C.c_uint64, C.c_uint32, _P, _P]),
     "rgl_query_pvalues": (C.c_int, [_P, C.POINTER(PValueBatch), C.c_uint32, _P, _P, _P, _P, _P, _P]),
     "rgl_synth_chrom_lengths": (C.c_int, [C.c_uint64, C.c_uint32, _P]),

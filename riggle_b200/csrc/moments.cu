@@ -549,3 +549,125 @@ int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_in
 }
 
 }  // extern "C"
+
+// ================================================================================================
+// Allocation-free depth signal.
+//
+// Some callers cannot allocate device memory while they call this library: code that is recording
+// a CUDA graph (cudaMalloc / cudaFree are not capturable operations), hosts that route every
+// device allocation through their own arena or memory pool and forbid allocations behind its back,
+// and latency-critical loops that cannot afford cudaMalloc's implicit device-wide synchronisation.
+// rgl_depth_signal_noalloc serves them: the same bit-exact depth signal as rgl_depth_signal, from
+// device-resident intervals into a caller-provided device buffer, with all of its scratch (impulse
+// records, sort buffers, per-chunk carries, CUB temporary storage) in one fixed array in this
+// file.  The array is a static device variable: every GPU that loads the library holds its
+// RGL_NOALLOC_SCRATCH_BYTES until the process exits.
+// ================================================================================================
+namespace {
+
+constexpr uint64_t kNaMaxIv = RGL_NOALLOC_MAX_INTERVALS;
+constexpr uint64_t kNaMaxBins = RGL_NOALLOC_MAX_BINS;
+constexpr uint64_t kNaKeys = 4 * kNaMaxIv * 8;           // one key array (u64 x 4 records per interval)
+constexpr uint64_t kNaVals = 4 * kNaMaxIv * 4;           // one value array (f32)
+constexpr uint64_t kNaChunks = kNaMaxBins / 8;
+constexpr uint64_t kNaOffKeyA = 0;
+constexpr uint64_t kNaOffKeyB = kNaOffKeyA + kNaKeys;
+constexpr uint64_t kNaOffValA = kNaOffKeyB + kNaKeys;
+constexpr uint64_t kNaOffValB = kNaOffValA + kNaVals;
+constexpr uint64_t kNaOffTot = kNaOffValB + kNaVals;
+constexpr uint64_t kNaOffIdx = kNaOffTot + kNaChunks * 4;
+constexpr uint64_t kNaOffCum = kNaOffIdx + kNaChunks * 4;
+constexpr uint64_t kNaOffNz = kNaOffCum + kNaChunks * 4;
+constexpr uint64_t kNaOffCnt = kNaOffNz + ((kNaChunks + 255) / 256) * 256;
+constexpr uint64_t kNaOffTmp = kNaOffCnt + 256;
+static_assert(kNaOffTmp < RGL_NOALLOC_SCRATCH_BYTES, "scratch layout exceeds its array");
+constexpr uint64_t kNaTmpBytes = RGL_NOALLOC_SCRATCH_BYTES - kNaOffTmp;
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[RGL_NOALLOC_SCRATCH_BYTES];
+
+namespace {
+std::mutex g_na_mu;
+unsigned char* g_na_ptr[64] = {nullptr};  // device address of g_noalloc_scratch, per device
+
+// Once per device, with that device current: the array's device address (the symbol itself is only
+// a host-side stand-in), and a check that CUB's temporary storage for the largest inputs fits.
+int noalloc_setup(int device, unsigned char** out) {
+    std::lock_guard<std::mutex> lk(g_na_mu);
+    if (!g_na_ptr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess)
+            return fail(RGL_ERR_DEVICE, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        size_t sort_b = 0, sel_b = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, sort_b, (uint64_t*)nullptr, (uint64_t*)nullptr, (float*)nullptr,
+                                        (float*)nullptr, (int)(4 * kNaMaxIv), 0, 64);
+        cub::DeviceSelect::Flagged(nullptr, sel_b, cub::CountingInputIterator<uint32_t>(0), (uint8_t*)nullptr,
+                                   (uint32_t*)nullptr, (int*)nullptr, (int)kNaChunks);
+        if (std::max(sort_b, sel_b) > kNaTmpBytes)
+            return fail(RGL_ERR_UNSUPPORTED, "CUB temporary storage exceeds the reserved scratch");
+        g_na_ptr[device] = static_cast<unsigned char*>(p);
+    }
+    *out = g_na_ptr[device];
+    return RGL_OK;
+}
+}  // namespace
+
+extern "C" int rgl_depth_signal_noalloc(int device, const rgl_interval* d_intervals, uint64_t n, uint64_t n_bins,
+                                        uint32_t bin_size, float* d_g, void* stream) {
+    clear_error();
+    if ((n && !d_intervals) || !d_g || bin_size == 0 || n_bins == 0) return fail(RGL_ERR_INVALID_ARGUMENT, "bad arguments");
+    if (n > kNaMaxIv)
+        return fail(RGL_ERR_INVALID_ARGUMENT, "rgl_depth_signal_noalloc takes at most " +
+                                                  std::to_string(kNaMaxIv) + " intervals (got " + std::to_string(n) + ")");
+    if (n_bins > kNaMaxBins)
+        return fail(RGL_ERR_INVALID_ARGUMENT, "rgl_depth_signal_noalloc takes at most " +
+                                                  std::to_string(kNaMaxBins) + " bins (got " + std::to_string(n_bins) + ")");
+    if (n_bins * (uint64_t)bin_size > 0xFFFFFFFFull) return fail(RGL_ERR_INVALID_ARGUMENT, "n_bins * bin_size overflows u32");
+    if (device < 0 || device >= 64) return fail(RGL_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    int prev = 0;
+    RGL_CUDA(cudaGetDevice(&prev));
+    RGL_CUDA(cudaSetDevice(device));
+    struct Restore {
+        int d;
+        ~Restore() { cudaSetDevice(d); }
+    } restore{prev};
+    unsigned char* base = nullptr;
+    RGL_TRY(noalloc_setup(device, &base));
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    uint64_t* key_a = reinterpret_cast<uint64_t*>(base + kNaOffKeyA);
+    uint64_t* key_b = reinterpret_cast<uint64_t*>(base + kNaOffKeyB);
+    float* val_a = reinterpret_cast<float*>(base + kNaOffValA);
+    float* val_b = reinterpret_cast<float*>(base + kNaOffValB);
+    float* totals = reinterpret_cast<float*>(base + kNaOffTot);
+    uint32_t* idx = reinterpret_cast<uint32_t*>(base + kNaOffIdx);
+    float* cum = reinterpret_cast<float*>(base + kNaOffCum);
+    uint8_t* nz = base + kNaOffNz;
+    int* cnt = reinterpret_cast<int*>(base + kNaOffCnt);
+    void* tmp = base + kNaOffTmp;
+    // the output and the compacted-chunk count start at zero; every other scratch word a call reads
+    // it writes first
+    RGL_CUDA(cudaMemsetAsync(d_g, 0, n_bins * 4, st));
+    RGL_CUDA(cudaMemsetAsync(cnt, 0, 4, st));
+    if (n) {
+        const uint64_t m = 4 * n;
+        k_spike_records<<<blocks_for(n), 256, 0, st>>>((uint32_t)n, d_intervals, (uint32_t)n_bins, bin_size, key_a, val_a);
+        size_t tb = kNaTmpBytes;
+        RGL_CUDA(cub::DeviceRadixSort::SortPairs(tmp, tb, key_a, key_b, val_a, val_b, (int)m, 0, 64, st));
+        k_bin_sums<<<blocks_for(m), 256, 0, st>>>(m, key_b, val_b, d_g);
+    }
+    if (n_bins > 1) {
+        const uint64_t full = n_bins / 8;
+        if (full) {
+            k_chunk_local<<<blocks_for(full), 256, 0, st>>>(full, d_g, totals, nz);
+            size_t tb = kNaTmpBytes;
+            RGL_CUDA(cub::DeviceSelect::Flagged(tmp, tb, cub::CountingInputIterator<uint32_t>(0), nz, idx, cnt,
+                                                (int)full, st));
+        }
+        k_carry_chain<<<1, 1, 0, st>>>(cnt, idx, totals, cum, d_g, n_bins, full);
+        if (full) k_apply_carry<<<blocks_for(full * 8), 256, 0, st>>>(full, cnt, idx, cum, d_g);
+    }
+    RGL_CUDA(cudaGetLastError());
+    return RGL_OK;
+}
