@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--chunk", type=int, default=0)
     ap.add_argument("--ctas-per-sm", type=int, default=0)
+    ap.add_argument("--pair-ratio", type=int, default=0,
+                    help="candidate/union ratio below which a range is swept pair by pair (0 = library default)")
     ap.add_argument("--db-intervals", type=int, default=2_000_000_000,
                     help="database size of the plain workload (smaller values for profiling captures)")
     ap.add_argument("--chroms", type=int, default=24,
@@ -258,7 +260,7 @@ def run_riggle(args, rank, world, local_rank, dist):
 
     stream = torch.cuda.ExternalStream(ctx.stream)
     shard_ids = np.arange(len(cl), dtype=np.uint32)
-    opts = _lib.QueryOpts(args.chunk, args.ctas_per_sm, 0, 0)
+    opts = _lib.QueryOpts(args.chunk, args.ctas_per_sm, 0, 0, args.pair_ratio)
     d_files = [torch.from_numpy(f[0].view(np.int32)).to(f"cuda:{dev}") for f in files]
     d_counts = torch.zeros((1, D), dtype=torch.int32, device=f"cuda:{dev}")
     d_bp = torch.zeros((1, D), dtype=torch.int64, device=f"cuda:{dev}")

@@ -166,10 +166,12 @@ typedef struct rgl_query_batch {
 
 /* Launch shape.  0 = default / autotuned. */
 typedef struct rgl_query_opts {
-    uint32_t chunk;       /* DB positions per work item */
+    uint32_t chunk;       /* positions per work item */
     uint32_t ctas_per_sm; /* persistent CTAs per SM */
     uint32_t block;       /* threads per CTA */
     uint32_t flags;       /* RGL_QF_* */
+    uint32_t pair_ratio;  /* a candidate range is swept pair by pair when its candidates are at most
+                             pair_ratio x its union size, else by rank differences (default 2) */
 } rgl_query_opts;
 
 #define RGL_QF_NO_OVERLAP 1u /* skip base-pair accumulation (counts only) */
@@ -177,6 +179,8 @@ typedef struct rgl_query_opts {
 typedef struct rgl_query_stats {
     uint64_t query_intervals;  /* intervals in the batch (on shards present in the index) */
     uint64_t db_swept;         /* DB intervals in the union of candidate ranges, all (shard, layer) */
+    uint64_t rank_positions;   /* union elements swept by rank differences */
+    uint64_t pair_candidates;  /* candidates swept pair by pair */
     uint64_t ranges;           /* merged candidate ranges */
     uint64_t work_items;       /* work items pulled by the sweep kernel */
     float sweep_ms;            /* sweep kernel time (CUDA events on the context stream) */

@@ -63,11 +63,13 @@ class QueryBatch(C.Structure):
 
 
 class QueryOpts(C.Structure):
-    _fields_ = [("chunk", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("block", C.c_uint32), ("flags", C.c_uint32)]
+    _fields_ = [("chunk", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("block", C.c_uint32), ("flags", C.c_uint32),
+                ("pair_ratio", C.c_uint32)]
 
 
 class QueryStats(C.Structure):
-    _fields_ = [("query_intervals", C.c_uint64), ("db_swept", C.c_uint64), ("ranges", C.c_uint64),
+    _fields_ = [("query_intervals", C.c_uint64), ("db_swept", C.c_uint64), ("rank_positions", C.c_uint64),
+                ("pair_candidates", C.c_uint64), ("ranges", C.c_uint64),
                 ("work_items", C.c_uint64), ("sweep_ms", C.c_float), ("device_ms", C.c_float),
                 ("chunk", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("block", C.c_uint32),
                 ("kernel_launches", C.c_uint32)]

@@ -143,10 +143,10 @@ class Context:
         check(load().rgl_context_sync(self._h))
 
     @staticmethod
-    def _opts(chunk=0, ctas_per_sm=0, counts_only=False):
-        return _lib.QueryOpts(chunk, ctas_per_sm, 0, 1 if counts_only else 0)
+    def _opts(chunk=0, ctas_per_sm=0, counts_only=False, pair_ratio=0):
+        return _lib.QueryOpts(chunk, ctas_per_sm, 0, 1 if counts_only else 0, pair_ratio)
 
-    def query_counts(self, shards, num_rows, with_overlap=True, chunk=0, ctas_per_sm=0, out=None):
+    def query_counts(self, shards, num_rows, with_overlap=True, chunk=0, ctas_per_sm=0, out=None, pair_ratio=0):
         """shards: {shard name (str) or id (int): uint32[n,3] (start, end, row)}.
 
         Returns (counts uint32[num_rows, D], overlap_bp uint64[num_rows, D] or None, stats dict).
@@ -168,7 +168,7 @@ class Context:
         else:
             counts, bp = out
         st = _lib.QueryStats()
-        opts = self._opts(chunk, ctas_per_sm, not with_overlap)
+        opts = self._opts(chunk, ctas_per_sm, not with_overlap, pair_ratio)
         check(load().rgl_query_counts(self._h, C.byref(batch), C.byref(opts), _ptr(counts), _ptr(bp), C.byref(st)))
         return counts, bp, st.as_dict()
 

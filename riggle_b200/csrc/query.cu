@@ -41,8 +41,16 @@ struct RangeDesc {
     uint32_t layer_idx;         // index into the layer table
     uint32_t qrow;              // query row (Q_SID)
     uint32_t seg;               // query segment (shard, row)
-    uint32_t pad;
+    uint32_t slot;              // layer slot K
 };
+
+// One query's candidate run for the pair sweep: DB elements [base, base + plen) of its layer.
+struct PairSeg {
+    uint64_t base;
+    uint32_t qs, qe, qrow, pad;
+};
+
+enum : uint8_t { M_RANK = 0, M_PAIR = 1 };
 
 // Rank table of one query segment: bin b (width 2^shift bp) holds, at tab[off + b], the number of
 // the segment's sorted starts (tab_s) or ends (tab_e) below b << shift, as absolute positions in
@@ -261,6 +269,7 @@ __global__ void k_range_emit(uint32_t n, uint32_t nslots, uint32_t rows, const u
         ranges[r].layer_idx = (uint32_t)li;
         ranges[r].qrow = sg % rows;
         ranges[r].seg = segnum[i] - 1;
+        ranges[r].slot = K;
     }
     bool last = (i + 1 == n) || segflag[i + 1] || rflag[t + 1];
     if (last) {
@@ -269,15 +278,68 @@ __global__ void k_range_emit(uint32_t n, uint32_t nslots, uint32_t rows, const u
     }
 }
 
-__global__ void k_range_len(uint64_t cap, const uint32_t* __restrict__ ridx_total_ptr,
-                            const RangeDesc* __restrict__ ranges, uint64_t* __restrict__ rlen) {
-    uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+// Per range: the reference's candidate count (sum over its queries of hi - lo) against the size of
+// the union.  Where the two are close (narrow layers) the pair sweep reads each candidate once with
+// trivial per-pair work; where candidate windows overlap heavily (broad layers) the rank sweep reads
+// each union element once.  rlen = union length of rank ranges (the rank work space), ulen = union
+// length of every range (the swept count of the metric).
+__global__ void k_range_method(uint64_t cap, uint32_t n, const uint32_t* __restrict__ ridx_total_ptr,
+                               const RangeDesc* __restrict__ ranges, const uint64_t* __restrict__ pc,
+                               uint32_t pair_ratio, uint8_t* __restrict__ method, uint64_t* __restrict__ rlen,
+                               uint64_t* __restrict__ ulen) {
+    const uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (r > cap) return;
-    uint32_t R = *ridx_total_ptr;
-    rlen[r] = (r < R) ? (uint64_t)(ranges[r].db_hi - ranges[r].db_lo) : 0ull;
+    const uint32_t R = *ridx_total_ptr;
+    if (r >= R) {
+        rlen[r] = 0;
+        ulen[r] = 0;
+        return;
+    }
+    const RangeDesc rd = ranges[r];
+    const uint64_t len = rd.db_hi - rd.db_lo;
+    const uint64_t t0 = (uint64_t)rd.slot * n + rd.i_first, t1 = (uint64_t)rd.slot * n + rd.i_last + 1;
+    const uint64_t cand = pc[t1] - pc[t0];
+    const uint8_t m = (cand <= (uint64_t)pair_ratio * len) ? M_PAIR : M_RANK;
+    method[r] = m;
+    rlen[r] = m == M_RANK ? len : 0;
+    ulen[r] = len;
 }
 
-// ---- 5. K2 sweep -----------------------------------------------------------------------------------
+__global__ void k_cand_len(uint64_t tot, const uint32_t* __restrict__ lo, const uint32_t* __restrict__ hi,
+                           uint64_t* __restrict__ cl) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t > tot) return;
+    cl[t] = t < tot ? (uint64_t)(hi[t] - lo[t]) : 0;
+}
+
+// Pair work space: each query of a pair range contributes its candidate run.
+__global__ void k_pair_len(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ seg,
+                           const int32_t* __restrict__ slot, const LayerDev* __restrict__ layers,
+                           const uint32_t* __restrict__ lo, const uint32_t* __restrict__ hi,
+                           const uint32_t* __restrict__ rflag, const uint32_t* __restrict__ ridx,
+                           const uint8_t* __restrict__ method, const uint32_t* __restrict__ starts,
+                           const uint32_t* __restrict__ qend, uint64_t* __restrict__ plen, PairSeg* __restrict__ psegs) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t tot = (uint64_t)n * nslots;
+    if (t > tot) return;
+    if (t == tot) {
+        plen[t] = 0;
+        return;
+    }
+    const uint32_t K = (uint32_t)(t / n), i = (uint32_t)(t % n);
+    const uint32_t sg = seg[i];
+    const int32_t li = slot[(uint64_t)(sg / rows) * nslots + K];
+    uint64_t len = 0;
+    if (li >= 0) {
+        const uint32_t r = ridx[t] + rflag[t] - 1;
+        if (method[r] == M_PAIR) {
+            len = hi[t] - lo[t];
+            psegs[t] = PairSeg{layers[li].off + lo[t], starts[i], qend[i], sg % rows, 0};
+        }
+    }
+    plen[t] = len;
+}
+
 struct SweepParams {
     const uint64_t* rpos;   // exclusive scan of range lengths, cap+1 entries; rpos[cap] = total
     uint64_t rcap;          // range capacity (entries of rpos minus one)
@@ -293,6 +355,9 @@ struct SweepParams {
     unsigned long long* bp;  // rows x D (may be null)
     uint32_t* queue;         // work counter
     const uint32_t* item_r0; // first range of each work item (items < item_cap)
+    const uint64_t* ppos;    // pair work space: exclusive scan of candidate runs, rcap + 1 entries
+    const PairSeg* psegs;
+    const uint32_t* item_t0; // first run of each pair work item
     const SegTab* segtabs;   // per query segment
     const uint32_t* tab_s;   // rank tables of sorted starts / ends
     const uint32_t* tab_e;
@@ -537,6 +602,72 @@ __global__ void __launch_bounds__(256, 3) k_sweep(SweepParams P) {
     }
 }
 
+// The pair sweep: the reference's scan (src/sweep/query.rs:147-158) over the candidate runs of the
+// queries of pair ranges, every candidate read once by one lane (lane l of a warp takes positions
+// p0 + l, p0 + l + 32, ...; consecutive positions of a run are consecutive DB elements, so the loads
+// coalesce).  A candidate d of query q overlaps when d.end > q.start (d.start < q.end and the
+// look-back bound hold by construction of the run); it adds 1 and min(ends) - max(starts).
+template <bool WITH_BP>
+__global__ void __launch_bounds__(256, 4) k_pairs(SweepParams P) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
+    uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t total = P.ppos[P.rcap];
+    if (P.smem_tally)
+        for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
+            s_cnt[k] = 0;
+            if (WITH_BP) s_bp[k] = 0;
+        }
+    __syncthreads();
+    for (;;) {
+        uint32_t item = 0;
+        if (lane == 0) item = atomicAdd(P.queue, 1u);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        const uint64_t p0 = (uint64_t)item * P.chunk;
+        if (p0 >= total) break;
+        const uint64_t p1 = min(p0 + P.chunk, total);
+        uint32_t t;
+        if (item < P.item_cap) {
+            t = __ldg(P.item_t0 + item);
+        } else {
+            uint64_t lo = 0, hi = P.rcap;
+            while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (__ldg(P.ppos + m) <= p0) lo = m; else hi = m - 1; }
+            t = (uint32_t)lo;
+        }
+        uint64_t rlo = __ldg(P.ppos + t), rhi = __ldg(P.ppos + t + 1);
+        PairSeg ps = P.psegs[t];
+        for (uint64_t p = p0 + lane; p < p1; p += 32) {
+            if (p >= rhi) {
+                t = range_advance(P.ppos, t, (uint32_t)P.rcap, p);
+                rlo = __ldg(P.ppos + t);
+                rhi = __ldg(P.ppos + t + 1);
+                ps = P.psegs[t];
+            }
+            const uint64_t di = ps.base + (p - rlo);
+            const uint2 d = __ldg(P.pos + di);
+            if (d.y > ps.qs) {
+                const uint32_t sid = __ldg(P.sid + di);
+                if (P.smem_tally) {
+                    atomicAdd(&s_cnt[sid], 1u);
+                    if (WITH_BP) atomicAdd(&s_bp[sid], (unsigned long long)(min(ps.qe, d.y) - max(ps.qs, d.x)));
+                } else {
+                    const uint64_t cell = (uint64_t)ps.qrow * P.D + sid;
+                    atomicAdd(&P.counts[cell], 1u);
+                    if (WITH_BP) atomicAdd(&P.bp[cell], (unsigned long long)(min(ps.qe, d.y) - max(ps.qs, d.x)));
+                }
+            }
+        }
+    }
+    if (P.smem_tally) {
+        __syncthreads();
+        for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
+            if (s_cnt[k]) atomicAdd(&P.counts[k], s_cnt[k]);
+            if (WITH_BP && s_bp[k]) atomicAdd(&P.bp[k], s_bp[k]);
+        }
+    }
+}
+
 }  // namespace rgl
 
 using namespace rgl;
@@ -554,6 +685,7 @@ struct rgl_context {
     DevBuf starts, ends, seg, segflag, segnum, seg_begin, ps_in, pe_in, ps, pe;
     DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp, item_r0;
     DevBuf segtab, tab_len, tab_off, tab_s, tab_e;
+    DevBuf cl, pc, method, ulen, plen, ppos, psegs, item_t0;
     uint32_t* h_small = nullptr;  // pinned mirror of `small`
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     uint64_t res_n = 0;
@@ -606,6 +738,14 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     RGL_TRY(c->rpos.ensure(tot * 8 + 16));
     RGL_TRY(c->small.ensure(256));
     RGL_TRY(c->item_r0.ensure(kItemCap * 4));
+    RGL_TRY(c->item_t0.ensure(kItemCap * 4));
+    RGL_TRY(c->cl.ensure(tot * 8 + 16));
+    RGL_TRY(c->pc.ensure(tot * 8 + 16));
+    RGL_TRY(c->method.ensure(tot + 16));
+    RGL_TRY(c->ulen.ensure(tot * 8 + 16));
+    RGL_TRY(c->plen.ensure(tot * 8 + 16));
+    RGL_TRY(c->ppos.ensure(tot * 8 + 16));
+    RGL_TRY(c->psegs.ensure(tot * sizeof(PairSeg) + sizeof(PairSeg)));
     RGL_TRY(c->segtab.ensure((n + 1) * sizeof(SegTab)));
     RGL_TRY(c->tab_len.ensure((n + 2) * 4));
     RGL_TRY(c->tab_off.ensure((n + 2) * 4));
@@ -631,6 +771,8 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, nn + 1, c->stream);
     need = std::max(need, b);
+    cub::DeviceReduce::Sum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nt, c->stream);
+    need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nt, c->stream);
     need = std::max(need, b);
     RGL_TRY(c->cub_tmp.ensure(need + 256));
@@ -646,16 +788,18 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
 inline unsigned grid_for(uint64_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
 
 struct Launch {
-    uint32_t chunk, ctas_per_sm, block;
+    uint32_t chunk, ctas_per_sm, block, pair_ratio;
 };
 
 Launch pick_launch(const rgl_query_opts* o) {
-    Launch l{512, 4, 256};
+    Launch l{2048, 4, 256, 2};
     if (o) {
         if (o->chunk) l.chunk = o->chunk;
         if (o->ctas_per_sm) l.ctas_per_sm = o->ctas_per_sm;
         if (o->block) l.block = 256;  // the kernel is compiled for 256 threads
+        if (o->pair_ratio) l.pair_ratio = o->pair_ratio;
     }
+    l.chunk = (l.chunk + 31) & ~31u;  // keep warps whole
     if (l.chunk < 32) l.chunk = 32;
     if (l.ctas_per_sm < 1) l.ctas_per_sm = 1;
     if (l.ctas_per_sm > 8) l.ctas_per_sm = 8;
@@ -690,7 +834,14 @@ int finish(rgl_context* c, const Launch& L, rgl_query_stats* stats) {
         uint64_t T = 0;
         if (c->last_n) std::memcpy(&T, c->h_small + 4, 8);
         stats->db_swept = T;
-        stats->work_items = (T + L.chunk - 1) / L.chunk;
+        uint64_t TR = 0, TP = 0;
+        if (c->last_n) {
+            std::memcpy(&TR, c->h_small + 6, 8);
+            std::memcpy(&TP, c->h_small + 8, 8);
+        }
+        stats->rank_positions = TR;
+        stats->pair_candidates = TP;
+        stats->work_items = (TR + L.chunk - 1) / L.chunk + (TP + L.chunk - 1) / L.chunk;
         stats->sweep_ms = c->last_n ? t_sweep : 0.f;
         stats->device_ms = c->last_n ? t_all : 0.f;
         stats->chunk = L.chunk;
@@ -797,18 +948,42 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
                                                      c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
                                                      c->ranges.as<RangeDesc>());
     launches++;
-    k_range_len<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, c->ridx.as<uint32_t>() + tot, c->ranges.as<RangeDesc>(),
-                                                        c->rlen.as<uint64_t>());
-    launches++;
+    // candidate counts per (K, query) -> per-range method; rank and pair work spaces
+    k_cand_len<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
+                                                       c->cl.as<uint64_t>());
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->cl.as<uint64_t>(), c->pc.as<uint64_t>(),
+                                           (int)(tot + 1), st));
+    k_range_method<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, n, c->ridx.as<uint32_t>() + tot,
+                                                           c->ranges.as<RangeDesc>(), c->pc.as<uint64_t>(),
+                                                           L.pair_ratio, c->method.as<uint8_t>(),
+                                                           c->rlen.as<uint64_t>(), c->ulen.as<uint64_t>());
+    k_pair_len<<<grid_for(tot + 1, 256), 256, 0, st>>>(n, ns, rows, c->seg.as<uint32_t>(), idx->d_slot,
+                                                       idx->d_layers, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
+                                                       c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
+                                                       c->method.as<uint8_t>(), c->starts.as<uint32_t>(),
+                                                       c->val_b.as<uint32_t>(), c->plen.as<uint64_t>(),
+                                                       c->psegs.as<PairSeg>());
+    launches += 3;
     tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(),
                                            (int)(tot + 1), st));
-
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->plen.as<uint64_t>(), c->ppos.as<uint64_t>(),
+                                           (int)(tot + 1), st));
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceReduce::Sum(c->cub_tmp.p, tb, c->ulen.as<uint64_t>(),
+                                    reinterpret_cast<uint64_t*>(d_small + 4), (int)tot, st));
     k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(tot, c->rpos.as<uint64_t>(), L.chunk, kItemCap,
                                                                c->item_r0.as<uint32_t>());
-    launches++;
+    k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(tot, c->ppos.as<uint64_t>(), L.chunk, kItemCap,
+                                                               c->item_t0.as<uint32_t>());
+    launches += 2;
     SweepParams P;
     P.item_r0 = c->item_r0.as<uint32_t>();
+    P.item_t0 = c->item_t0.as<uint32_t>();
+    P.ppos = c->ppos.as<uint64_t>();
+    P.psegs = c->psegs.as<PairSeg>();
     P.segtabs = c->segtab.as<SegTab>();
     P.tab_s = c->tab_s.as<uint32_t>();
     P.tab_e = c->tab_e.as<uint32_t>();
@@ -835,15 +1010,18 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
     unsigned grid = (unsigned)(c->num_sms * L.ctas_per_sm);
     if (stats) RGL_CUDA(cudaEventRecord(c->ev[1], st));
     if (c->timing) RGL_TRY(timing_record(c, true));
-    if (with_bp) {
-        if (smem > 48 * 1024)
-            RGL_CUDA(cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_sweep<true><<<grid, 256, smem, st>>>(P);
-    } else {
-        if (smem > 48 * 1024)
-            RGL_CUDA(cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_sweep<false><<<grid, 256, smem, st>>>(P);
+    if (smem > 48 * 1024) {
+        RGL_CUDA(cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RGL_CUDA(cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RGL_CUDA(cudaFuncSetAttribute(k_pairs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        RGL_CUDA(cudaFuncSetAttribute(k_pairs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     }
+    if (with_bp) k_sweep<true><<<grid, 256, smem, st>>>(P);
+    else k_sweep<false><<<grid, 256, smem, st>>>(P);
+    P.queue = d_small + 2;  // the pair sweep pulls from its own counter
+    if (with_bp) k_pairs<true><<<grid, 256, smem, st>>>(P);
+    else k_pairs<false><<<grid, 256, smem, st>>>(P);
+    launches++;
     launches++;
     RGL_CUDA(cudaGetLastError());
     if (c->timing) RGL_TRY(timing_record(c, false));
@@ -853,7 +1031,9 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
     if (stats) {
         RGL_CUDA(cudaEventRecord(c->ev[2], st));
         RGL_CUDA(cudaMemcpyAsync(c->h_small + 2, c->ridx.as<uint32_t>() + tot, 4, cudaMemcpyDeviceToHost, st));
-        RGL_CUDA(cudaMemcpyAsync(c->h_small + 4, c->rpos.as<uint64_t>() + tot, 8, cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaMemcpyAsync(c->h_small + 4, d_small + 4, 8, cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaMemcpyAsync(c->h_small + 6, c->rpos.as<uint64_t>() + tot, 8, cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaMemcpyAsync(c->h_small + 8, c->ppos.as<uint64_t>() + tot, 8, cudaMemcpyDeviceToHost, st));
     }
     RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
     return RGL_OK;
@@ -925,7 +1105,8 @@ int rgl_context_destroy(rgl_context* c) {
                       &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps, &c->pe, &c->lo, &c->hi, &c->maxhi,
                       &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos, &c->cub_tmp, &c->small,
                       &c->out_counts, &c->out_bp, &c->item_r0,
-                      &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e};
+                      &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e,
+                      &c->cl, &c->pc, &c->method, &c->ulen, &c->plen, &c->ppos, &c->psegs, &c->item_t0};
     for (DevBuf* b : bufs) b->release();
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);

@@ -46,6 +46,9 @@ def test_random_parity_with_oracle(seed):
     c, bp, st = gpu_counts(layers, {f"s{k}": v for k, v in qsh.items()}, rows, D, nsh)
     assert (c == oc).all()
     assert (bp == obp).all()
+    for ratio in (1, 1000000):  # all ranges by rank differences / all pair by pair
+        c2, bp2, _ = gpu_counts(layers, {f"s{k}": v for k, v in qsh.items()}, rows, D, nsh, pair_ratio=ratio)
+        assert (c2 == oc).all() and (bp2 == obp).all()
     # the device sweeps the union of candidate ranges once per (shard, query row)
     per_row = 0
     for r in range(rows):
@@ -117,8 +120,8 @@ def test_launch_shapes_do_not_change_results():
     ctx = rg.Context(idx)
     ref = None
     for chunk in (256, 1024, 4096, 16384):
-        for cps in (1, 2, 4, 8):
-            c, bp, _ = ctx.query_counts({0: q}, 1, chunk=chunk, ctas_per_sm=cps)
+        for cps, ratio in ((1, 1), (2, 4), (4, 0), (8, 1000000)):
+            c, bp, _ = ctx.query_counts({0: q}, 1, chunk=chunk, ctas_per_sm=cps, pair_ratio=ratio)
             if ref is None:
                 ref = (c, bp)
             assert (c == ref[0]).all() and (bp == ref[1]).all()
