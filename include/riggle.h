@@ -206,6 +206,72 @@ int rgl_query_counts_device(rgl_context* ctx, uint32_t num_rows, uint32_t num_sh
                             const rgl_query_opts* opts, uint32_t* d_counts, uint64_t* d_overlap_bp,
                             rgl_query_stats* stats);
 
+/* ---- Batched form: many query files in one call -------------------------------------------------
+ * Replaces query_database's loop over batches of query files (src/tasks/query/mod.rs:182-307) for a
+ * whole set of files at once; the reference has no single entry point for it.  Block b holds
+ * d_intervals[block_offsets[b] .. block_offsets[b+1]) on index shard block_shards[b]; blocks are laid
+ * end to end (offsets non-decreasing).  Every interval's sid is its output row (query file).  With
+ * block_rows given, all intervals of block b have sid == block_rows[b], which narrows the rows each
+ * sub-batch touches; with NULL they may lie anywhere in [0, num_rows). */
+typedef struct rgl_batch {
+    uint32_t num_rows;
+    uint32_t num_blocks;
+    const uint32_t* block_shards;    /* host, num_blocks */
+    const uint32_t* block_rows;      /* host, num_blocks, or NULL */
+    const uint64_t* block_offsets;   /* host, num_blocks + 1 */
+    const rgl_interval* d_intervals; /* device */
+} rgl_batch;
+
+typedef struct rgl_batch_opts {
+    rgl_query_opts query; /* launch shape of every sub-batch (zeros: tuned shape or defaults) */
+    uint64_t sub_batch;   /* query intervals per sub-batch, the unit of device workspace (0: 2^24) */
+    uint32_t flags;       /* RGL_BF_* */
+} rgl_batch_opts;
+
+#define RGL_BF_GRAPH 1u /* capture the batch as one CUDA graph and replay it while the batch (its block
+                           tables, buffers and launch shape) is unchanged */
+#define RGL_BF_TUNED 2u /* fill zero launch fields from the context's rgl_batch_autotune result */
+
+typedef struct rgl_batch_stats {
+    uint64_t query_intervals;  /* intervals in the batch */
+    uint64_t db_swept;         /* per query file: the union of its candidate ranges, summed */
+    uint64_t rank_positions;   /* union elements swept by rank differences */
+    uint64_t pair_candidates;  /* candidates swept pair by pair */
+    uint64_t ranges;           /* merged candidate ranges */
+    uint32_t sub_batches;      /* pipeline runs */
+    uint32_t kernel_launches;  /* kernels of this library launched (CUB's not counted) */
+    uint32_t graph_nodes;      /* nodes of the captured graph (0 without RGL_BF_GRAPH) */
+    uint32_t graph_replayed;   /* 1: an identical earlier batch's graph was launched again */
+    float device_ms;           /* CUDA events around the whole batch on the context stream */
+    uint32_t chunk, ctas_per_sm, pair_ratio;
+} rgl_batch_stats;
+
+/* Zeroes d_counts (num_rows x D) and d_overlap_bp, then accumulates every sub-batch into them.
+ * Asynchronous on the context stream unless stats is non-NULL; errors in the intervals are then
+ * reported by rgl_context_check.  The first call with RGL_BF_GRAPH sizes the workspace, captures and
+ * launches; later identical calls launch the cached graph without host work per sub-batch. */
+int rgl_query_batch_device(rgl_context* ctx, const rgl_batch* batch, const rgl_batch_opts* opts,
+                           uint32_t* d_counts, uint64_t* d_overlap_bp, rgl_batch_stats* stats);
+
+/* The batched form with the intervals in host memory (page-locked for full speed; batch->d_intervals
+ * is ignored): sub-batch k + 1 is copied to the device on a second stream while sub-batch k is swept.
+ * counts / overlap_bp are host buffers (num_rows x D).  Synchronous; not graph-captured. */
+int rgl_query_batch_host(rgl_context* ctx, const rgl_batch* batch, const rgl_interval* h_intervals,
+                         const rgl_batch_opts* opts, uint32_t* counts, uint64_t* overlap_bp,
+                         rgl_batch_stats* stats);
+
+typedef struct rgl_tune_trial {
+    uint32_t chunk, ctas_per_sm, pair_ratio;
+    float sweep_ms; /* best of two runs of the sweep kernels of the largest sub-batch */
+} rgl_tune_trial;
+
+/* Autotuner: times the sweep kernels of the batch's largest sub-batch for pair_ratio in {1,2,4,8}
+ * at the default shape, then for work-item size {512..8192} x CTAs per SM {2,3,4,6,8}; stores the
+ * fastest shape in the context (used by RGL_BF_TUNED) and returns it in *best.  trials (optional)
+ * receives up to max_trials measurements. */
+int rgl_batch_autotune(rgl_context* ctx, const rgl_batch* batch, uint64_t sub_batch, rgl_query_opts* best,
+                       rgl_tune_trial* trials, uint32_t max_trials, uint32_t* num_trials);
+
 /* ------------------------------------------------------------------------------------------ */
 /* Sliding-window moment store and analytic p-values.                                           */
 /* ------------------------------------------------------------------------------------------ */
@@ -326,6 +392,15 @@ int rgl_synth_chrom_layers_host(const rgl_synth_spec* spec, uint32_t chrom, uint
  * start all on the device).  Same content as bucketing the host blocks. */
 int rgl_index_synth(const rgl_synth_spec* spec, uint32_t min_size, uint32_t growth_factor, int device,
                     rgl_index** out);
+/* File-major layout of a query batch drawn from a spec: block f * num_chroms + c holds the intervals
+ * of (file f, chromosome c), sized as rgl_synth_file_chrom_counts.  block_offsets receives
+ * num_files * num_chroms + 1 entries; block_shards (= c) and block_rows (= f) are optional. */
+int rgl_synth_batch_layout(const rgl_synth_spec* spec, uint64_t* block_offsets, uint32_t* block_shards,
+                           uint32_t* block_rows);
+/* Generates that batch into device memory: block (f, c) holds the intervals rgl_synth_block_host
+ * returns for (f, c), in generation order (unsorted), sid = sid_base + f.  Synchronises `stream`. */
+int rgl_synth_batch_device(const rgl_synth_spec* spec, int device, const uint64_t* block_offsets,
+                           rgl_interval* d_out, void* stream);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Stream helpers, timing and pinned host memory (no counterpart in the reference).              */

@@ -6,10 +6,13 @@ from ._lib import RiggleError, load, LIB_PATH  # noqa: F401
 from .api import (  # noqa: F401
     CHROM_NAMES_24,
     Context,
+    DeviceBatch,
     Index,
     LayerConfig,
     SynthSpec,
     bucket_layers,
+    synth_batch_device,
+    synth_batch_layout,
     synth_chrom_lengths,
     synth_loguniform_sizes,
     synth_zipf_sizes,

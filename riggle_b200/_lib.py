@@ -78,6 +78,35 @@ class QueryStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchDesc(C.Structure):
+    _fields_ = [("num_rows", C.c_uint32), ("num_blocks", C.c_uint32), ("block_shards", C.c_void_p),
+                ("block_rows", C.c_void_p), ("block_offsets", C.c_void_p), ("d_intervals", C.c_void_p)]
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("query", QueryOpts), ("sub_batch", C.c_uint64), ("flags", C.c_uint32)]
+
+
+RGL_BF_GRAPH = 1
+RGL_BF_TUNED = 2
+
+
+class BatchStats(C.Structure):
+    _fields_ = [("query_intervals", C.c_uint64), ("db_swept", C.c_uint64), ("rank_positions", C.c_uint64),
+                ("pair_candidates", C.c_uint64), ("ranges", C.c_uint64), ("sub_batches", C.c_uint32),
+                ("kernel_launches", C.c_uint32), ("graph_nodes", C.c_uint32), ("graph_replayed", C.c_uint32),
+                ("device_ms", C.c_float), ("chunk", C.c_uint32), ("ctas_per_sm", C.c_uint32),
+                ("pair_ratio", C.c_uint32)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class TuneTrial(C.Structure):
+    _fields_ = [("chunk", C.c_uint32), ("ctas_per_sm", C.c_uint32), ("pair_ratio", C.c_uint32),
+                ("sweep_ms", C.c_float)]
+
+
 class SynthSpec(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("num_chroms", C.c_uint32), ("chrom_len", C.POINTER(C.c_uint32)),
                 ("num_files", C.c_uint32), ("file_sizes", C.POINTER(C.c_uint64)),
@@ -117,6 +146,12 @@ _SIGS = {
                                    C.POINTER(QueryStats)]),
     "rgl_query_counts_device": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, _P, C.POINTER(QueryOpts), _P, _P,
                                           C.POINTER(QueryStats)]),
+    "rgl_query_batch_device": (C.c_int, [_P, C.POINTER(BatchDesc), C.POINTER(BatchOpts), _P, _P,
+                                         C.POINTER(BatchStats)]),
+    "rgl_query_batch_host": (C.c_int, [_P, C.POINTER(BatchDesc), _P, C.POINTER(BatchOpts), _P, _P,
+                                       C.POINTER(BatchStats)]),
+    "rgl_batch_autotune": (C.c_int, [_P, C.POINTER(BatchDesc), C.c_uint64, C.POINTER(QueryOpts),
+                                     C.POINTER(TuneTrial), C.c_uint32, C.POINTER(C.c_uint32)]),
     "rgl_context_check": (C.c_int, [_P]),
     "rgl_context_set_timing": (C.c_int, [_P, C.c_int]),
     "rgl_context_sweep_times": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),
@@ -144,6 +179,8 @@ _SIGS = {
     "rgl_synth_chrom_layers_host": (C.c_int, [C.POINTER(SynthSpec), C.c_uint32, C.c_uint32, C.c_uint32, _P,
                                               C.c_uint32, _P, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
     "rgl_index_synth": (C.c_int, [C.POINTER(SynthSpec), C.c_uint32, C.c_uint32, C.c_int, C.POINTER(_P)]),
+    "rgl_synth_batch_layout": (C.c_int, [C.POINTER(SynthSpec), _P, _P, _P]),
+    "rgl_synth_batch_device": (C.c_int, [C.POINTER(SynthSpec), C.c_int, _P, _P, _P]),
 }
 
 EXPORTED = tuple(_SIGS)

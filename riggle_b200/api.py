@@ -172,6 +172,53 @@ class Context:
         check(load().rgl_query_counts(self._h, C.byref(batch), C.byref(opts), _ptr(counts), _ptr(bp), C.byref(st)))
         return counts, bp, st.as_dict()
 
+    def query_batch_device(self, batch, d_counts, d_bp=None, graph=False, tuned=False, sub_batch=0, chunk=0,
+                           ctas_per_sm=0, pair_ratio=0, counts_only=False, stats=True):
+        """Batched form over a DeviceBatch; d_counts / d_bp are device pointers (int) to num_rows x D
+        uint32 / uint64.  Returns the stats dict (synchronising) or None (asynchronous)."""
+        flags = (_lib.RGL_BF_GRAPH if graph else 0) | (_lib.RGL_BF_TUNED if tuned else 0)
+        o = _lib.BatchOpts(self._opts(chunk, ctas_per_sm, counts_only, pair_ratio), int(sub_batch), flags)
+        st = _lib.BatchStats() if stats else None
+        check(load().rgl_query_batch_device(self._h, C.byref(batch.c), C.byref(o), C.c_void_p(d_counts),
+                                            C.c_void_p(d_bp) if d_bp else None, C.byref(st) if stats else None))
+        return st.as_dict() if stats else None
+
+    def query_batch_host(self, batch, h_intervals, with_overlap=True, tuned=False, sub_batch=0, chunk=0,
+                         ctas_per_sm=0, pair_ratio=0, out=None):
+        """Batched form with host intervals (uint32[n,3] array or an int pointer to pinned memory);
+        returns (counts uint32[R, D], overlap_bp uint64[R, D] or None, stats dict)."""
+        R, D = batch.num_rows, self.index.num_sources
+        if out is None:
+            counts = np.empty((R, D), np.uint32)
+            bp = np.empty((R, D), np.uint64) if with_overlap else None
+        else:
+            counts, bp = out
+        if isinstance(h_intervals, np.ndarray):
+            h = np.ascontiguousarray(h_intervals, np.uint32)
+            hp = _ptr(h)
+        else:
+            hp = C.c_void_p(int(h_intervals))
+        flags = _lib.RGL_BF_TUNED if tuned else 0
+        o = _lib.BatchOpts(self._opts(chunk, ctas_per_sm, not with_overlap, pair_ratio), int(sub_batch), flags)
+        st = _lib.BatchStats()
+        check(load().rgl_query_batch_host(self._h, C.byref(batch.c), hp, C.byref(o), _ptr(counts), _ptr(bp),
+                                          C.byref(st)))
+        return counts, bp, st.as_dict()
+
+    def autotune(self, batch, sub_batch=0, max_trials=64):
+        """Runs the launch-shape autotuner on the batch; returns (best opts dict, list of trials)."""
+        best = _lib.QueryOpts()
+        trials = (_lib.TuneTrial * max_trials)()
+        nt = C.c_uint32()
+        check(load().rgl_batch_autotune(self._h, C.byref(batch.c), int(sub_batch), C.byref(best), trials, max_trials,
+                                        C.byref(nt)))
+        out = [dict(chunk=t.chunk, ctas_per_sm=t.ctas_per_sm, pair_ratio=t.pair_ratio, sweep_ms=t.sweep_ms)
+               for t in trials[:min(nt.value, max_trials)]]
+        return dict(chunk=best.chunk, ctas_per_sm=best.ctas_per_sm, pair_ratio=best.pair_ratio), out
+
+    def check(self):
+        check(load().rgl_context_check(self._h))
+
     def close(self):
         if self._h:
             load().rgl_context_destroy(self._h)
@@ -182,6 +229,41 @@ class Context:
             self.close()
         except Exception:
             pass
+
+
+class DeviceBatch:
+    """A file-major query batch whose intervals are in device memory (rgl_batch): block b holds
+    intervals [offsets[b], offsets[b+1]) on shard shards[b]; rows[b] (optional) is their file."""
+
+    def __init__(self, num_rows, shards, offsets, d_intervals, rows=None):
+        self.num_rows = int(num_rows)
+        self.shards = np.ascontiguousarray(shards, np.uint32)
+        self.offsets = np.ascontiguousarray(offsets, np.uint64)
+        self.rows = None if rows is None else np.ascontiguousarray(rows, np.uint32)
+        self.d_intervals = int(d_intervals)
+        self.c = _lib.BatchDesc(self.num_rows, len(self.shards), _ptr(self.shards), _ptr(self.rows),
+                                _ptr(self.offsets), C.c_void_p(self.d_intervals))
+
+    @property
+    def num_intervals(self):
+        return int(self.offsets[-1]) if len(self.offsets) else 0
+
+
+def synth_batch_layout(spec):
+    """(offsets uint64[F*C+1], shards uint32[F*C], rows uint32[F*C]) of a file-major batch."""
+    nb = spec.num_files * spec.num_chroms
+    off = np.empty(nb + 1, np.uint64)
+    sh = np.empty(nb, np.uint32)
+    rw = np.empty(nb, np.uint32)
+    check(load().rgl_synth_batch_layout(C.byref(spec.c), _ptr(off), _ptr(sh), _ptr(rw)))
+    return off, sh, rw
+
+
+def synth_batch_device(spec, offsets, d_out, device=0, stream=None):
+    """Generates the batch of `spec` into device memory at d_out (int pointer)."""
+    offsets = np.ascontiguousarray(offsets, np.uint64)
+    check(load().rgl_synth_batch_device(C.byref(spec.c), device, _ptr(offsets), C.c_void_p(d_out),
+                                        C.c_void_p(stream) if stream else None))
 
 
 class SynthSpec:

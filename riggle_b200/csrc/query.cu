@@ -97,8 +97,8 @@ __device__ __forceinline__ uint32_t pp_layer(const uint2* __restrict__ pos, uint
 
 // ---- 1. keys ------------------------------------------------------------------------------------
 __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, const uint64_t* __restrict__ blk_off,
-                              const uint32_t* __restrict__ blk_shard, uint32_t nblk, uint32_t rows,
-                              uint64_t* __restrict__ key, uint32_t* __restrict__ val, uint64_t* __restrict__ ekey,
+                              const uint32_t* __restrict__ blk_shard, const uint32_t* __restrict__ blk_row,
+                              uint32_t nblk, uint32_t rows, uint32_t row_base, uint64_t* __restrict__ key, uint32_t* __restrict__ val, uint64_t* __restrict__ ekey,
                               uint32_t* __restrict__ err) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -108,10 +108,10 @@ __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, c
         if (blk_off[m] <= i) lo = m; else hi = m;
     }
     const uint32_t* w = reinterpret_cast<const uint32_t*>(iv) + 3ull * i;
-    uint32_t s = w[0], e = w[1], q = w[2];
+    uint32_t s = w[0], e = w[1], q = w[2] - row_base;  // rows below row_base wrap to >= rows
     uint32_t bad = 0;
     if (s >= e) bad |= ERR_BAD_INTERVAL;
-    if (q >= rows) { bad |= ERR_BAD_ROW; q = 0; }
+    if (q >= rows || (blk_row && w[2] != blk_row[lo])) { bad |= ERR_BAD_ROW; q = 0; }
     if (bad) atomicOr(err, bad);
     uint64_t seg = (uint64_t)blk_shard[lo] * rows + q;
     key[i] = (seg << 32) | s;
@@ -149,10 +149,11 @@ __global__ void k_seg_begin(uint32_t n, const uint32_t* __restrict__ segflag, co
     if (i == n - 1) seg_begin[segnum[i]] = n;
 }
 
-// Bin width per segment: about four bins per query, at least 64 bp; tab_len = nbins + 1.
+// Bin width per segment: about four bins per query, at least 64 bp; tab_len = nbins + 1 for the
+// segments that have a rank-difference range, 0 for the rest.
 __global__ void k_seg_tabsize(uint32_t n, const uint32_t* __restrict__ segnum, const uint32_t* __restrict__ seg_begin,
-                              const uint32_t* __restrict__ ends_s, SegTab* __restrict__ tabs,
-                              uint32_t* __restrict__ tab_len) {
+                              const uint32_t* __restrict__ need, const uint32_t* __restrict__ ends_s,
+                              SegTab* __restrict__ tabs, uint32_t* __restrict__ tab_len) {
     uint32_t sgi = blockIdx.x * blockDim.x + threadIdx.x;
     if (sgi > n) return;
     const uint32_t nseg = segnum[n - 1];
@@ -161,6 +162,11 @@ __global__ void k_seg_tabsize(uint32_t n, const uint32_t* __restrict__ segnum, c
         return;
     }
     const uint32_t beg = seg_begin[sgi], end = seg_begin[sgi + 1];
+    if (!need[sgi]) {  // no range of this segment is swept by rank differences
+        tabs[sgi] = SegTab{beg, end, 6, 0, 0, 0};
+        tab_len[sgi] = 0;
+        return;
+    }
     const uint64_t extent = (uint64_t)ends_s[end - 1] + 1;  // covers every start and end of the segment
     const uint64_t want = extent / (4ull * (end - beg));
     uint32_t shift = want > 1 ? 63u - __clzll(want) : 0u;
@@ -286,7 +292,7 @@ __global__ void k_range_emit(uint32_t n, uint32_t nslots, uint32_t rows, const u
 __global__ void k_range_method(uint64_t cap, uint32_t n, const uint32_t* __restrict__ ridx_total_ptr,
                                const RangeDesc* __restrict__ ranges, const uint64_t* __restrict__ pc,
                                uint32_t pair_ratio, uint8_t* __restrict__ method, uint64_t* __restrict__ rlen,
-                               uint64_t* __restrict__ ulen) {
+                               uint64_t* __restrict__ ulen, uint32_t* __restrict__ seg_need) {
     const uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (r > cap) return;
     const uint32_t R = *ridx_total_ptr;
@@ -301,6 +307,7 @@ __global__ void k_range_method(uint64_t cap, uint32_t n, const uint32_t* __restr
     const uint64_t cand = pc[t1] - pc[t0];
     const uint8_t m = (cand <= (uint64_t)pair_ratio * len) ? M_PAIR : M_RANK;
     method[r] = m;
+    if (m == M_RANK && len) seg_need[rd.seg] = 1u;
     rlen[r] = m == M_RANK ? len : 0;
     ulen[r] = len;
 }
@@ -685,8 +692,25 @@ struct rgl_context {
     DevBuf starts, ends, seg, segflag, segnum, seg_begin, ps_in, pe_in, ps, pe;
     DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp, item_r0;
     DevBuf segtab, tab_len, tab_off, tab_s, tab_e;
-    DevBuf cl, pc, method, ulen, plen, ppos, psegs, item_t0;
+    DevBuf cl, pc, method, ulen, plen, ppos, psegs, item_t0, seg_need;
+    DevBuf bt_off, bt_shard, acc;  // batched form: sub-batch block tables (offsets; shards then rows), stats
     uint32_t* h_small = nullptr;  // pinned mirror of `small`
+    unsigned long long* h_acc = nullptr;  // pinned mirror of `acc`
+    uint64_t ws_sig = 0;          // changes whenever a workspace buffer is reallocated
+    // the CUDA graph of the last batch run with RGL_BF_GRAPH, replayed while the batch is unchanged
+    struct GraphCache {
+        std::vector<uint64_t> key;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        DevBuf t_off, t_shard;  // the graph's own copies of the block tables
+        uint32_t nodes = 0, launches = 0, subs = 0;
+    } gc;
+    // host-input batches: two staging buffers filled on a copy stream while the other is swept
+    DevBuf stage[2];
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_used[2] = {nullptr, nullptr};
+    bool has_tuned = false;       // rgl_batch_autotune result
+    rgl_query_opts tuned{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     uint64_t res_n = 0;
     uint32_t res_rows = 0;
@@ -724,6 +748,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     RGL_TRY(c->segflag.ensure(n * 4 + 4));
     RGL_TRY(c->segnum.ensure(n * 4 + 4));
     RGL_TRY(c->seg_begin.ensure(n * 4 + 4));
+    RGL_TRY(c->seg_need.ensure(n * 4 + 4));
     RGL_TRY(c->ps_in.ensure(n * 8 + 16));
     RGL_TRY(c->pe_in.ensure(n * 8 + 16));
     RGL_TRY(c->ps.ensure(n * 8 + 16));
@@ -751,6 +776,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     RGL_TRY(c->tab_off.ensure((n + 2) * 4));
     RGL_TRY(c->tab_s.ensure((10 * n + 16) * 4));
     RGL_TRY(c->tab_e.ensure((10 * n + 16) * 4));
+    RGL_TRY(c->acc.ensure(64));
     // CUB temporary storage: the maximum over every primitive used, at these sizes.
     size_t need = 0, b = 0;
     int nn = (int)std::max<uint64_t>(n, 1);
@@ -782,6 +808,15 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     }
     c->res_n = std::max(c->res_n, n);
     c->res_rows = std::max(c->res_rows, rows);
+    uint64_t sig = 1469598103934665603ull;
+    for (DevBuf* b : {&c->iv, &c->key_a, &c->key_b, &c->val_a, &c->val_b, &c->ekey_a, &c->ekey_b, &c->starts,
+                      &c->ends, &c->seg, &c->segflag, &c->segnum, &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps,
+                      &c->pe, &c->lo, &c->hi, &c->maxhi, &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos,
+                      &c->cub_tmp, &c->small, &c->item_r0, &c->item_t0, &c->segtab, &c->tab_len, &c->tab_off,
+                      &c->tab_s, &c->tab_e, &c->cl, &c->pc, &c->method, &c->ulen, &c->plen, &c->ppos, &c->psegs,
+                      &c->seg_need, &c->acc})
+        sig = (sig ^ (uint64_t)(uintptr_t)b->p ^ ((uint64_t)b->cap << 17)) * 1099511628211ull;
+    c->ws_sig = sig;
     return RGL_OK;
 }
 
@@ -854,27 +889,64 @@ int finish(rgl_context* c, const Launch& L, rgl_query_stats* stats) {
     return RGL_OK;
 }
 
-// Runs steps 1-5 for n intervals already in c->iv with block table in c->blk_off/c->blk_shard.
-int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, const rgl_query_opts* opts,
-                 uint32_t* d_counts, unsigned long long* d_bp, rgl_query_stats* stats) {
+// Input of one pipeline run: n intervals at `iv` (device), block b = [blk_off[b], blk_off[b+1]) on
+// shard blk_shard[b] (both tables on the device), rows [row_base, row_base + rows) of the output.
+struct PipeIn {
+    const rgl_interval* iv;
+    uint64_t n;
+    uint32_t rows, row_base, nblk;
+    const uint64_t* blk_off;
+    const uint32_t* blk_shard;
+    const uint32_t* blk_row;  // optional: the row every interval of the block must carry
+};
+
+// What a run does besides the sweep: the single-call entry points zero their rows, reset the error
+// word and record stats events; the sub-batches of a batched call leave all of that to the caller
+// and add their stats into a device accumulator.
+struct PipeMode {
+    bool zero_out = true;
+    bool reset_err = true;
+    bool events = true;  // stats events and sweep timing (off inside a graph capture)
+    unsigned long long* acc = nullptr;
+};
+
+__global__ void k_acc_stats(unsigned long long* acc, const uint32_t* ranges, const unsigned long long* uni,
+                            const unsigned long long* rank_pos, const unsigned long long* pair_cand, uint32_t n) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        acc[0] += *ranges;
+        acc[1] += *uni;
+        acc[2] += *rank_pos;
+        acc[3] += *pair_cand;
+        acc[4] += n;
+    }
+}
+
+// Runs steps 1-5 of the pipeline on the context stream, with no host synchronisation.
+int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, uint32_t* d_counts,
+                 unsigned long long* d_bp, rgl_query_stats* stats, const PipeMode& mode = PipeMode()) {
     rgl_index* idx = c->idx;
     cudaStream_t st = c->stream;
     const uint32_t D = idx->num_sources;
     const uint32_t ns = idx->num_slots;
-    const uint32_t n = (uint32_t)n64;
+    const uint32_t n = (uint32_t)in.n;
+    const uint32_t rows = in.rows;
     Launch L = pick_launch(opts);
     const bool with_bp = d_bp != nullptr && !(opts && (opts->flags & RGL_QF_NO_OVERLAP));
+    const bool ev = mode.events && stats;
 
     uint32_t* d_small = c->small.as<uint32_t>();  // [0] error bits, [1] queue, [2..] scratch
-    RGL_CUDA(cudaMemsetAsync(d_small, 0, 64, st));
-    if (d_counts) RGL_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)rows * D * 4, st));
-    if (d_bp) RGL_CUDA(cudaMemsetAsync(d_bp, 0, (size_t)rows * D * 8, st));
+    if (mode.reset_err) RGL_CUDA(cudaMemsetAsync(d_small, 0, 64, st));
+    else RGL_CUDA(cudaMemsetAsync(d_small + 1, 0, 60, st));
+    if (mode.zero_out) {
+        if (d_counts) RGL_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)rows * D * 4, st));
+        if (d_bp) RGL_CUDA(cudaMemsetAsync(d_bp, 0, (size_t)rows * D * 8, st));
+    }
     if (n == 0 || ns == 0) {
         c->last_n = 0;
         c->last_tot = 0;
         c->last_launches = 0;
         if (stats) std::memset(stats, 0, sizeof(*stats));
-        RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
+        if (mode.reset_err) RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
         return RGL_OK;
     }
     // key width: segment = shard * rows + row
@@ -883,11 +955,12 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
     while (segbits < 32 && (1ull << segbits) < nseg) segbits++;
     if (nseg >= (1ull << 32)) return fail(RGL_ERR_INVALID_ARGUMENT, "num_shards * num_rows must be < 2^32");
 
-    if (stats) RGL_CUDA(cudaEventRecord(c->ev[0], st));
+    if (ev) RGL_CUDA(cudaEventRecord(c->ev[0], st));
     uint32_t launches = 0;
-    k_expand_keys<<<grid_for(n, 256), 256, 0, st>>>(n, c->iv.as<rgl_interval>(), c->blk_off.as<uint64_t>(),
-                                                    c->blk_shard.as<uint32_t>(), nblk, rows, c->key_a.as<uint64_t>(),
-                                                    c->val_a.as<uint32_t>(), c->ekey_a.as<uint64_t>(), d_small);
+    k_expand_keys<<<grid_for(n, 256), 256, 0, st>>>(n, in.iv, in.blk_off, in.blk_shard, in.blk_row, in.nblk, rows,
+                                                    in.row_base,
+                                                    c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
+                                                    c->ekey_a.as<uint64_t>(), d_small);
     launches++;
     size_t tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tb, c->key_a.as<uint64_t>(), c->key_b.as<uint64_t>(),
@@ -910,19 +983,10 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
     tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->pe_in.as<uint64_t>(), c->pe.as<uint64_t>(),
                                            (int)n + 1, st));
-    // rank tables of every query segment
     k_seg_begin<<<grid_for(n, 256), 256, 0, st>>>(n, c->segflag.as<uint32_t>(), c->segnum.as<uint32_t>(),
                                                   c->seg_begin.as<uint32_t>());
-    k_seg_tabsize<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->seg_begin.as<uint32_t>(),
-                                                        c->ends.as<uint32_t>(), c->segtab.as<SegTab>(),
-                                                        c->tab_len.as<uint32_t>());
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->tab_len.as<uint32_t>(), c->tab_off.as<uint32_t>(),
-                                           (int)n + 1, st));
-    k_seg_tabfill<<<(unsigned)std::min<uint64_t>((10 * n + 255) / 256, (uint64_t)c->num_sms * 16), 256, 0, st>>>(
-        n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(), c->tab_off.as<uint32_t>(), c->starts.as<uint32_t>(),
-        c->ends.as<uint32_t>(), c->tab_s.as<uint32_t>(), c->tab_e.as<uint32_t>());
-    launches += 3;
+    launches++;
+    RGL_CUDA(cudaMemsetAsync(c->seg_need.p, 0, (size_t)(n + 1) * 4, st));
     const uint64_t tot = (uint64_t)n * ns;
     k_lohi<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, rows, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
                                                 c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, idx->d_pos,
@@ -957,7 +1021,19 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
     k_range_method<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, n, c->ridx.as<uint32_t>() + tot,
                                                            c->ranges.as<RangeDesc>(), c->pc.as<uint64_t>(),
                                                            L.pair_ratio, c->method.as<uint8_t>(),
-                                                           c->rlen.as<uint64_t>(), c->ulen.as<uint64_t>());
+                                                           c->rlen.as<uint64_t>(), c->ulen.as<uint64_t>(),
+                                                           c->seg_need.as<uint32_t>());
+    // rank tables of the query segments that have a rank-difference range
+    k_seg_tabsize<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->seg_begin.as<uint32_t>(),
+                                                        c->seg_need.as<uint32_t>(), c->ends.as<uint32_t>(), c->segtab.as<SegTab>(),
+                                                        c->tab_len.as<uint32_t>());
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->tab_len.as<uint32_t>(), c->tab_off.as<uint32_t>(),
+                                           (int)n + 1, st));
+    k_seg_tabfill<<<(unsigned)std::min<uint64_t>((10 * n + 255) / 256, (uint64_t)c->num_sms * 16), 256, 0, st>>>(
+        n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(), c->tab_off.as<uint32_t>(), c->starts.as<uint32_t>(),
+        c->ends.as<uint32_t>(), c->tab_s.as<uint32_t>(), c->tab_e.as<uint32_t>());
+    launches += 2;
     k_pair_len<<<grid_for(tot + 1, 256), 256, 0, st>>>(n, ns, rows, c->seg.as<uint32_t>(), idx->d_slot,
                                                        idx->d_layers, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
                                                        c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
@@ -1008,14 +1084,8 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
     P.smem_tally = (rows == 1 && smem <= 160 * 1024) ? 1 : 0;
     if (!P.smem_tally) smem = 0;
     unsigned grid = (unsigned)(c->num_sms * L.ctas_per_sm);
-    if (stats) RGL_CUDA(cudaEventRecord(c->ev[1], st));
-    if (c->timing) RGL_TRY(timing_record(c, true));
-    if (smem > 48 * 1024) {
-        RGL_CUDA(cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        RGL_CUDA(cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        RGL_CUDA(cudaFuncSetAttribute(k_pairs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        RGL_CUDA(cudaFuncSetAttribute(k_pairs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    }
+    if (ev) RGL_CUDA(cudaEventRecord(c->ev[1], st));
+    if (c->timing && mode.events) RGL_TRY(timing_record(c, true));
     if (with_bp) k_sweep<true><<<grid, 256, smem, st>>>(P);
     else k_sweep<false><<<grid, 256, smem, st>>>(P);
     P.queue = d_small + 2;  // the pair sweep pulls from its own counter
@@ -1024,18 +1094,25 @@ int run_pipeline(rgl_context* c, uint64_t n64, uint32_t rows, uint32_t nblk, con
     launches++;
     launches++;
     RGL_CUDA(cudaGetLastError());
-    if (c->timing) RGL_TRY(timing_record(c, false));
+    if (c->timing && mode.events) RGL_TRY(timing_record(c, false));
+    if (mode.acc) {
+        k_acc_stats<<<1, 32, 0, st>>>(mode.acc, c->ridx.as<uint32_t>() + tot,
+                                      reinterpret_cast<unsigned long long*>(d_small + 4),
+                                      c->rpos.as<unsigned long long>() + tot, c->ppos.as<unsigned long long>() + tot,
+                                      n);
+        launches++;
+    }
     c->last_tot = tot;
     c->last_launches = launches;
     c->last_n = n;
-    if (stats) {
+    if (ev) {
         RGL_CUDA(cudaEventRecord(c->ev[2], st));
         RGL_CUDA(cudaMemcpyAsync(c->h_small + 2, c->ridx.as<uint32_t>() + tot, 4, cudaMemcpyDeviceToHost, st));
         RGL_CUDA(cudaMemcpyAsync(c->h_small + 4, d_small + 4, 8, cudaMemcpyDeviceToHost, st));
         RGL_CUDA(cudaMemcpyAsync(c->h_small + 6, c->rpos.as<uint64_t>() + tot, 8, cudaMemcpyDeviceToHost, st));
         RGL_CUDA(cudaMemcpyAsync(c->h_small + 8, c->ppos.as<uint64_t>() + tot, 8, cudaMemcpyDeviceToHost, st));
     }
-    RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
+    if (mode.reset_err) RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
     return RGL_OK;
 }
 
@@ -1062,6 +1139,149 @@ int resolve_blocks(rgl_context* c, const rgl_query_batch* b, std::vector<uint32_
     return RGL_OK;
 }
 
+// ---- batched form ------------------------------------------------------------------------------
+// A batch is cut into sub-batches of at most `sub` intervals (cutting blocks where needed: counts and
+// base pairs are sums over pairs, so a row split across sub-batches adds up to the same cells).
+struct SubBatch {
+    uint64_t begin, n;        // element range in d_intervals
+    uint32_t row_lo, rows;    // output rows the sub-batch may touch
+    uint32_t tab_at, nblk;    // its block table: entries [tab_at, tab_at + nblk] of the offsets, [tab_at, +nblk) of shards
+};
+
+struct BatchPlan {
+    std::vector<SubBatch> subs;
+    std::vector<uint64_t> off;   // per sub-batch: nblk + 1 offsets relative to its begin
+    std::vector<uint32_t> shard; // per sub-batch: nblk shard ids (padded to the offsets' layout)
+    std::vector<uint32_t> row;   // per sub-batch: nblk block rows (same layout; unused without block_rows)
+    uint64_t max_n = 0;
+    uint32_t max_rows = 0, max_blk = 0;
+    std::vector<uint32_t> shard_rows() const {  // the device table: shards, then rows
+        std::vector<uint32_t> v(shard);
+        v.insert(v.end(), row.begin(), row.end());
+        return v;
+    }
+};
+
+int plan_batch(rgl_context* c, const rgl_batch* b, uint64_t sub, BatchPlan* P) {
+    const uint64_t* bo = b->block_offsets;
+    for (uint32_t i = 0; i < b->num_blocks; i++) {
+        if (bo[i + 1] < bo[i]) return fail(RGL_ERR_INVALID_ARGUMENT, "block offsets must be non-decreasing");
+        if (b->block_shards[i] >= c->idx->num_shards) return fail(RGL_ERR_INVALID_ARGUMENT, "shard id out of range");
+        if (b->block_rows && b->block_rows[i] >= b->num_rows)
+            return fail(RGL_ERR_INVALID_ARGUMENT, "block row >= num_rows");
+    }
+    SubBatch cur{};
+    uint32_t rlo = 0xFFFFFFFFu, rhi = 0;
+    bool open = false;
+    auto close = [&]() {
+        if (!open) return;
+        P->off.push_back(cur.n);
+        P->shard.push_back(0);  // keeps the three tables indexed alike
+        P->row.push_back(0);
+        cur.row_lo = b->block_rows ? rlo : 0;
+        cur.rows = b->block_rows ? rhi - rlo + 1 : b->num_rows;
+        P->max_n = std::max(P->max_n, cur.n);
+        P->max_rows = std::max(P->max_rows, cur.rows);
+        P->max_blk = std::max(P->max_blk, cur.nblk);
+        P->subs.push_back(cur);
+        open = false;
+    };
+    for (uint32_t i = 0; i < b->num_blocks; i++) {
+        uint64_t at = bo[i], end = bo[i + 1];
+        while (at < end) {
+            if (!open) {
+                cur = SubBatch{at, 0, 0, 0, (uint32_t)P->off.size(), 0};
+                rlo = 0xFFFFFFFFu;
+                rhi = 0;
+                open = true;
+            }
+            const uint64_t take = std::min(end - at, sub - cur.n);
+            P->off.push_back(cur.n);
+            P->shard.push_back(b->block_shards[i]);
+            P->row.push_back(b->block_rows ? b->block_rows[i] : 0);
+            cur.nblk++;
+            cur.n += take;
+            if (b->block_rows) {
+                rlo = std::min(rlo, b->block_rows[i]);
+                rhi = std::max(rhi, b->block_rows[i]);
+            }
+            at += take;
+            if (cur.n == sub) close();
+        }
+    }
+    close();
+    return RGL_OK;
+}
+
+Launch batch_launch(rgl_context* c, const rgl_batch_opts* o, rgl_query_opts* q) {
+    *q = o ? o->query : rgl_query_opts{};
+    if (o && (o->flags & RGL_BF_TUNED) && c->has_tuned) {
+        if (!q->chunk) q->chunk = c->tuned.chunk;
+        if (!q->ctas_per_sm) q->ctas_per_sm = c->tuned.ctas_per_sm;
+        if (!q->pair_ratio) q->pair_ratio = c->tuned.pair_ratio;
+    }
+    return pick_launch(q);
+}
+
+// Enqueues a whole batch on the context stream: zero the outputs, one pipeline run per sub-batch,
+// then the error word and the stats accumulator to pinned host memory.
+int enqueue_batch(rgl_context* c, const rgl_batch* b, const BatchPlan& P, const uint64_t* d_off,
+                  const uint32_t* d_sr, const rgl_query_opts* q, uint32_t* d_counts, unsigned long long* d_bp,
+                  bool events, uint32_t* launches) {
+    cudaStream_t st = c->stream;
+    const uint32_t D = c->idx->num_sources;
+    uint32_t* d_small = c->small.as<uint32_t>();
+    RGL_CUDA(cudaMemsetAsync(d_small, 0, 64, st));
+    RGL_CUDA(cudaMemsetAsync(c->acc.p, 0, 64, st));
+    RGL_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)b->num_rows * D * 4, st));
+    if (d_bp) RGL_CUDA(cudaMemsetAsync(d_bp, 0, (size_t)b->num_rows * D * 8, st));
+    PipeMode m;
+    m.zero_out = false;
+    m.reset_err = false;
+    m.events = events;
+    m.acc = c->acc.as<unsigned long long>();
+    uint32_t nl = 0;
+    for (const SubBatch& sb : P.subs) {
+        PipeIn in{b->d_intervals + sb.begin, sb.n, sb.rows, sb.row_lo, sb.nblk, d_off + sb.tab_at,
+                  d_sr + sb.tab_at, b->block_rows ? d_sr + P.shard.size() + sb.tab_at : nullptr};
+        RGL_TRY(run_pipeline(c, in, q, d_counts + (uint64_t)sb.row_lo * D,
+                             d_bp ? d_bp + (uint64_t)sb.row_lo * D : nullptr, nullptr, m));
+        nl += c->last_launches;
+    }
+    RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
+    RGL_CUDA(cudaMemcpyAsync(c->h_acc, c->acc.p, 64, cudaMemcpyDeviceToHost, st));
+    *launches = nl;
+    return RGL_OK;
+}
+
+void graph_drop(rgl_context* c) {
+    if (c->gc.exec) cudaGraphExecDestroy(c->gc.exec);
+    if (c->gc.graph) cudaGraphDestroy(c->gc.graph);
+    c->gc.exec = nullptr;
+    c->gc.graph = nullptr;
+    c->gc.key.clear();
+}
+
+std::vector<uint64_t> batch_key(rgl_context* c, const rgl_batch* b, const rgl_batch_opts* o, const Launch& L,
+                                const void* d_counts, const void* d_bp) {
+    std::vector<uint64_t> k;
+    k.reserve(16 + 3ull * b->num_blocks);
+    k.push_back(b->num_rows);
+    k.push_back(b->num_blocks);
+    k.push_back((uint64_t)(uintptr_t)b->d_intervals);
+    k.push_back((uint64_t)(uintptr_t)d_counts);
+    k.push_back((uint64_t)(uintptr_t)d_bp);
+    k.push_back(((uint64_t)L.chunk << 32) | L.ctas_per_sm);
+    k.push_back(((uint64_t)L.pair_ratio << 32) | (o ? o->query.flags : 0));
+    k.push_back(o ? o->sub_batch : 0);
+    k.push_back(c->ws_sig);
+    k.push_back(b->block_rows ? 1 : 0);
+    for (uint32_t i = 0; i <= b->num_blocks; i++) k.push_back(b->block_offsets[i]);
+    for (uint32_t i = 0; i < b->num_blocks; i++)
+        k.push_back(((uint64_t)b->block_shards[i] << 32) | (b->block_rows ? b->block_rows[i] : 0));
+    return k;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1083,9 +1303,20 @@ int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
             c->own_stream = true;
     }
     if (s == RGL_OK) cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, index->device);
+    // shared-memory tallies of up to 160 KB (one row, D x 12 B); set once here so that no launch
+    // path changes function attributes (graph capture included)
+    if (s == RGL_OK) {
+        const int mx = 160 * 1024;
+        if (cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+            cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+            cudaFuncSetAttribute(k_pairs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+            cudaFuncSetAttribute(k_pairs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess)
+            s = fail(RGL_ERR_DEVICE, "cudaFuncSetAttribute");
+    }
     for (int i = 0; i < 4 && s == RGL_OK; i++)
         if (cudaEventCreate(&c->ev[i]) != cudaSuccess) s = fail(RGL_ERR_DEVICE, "cudaEventCreate");
     if (s == RGL_OK && cudaMallocHost(&c->h_small, 256) != cudaSuccess) s = fail(RGL_ERR_OOM, "pinned");
+    if (s == RGL_OK && cudaMallocHost(&c->h_acc, 64) != cudaSuccess) s = fail(RGL_ERR_OOM, "pinned");
     if (s == RGL_OK) s = c->small.ensure(256);
     if (s != RGL_OK) {
         rgl_context_destroy(c);
@@ -1106,12 +1337,23 @@ int rgl_context_destroy(rgl_context* c) {
                       &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos, &c->cub_tmp, &c->small,
                       &c->out_counts, &c->out_bp, &c->item_r0,
                       &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e,
-                      &c->cl, &c->pc, &c->method, &c->ulen, &c->plen, &c->ppos, &c->psegs, &c->item_t0};
+                      &c->cl, &c->pc, &c->method, &c->ulen, &c->plen, &c->ppos, &c->psegs, &c->item_t0,
+                      &c->seg_need, &c->bt_off, &c->bt_shard, &c->acc, &c->gc.t_off, &c->gc.t_shard};
+    if (c->gc.exec) cudaGraphExecDestroy(c->gc.exec);
+    if (c->gc.graph) cudaGraphDestroy(c->gc.graph);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
     for (DevBuf* b : bufs) b->release();
+    for (int i = 0; i < 2; i++) {
+        c->stage[i].release();
+        if (c->ev_copied[i]) cudaEventDestroy(c->ev_copied[i]);
+        if (c->ev_used[i]) cudaEventDestroy(c->ev_used[i]);
+    }
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     for (auto& e : c->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : c->tev) cudaEventDestroy(e);
     if (c->h_small) cudaFreeHost(c->h_small);
+    if (c->h_acc) cudaFreeHost(c->h_acc);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     index_release(c->idx);
     delete c;
@@ -1155,8 +1397,9 @@ int rgl_query_counts_device(rgl_context* c, uint32_t num_rows, uint32_t num_shar
         RGL_CUDA(cudaMemcpyAsync(c->iv.p, d_intervals + shard_offsets[0], n * sizeof(rgl_interval),
                                  cudaMemcpyDeviceToDevice, c->stream));
     }
-    RGL_TRY(run_pipeline(c, n, num_rows, num_shards, opts, d_counts,
-                         reinterpret_cast<unsigned long long*>(d_overlap_bp), stats));
+    PipeIn in{c->iv.as<rgl_interval>(), n, num_rows, 0, num_shards, c->blk_off.as<uint64_t>(),
+              c->blk_shard.as<uint32_t>(), nullptr};
+    RGL_TRY(run_pipeline(c, in, opts, d_counts, reinterpret_cast<unsigned long long*>(d_overlap_bp), stats));
     if (!stats) return RGL_OK;
     RGL_CUDA(cudaStreamSynchronize(c->stream));
     return finish(c, pick_launch(opts), stats);
@@ -1189,7 +1432,9 @@ int rgl_query_counts(rgl_context* c, const rgl_query_batch* b, const rgl_query_o
         RGL_CUDA(cudaMemcpyAsync(c->blk_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st));
         RGL_CUDA(cudaMemcpyAsync(c->blk_shard.p, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st));
     }
-    RGL_TRY(run_pipeline(c, n, rows, (uint32_t)blocks.size(), opts, c->out_counts.as<uint32_t>(),
+    PipeIn in{c->iv.as<rgl_interval>(), n, rows, 0, (uint32_t)blocks.size(), c->blk_off.as<uint64_t>(),
+              c->blk_shard.as<uint32_t>(), nullptr};
+    RGL_TRY(run_pipeline(c, in, opts, c->out_counts.as<uint32_t>(),
                          overlap_bp ? c->out_bp.as<unsigned long long>() : nullptr, stats));
     if (cells) {
         RGL_CUDA(cudaMemcpyAsync(counts, c->out_counts.p, cells * 4, cudaMemcpyDeviceToHost, st));
@@ -1197,6 +1442,287 @@ int rgl_query_counts(rgl_context* c, const rgl_query_batch* b, const rgl_query_o
     }
     RGL_CUDA(cudaStreamSynchronize(st));
     return finish(c, pick_launch(opts), stats);
+}
+
+int rgl_query_batch_device(rgl_context* c, const rgl_batch* b, const rgl_batch_opts* o, uint32_t* d_counts,
+                           uint64_t* d_overlap_bp, rgl_batch_stats* stats) {
+    clear_error();
+    if (!c || !b || !d_counts) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    if (b->num_blocks && (!b->block_offsets || !b->block_shards || !b->d_intervals))
+        return fail(RGL_ERR_INVALID_ARGUMENT, "incomplete batch");
+    RGL_CUDA(cudaSetDevice(c->idx->device));
+    const uint64_t sub = (o && o->sub_batch) ? std::min<uint64_t>(o->sub_batch, (1ull << 31) - 1) : (1ull << 24);
+    rgl_query_opts q;
+    const Launch L = batch_launch(c, o, &q);
+    const bool graph = o && (o->flags & RGL_BF_GRAPH);
+    unsigned long long* d_bp = (d_overlap_bp && !(q.flags & RGL_QF_NO_OVERLAP))
+                                   ? reinterpret_cast<unsigned long long*>(d_overlap_bp) : nullptr;
+    cudaStream_t st = c->stream;
+    BatchPlan P;
+    std::vector<uint64_t> key;
+    bool replay = false;
+    if (graph) {
+        key = batch_key(c, b, o, L, d_counts, d_bp);
+        replay = c->gc.exec && key == c->gc.key;
+    }
+    if (!replay) {
+        RGL_TRY(plan_batch(c, b, sub, &P));
+        RGL_TRY(ensure_workspace(c, P.max_n, 0, P.max_blk));
+    }
+    if (stats) RGL_CUDA(cudaEventRecord(c->ev[0], st));
+    uint32_t launches = 0, subs = 0, nodes = 0;
+    if (replay) {
+        RGL_CUDA(cudaGraphLaunch(c->gc.exec, st));
+        launches = c->gc.launches;
+        subs = c->gc.subs;
+        nodes = c->gc.nodes;
+    } else if (graph) {
+        RGL_CUDA(cudaStreamSynchronize(st));  // the previous graph may still read its tables
+        graph_drop(c);
+        RGL_TRY(c->gc.t_off.ensure(P.off.size() * 8 + 8));
+        const std::vector<uint32_t> sr = P.shard_rows();
+        RGL_TRY(c->gc.t_shard.ensure(sr.size() * 4 + 4));
+        RGL_CUDA(cudaMemcpy(c->gc.t_off.p, P.off.data(), P.off.size() * 8, cudaMemcpyHostToDevice));
+        RGL_CUDA(cudaMemcpy(c->gc.t_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice));
+        // the key is taken after the workspace is sized, so that a later reallocation invalidates it
+        key = batch_key(c, b, o, L, d_counts, d_bp);
+        RGL_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        int s = enqueue_batch(c, b, P, c->gc.t_off.as<uint64_t>(), c->gc.t_shard.as<uint32_t>(), &q, d_counts, d_bp,
+                              false, &launches);
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamEndCapture(st, &g);
+        if (s != RGL_OK) {
+            if (g) cudaGraphDestroy(g);
+            return s;
+        }
+        if (e != cudaSuccess) return fail(RGL_ERR_DEVICE, std::string("stream capture: ") + cudaGetErrorString(e));
+        cudaGraphExec_t x = nullptr;
+        e = cudaGraphInstantiate(&x, g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(g);
+            return fail(RGL_ERR_DEVICE, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+        size_t nn = 0;
+        cudaGraphGetNodes(g, nullptr, &nn);
+        c->gc.graph = g;
+        c->gc.exec = x;
+        c->gc.key = std::move(key);
+        c->gc.nodes = nodes = (uint32_t)nn;
+        c->gc.launches = launches;
+        c->gc.subs = subs = (uint32_t)P.subs.size();
+        RGL_CUDA(cudaGraphLaunch(x, st));
+    } else {
+        RGL_TRY(c->bt_off.ensure(P.off.size() * 8 + 8));
+        const std::vector<uint32_t> sr = P.shard_rows();
+        RGL_TRY(c->bt_shard.ensure(sr.size() * 4 + 4));
+        RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, P.off.data(), P.off.size() * 8, cudaMemcpyHostToDevice, st));
+        RGL_CUDA(cudaMemcpyAsync(c->bt_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
+        RGL_TRY(enqueue_batch(c, b, P, c->bt_off.as<uint64_t>(), c->bt_shard.as<uint32_t>(), &q, d_counts, d_bp, true,
+                              &launches));
+        subs = (uint32_t)P.subs.size();
+    }
+    c->last_n = 0;  // the single-call stats of finish() do not apply to a batch
+    if (!stats) return RGL_OK;
+    RGL_CUDA(cudaEventRecord(c->ev[2], st));
+    RGL_CUDA(cudaStreamSynchronize(st));
+    float ms = 0;
+    RGL_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[2]));
+    std::memset(stats, 0, sizeof(*stats));
+    stats->ranges = c->h_acc[0];
+    stats->db_swept = c->h_acc[1];
+    stats->rank_positions = c->h_acc[2];
+    stats->pair_candidates = c->h_acc[3];
+    stats->query_intervals = c->h_acc[4];
+    stats->sub_batches = subs;
+    stats->kernel_launches = launches;
+    stats->graph_nodes = nodes;
+    stats->graph_replayed = replay ? 1 : 0;
+    stats->device_ms = ms;
+    stats->chunk = L.chunk;
+    stats->ctas_per_sm = L.ctas_per_sm;
+    stats->pair_ratio = L.pair_ratio;
+    return finish(c, L, nullptr);
+}
+
+int rgl_query_batch_host(rgl_context* c, const rgl_batch* b, const rgl_interval* h_intervals, const rgl_batch_opts* o,
+                    uint32_t* counts, uint64_t* overlap_bp, rgl_batch_stats* stats) {
+    clear_error();
+    if (!c || !b || !counts) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    if (b->num_blocks && (!b->block_offsets || !b->block_shards || !h_intervals))
+        return fail(RGL_ERR_INVALID_ARGUMENT, "incomplete batch");
+    RGL_CUDA(cudaSetDevice(c->idx->device));
+    const uint64_t sub = (o && o->sub_batch) ? std::min<uint64_t>(o->sub_batch, (1ull << 31) - 1) : (1ull << 24);
+    rgl_query_opts q;
+    const Launch L = batch_launch(c, o, &q);
+    const bool want_bp = overlap_bp && !(q.flags & RGL_QF_NO_OVERLAP);
+    const uint32_t D = c->idx->num_sources;
+    const uint64_t cells = (uint64_t)b->num_rows * D;
+    BatchPlan P;
+    RGL_TRY(plan_batch(c, b, sub, &P));
+    RGL_TRY(ensure_workspace(c, P.max_n, b->num_rows, P.max_blk));
+    for (int i = 0; i < 2; i++) {
+        RGL_TRY(c->stage[i].ensure(std::max<uint64_t>(P.max_n, 1) * sizeof(rgl_interval)));
+        if (!c->ev_copied[i]) RGL_CUDA(cudaEventCreateWithFlags(&c->ev_copied[i], cudaEventDisableTiming));
+        if (!c->ev_used[i]) RGL_CUDA(cudaEventCreateWithFlags(&c->ev_used[i], cudaEventDisableTiming));
+    }
+    if (!c->copy_stream) RGL_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+    cudaStream_t st = c->stream, cs = c->copy_stream;
+    const std::vector<uint32_t> sr = P.shard_rows();
+    RGL_TRY(c->bt_off.ensure(P.off.size() * 8 + 8));
+    RGL_TRY(c->bt_shard.ensure(sr.size() * 4 + 4));
+    if (stats) RGL_CUDA(cudaEventRecord(c->ev[0], st));
+    RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, P.off.data(), P.off.size() * 8, cudaMemcpyHostToDevice, st));
+    RGL_CUDA(cudaMemcpyAsync(c->bt_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
+    uint32_t* d_counts = c->out_counts.as<uint32_t>();
+    unsigned long long* d_bp = want_bp ? c->out_bp.as<unsigned long long>() : nullptr;
+    uint32_t* d_small = c->small.as<uint32_t>();
+    RGL_CUDA(cudaMemsetAsync(d_small, 0, 64, st));
+    RGL_CUDA(cudaMemsetAsync(c->acc.p, 0, 64, st));
+    RGL_CUDA(cudaMemsetAsync(d_counts, 0, cells * 4, st));
+    if (d_bp) RGL_CUDA(cudaMemsetAsync(d_bp, 0, cells * 8, st));
+    PipeMode m;
+    m.zero_out = false;
+    m.reset_err = false;
+    m.acc = c->acc.as<unsigned long long>();
+    uint32_t launches = 0;
+    const uint64_t* d_off = c->bt_off.as<uint64_t>();
+    const uint32_t* d_sr = c->bt_shard.as<uint32_t>();
+    for (size_t k = 0; k < P.subs.size(); k++) {
+        const SubBatch& sb = P.subs[k];
+        const int slot = (int)(k & 1);
+        rgl_interval* stage = c->stage[slot].as<rgl_interval>();
+        // the staging buffer is free once the sub-batch two back has been swept
+        if (k >= 2) RGL_CUDA(cudaStreamWaitEvent(cs, c->ev_used[slot], 0));
+        RGL_CUDA(cudaMemcpyAsync(stage, h_intervals + sb.begin, sb.n * sizeof(rgl_interval), cudaMemcpyHostToDevice, cs));
+        RGL_CUDA(cudaEventRecord(c->ev_copied[slot], cs));
+        RGL_CUDA(cudaStreamWaitEvent(st, c->ev_copied[slot], 0));
+        PipeIn in{stage, sb.n, sb.rows, sb.row_lo, sb.nblk, d_off + sb.tab_at, d_sr + sb.tab_at,
+                  b->block_rows ? d_sr + P.shard.size() + sb.tab_at : nullptr};
+        RGL_TRY(run_pipeline(c, in, &q, d_counts + (uint64_t)sb.row_lo * D, d_bp ? d_bp + (uint64_t)sb.row_lo * D : nullptr,
+                             nullptr, m));
+        RGL_CUDA(cudaEventRecord(c->ev_used[slot], st));
+        launches += c->last_launches;
+    }
+    RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
+    RGL_CUDA(cudaMemcpyAsync(c->h_acc, c->acc.p, 64, cudaMemcpyDeviceToHost, st));
+    if (cells) {
+        RGL_CUDA(cudaMemcpyAsync(counts, d_counts, cells * 4, cudaMemcpyDeviceToHost, st));
+        if (overlap_bp) {
+            if (d_bp) RGL_CUDA(cudaMemcpyAsync(overlap_bp, d_bp, cells * 8, cudaMemcpyDeviceToHost, st));
+            else std::memset(overlap_bp, 0, cells * 8);
+        }
+    }
+    if (stats) RGL_CUDA(cudaEventRecord(c->ev[2], st));
+    RGL_CUDA(cudaStreamSynchronize(st));
+    c->last_n = 0;
+    if (stats) {
+        float ms = 0;
+        RGL_CUDA(cudaEventElapsedTime(&ms, c->ev[0], c->ev[2]));
+        std::memset(stats, 0, sizeof(*stats));
+        stats->ranges = c->h_acc[0];
+        stats->db_swept = c->h_acc[1];
+        stats->rank_positions = c->h_acc[2];
+        stats->pair_candidates = c->h_acc[3];
+        stats->query_intervals = c->h_acc[4];
+        stats->sub_batches = (uint32_t)P.subs.size();
+        stats->kernel_launches = launches;
+        stats->device_ms = ms;
+        stats->chunk = L.chunk;
+        stats->ctas_per_sm = L.ctas_per_sm;
+        stats->pair_ratio = L.pair_ratio;
+    }
+    return finish(c, L, nullptr);
+}
+
+// Autotuner: times the sweep kernels of the batch's largest sub-batch over a grid of launch shapes
+// (pair_ratio first at the default shape, then work-item size x CTAs per SM) and keeps the fastest.
+int rgl_batch_autotune(rgl_context* c, const rgl_batch* b, uint64_t sub_batch, rgl_query_opts* best,
+                       rgl_tune_trial* trials, uint32_t max_trials, uint32_t* num_trials) {
+    clear_error();
+    if (!c || !b || !best) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    RGL_CUDA(cudaSetDevice(c->idx->device));
+    BatchPlan P;
+    const uint64_t sub = sub_batch ? std::min<uint64_t>(sub_batch, (1ull << 31) - 1) : (1ull << 24);
+    RGL_TRY(plan_batch(c, b, sub, &P));
+    if (P.subs.empty()) return fail(RGL_ERR_INVALID_ARGUMENT, "empty batch");
+    size_t big = 0;
+    for (size_t i = 1; i < P.subs.size(); i++)
+        if (P.subs[i].n > P.subs[big].n) big = i;
+    const SubBatch sb = P.subs[big];
+    RGL_TRY(ensure_workspace(c, sb.n, sb.rows, sb.nblk));
+    cudaStream_t st = c->stream;
+    RGL_TRY(c->bt_off.ensure(P.off.size() * 8 + 8));
+    const std::vector<uint32_t> sr = P.shard_rows();
+    RGL_TRY(c->bt_shard.ensure(sr.size() * 4 + 4));
+    RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, P.off.data(), P.off.size() * 8, cudaMemcpyHostToDevice, st));
+    RGL_CUDA(cudaMemcpyAsync(c->bt_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
+    PipeIn in{b->d_intervals + sb.begin, sb.n, sb.rows, sb.row_lo, sb.nblk, c->bt_off.as<uint64_t>() + sb.tab_at,
+              c->bt_shard.as<uint32_t>() + sb.tab_at,
+              b->block_rows ? c->bt_shard.as<uint32_t>() + P.shard.size() + sb.tab_at : nullptr};
+    const bool was_timing = c->timing;
+    *best = rgl_query_opts{};
+    uint32_t nt = 0;
+    auto trial = [&](rgl_query_opts q, float* out_ms) -> int {
+        float best_ms = 1e30f;
+        for (int rep = 0; rep < 2; rep++) {
+            c->timing = true;
+            c->tev_used = 0;
+            RGL_TRY(run_pipeline(c, in, &q, c->out_counts.as<uint32_t>(), c->out_bp.as<unsigned long long>(), nullptr));
+            RGL_CUDA(cudaStreamSynchronize(st));
+            float ms = 0;
+            RGL_CUDA(cudaEventElapsedTime(&ms, c->tev[0], c->tev[1]));
+            c->tev_used = 0;
+            best_ms = std::min(best_ms, ms);
+        }
+        *out_ms = best_ms;
+        const Launch L = pick_launch(&q);
+        if (trials && nt < max_trials) trials[nt] = rgl_tune_trial{L.chunk, L.ctas_per_sm, L.pair_ratio, best_ms};
+        nt++;
+        return RGL_OK;
+    };
+    int s = RGL_OK;
+    rgl_query_opts cur{};
+    cur.flags = 0;
+    float cur_ms = 1e30f;
+    for (uint32_t pr : {1u, 2u, 4u, 8u}) {
+        rgl_query_opts q = cur;
+        q.pair_ratio = pr;
+        float ms;
+        if ((s = trial(q, &ms)) != RGL_OK) break;
+        if (ms < cur_ms) {
+            cur_ms = ms;
+            best->pair_ratio = pr;
+        }
+    }
+    cur.pair_ratio = best->pair_ratio;
+    for (uint32_t ch : {512u, 1024u, 2048u, 4096u, 8192u}) {
+        if (s != RGL_OK) break;
+        for (uint32_t ct : {2u, 3u, 4u, 6u, 8u}) {
+            rgl_query_opts q = cur;
+            q.chunk = ch;
+            q.ctas_per_sm = ct;
+            float ms;
+            if ((s = trial(q, &ms)) != RGL_OK) break;
+            if (ms < cur_ms) {
+                cur_ms = ms;
+                best->chunk = ch;
+                best->ctas_per_sm = ct;
+            }
+        }
+    }
+    c->timing = was_timing;
+    if (s != RGL_OK) return s;
+    const Launch L = pick_launch(best);
+    best->chunk = L.chunk;
+    best->ctas_per_sm = L.ctas_per_sm;
+    best->pair_ratio = L.pair_ratio;
+    best->block = 256;
+    best->flags = 0;
+    c->tuned = *best;
+    c->has_tuned = true;
+    if (num_trials) *num_trials = nt;
+    RGL_CUDA(cudaStreamSynchronize(st));
+    return finish(c, L, nullptr);
 }
 
 int rgl_context_check(rgl_context* c) {

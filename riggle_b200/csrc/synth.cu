@@ -209,6 +209,23 @@ __global__ void k_synth_unpack(uint64_t total, const uint64_t* __restrict__ key,
     sid[dst] = (uint32_t)v;
 }
 
+// One thread per interval of a file-major query batch: block b = (file b / C, chromosome b % C).
+__global__ void k_synth_batch(GenParams g, const uint32_t* __restrict__ t_logn, const uint32_t* __restrict__ t_logu,
+                              const uint32_t* __restrict__ chrom_len, uint32_t C, const uint64_t* __restrict__ off,
+                              uint32_t nblk, uint64_t total, rgl_interval* __restrict__ out) {
+    const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (j >= total) return;
+    uint32_t lo = 0, hi = nblk;  // last block with off[b] <= j
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (off[m] <= j) lo = m; else hi = m;
+    }
+    const uint32_t f = lo / C, c = lo % C;
+    uint32_t s, e;
+    gen_interval(g, t_logn, t_logu, f, c, chrom_len[c], j - off[lo], &s, &e);
+    out[j] = rgl_interval{s, e, g.sid_base + f};
+}
+
 }  // namespace rgl
 
 using namespace rgl;
@@ -329,6 +346,62 @@ int rgl_synth_chrom_layers_host(const rgl_synth_spec* sp, uint32_t chrom, uint32
         sid[j] = (uint32_t)v;
     }
     return RGL_OK;
+}
+
+int rgl_synth_batch_layout(const rgl_synth_spec* sp, uint64_t* block_offsets, uint32_t* block_shards,
+                           uint32_t* block_rows) {
+    RGL_TRY(check_spec(sp));
+    if (!block_offsets) return fail(RGL_ERR_INVALID_ARGUMENT, "null output");
+    const uint32_t C = sp->num_chroms;
+    std::vector<uint64_t> per(C);
+    uint64_t acc = 0;
+    for (uint32_t f = 0; f < sp->num_files; f++) {
+        chrom_split(sp, sp->file_sizes[f], per.data());
+        for (uint32_t c = 0; c < C; c++) {
+            const uint64_t b = (uint64_t)f * C + c;
+            block_offsets[b] = acc;
+            if (block_shards) block_shards[b] = c;
+            if (block_rows) block_rows[b] = f;
+            acc += per[c];
+        }
+    }
+    block_offsets[(uint64_t)sp->num_files * C] = acc;
+    return RGL_OK;
+}
+
+int rgl_synth_batch_device(const rgl_synth_spec* sp, int device, const uint64_t* block_offsets, rgl_interval* d_out,
+                           void* stream) {
+    clear_error();
+    RGL_TRY(check_spec(sp));
+    if (!block_offsets) return fail(RGL_ERR_INVALID_ARGUMENT, "null block offsets");
+    const uint64_t nblk = (uint64_t)sp->num_files * sp->num_chroms;
+    const uint64_t total = block_offsets[nblk];
+    if (total && !d_out) return fail(RGL_ERR_INVALID_ARGUMENT, "null output");
+    if (nblk >= (1ull << 32)) return fail(RGL_ERR_INVALID_ARGUMENT, "too many blocks");
+    RGL_CUDA(cudaSetDevice(device));
+    if (!total) return RGL_OK;
+    cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);
+    const SynthTables& T = synth_tables();
+    DevBuf tn, tu, cl, off;
+    int s = tn.ensure(65537 * 4);
+    if (s == RGL_OK) s = tu.ensure(65537 * 4);
+    if (s == RGL_OK) s = cl.ensure(sp->num_chroms * 4ull);
+    if (s == RGL_OK) s = off.ensure((nblk + 1) * 8);
+    if (s == RGL_OK &&
+        (cudaMemcpy(tn.p, T.lognormal.data(), 65537 * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(tu.p, T.loguniform.data(), 65537 * 4, cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(cl.p, sp->chrom_len, sp->num_chroms * 4ull, cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(off.p, block_offsets, (nblk + 1) * 8, cudaMemcpyHostToDevice) != cudaSuccess))
+        s = fail(RGL_ERR_DEVICE, "synth upload");
+    if (s == RGL_OK) {
+        k_synth_batch<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(
+            make_params(sp), tn.as<uint32_t>(), tu.as<uint32_t>(), cl.as<uint32_t>(), sp->num_chroms,
+            off.as<uint64_t>(), (uint32_t)nblk + 1, total, d_out);
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(st) != cudaSuccess)
+            s = fail(RGL_ERR_DEVICE, "synth batch kernel");
+    }
+    for (DevBuf* b : {&tn, &tu, &cl, &off}) b->release();
+    return s;
 }
 
 int rgl_index_synth(const rgl_synth_spec* sp, uint32_t min_size, uint32_t gf, int device, rgl_index** out) {
