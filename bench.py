@@ -1,21 +1,31 @@
 #!/usr/bin/env python
-"""Benchmark of the interval sweep: intervals swept per second on B200.
+"""Benchmark of the interval sweep on B200: intervals swept per second, batched vs plain, and the
+serving loop's latency, counts exact.
 
-Default workload ("plain"): the GPU-scale plain configuration — 24 chromosomes with lengths
-uniform in [50M, 250M] bp, a database of 1,000 files with rank-Zipf(1.1) sizes clamped to
-[1e3, 1e7] intervals summing to 2e9 (log-normal lengths, median 500 bp, sigma 1, clipped to
-[20, 100k], plus 5% log-uniform [10k, 1M] broad intervals), u32 start/end/file-id resident in HBM
-(~24 GB), and one query file of 1e5 intervals per step (a different seeded file every step).
-A step is one pass of the hot path: sort the query file, partition the candidate ranges, sweep and
-tally the 1 x 1000 count vector and overlap base pairs.
+One JSON line with three parts:
+  value (primary, the GPU-scale plain configuration): 24 chromosomes with lengths uniform in
+    [50M, 250M] bp, a database of 1,000 files with rank-Zipf(1.1) sizes clamped to [1e3, 1e7]
+    intervals summing to 2e9 (log-normal lengths, median 500 bp, sigma 1, clipped to [20, 100k], plus
+    5% log-uniform [10k, 1M] broad intervals), u32 start/end/file-id resident in HBM (~24 GB), and one
+    query file of 1e5 intervals per step (a different seeded file every step).  A step is one pass of
+    the hot path: sort the query file, partition the candidate ranges, sweep and tally the 1 x 1000
+    count vector and overlap base pairs.  Carries roofline, cpu_baseline, e2e and clocks.
+  "batched": 4,096 query files (log-uniform [1e2, 1e6] intervals, 10% in 1 Mbp hot spots) against
+    the 64-file x 50k database in one call (CUDA graph replay, autotuned launch shape), next to the
+    plain form on the same files (one call per file), with the results compared cell by cell.
+  "serving": Poisson arrivals at 200 query files/s (log-uniform [1e3, 1e6] intervals) against the
+    resident 64-file database through the request server: p50/p99/p99.9 latency and sustained rate,
+    continuous batching vs one query file per launch.
 
 "intervals swept" = query intervals + database intervals in the union of the reference's candidate
-ranges [q.start - layer_max_K, q.end) over all (shard, layer) (computed by the pipeline itself).
+ranges [q.start - layer_max_K, q.end) over all (shard, layer), per query file (computed by the
+pipeline itself).
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl riggle|reference]
-       [--workload plain|config1]
+       [--workload plain|config1] [--batch-files F] [--serve-seconds S] [--only all|plain|batched|serving]
 For N > 1 launch with torch.distributed.run: every rank holds a replica of the index and sweeps its
-own query files (weak scaling, no data-path collective); timing is the max over ranks.
+own query files (weak scaling, no data-path collective); timing is the max over ranks.  The batched
+and serving parts run at N = 1 only.
 """
 import argparse
 import ctypes as C
@@ -31,14 +41,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "intervals swept/s (plain one-query-file-per-launch form, counts exact)"
+METRIC = "intervals swept/s + p99 latency, batched vs plain, 1 B200, counts exact"
 UNIT = "intervals/s"
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["riggle", "reference"], default="riggle")
     ap.add_argument("--workload", choices=["plain", "config1"], default="plain")
@@ -53,6 +63,14 @@ def parse():
     ap.add_argument("--chroms", type=int, default=24,
                     help="keep only the first N chromosomes, scaling database and query sizes by their share "
                          "of the genome (same per-bp density; for profiling captures)")
+    ap.add_argument("--batch-files", type=int, default=4096,
+                    help="query files of the batched measurement (0 skips it)")
+    ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--serve-seconds", type=float, default=5.0,
+                    help="length of the Poisson arrival trace of the serving measurement (0 skips it)")
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--only", choices=["all", "plain", "batched", "serving"], default="all",
+                    help="run one part only (profiling captures)")
     return ap.parse_args()
 
 
@@ -103,6 +121,9 @@ def query_file(cl, seed, qsize):
 # clocks sampled during the timed region
 # ---------------------------------------------------------------------------------------------
 class ClockSampler:
+    """nvidia-smi samples every 50 ms, each stamped on arrival; stop(t0, t1) keeps the samples taken
+    inside the timed region [t0, t1] (perf_counter), or, for a region shorter than the sampling
+    period, the samples within 250 ms of it (marked in "window")."""
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -115,18 +136,19 @@ class ClockSampler:
     def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
         except Exception:
             self.proc = None
+        return self
 
     def _read(self):
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            self.lines.append((time.perf_counter(), line.strip()))
 
-    def stop(self):
+    def stop(self, t0=None, t1=None):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -134,9 +156,17 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
+        lines = self.lines
+        window = "timed region"
+        if t0 is not None:
+            inside = [x for x in lines if t0 <= x[0] <= t1]
+            if not inside:
+                inside = [x for x in lines if t0 - 0.25 <= x[0] <= t1 + 0.25]
+                window = "timed region +- 250 ms (region shorter than the 50 ms sampling period allows)"
+            lines = inside
         sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
+        for _, ln in lines:
             p = [x.strip() for x in ln.split(",")]
             if len(p) < 9:
                 continue
@@ -149,7 +179,7 @@ class ClockSampler:
                 if v.lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "window": window}
 
 
 def measured_peak():
@@ -284,6 +314,8 @@ def run_riggle(args, rank, world, local_rank, dist):
     work = np.array(swept, np.float64)
 
     # ---- device-resident timing (value) ----
+    clocks = ClockSampler(dev).start()
+    time.sleep(0.3)  # the sampler's first line
     for i in range(args.warmup):
         dev_step(i)
     _lib.check(lib.rgl_context_check(ctx._h))
@@ -292,19 +324,19 @@ def run_riggle(args, rank, world, local_rank, dist):
     if dist:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    clocks = ClockSampler(dev)
-    clocks.start()
     lib.rgl_context_set_timing(ctx._h, 1)
+    tc0 = time.perf_counter()
     e0.record(stream)
     for i in range(args.warmup, nfiles):
         dev_step(i)
     e1.record(stream)
     torch.cuda.synchronize()
+    tc1 = time.perf_counter()
     sweep_ms = C.c_float()
     launches = C.c_uint32()
     _lib.check(lib.rgl_context_sweep_times(ctx._h, C.byref(sweep_ms), C.byref(launches)))
     lib.rgl_context_set_timing(ctx._h, 0)
-    clk = clocks.stop()
+    clk = clocks.stop(tc0, tc1)
     _lib.check(lib.rgl_context_check(ctx._h))
     ms = e0.elapsed_time(e1)
     units = float(work[args.warmup:].sum())
@@ -379,6 +411,7 @@ def run_riggle(args, rank, world, local_rank, dist):
                          "structure (one query file = one 64-row window = one thread)"}
 
     own_launches = first_stats["kernel_launches"]
+    out = None
     if rank == 0:
         out = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -393,13 +426,238 @@ def run_riggle(args, rank, world, local_rank, dist):
                "extra": {"index_build_s": build_s, "db_swept_first": first_stats["db_swept"],
                          "ranges_first": first_stats["ranges"], "device_ms_first": first_stats["device_ms"],
                          "sweep_ms_first": first_stats["sweep_ms"], "own_kernels_per_step": own_launches}}
-        print(json.dumps(out), flush=True)
     for p in pin_q:
         lib.rgl_host_free(p)
     lib.rgl_host_free(pc)
     lib.rgl_host_free(pb)
     ctx.close()
     idx.close()
+    return out
+
+
+# ---------------------------------------------------------------------------------------------
+# batched form (4,096 query files in one call) against the plain one-file-per-launch form
+# ---------------------------------------------------------------------------------------------
+def batched_workload(nfiles):
+    """The 64-file x 50k database and a seeded batch of query files with log-uniform [1e2, 1e6] sizes,
+    10% of each file's intervals in 1 Mbp hot spots (8 spots per chromosome shared by all files)."""
+    import riggle_b200 as rg
+
+    cl = rg.synth_chrom_lengths(1, 24)
+    db = rg.SynthSpec(2, cl, np.full(64, 50_000, np.uint64))
+    sizes = rg.synth_loguniform_sizes(4242, nfiles, 100, 1_000_000) if nfiles else np.zeros(0, np.uint64)
+    q = rg.SynthSpec(5000, cl, sizes, hotspot_fraction=0.1, num_hotspots=8)
+    return cl, db, q
+
+
+def run_batched(args, dev):
+    import torch
+
+    import riggle_b200 as rg
+    from riggle_b200 import _lib
+
+    lib = rg.load()
+    cl, dbspec, qspec = batched_workload(args.batch_files)
+    idx = rg.Index.synth(dbspec, device=dev)
+    D = idx.num_sources
+    off, sh, rw = rg.synth_batch_layout(qspec)
+    N, F = int(off[-1]), qspec.num_files
+    cuda = f"cuda:{dev}"
+    t_iv = torch.empty((N, 3), dtype=torch.int32, device=cuda)
+    rg.synth_batch_device(qspec, off, t_iv.data_ptr(), device=dev)
+    ctx = rg.Context(idx)
+    batch = rg.DeviceBatch(F, sh, off, t_iv.data_ptr(), rw)
+    dc = torch.empty((F, D), dtype=torch.int32, device=cuda)
+    dbp = torch.empty((F, D), dtype=torch.int64, device=cuda)
+    t0 = time.perf_counter()
+    best, trials = ctx.autotune(batch)
+    tune_s = time.perf_counter() - t0
+    # capture, then replays: the timed steps launch the cached graph
+    for _ in range(2):
+        st = ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), graph=True, tuned=True)
+    units = float(st["db_swept"] + st["query_intervals"])
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(dev).start()
+    time.sleep(0.3)  # the sampler's first line
+    torch.cuda.synchronize()
+    tc0 = time.perf_counter()
+    e0.record(stream)
+    for _ in range(args.batch_steps):
+        ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), graph=True, tuned=True, stats=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop(tc0, time.perf_counter())
+    ctx.check()
+    ms = e0.elapsed_time(e1) / args.batch_steps
+    value = units / (ms / 1e3)
+    bc = dc.cpu().numpy().view(np.uint32)
+    bb = dbp.cpu().numpy().view(np.uint64)
+
+    # the plain form on the same files: one rgl_query_counts_device call (one pipeline) per file
+    t_plain = t_iv.clone()
+    t_plain[:, 2] = 0
+    pc = torch.empty((F, D), dtype=torch.int32, device=cuda)
+    pb = torch.empty((F, D), dtype=torch.int64, device=cuda)
+    shard_ids = np.arange(len(cl), dtype=np.uint32)
+    opts = _lib.QueryOpts(0, 0, 0, 0, 0)
+    C_ = len(cl)
+    offs_f = [np.ascontiguousarray(off[f * C_:(f + 1) * C_ + 1]) for f in range(F)]
+    ctx.reserve(int(max(qspec.file_sizes)) + 16, 1)
+
+    def plain_pass(files):
+        for f in files:
+            _lib.check(lib.rgl_query_counts_device(ctx._h, 1, C_, C.c_void_p(shard_ids.ctypes.data),
+                                                   C.c_void_p(offs_f[f].ctypes.data), C.c_void_p(t_plain.data_ptr()),
+                                                   C.byref(opts), C.c_void_p(pc.data_ptr() + f * D * 4),
+                                                   C.c_void_p(pb.data_ptr() + f * D * 8), None))
+
+    plain_pass(range(min(F, 64)))
+    torch.cuda.synchronize()
+    e0.record(stream)
+    plain_pass(range(F))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.check()
+    plain_ms = e0.elapsed_time(e1)
+    plain_value = units / (plain_ms / 1e3)
+    exact = bool((pc.cpu().numpy().view(np.uint32) == bc).all() and (pb.cpu().numpy().view(np.uint64) == bb).all())
+    if not exact:
+        raise RuntimeError("batched and plain forms disagree")
+    del t_plain
+
+    # end to end: host intervals in page-locked memory, copies overlapped with the sweep
+    hp = C.c_void_p()
+    _lib.check(lib.rgl_host_alloc(N * 12, C.byref(hp)))
+    hv = np.ctypeslib.as_array((C.c_uint32 * (N * 3)).from_address(hp.value))
+    hv[:] = t_iv.cpu().numpy().view(np.uint32).reshape(-1)
+    hc = np.empty((F, D), np.uint32)
+    hb = np.empty((F, D), np.uint64)
+    ctx.query_batch_host(batch, hp.value, tuned=True, out=(hc, hb))
+    walls = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        ctx.query_batch_host(batch, hp.value, tuned=True, out=(hc, hb))
+        walls.append(time.perf_counter() - t0)
+    e2e_s = min(walls)
+    if not ((hc == bc).all() and (hb == bb).all()):
+        raise RuntimeError("host-input batch disagrees")
+    lib.rgl_host_free(hp)
+
+    # CPU: the oracle's restatement on a bounded sample of the batch's files
+    cpu = None
+    if not args.no_cpu_baseline:
+        import oracle as O
+
+        sample = list(range(0, F, max(1, F // 48)))[:48]
+        host = t_iv.cpu().numpy().view(np.uint32)
+        layers = {}
+        for c in range(C_):
+            layers.update(dbspec.chrom_layers(c))
+        jumps = O.jump_tables(layers)
+        n_s = 0.0
+        t_s = 0.0
+        for f in sample:
+            per = {}
+            for c in range(C_):
+                a = host[int(off[f * C_ + c]):int(off[f * C_ + c + 1])].copy()
+                if len(a):
+                    a[:, 2] = 0
+                    per[c] = a
+            t0 = time.perf_counter()
+            _, _, _, ost = O.query_database(layers, per, 1, D, threads=1, mode=0, jumps=jumps)
+            t_s += time.perf_counter() - t0
+            n_s += ost["db_swept"] + ost["query_intervals"]
+        cpu = {"value": n_s / t_s, "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{len(sample)} of the {F} query files (every {max(1, F // 48)}th), all chromosomes, "
+                         "restatement of query_database/query_sweep_windowed, one thread per query file"}
+    out = {"workload": f"batched: {F} query files, log-uniform [1e2, 1e6] intervals (10% in 1 Mbp hot spots), "
+                       "against the 64-file x 50k database, one call (graph replay, autotuned launch shape)",
+           "value": value, "unit": UNIT, "ms_per_step": ms, "steps": args.batch_steps, "query_files": F,
+           "query_intervals": int(st["query_intervals"]), "db_swept": int(st["db_swept"]),
+           "sub_batches": st["sub_batches"], "graph_nodes": st["graph_nodes"],
+           "gpu_launches_per_step": st["kernel_launches"],
+           "tuned": best, "tune_trials": len(trials), "tune_s": tune_s,
+           "plain": {"value": plain_value, "ms_per_step": plain_ms,
+                     "form": "one rgl_query_counts_device call per query file, same files, same units"},
+           "batched_vs_plain": value / plain_value, "counts_exact_vs_plain": exact,
+           "e2e": {"value": units / e2e_s, "unit": UNIT, "ms_per_step": e2e_s * 1e3, "h2d_bytes_per_step": N * 12,
+                   "d2h_bytes_per_step": F * D * 12, "api": "rgl_query_batch_host (page-locked host intervals)"},
+           "cpu_baseline": cpu, "clocks": clk, "l2": "the batch's 5.6 GB of query intervals exceed L2"}
+    ctx.close()
+    return out, idx
+
+
+# ---------------------------------------------------------------------------------------------
+# serving: Poisson arrivals against the resident 64-file database
+# ---------------------------------------------------------------------------------------------
+def serve_trace(srv, reqs, arrivals, hp):
+    tickets = []
+    t0 = time.perf_counter()
+    for k, blocks in enumerate(reqs):
+        dt = t0 + arrivals[k] - time.perf_counter()
+        if dt > 0:
+            time.sleep(dt)
+        tickets.append(srv.submit(blocks, intervals_ptr=hp))
+    infos = [srv.wait(t, 120_000)[2] for t in tickets]
+    return infos
+
+
+def run_serving(args, dev, idx):
+    import torch
+
+    import riggle_b200 as rg
+    from riggle_b200 import _lib
+
+    lib = rg.load()
+    cl = rg.synth_chrom_lengths(1, 24)
+    rng = np.random.default_rng(77)
+    lam, T = args.serve_rate, args.serve_seconds
+    arr = np.cumsum(rng.exponential(1.0 / lam, size=int(lam * T * 2) + 64))
+    arr = arr[arr < T]
+    nreq = len(arr)
+    sizes = rg.synth_loguniform_sizes(777, nreq, 1000, 1_000_000)
+    spec = rg.SynthSpec(7000, cl, sizes)
+    off, sh, _ = rg.synth_batch_layout(spec)
+    N = int(off[-1])
+    t_iv = torch.empty((max(N, 1), 3), dtype=torch.int32, device=f"cuda:{dev}")
+    rg.synth_batch_device(spec, off, t_iv.data_ptr(), device=dev)
+    hp = C.c_void_p()
+    _lib.check(lib.rgl_host_alloc(max(N, 1) * 12, C.byref(hp)))
+    hv = np.ctypeslib.as_array((C.c_uint32 * (max(N, 1) * 3)).from_address(hp.value))
+    hv[:] = t_iv.cpu().numpy().view(np.uint32).reshape(-1)
+    del t_iv
+    C_ = len(cl)
+    reqs = [[(int(sh[b]), int(off[b]), int(off[b + 1])) for b in range(k * C_, (k + 1) * C_) if off[b + 1] > off[b]]
+            for k in range(nreq)]
+
+    def measure(**kw):
+        srv = rg.Server(idx, **kw)
+        serve_trace(srv, reqs[:32], np.zeros(32), hp.value)  # warm-up burst
+        srv.reset_stats()
+        infos = serve_trace(srv, reqs, arr, hp.value)
+        st = srv.stats()
+        srv.close()
+        lat = np.array([(i["done_s"] - i["submit_s"]) * 1e3 for i in infos])
+        n = np.array([i["intervals"] for i in infos])
+        near = lat[(n >= 50_000) & (n <= 200_000)]
+        return {"p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "p999_ms": st["p999_ms"], "max_ms": st["max_ms"],
+                "mean_ms": st["mean_ms"],
+                "p99_ms_1e5_requests": float(np.percentile(near, 99, method="inverted_cdf")) if len(near) else None,
+                "requests_1e5": int(len(near)),
+                "sustained_query_intervals_per_s": st["intervals"] / max(1e-9, st["last_done_s"] - st["first_submit_s"]),
+                "batches": st["batches"], "mean_batch_requests": st["mean_batch_requests"],
+                "workers": st["workers"], "failed": st["failed"]}
+
+    batched = measure()
+    plain = measure(workers=1, max_batch_requests=1)
+    lib.rgl_host_free(hp)
+    return {"workload": f"serving: Poisson arrivals at {lam:g}/s for {T:g} s ({nreq} query files, log-uniform "
+                        "[1e3, 1e6] intervals) against the resident 64-file x 50k database; latency = submit to "
+                        "count and overlap rows in host memory",
+            "offered_query_intervals_per_s": float(sizes.sum()) / T, "requests": nreq,
+            "continuous_batching": batched, "plain_one_file_per_launch": plain}
 
 
 def main():
@@ -420,7 +678,33 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         dist = True
     try:
-        run_riggle(args, rank, world, local_rank, dist)
+        out = None
+        if args.only in ("all", "plain"):
+            out = run_riggle(args, rank, world, local_rank, dist)
+        if rank == 0 and world == 1 and args.only != "plain":
+            idx = None
+            if args.batch_files and args.only in ("all", "batched"):
+                b, idx = run_batched(args, local_rank)
+                if out is None:  # the batched measurement alone (profiling)
+                    out = {"metric": METRIC, "value": b["value"], "unit": UNIT, "n_gpus": 1,
+                           "steps": args.batch_steps, "warmup": 2, "higher_is_better": True, "scaling": "weak",
+                           "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+                           "config": {"workload": b["workload"]}}
+                out["batched"] = b
+            if args.serve_seconds and args.only in ("all", "serving"):
+                import riggle_b200 as rg
+
+                if idx is None:
+                    idx = rg.Index.synth(batched_workload(0)[1], device=local_rank)
+                sv = run_serving(args, local_rank, idx)
+                if out is None:
+                    out = {"metric": METRIC, "value": sv["continuous_batching"]["p99_ms"], "unit": "ms (p99)",
+                           "n_gpus": 1, "higher_is_better": False, "config": {"workload": sv["workload"]}}
+                out["serving"] = sv
+            if idx is not None:
+                idx.close()
+        if rank == 0 and out is not None:
+            print(json.dumps(out), flush=True)
     finally:
         if dist:
             import torch

@@ -403,6 +403,69 @@ int rgl_synth_batch_device(const rgl_synth_spec* spec, int device, const uint64_
                            rgl_interval* d_out, void* stream);
 
 /* ------------------------------------------------------------------------------------------ */
+/* Request server (no counterpart in the reference, whose query_database answers one set of     */
+/* files per process run).  The index stays resident; query files arrive one at a time and are   */
+/* batched as they come: each worker owns a query context on its own stream and, whenever it is  */
+/* idle, takes the oldest pending requests (up to max_batch_requests and batch_intervals) as one */
+/* batch, so requests that arrive while others are on the GPU overlap with them on the device.   */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct rgl_server rgl_server;
+
+typedef struct rgl_server_opts {
+    uint32_t workers;               /* batches in flight at once (default 3; fewer when HBM is short) */
+    uint32_t max_batch_requests;    /* requests per batch (default 256; 1 = one query file per launch) */
+    uint64_t batch_intervals;       /* intervals per batch, also the largest admissible request (default 2^23) */
+    uint64_t hbm_reserve_bytes;     /* device memory left free when sizing workers (default 4 GiB) */
+    uint64_t max_pending_intervals; /* host queue bound: submit refuses beyond it (default 2^28) */
+    rgl_query_opts query;           /* launch shape (zeros: defaults); RGL_QF_NO_OVERLAP */
+} rgl_server_opts;
+
+/* One query file.  The server copies the block tables at submit; `intervals` (page-locked for
+ * asynchronous copies) must stay valid until the request completes; counts / overlap_bp (D entries
+ * each, overlap_bp may be NULL) are written when it completes.  Interval sids are ignored. */
+typedef struct rgl_request {
+    uint32_t num_blocks;
+    const uint32_t* block_shards;  /* index shard of each block */
+    const uint64_t* block_offsets; /* num_blocks + 1 element offsets into intervals */
+    const rgl_interval* intervals;
+    uint32_t* counts;
+    uint64_t* overlap_bp;
+} rgl_request;
+
+typedef struct rgl_request_info {
+    int status;               /* rgl_status of this request */
+    uint32_t batch_requests;  /* requests in the batch it ran in */
+    uint64_t batch_intervals; /* intervals in that batch */
+    uint64_t intervals;       /* this request's intervals */
+    double submit_s, start_s, done_s; /* steady-clock seconds since the server was created */
+} rgl_request_info;
+
+typedef struct rgl_server_stats {
+    uint64_t submitted, completed, failed, batches, intervals;
+    uint32_t workers;           /* workers admitted by free HBM */
+    uint32_t pending;           /* requests waiting now */
+    double mean_batch_requests;
+    double p50_ms, p99_ms, p999_ms, max_ms, mean_ms; /* submit -> results in host memory */
+    double first_submit_s, last_done_s;
+    double worker_bytes;        /* device memory reserved per worker */
+} rgl_server_stats;
+
+/* Sizes the workers by free device memory (each reserves its workspace for batch_intervals). */
+int rgl_server_create(rgl_index* index, const rgl_server_opts* opts, rgl_server** out);
+/* Queues one request; RGL_ERR_INVALID_ARGUMENT for a bad block table or a request larger than
+ * batch_intervals, RGL_ERR_OOM when the queue is full. */
+int rgl_server_submit(rgl_server* server, const rgl_request* req, uint64_t* ticket);
+/* Waits up to timeout_ms (0: poll) for a request; RGL_ERR_TIMEOUT while it is not done.  A completed
+ * ticket is released by this call.  A batch that fails is retried request by request, so only the
+ * request with invalid intervals fails. */
+int rgl_server_wait(rgl_server* server, uint64_t ticket, uint32_t timeout_ms, rgl_request_info* info);
+int rgl_server_get_stats(rgl_server* server, rgl_server_stats* out);
+/* Clears the latency record and counters (between a warm-up and a measured run). */
+int rgl_server_reset_stats(rgl_server* server);
+/* Finishes the queued requests, stops the workers and frees everything. */
+int rgl_server_destroy(rgl_server* server);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Stream helpers, timing and pinned host memory (no counterpart in the reference).              */
 /* ------------------------------------------------------------------------------------------ */
 int rgl_context_sync(rgl_context* ctx);

@@ -9,6 +9,7 @@ from .api import (  # noqa: F401
     DeviceBatch,
     Index,
     LayerConfig,
+    Server,
     SynthSpec,
     bucket_layers,
     synth_batch_device,

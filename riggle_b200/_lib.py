@@ -107,6 +107,36 @@ class TuneTrial(C.Structure):
                 ("sweep_ms", C.c_float)]
 
 
+class ServerOpts(C.Structure):
+    _fields_ = [("workers", C.c_uint32), ("max_batch_requests", C.c_uint32), ("batch_intervals", C.c_uint64),
+                ("hbm_reserve_bytes", C.c_uint64), ("max_pending_intervals", C.c_uint64), ("query", QueryOpts)]
+
+
+class Request(C.Structure):
+    _fields_ = [("num_blocks", C.c_uint32), ("block_shards", C.c_void_p), ("block_offsets", C.c_void_p),
+                ("intervals", C.c_void_p), ("counts", C.c_void_p), ("overlap_bp", C.c_void_p)]
+
+
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int), ("batch_requests", C.c_uint32), ("batch_intervals", C.c_uint64),
+                ("intervals", C.c_uint64), ("submit_s", C.c_double), ("start_s", C.c_double),
+                ("done_s", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("failed", C.c_uint64),
+                ("batches", C.c_uint64), ("intervals", C.c_uint64), ("workers", C.c_uint32),
+                ("pending", C.c_uint32), ("mean_batch_requests", C.c_double), ("p50_ms", C.c_double),
+                ("p99_ms", C.c_double), ("p999_ms", C.c_double), ("max_ms", C.c_double), ("mean_ms", C.c_double),
+                ("first_submit_s", C.c_double), ("last_done_s", C.c_double), ("worker_bytes", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class SynthSpec(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("num_chroms", C.c_uint32), ("chrom_len", C.POINTER(C.c_uint32)),
                 ("num_files", C.c_uint32), ("file_sizes", C.POINTER(C.c_uint64)),
@@ -152,6 +182,12 @@ _SIGS = {
                                        C.POINTER(BatchStats)]),
     "rgl_batch_autotune": (C.c_int, [_P, C.POINTER(BatchDesc), C.c_uint64, C.POINTER(QueryOpts),
                                      C.POINTER(TuneTrial), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "rgl_server_create": (C.c_int, [_P, C.POINTER(ServerOpts), C.POINTER(_P)]),
+    "rgl_server_submit": (C.c_int, [_P, C.POINTER(Request), C.POINTER(C.c_uint64)]),
+    "rgl_server_wait": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.POINTER(RequestInfo)]),
+    "rgl_server_get_stats": (C.c_int, [_P, C.POINTER(ServerStats)]),
+    "rgl_server_reset_stats": (C.c_int, [_P]),
+    "rgl_server_destroy": (C.c_int, [_P]),
     "rgl_context_check": (C.c_int, [_P]),
     "rgl_context_set_timing": (C.c_int, [_P, C.c_int]),
     "rgl_context_sweep_times": (C.c_int, [_P, C.POINTER(C.c_float), C.POINTER(C.c_uint32)]),

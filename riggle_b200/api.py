@@ -231,6 +231,78 @@ class Context:
             pass
 
 
+class Server:
+    """Request server over a resident Index (rgl_server_*): submit query files as they arrive, wait
+    for their count / overlap rows; p50/p99/p99.9 latency in stats()."""
+
+    def __init__(self, index, workers=0, max_batch_requests=0, batch_intervals=0, hbm_reserve_bytes=0,
+                 max_pending_intervals=0, counts_only=False, chunk=0, ctas_per_sm=0, pair_ratio=0):
+        self.index = index
+        o = _lib.ServerOpts(workers, max_batch_requests, batch_intervals, hbm_reserve_bytes, max_pending_intervals,
+                            Context._opts(chunk, ctas_per_sm, counts_only, pair_ratio))
+        h = C.c_void_p()
+        check(load().rgl_server_create(index._h, C.byref(o), C.byref(h)))
+        self._h = h
+        self._live = {}  # ticket -> arrays that must outlive the request
+
+    def submit(self, blocks, intervals_ptr=None, with_overlap=True):
+        """blocks: {shard id: uint32[n,3]} (copied into one array), or, with intervals_ptr (an int
+        pointer to page-locked intervals), a list of (shard id, begin, end) element ranges of it.
+        Returns the ticket."""
+        D = self.index.num_sources
+        keep = []
+        if intervals_ptr is None:
+            items = [(int(k), np.ascontiguousarray(v, np.uint32).reshape(-1, 3)) for k, v in blocks.items()]
+            items = [(k, v) for k, v in items if len(v)]
+            iv = np.concatenate([v for _, v in items]) if items else np.zeros((0, 3), np.uint32)
+            shards = np.array([k for k, _ in items], np.uint32)
+            offs = np.zeros(len(items) + 1, np.uint64)
+            offs[1:] = np.cumsum([len(v) for _, v in items])
+            keep.append(iv)
+            ptr = iv.ctypes.data if len(iv) else None
+        else:
+            shards = np.array([b[0] for b in blocks], np.uint32)
+            offs = np.array([blocks[0][1]] + [b[2] for b in blocks], np.uint64) if blocks else np.zeros(1, np.uint64)
+            ptr = intervals_ptr
+        counts = np.zeros(D, np.uint32)
+        bp = np.zeros(D, np.uint64) if with_overlap else None
+        keep += [shards, offs, counts, bp]
+        req = _lib.Request(len(shards), _ptr(shards), _ptr(offs), C.c_void_p(ptr) if ptr else None, _ptr(counts),
+                           _ptr(bp))
+        t = C.c_uint64()
+        check(load().rgl_server_submit(self._h, C.byref(req), C.byref(t)))
+        self._live[t.value] = (keep, counts, bp)
+        return t.value
+
+    def wait(self, ticket, timeout_ms=60_000):
+        """Returns (counts uint32[D], overlap_bp uint64[D] or None, info dict)."""
+        info = _lib.RequestInfo()
+        check(load().rgl_server_wait(self._h, ticket, timeout_ms, C.byref(info)))
+        _, counts, bp = self._live.pop(ticket)
+        if info.status:
+            raise _lib.RiggleError(info.status, "request failed")
+        return counts, bp, info.as_dict()
+
+    def stats(self):
+        st = _lib.ServerStats()
+        check(load().rgl_server_get_stats(self._h, C.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self):
+        check(load().rgl_server_reset_stats(self._h))
+
+    def close(self):
+        if self._h:
+            load().rgl_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class DeviceBatch:
     """A file-major query batch whose intervals are in device memory (rgl_batch): block b holds
     intervals [offsets[b], offsets[b+1]) on shard shards[b]; rows[b] (optional) is their file."""

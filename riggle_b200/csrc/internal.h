@@ -115,4 +115,16 @@ struct SynthTables {
 };
 const SynthTables& synth_tables();
 
+// ---- query contexts, for the request server --------------------------------------------------
+cudaStream_t context_stream(rgl_context* c);
+int context_reserve_rows(rgl_context* c, uint64_t max_intervals, uint32_t max_rows, uint32_t max_blocks);
+// One batch with rows taken from the blocks (interval sids ignored); asynchronous on the context
+// stream.  off holds nblk + 1 element offsets into d_iv.
+int enqueue_block_rows(rgl_context* c, uint32_t num_rows, uint32_t nblk, const uint32_t* shards, const uint32_t* rows,
+                       const uint64_t* off, const rgl_interval* d_iv, const rgl_query_opts* q, uint32_t* d_counts,
+                       unsigned long long* d_bp);
+// Error bits of the last run, read after the stream has been synchronised.
+int context_errors(rgl_context* c);
+uint32_t context_last_launches(rgl_context* c);
+
 }  // namespace rgl

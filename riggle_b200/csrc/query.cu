@@ -98,7 +98,8 @@ __device__ __forceinline__ uint32_t pp_layer(const uint2* __restrict__ pos, uint
 // ---- 1. keys ------------------------------------------------------------------------------------
 __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, const uint64_t* __restrict__ blk_off,
                               const uint32_t* __restrict__ blk_shard, const uint32_t* __restrict__ blk_row,
-                              uint32_t nblk, uint32_t rows, uint32_t row_base, uint64_t* __restrict__ key, uint32_t* __restrict__ val, uint64_t* __restrict__ ekey,
+                              int row_from_block, uint32_t nblk, uint32_t rows, uint32_t row_base,
+                              uint64_t* __restrict__ key, uint32_t* __restrict__ val, uint64_t* __restrict__ ekey,
                               uint32_t* __restrict__ err) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -108,10 +109,12 @@ __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, c
         if (blk_off[m] <= i) lo = m; else hi = m;
     }
     const uint32_t* w = reinterpret_cast<const uint32_t*>(iv) + 3ull * i;
-    uint32_t s = w[0], e = w[1], q = w[2] - row_base;  // rows below row_base wrap to >= rows
+    // the row is the interval's sid, or with row_from_block its block's row (sid ignored)
+    const uint32_t row = row_from_block ? blk_row[lo] : w[2];
+    uint32_t s = w[0], e = w[1], q = row - row_base;  // rows below row_base wrap to >= rows
     uint32_t bad = 0;
     if (s >= e) bad |= ERR_BAD_INTERVAL;
-    if (q >= rows || (blk_row && w[2] != blk_row[lo])) { bad |= ERR_BAD_ROW; q = 0; }
+    if (q >= rows || (blk_row && row != blk_row[lo])) { bad |= ERR_BAD_ROW; q = 0; }
     if (bad) atomicOr(err, bad);
     uint64_t seg = (uint64_t)blk_shard[lo] * rows + q;
     key[i] = (seg << 32) | s;
@@ -898,6 +901,7 @@ struct PipeIn {
     const uint64_t* blk_off;
     const uint32_t* blk_shard;
     const uint32_t* blk_row;  // optional: the row every interval of the block must carry
+    int row_from_block = 0;   // 1: rows come from blk_row, interval sids are ignored
 };
 
 // What a run does besides the sweep: the single-call entry points zero their rows, reset the error
@@ -957,8 +961,8 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
 
     if (ev) RGL_CUDA(cudaEventRecord(c->ev[0], st));
     uint32_t launches = 0;
-    k_expand_keys<<<grid_for(n, 256), 256, 0, st>>>(n, in.iv, in.blk_off, in.blk_shard, in.blk_row, in.nblk, rows,
-                                                    in.row_base,
+    k_expand_keys<<<grid_for(n, 256), 256, 0, st>>>(n, in.iv, in.blk_off, in.blk_shard, in.blk_row,
+                                                    in.row_from_block, in.nblk, rows, in.row_base,
                                                     c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
                                                     c->ekey_a.as<uint64_t>(), d_small);
     launches++;
@@ -1283,6 +1287,58 @@ std::vector<uint64_t> batch_key(rgl_context* c, const rgl_batch* b, const rgl_ba
 }
 
 }  // namespace
+
+namespace rgl {
+
+cudaStream_t context_stream(rgl_context* c) { return c->stream; }
+
+int context_reserve_rows(rgl_context* c, uint64_t max_intervals, uint32_t max_rows, uint32_t max_blocks) {
+    RGL_CUDA(cudaSetDevice(c->idx->device));
+    return ensure_workspace(c, max_intervals, max_rows, max_blocks);
+}
+
+// One batch whose intervals are already on the device, rows taken from the blocks (interval sids are
+// ignored), as a single pipeline run: zero the num_rows x D outputs, sweep, error word to the host.
+// Asynchronous on the context stream; the caller synchronises and then calls context_errors.
+int enqueue_block_rows(rgl_context* c, uint32_t num_rows, uint32_t nblk, const uint32_t* shards, const uint32_t* rows,
+                       const uint64_t* off, const rgl_interval* d_iv, const rgl_query_opts* q, uint32_t* d_counts,
+                       unsigned long long* d_bp) {
+    cudaStream_t st = c->stream;
+    const uint32_t D = c->idx->num_sources;
+    for (uint32_t i = 0; i < nblk; i++)
+        if (shards[i] >= c->idx->num_shards || rows[i] >= num_rows)
+            return fail(RGL_ERR_INVALID_ARGUMENT, "block shard or row out of range");
+    const uint64_t n = nblk ? off[nblk] - off[0] : 0;
+    RGL_TRY(ensure_workspace(c, n, 0, nblk));
+    std::vector<uint64_t> rel(nblk + 1);
+    for (uint32_t i = 0; i <= nblk; i++) rel[i] = off[i] - off[0];
+    std::vector<uint32_t> sr(2ull * nblk + 2, 0);
+    for (uint32_t i = 0; i < nblk; i++) {
+        sr[i] = shards[i];
+        sr[nblk + 1 + i] = rows[i];
+    }
+    RGL_TRY(c->bt_off.ensure(rel.size() * 8 + 8));
+    RGL_TRY(c->bt_shard.ensure(sr.size() * 4 + 4));
+    RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, rel.data(), rel.size() * 8, cudaMemcpyHostToDevice, st));
+    RGL_CUDA(cudaMemcpyAsync(c->bt_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
+    // the interval copies and table uploads above are ordered before the pipeline on this stream
+    RGL_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)num_rows * D * 4, st));
+    if (d_bp) RGL_CUDA(cudaMemsetAsync(d_bp, 0, (size_t)num_rows * D * 8, st));
+    PipeIn in{d_iv + off[0], n, num_rows, 0, nblk, c->bt_off.as<uint64_t>(), c->bt_shard.as<uint32_t>(),
+              c->bt_shard.as<uint32_t>() + nblk + 1, 1};
+    PipeMode m;
+    m.zero_out = false;
+    // the table uploads read pageable vectors that die here: an asynchronous copy from pageable
+    // memory has staged its source before it returns
+    return run_pipeline(c, in, q, d_counts, d_bp, nullptr, m);
+}
+
+// After the stream has been synchronised: the error bits of the last run.
+int context_errors(rgl_context* c) { return finish(c, pick_launch(nullptr), nullptr); }
+
+uint32_t context_last_launches(rgl_context* c) { return c->last_launches; }
+
+}  // namespace rgl
 
 extern "C" {
 

@@ -1,0 +1,373 @@
+// Request server: continuous batching of query files against a resident index.
+//
+// Worker threads each own a query context (its own CUDA stream and workspace), a device staging
+// buffer for the intervals of one batch and page-locked output rows.  An idle worker takes the
+// oldest pending requests that fit its capacity (intervals and rows) as one batch: one host-to-device
+// copy per request, one pipeline run with the rows taken from the blocks, one device-to-host copy of
+// the batch's count and overlap rows, then the rows are handed to their requests.  With several
+// workers, requests that arrive while a batch is on the GPU start on another stream at once, so
+// their work overlaps on the device.  Workers are admitted by free device memory at creation: each
+// reserves its full workspace up front, so a running server never allocates device memory.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <memory>
+#include <thread>
+#include <unordered_map>
+
+#include "internal.h"
+
+namespace rgl {
+namespace {
+
+struct Req {
+    rgl_request r;
+    std::vector<uint32_t> shards;
+    std::vector<uint64_t> offsets;
+    uint64_t n = 0;
+    uint64_t ticket = 0;
+    double t_submit = 0, t_start = 0, t_done = 0;
+    int status = RGL_OK;
+    bool done = false;
+    uint32_t batch_requests = 0;
+    uint64_t batch_intervals = 0;
+};
+
+struct Worker {
+    rgl_context* ctx = nullptr;
+    DevBuf stage, dc, dbp;
+    uint32_t* h_counts = nullptr;
+    uint64_t* h_bp = nullptr;
+    std::thread th;
+};
+
+}  // namespace
+}  // namespace rgl
+
+using namespace rgl;
+
+struct rgl_server {
+    rgl_index* idx = nullptr;
+    int device = 0;
+    uint32_t D = 0;
+    rgl_server_opts o{};
+    bool with_bp = true;
+    std::chrono::steady_clock::time_point t0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Req*> pending;
+    uint64_t pending_n = 0;
+    std::unordered_map<uint64_t, Req*> reqs;
+    uint64_t next_ticket = 1;
+    bool stop = false;
+    std::vector<std::unique_ptr<Worker>> workers;
+    double worker_bytes = 0;
+    // stats
+    uint64_t submitted = 0, completed = 0, failed = 0, batches = 0, intervals = 0, batch_req_sum = 0;
+    std::vector<double> lat_ms;
+    double first_submit = -1, last_done = 0;
+
+    double now() const {
+        return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+};
+
+namespace {
+
+// One batch on worker W: copies, pipeline, results.  Returns the batch status.
+int run_batch(rgl_server* S, Worker* W, const std::vector<Req*>& batch) {
+    rgl_context* c = W->ctx;
+    cudaStream_t st = context_stream(c);
+    const uint32_t R = (uint32_t)batch.size();
+    std::vector<uint32_t> shards, rows;
+    std::vector<uint64_t> off(1, 0);
+    uint64_t at = 0;
+    for (uint32_t j = 0; j < R; j++) {
+        const Req* q = batch[j];
+        if (q->n) {
+            RGL_CUDA(cudaMemcpyAsync(W->stage.as<rgl_interval>() + at, q->r.intervals + q->offsets[0],
+                                     q->n * sizeof(rgl_interval), cudaMemcpyHostToDevice, st));
+        }
+        for (size_t b = 0; b + 1 < q->offsets.size(); b++) {
+            const uint64_t cnt = q->offsets[b + 1] - q->offsets[b];
+            if (!cnt) continue;
+            shards.push_back(q->shards[b]);
+            rows.push_back(j);
+            at += cnt;
+            off.push_back(at);
+        }
+    }
+    unsigned long long* d_bp = S->with_bp ? W->dbp.as<unsigned long long>() : nullptr;
+    RGL_TRY(enqueue_block_rows(c, R, (uint32_t)shards.size(), shards.data(), rows.data(), off.data(),
+                               W->stage.as<rgl_interval>(), &S->o.query, W->dc.as<uint32_t>(), d_bp));
+    RGL_CUDA(cudaMemcpyAsync(W->h_counts, W->dc.p, (size_t)R * S->D * 4, cudaMemcpyDeviceToHost, st));
+    if (d_bp) RGL_CUDA(cudaMemcpyAsync(W->h_bp, W->dbp.p, (size_t)R * S->D * 8, cudaMemcpyDeviceToHost, st));
+    RGL_CUDA(cudaStreamSynchronize(st));
+    RGL_TRY(context_errors(c));
+    for (uint32_t j = 0; j < R; j++) {
+        const Req* q = batch[j];
+        if (q->r.counts) std::memcpy(q->r.counts, W->h_counts + (size_t)j * S->D, S->D * 4ull);
+        if (q->r.overlap_bp) {
+            if (d_bp) std::memcpy(q->r.overlap_bp, W->h_bp + (size_t)j * S->D, S->D * 8ull);
+            else std::memset(q->r.overlap_bp, 0, S->D * 8ull);
+        }
+    }
+    return RGL_OK;
+}
+
+void complete(rgl_server* S, const std::vector<Req*>& batch, const std::vector<int>& status, uint64_t n) {
+    std::lock_guard<std::mutex> lk(S->mu);
+    const double t = S->now();
+    S->batches++;
+    S->batch_req_sum += batch.size();
+    for (size_t j = 0; j < batch.size(); j++) {
+        Req* q = batch[j];
+        q->status = status[j];
+        q->t_done = t;
+        q->done = true;
+        q->batch_requests = (uint32_t)batch.size();
+        q->batch_intervals = n;
+        if (status[j] == RGL_OK) {
+            S->completed++;
+            S->intervals += q->n;
+            S->lat_ms.push_back((t - q->t_submit) * 1e3);
+        } else {
+            S->failed++;
+        }
+        S->last_done = std::max(S->last_done, t);
+    }
+}
+
+void worker_main(rgl_server* S, Worker* W) {
+    cudaSetDevice(S->device);
+    std::vector<Req*> batch;
+    for (;;) {
+        uint64_t n = 0;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty(); });
+            if (S->pending.empty()) return;  // stop requested and the queue is drained
+            batch.clear();
+            while (!S->pending.empty() && batch.size() < S->o.max_batch_requests) {
+                Req* q = S->pending.front();
+                if (!batch.empty() && n + q->n > S->o.batch_intervals) break;
+                batch.push_back(q);
+                n += q->n;
+                S->pending.pop_front();
+            }
+            S->pending_n -= n;
+            const double t = S->now();
+            for (Req* q : batch) q->t_start = t;
+        }
+        std::vector<int> status(batch.size(), RGL_OK);
+        int s = run_batch(S, W, batch);
+        if (s != RGL_OK && batch.size() > 1) {
+            // isolate the failing request: every request of the batch again on its own
+            std::vector<Req*> one(1);
+            for (size_t j = 0; j < batch.size(); j++) {
+                one[0] = batch[j];
+                status[j] = run_batch(S, W, one);
+            }
+        } else if (s != RGL_OK) {
+            status[0] = s;
+        }
+        complete(S, batch, status, n);
+        S->cv_done.notify_all();
+    }
+}
+
+void destroy_worker(Worker* W) {
+    if (W->ctx) rgl_context_destroy(W->ctx);
+    W->stage.release();
+    W->dc.release();
+    W->dbp.release();
+    if (W->h_counts) cudaFreeHost(W->h_counts);
+    if (W->h_bp) cudaFreeHost(W->h_bp);
+}
+
+int make_worker(rgl_server* S, Worker* W) {
+    RGL_TRY(rgl_context_create(S->idx, nullptr, &W->ctx));
+    const uint64_t cap = S->o.batch_intervals;
+    const uint32_t R = S->o.max_batch_requests;
+    // blocks per batch: at most one per (request, shard) for requests built from the shard list;
+    // larger block tables grow the workspace on demand
+    RGL_TRY(context_reserve_rows(W->ctx, cap, 0, R * std::max<uint32_t>(S->idx->num_shards, 1)));
+    RGL_TRY(W->stage.ensure(cap * sizeof(rgl_interval)));
+    RGL_TRY(W->dc.ensure((size_t)R * S->D * 4 + 16));
+    RGL_TRY(W->dbp.ensure((size_t)R * S->D * 8 + 16));
+    RGL_CUDA(cudaMallocHost(&W->h_counts, (size_t)R * S->D * 4 + 16));
+    RGL_CUDA(cudaMallocHost(&W->h_bp, (size_t)R * S->D * 8 + 16));
+    return RGL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rgl_server_create(rgl_index* index, const rgl_server_opts* opts, rgl_server** out) {
+    clear_error();
+    if (!index || !out) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    auto S = std::make_unique<rgl_server>();
+    S->idx = index;
+    S->device = index->device;
+    S->D = index->num_sources;
+    S->t0 = std::chrono::steady_clock::now();
+    if (opts) S->o = *opts;
+    if (!S->o.workers) S->o.workers = 3;
+    if (!S->o.max_batch_requests) S->o.max_batch_requests = 256;
+    if (!S->o.batch_intervals) S->o.batch_intervals = 1ull << 23;
+    if (!S->o.hbm_reserve_bytes) S->o.hbm_reserve_bytes = 4ull << 30;
+    if (!S->o.max_pending_intervals) S->o.max_pending_intervals = 1ull << 28;
+    S->o.batch_intervals = std::min<uint64_t>(S->o.batch_intervals, (1ull << 31) - 1);
+    S->with_bp = !(S->o.query.flags & RGL_QF_NO_OVERLAP);
+    RGL_CUDA(cudaSetDevice(S->device));
+    // admission of workers by free device memory: the first worker's reservation is the unit
+    for (uint32_t w = 0; w < S->o.workers; w++) {
+        size_t free0 = 0, total = 0;
+        RGL_CUDA(cudaMemGetInfo(&free0, &total));
+        if (w > 0 && (double)free0 < S->worker_bytes + (double)S->o.hbm_reserve_bytes) break;
+        auto W = std::make_unique<Worker>();
+        int s = make_worker(S.get(), W.get());
+        if (s != RGL_OK) {
+            destroy_worker(W.get());
+            if (w == 0) {
+                for (auto& x : S->workers) destroy_worker(x.get());
+                return s;
+            }
+            clear_error();
+            break;
+        }
+        size_t free1 = 0;
+        RGL_CUDA(cudaMemGetInfo(&free1, &total));
+        if (w == 0) S->worker_bytes = (double)(free0 > free1 ? free0 - free1 : 0);
+        S->workers.push_back(std::move(W));
+    }
+    rgl_server* raw = S.release();
+    for (auto& W : raw->workers) W->th = std::thread(worker_main, raw, W.get());
+    *out = raw;
+    return RGL_OK;
+}
+
+int rgl_server_submit(rgl_server* S, const rgl_request* req, uint64_t* ticket) {
+    clear_error();
+    if (!S || !req || !ticket) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    if (req->num_blocks && (!req->block_shards || !req->block_offsets || !req->intervals))
+        return fail(RGL_ERR_INVALID_ARGUMENT, "incomplete request");
+    auto q = std::make_unique<Req>();
+    q->r = *req;
+    q->shards.assign(req->block_shards, req->block_shards + req->num_blocks);
+    q->offsets.assign(req->block_offsets, req->block_offsets + req->num_blocks + 1);
+    if (!req->num_blocks) q->offsets.assign(1, 0);
+    for (uint32_t b = 0; b < req->num_blocks; b++) {
+        if (q->offsets[b + 1] < q->offsets[b]) return fail(RGL_ERR_INVALID_ARGUMENT, "block offsets must be non-decreasing");
+        if (q->shards[b] >= S->idx->num_shards) return fail(RGL_ERR_INVALID_ARGUMENT, "shard id out of range");
+    }
+    q->n = q->offsets.back() - q->offsets.front();
+    if (q->n > S->o.batch_intervals)
+        return fail(RGL_ERR_INVALID_ARGUMENT, "request larger than the server's batch_intervals");
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) return fail(RGL_ERR_INVALID_ARGUMENT, "server is stopping");
+    if (S->pending_n + q->n > S->o.max_pending_intervals)
+        return fail(RGL_ERR_OOM, "request queue full (max_pending_intervals)");
+    q->ticket = S->next_ticket++;
+    q->t_submit = S->now();
+    if (S->first_submit < 0) S->first_submit = q->t_submit;
+    S->submitted++;
+    S->pending_n += q->n;
+    *ticket = q->ticket;
+    Req* raw = q.release();
+    S->reqs[raw->ticket] = raw;
+    S->pending.push_back(raw);
+    S->cv_work.notify_one();
+    return RGL_OK;
+}
+
+int rgl_server_wait(rgl_server* S, uint64_t ticket, uint32_t timeout_ms, rgl_request_info* info) {
+    clear_error();
+    if (!S) return fail(RGL_ERR_INVALID_ARGUMENT, "null server");
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->reqs.find(ticket);
+    if (it == S->reqs.end()) return fail(RGL_ERR_INVALID_ARGUMENT, "unknown ticket");
+    Req* q = it->second;
+    if (!S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return q->done; }))
+        return fail(RGL_ERR_TIMEOUT, "request not done yet");
+    if (info) {
+        info->status = q->status;
+        info->batch_requests = q->batch_requests;
+        info->batch_intervals = q->batch_intervals;
+        info->intervals = q->n;
+        info->submit_s = q->t_submit;
+        info->start_s = q->t_start;
+        info->done_s = q->t_done;
+    }
+    S->reqs.erase(it);
+    delete q;
+    return RGL_OK;
+}
+
+int rgl_server_get_stats(rgl_server* S, rgl_server_stats* out) {
+    if (!S || !out) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(S->mu);
+    std::memset(out, 0, sizeof(*out));
+    out->submitted = S->submitted;
+    out->completed = S->completed;
+    out->failed = S->failed;
+    out->batches = S->batches;
+    out->intervals = S->intervals;
+    out->workers = (uint32_t)S->workers.size();
+    out->pending = (uint32_t)S->pending.size();
+    out->mean_batch_requests = S->batches ? (double)S->batch_req_sum / (double)S->batches : 0.0;
+    out->first_submit_s = S->first_submit < 0 ? 0 : S->first_submit;
+    out->last_done_s = S->last_done;
+    out->worker_bytes = S->worker_bytes;
+    if (!S->lat_ms.empty()) {
+        std::vector<double> v(S->lat_ms);
+        std::sort(v.begin(), v.end());
+        // nearest-rank percentiles
+        auto pct = [&](double p) {
+            size_t k = (size_t)std::ceil(p / 100.0 * (double)v.size());
+            return v[std::min(v.size(), std::max<size_t>(k, 1)) - 1];
+        };
+        out->p50_ms = pct(50);
+        out->p99_ms = pct(99);
+        out->p999_ms = pct(99.9);
+        out->max_ms = v.back();
+        double sum = 0;
+        for (double x : v) sum += x;
+        out->mean_ms = sum / (double)v.size();
+    }
+    return RGL_OK;
+}
+
+int rgl_server_reset_stats(rgl_server* S) {
+    if (!S) return fail(RGL_ERR_INVALID_ARGUMENT, "null server");
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->submitted = S->completed = S->failed = S->batches = S->intervals = S->batch_req_sum = 0;
+    S->lat_ms.clear();
+    S->first_submit = -1;
+    S->last_done = 0;
+    return RGL_OK;
+}
+
+int rgl_server_destroy(rgl_server* S) {
+    clear_error();
+    if (!S) return RGL_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+    }
+    S->cv_work.notify_all();
+    for (auto& W : S->workers)
+        if (W->th.joinable()) W->th.join();
+    cudaSetDevice(S->device);
+    for (auto& W : S->workers) destroy_worker(W.get());
+    for (auto& kv : S->reqs) delete kv.second;
+    delete S;
+    return RGL_OK;
+}
+
+}  // extern "C"
