@@ -152,8 +152,8 @@ __global__ void k_seg_begin(uint32_t n, const uint32_t* __restrict__ segflag, co
     if (i == n - 1) seg_begin[segnum[i]] = n;
 }
 
-// Bin width per segment: about four bins per query, at least 64 bp; tab_len = nbins + 1 for the
-// segments that have a rank-difference range, 0 for the rest.
+// Bin width per segment: about four bins per query, at least 64 bp.  A segment with a rank-
+// difference range gets nbins + 1 table entries, any other segment a single entry (see k_tab_place).
 __global__ void k_seg_tabsize(uint32_t n, const uint32_t* __restrict__ segnum, const uint32_t* __restrict__ seg_begin,
                               const uint32_t* __restrict__ need, const uint32_t* __restrict__ ends_s,
                               SegTab* __restrict__ tabs, uint32_t* __restrict__ tab_len) {
@@ -167,7 +167,7 @@ __global__ void k_seg_tabsize(uint32_t n, const uint32_t* __restrict__ segnum, c
     const uint32_t beg = seg_begin[sgi], end = seg_begin[sgi + 1];
     if (!need[sgi]) {  // no range of this segment is swept by rank differences
         tabs[sgi] = SegTab{beg, end, 6, 0, 0, 0};
-        tab_len[sgi] = 0;
+        tab_len[sgi] = 1;
         return;
     }
     const uint64_t extent = (uint64_t)ends_s[end - 1] + 1;  // covers every start and end of the segment
@@ -175,40 +175,37 @@ __global__ void k_seg_tabsize(uint32_t n, const uint32_t* __restrict__ segnum, c
     uint32_t shift = want > 1 ? 63u - __clzll(want) : 0u;
     if (shift < 6) shift = 6;
     if (shift > 31) shift = 31;
-    const uint32_t nbins = (uint32_t)(extent >> shift) + 1;
+    const uint32_t nbins = (uint32_t)(extent >> shift) + 1;  // <= 8 (end - beg): tables fit 10 n entries
     tabs[sgi] = SegTab{beg, end, shift, nbins, 0, 0};
     tab_len[sgi] = nbins + 1;
 }
 
-// One thread per table entry (grid-stride over all segments' entries): the entry's segment is found
-// by binary search over the table offsets, then tab_s[b] = #starts < b << shift and
-// tab_e[b] = #ends < b << shift within the segment.
-__global__ void k_seg_tabfill(uint32_t n, const uint32_t* __restrict__ segnum, SegTab* __restrict__ tabs,
-                              const uint32_t* __restrict__ tab_off, const uint32_t* __restrict__ starts,
-                              const uint32_t* __restrict__ ends_s, uint32_t* __restrict__ tab_s,
-                              uint32_t* __restrict__ tab_e) {
-    const uint32_t nseg = segnum[n - 1];
-    const uint32_t total = tab_off[nseg];
-    for (uint32_t e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
-        uint32_t lo = 0, hi = nseg - 1;  // last segment with tab_off <= e
-        while (lo < hi) {
-            uint32_t m = (lo + hi + 1) >> 1;
-            if (__ldg(tab_off + m) <= e) lo = m; else hi = m - 1;
-        }
-        const SegTab t = tabs[lo];
-        const uint32_t b = e - __ldg(tab_off + lo);
-        if (b == 0) tabs[lo].off = e;
-        const uint64_t x = (uint64_t)b << t.shift;
-        uint32_t rs, re;
-        if (x > 0xFFFFFFFFull) {
-            rs = re = t.end;
-        } else {
-            rs = lb_u32(starts, t.beg, t.end, (uint32_t)x);
-            re = lb_u32(ends_s, t.beg, t.end, (uint32_t)x);
-        }
-        tab_s[e] = rs;
-        tab_e[e] = re;
+// Rank tables by counting.  Entry b of a segment's table must hold beg + #{elements with bin < b}.
+// With the per-bin counts placed one entry to the right (bin b at entry b + 1) and every other
+// segment's single entry holding its element count, an inclusive scan over all segments' entries
+// yields exactly that: everything before a segment's first entry sums to its `beg`.
+__global__ void k_tab_place(uint32_t n, const uint32_t* __restrict__ segnum, SegTab* __restrict__ tabs,
+                            const uint32_t* __restrict__ tab_off, uint32_t* __restrict__ xs, uint32_t* __restrict__ xe) {
+    const uint32_t sgi = blockIdx.x * blockDim.x + threadIdx.x;
+    if (sgi >= segnum[n - 1]) return;
+    const uint32_t off = tab_off[sgi];
+    tabs[sgi].off = off;
+    const SegTab t = tabs[sgi];
+    if (t.nbins == 0) {
+        xs[off] = t.end - t.beg;
+        xe[off] = t.end - t.beg;
     }
+}
+
+__global__ void k_tab_count(uint32_t n, const uint32_t* __restrict__ segnum, const SegTab* __restrict__ tabs,
+                            const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends_s,
+                            uint32_t* __restrict__ xs, uint32_t* __restrict__ xe) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const SegTab t = tabs[segnum[j] - 1];
+    if (t.nbins == 0) return;
+    atomicAdd(xs + t.off + (starts[j] >> t.shift) + 1, 1u);
+    atomicAdd(xe + t.off + (ends_s[j] >> t.shift) + 1, 1u);
 }
 
 // ---- 4. K1 partition -----------------------------------------------------------------------------
@@ -694,7 +691,7 @@ struct rgl_context {
     DevBuf iv, blk_off, blk_shard, key_a, key_b, val_a, val_b, ekey_a, ekey_b;
     DevBuf starts, ends, seg, segflag, segnum, seg_begin, ps_in, pe_in, ps, pe;
     DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp, item_r0;
-    DevBuf segtab, tab_len, tab_off, tab_s, tab_e;
+    DevBuf segtab, tab_len, tab_off, tab_s, tab_e, tab_xs, tab_xe;
     DevBuf cl, pc, method, ulen, plen, ppos, psegs, item_t0, seg_need;
     DevBuf bt_off, bt_shard, acc;  // batched form: sub-batch block tables (offsets; shards then rows), stats
     uint32_t* h_small = nullptr;  // pinned mirror of `small`
@@ -732,8 +729,12 @@ namespace {
 // Work items whose first range is precomputed; items beyond it search the range list themselves.
 constexpr uint64_t kItemCap = 1ull << 22;
 
+// Query intervals per pipeline run: the rank tables (up to 10 entries per interval) use 31-bit offsets.
+constexpr uint64_t kMaxRunIntervals = 200000000ull;
+
 int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     rgl_index* idx = c->idx;
+    if (n > kMaxRunIntervals) return fail(RGL_ERR_INVALID_ARGUMENT, "at most 200,000,000 query intervals per run");
     const uint64_t ns = std::max<uint32_t>(idx->num_slots, 1);
     const uint64_t tot = n * ns;
     RGL_TRY(c->iv.ensure(n * sizeof(rgl_interval) + 16));
@@ -779,6 +780,8 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     RGL_TRY(c->tab_off.ensure((n + 2) * 4));
     RGL_TRY(c->tab_s.ensure((10 * n + 16) * 4));
     RGL_TRY(c->tab_e.ensure((10 * n + 16) * 4));
+    RGL_TRY(c->tab_xs.ensure((10 * n + 16) * 4));
+    RGL_TRY(c->tab_xe.ensure((10 * n + 16) * 4));
     RGL_TRY(c->acc.ensure(64));
     // CUB temporary storage: the maximum over every primitive used, at these sizes.
     size_t need = 0, b = 0;
@@ -790,6 +793,8 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     cub::DeviceRadixSort::SortKeys(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nn, 0, 64, c->stream);
     need = std::max(need, b);
     cub::DeviceScan::InclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, nn, c->stream);
+    need = std::max(need, b);
+    cub::DeviceScan::InclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)(10 * n + 16), c->stream);
     need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nn + 1, c->stream);
     need = std::max(need, b);
@@ -816,7 +821,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
                       &c->ends, &c->seg, &c->segflag, &c->segnum, &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps,
                       &c->pe, &c->lo, &c->hi, &c->maxhi, &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos,
                       &c->cub_tmp, &c->small, &c->item_r0, &c->item_t0, &c->segtab, &c->tab_len, &c->tab_off,
-                      &c->tab_s, &c->tab_e, &c->cl, &c->pc, &c->method, &c->ulen, &c->plen, &c->ppos, &c->psegs,
+                      &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->cl, &c->pc, &c->method, &c->ulen, &c->plen, &c->ppos, &c->psegs,
                       &c->seg_need, &c->acc})
         sig = (sig ^ (uint64_t)(uintptr_t)b->p ^ ((uint64_t)b->cap << 17)) * 1099511628211ull;
     c->ws_sig = sig;
@@ -1029,15 +1034,27 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                                            c->seg_need.as<uint32_t>());
     // rank tables of the query segments that have a rank-difference range
     k_seg_tabsize<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->seg_begin.as<uint32_t>(),
-                                                        c->seg_need.as<uint32_t>(), c->ends.as<uint32_t>(), c->segtab.as<SegTab>(),
-                                                        c->tab_len.as<uint32_t>());
+                                                        c->seg_need.as<uint32_t>(), c->ends.as<uint32_t>(),
+                                                        c->segtab.as<SegTab>(), c->tab_len.as<uint32_t>());
     tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->tab_len.as<uint32_t>(), c->tab_off.as<uint32_t>(),
                                            (int)n + 1, st));
-    k_seg_tabfill<<<(unsigned)std::min<uint64_t>((10 * n + 255) / 256, (uint64_t)c->num_sms * 16), 256, 0, st>>>(
-        n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(), c->tab_off.as<uint32_t>(), c->starts.as<uint32_t>(),
-        c->ends.as<uint32_t>(), c->tab_s.as<uint32_t>(), c->tab_e.as<uint32_t>());
-    launches += 2;
+    const uint64_t tab_cap = 10ull * n + 16;
+    RGL_CUDA(cudaMemsetAsync(c->tab_xs.p, 0, tab_cap * 4, st));
+    RGL_CUDA(cudaMemsetAsync(c->tab_xe.p, 0, tab_cap * 4, st));
+    k_tab_place<<<grid_for(n, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
+                                                  c->tab_off.as<uint32_t>(), c->tab_xs.as<uint32_t>(),
+                                                  c->tab_xe.as<uint32_t>());
+    k_tab_count<<<grid_for(n, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
+                                                  c->starts.as<uint32_t>(), c->ends.as<uint32_t>(),
+                                                  c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>());
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tb, c->tab_xs.as<uint32_t>(), c->tab_s.as<uint32_t>(),
+                                           (int)tab_cap, st));
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tb, c->tab_xe.as<uint32_t>(), c->tab_e.as<uint32_t>(),
+                                           (int)tab_cap, st));
+    launches += 3;
     k_pair_len<<<grid_for(tot + 1, 256), 256, 0, st>>>(n, ns, rows, c->seg.as<uint32_t>(), idx->d_slot,
                                                        idx->d_layers, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
                                                        c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
@@ -1392,7 +1409,7 @@ int rgl_context_destroy(rgl_context* c) {
                       &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps, &c->pe, &c->lo, &c->hi, &c->maxhi,
                       &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos, &c->cub_tmp, &c->small,
                       &c->out_counts, &c->out_bp, &c->item_r0,
-                      &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e,
+                      &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe,
                       &c->cl, &c->pc, &c->method, &c->ulen, &c->plen, &c->ppos, &c->psegs, &c->item_t0,
                       &c->seg_need, &c->bt_off, &c->bt_shard, &c->acc, &c->gc.t_off, &c->gc.t_shard};
     if (c->gc.exec) cudaGraphExecDestroy(c->gc.exec);
@@ -1507,7 +1524,7 @@ int rgl_query_batch_device(rgl_context* c, const rgl_batch* b, const rgl_batch_o
     if (b->num_blocks && (!b->block_offsets || !b->block_shards || !b->d_intervals))
         return fail(RGL_ERR_INVALID_ARGUMENT, "incomplete batch");
     RGL_CUDA(cudaSetDevice(c->idx->device));
-    const uint64_t sub = (o && o->sub_batch) ? std::min<uint64_t>(o->sub_batch, (1ull << 31) - 1) : (1ull << 24);
+    const uint64_t sub = (o && o->sub_batch) ? std::min<uint64_t>(o->sub_batch, kMaxRunIntervals) : (1ull << 24);
     rgl_query_opts q;
     const Launch L = batch_launch(c, o, &q);
     const bool graph = o && (o->flags & RGL_BF_GRAPH);
@@ -1607,7 +1624,7 @@ int rgl_query_batch_host(rgl_context* c, const rgl_batch* b, const rgl_interval*
     if (b->num_blocks && (!b->block_offsets || !b->block_shards || !h_intervals))
         return fail(RGL_ERR_INVALID_ARGUMENT, "incomplete batch");
     RGL_CUDA(cudaSetDevice(c->idx->device));
-    const uint64_t sub = (o && o->sub_batch) ? std::min<uint64_t>(o->sub_batch, (1ull << 31) - 1) : (1ull << 24);
+    const uint64_t sub = (o && o->sub_batch) ? std::min<uint64_t>(o->sub_batch, kMaxRunIntervals) : (1ull << 24);
     rgl_query_opts q;
     const Launch L = batch_launch(c, o, &q);
     const bool want_bp = overlap_bp && !(q.flags & RGL_QF_NO_OVERLAP);
@@ -1698,7 +1715,7 @@ int rgl_batch_autotune(rgl_context* c, const rgl_batch* b, uint64_t sub_batch, r
     if (!c || !b || !best) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
     RGL_CUDA(cudaSetDevice(c->idx->device));
     BatchPlan P;
-    const uint64_t sub = sub_batch ? std::min<uint64_t>(sub_batch, (1ull << 31) - 1) : (1ull << 24);
+    const uint64_t sub = sub_batch ? std::min<uint64_t>(sub_batch, kMaxRunIntervals) : (1ull << 24);
     RGL_TRY(plan_batch(c, b, sub, &P));
     if (P.subs.empty()) return fail(RGL_ERR_INVALID_ARGUMENT, "empty batch");
     size_t big = 0;

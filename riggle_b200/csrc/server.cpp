@@ -222,7 +222,7 @@ int rgl_server_create(rgl_index* index, const rgl_server_opts* opts, rgl_server*
     if (!S->o.batch_intervals) S->o.batch_intervals = 1ull << 23;
     if (!S->o.hbm_reserve_bytes) S->o.hbm_reserve_bytes = 4ull << 30;
     if (!S->o.max_pending_intervals) S->o.max_pending_intervals = 1ull << 28;
-    S->o.batch_intervals = std::min<uint64_t>(S->o.batch_intervals, (1ull << 31) - 1);
+    S->o.batch_intervals = std::min<uint64_t>(S->o.batch_intervals, 200000000ull);  // one pipeline run
     S->with_bp = !(S->o.query.flags & RGL_QF_NO_OVERLAP);
     RGL_CUDA(cudaSetDevice(S->device));
     // admission of workers by free device memory: the first worker's reservation is the unit
