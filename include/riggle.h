@@ -353,6 +353,20 @@ typedef struct rgl_pvalue_batch {
 int rgl_query_pvalues(rgl_moments* m, const rgl_pvalue_batch* batch, uint32_t bin_size, const uint32_t* counts,
                       const uint64_t* overlap_bp, double* p, double* llr, double* log_p, uint8_t* flags);
 
+/* The stats stage of the batched form, all on the device: compute_analytic_pvalues
+ * (src/tasks/query/pvalues.rs:22-77) for every (row, source) cell of a batch whose counts and overlap
+ * are in device memory (the outputs of rgl_query_batch_device), with the query length groups
+ * (build_query_chrom_data, src/fourier/moments.rs:138-177) built on the device from the batch's own
+ * intervals.  The group sums come from exact integer sums of lengths and squared lengths (one
+ * rounding each; the reference rounds sequentially, ~1e-15 relative apart).  shard_chrom maps index
+ * shard -> moment-store chromosome (UINT32_MAX: none); batch->block_rows is required.  Outputs are
+ * device arrays of num_rows x D (d_log_p may be NULL), written asynchronously on the context
+ * stream; *out_groups (optional, synchronises) receives the number of groups. */
+int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* moments, const rgl_batch* batch,
+                             const uint32_t* shard_chrom, uint32_t num_shards, uint32_t bin_size,
+                             const uint32_t* d_counts, const uint64_t* d_overlap_bp, double* d_p, double* d_llr,
+                             double* d_log_p, uint8_t* d_flags, uint64_t* out_groups);
+
 /* ------------------------------------------------------------------------------------------ */
 /* Seeded synthetic workloads (no counterpart in the reference; used by tests and benchmarks).  */
 /* SplitMix64 counter streams (Steele, Lea & Flood 2014) drive identical host and device        */

@@ -11,6 +11,8 @@
 // lanes stride over the row's groups, accumulate mu, sigma^2 and mu_raw in FP64, reduce, and lane
 // 0 dispatches NB / Poisson, evaluates the LLR and the A&S 7.1.26 tail exactly as the reference
 // writes it (src/fourier/stats.rs:65-126).
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -155,6 +157,91 @@ __global__ void k_pvalues(uint32_t rows, uint32_t D, uint32_t C, const uint32_t*
     }
 }
 
+// ---- query length groups of a whole device-resident batch ------------------------------------
+// build_query_chrom_data (src/fourier/moments.rs:138-177) groups a file's lengths on one chromosome
+// by l_int = max(ceil(len / bin), 1) and sums s = (len / bin) / l_int and s^2.  Here every interval
+// of the batch gets the key (row * C + chrom) << 32 | l_int, the keys are sorted and each run is
+// reduced with exact integer sums of len and len^2, so that sum_s = sum_len / (bin * l_int) and
+// sum_s2 = sum_len2 / (bin * l_int)^2 carry one rounding each instead of the reference's sequential
+// f64 rounding (they agree to ~1e-15 relative).
+struct LenAgg {
+    unsigned long long cnt, s1, s2lo, s2hi;  // count, sum of len, sum of len^2 (128-bit)
+};
+struct LenAggOp {
+    __device__ __forceinline__ LenAgg operator()(const LenAgg& a, const LenAgg& b) const {
+        LenAgg r;
+        r.cnt = a.cnt + b.cnt;
+        r.s1 = a.s1 + b.s1;
+        r.s2lo = a.s2lo + b.s2lo;
+        r.s2hi = a.s2hi + b.s2hi + (r.s2lo < a.s2lo ? 1ull : 0ull);
+        return r;
+    }
+};
+struct LenToAgg {
+    __device__ __forceinline__ LenAgg operator()(uint32_t len) const {
+        const unsigned long long l = len;
+        return LenAgg{1ull, l, l * l, 0ull};  // len < 2^32: len^2 fits 64 bits
+    }
+};
+
+constexpr uint64_t kNoGroup = ~0ull;
+
+__global__ void k_group_keys(uint64_t n, const rgl_interval* __restrict__ iv, const uint64_t* __restrict__ blk_off,
+                             const uint32_t* __restrict__ blk_shard, const uint32_t* __restrict__ blk_row, uint32_t nblk,
+                             const uint32_t* __restrict__ shard_chrom, uint32_t nshards, uint32_t C,
+                             const uint64_t* __restrict__ n_bins, double bin, uint64_t* __restrict__ key,
+                             uint32_t* __restrict__ len_out) {
+    const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    uint32_t lo = 0, hi = nblk;  // last block with blk_off[b] <= j
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (blk_off[m] <= j) lo = m; else hi = m;
+    }
+    const rgl_interval v = iv[j];
+    const uint32_t sh = blk_shard[lo];
+    const uint32_t c = sh < nshards ? shard_chrom[sh] : 0xFFFFFFFFu;
+    uint64_t k = kNoGroup;
+    const uint32_t len = v.end > v.start ? v.end - v.start : 0u;
+    if (c < C && len) {
+        const double l = (double)len / bin;  // as build_query_chrom_data: lengths in bins, f64
+        const double ce = ceil(l);
+        const uint64_t li = ce < 1.0 ? 1ull : (uint64_t)ce;
+        // groups with l_int >= n_bins never meet a moment (src/io/momentstore.rs:66-79)
+        if (li < n_bins[c]) k = (((uint64_t)blk_row[lo] * C + c) << 32) | li;
+    }
+    key[j] = k;
+    len_out[j] = len;
+}
+
+// One thread per group: FP64 sums, the host-made slot table, and the per-row group offsets.
+__global__ void k_group_finish(const uint64_t* __restrict__ ukey, const LenAgg* __restrict__ agg,
+                               const uint32_t* __restrict__ num_runs, uint32_t rows, uint32_t C, double bin,
+                               const uint32_t* __restrict__ slot_tab, uint64_t slot_tab_len,
+                               QGroupDev* __restrict__ groups, uint64_t* __restrict__ g_off) {
+    const uint32_t runs = *num_runs;
+    // a trailing run of unusable intervals (key kNoGroup) sorts last and is dropped
+    const uint32_t ng = (runs && ukey[runs - 1] == kNoGroup) ? runs - 1 : runs;
+    const uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (g > ng) return;
+    if (g == ng) {  // rows after the last group's row
+        const uint32_t r0 = ng ? (uint32_t)((ukey[ng - 1] >> 32) / C) + 1 : 0;
+        for (uint32_t r = r0; r <= rows; r++) g_off[r] = ng;
+        return;
+    }
+    const uint64_t k = ukey[g];
+    const uint32_t rc = (uint32_t)(k >> 32), row = rc / C, chrom = rc % C;
+    const uint64_t li = k & 0xFFFFFFFFull;
+    const LenAgg a = agg[g];
+    const double den = bin * (double)li;
+    const double s2 = (double)a.s2hi * 18446744073709551616.0 + (double)a.s2lo;
+    groups[g] = QGroupDev{chrom, li < slot_tab_len ? slot_tab[li] : 0xFFFFFFFFu, (double)a.s1 / den,
+                          s2 / (den * den), (double)li, (double)a.cnt};
+    const uint32_t prev = g ? (uint32_t)((ukey[g - 1] >> 32) / C) : 0xFFFFFFFFu;
+    if (prev != row)  // rows (prev, row] start at this group
+        for (uint32_t r = (prev == 0xFFFFFFFFu ? 0 : prev + 1); r <= row; r++) g_off[r] = g;
+}
+
 }  // namespace rgl
 
 using namespace rgl;
@@ -167,6 +254,8 @@ struct rgl_moments {
     float2* d_mv = nullptr;
     uint32_t* d_len = nullptr;
     std::vector<uint32_t> len;  // host mirror of the per-(source, chromosome) table lengths
+    // batched stats: compact_index table (slot of every l_int below the largest n_bins) and scratch
+    DevBuf slot_tab, coff, key_a, key_b, len_a, len_b, ukey, agg, runs, groups, goff, tmp, nb;
 };
 
 namespace rgl {
@@ -285,6 +374,9 @@ int rgl_moments_destroy(rgl_moments* m) {
     clear_error();
     if (!m) return RGL_OK;
     cudaSetDevice(m->device);
+    for (DevBuf* b : {&m->slot_tab, &m->coff, &m->key_a, &m->key_b, &m->len_a, &m->len_b, &m->ukey, &m->agg,
+                      &m->runs, &m->groups, &m->goff, &m->tmp, &m->nb})
+        b->release();
     if (m->d_mv) cudaFree(m->d_mv);
     if (m->d_len) cudaFree(m->d_len);
     delete m;
@@ -394,6 +486,121 @@ int rgl_query_pvalues(rgl_moments* m, const rgl_pvalue_batch* b, uint32_t bin_si
     back(flags, d_f.p, cells);
     for (DevBuf* x : {&d_goff, &d_g, &d_coff, &d_cnt, &d_bp, &d_p, &d_llr, &d_lp, &d_f}) x->release();
     return s;
+}
+
+int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* m, const rgl_batch* b, const uint32_t* shard_chrom,
+                             uint32_t num_shards, uint32_t bin_size, const uint32_t* d_counts,
+                             const uint64_t* d_overlap_bp, double* d_p, double* d_llr, double* d_log_p,
+                             uint8_t* d_flags, uint64_t* out_groups) {
+    clear_error();
+    if (!ctx || !m || !b || !d_counts || !d_overlap_bp || !d_p || !d_llr || !d_flags || !bin_size ||
+        (num_shards && !shard_chrom))
+        return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    if (b->num_blocks && (!b->block_offsets || !b->block_shards || !b->d_intervals))
+        return fail(RGL_ERR_INVALID_ARGUMENT, "incomplete batch");
+    const uint32_t rows = b->num_rows, D = m->num_sources, C = m->num_chroms;
+    const uint64_t n = b->num_blocks ? b->block_offsets[b->num_blocks] - b->block_offsets[0] : 0;
+    if ((uint64_t)rows * C >= (1ull << 32)) return fail(RGL_ERR_INVALID_ARGUMENT, "num_rows x chromosomes must be < 2^32");
+    if (n >= (1ull << 31)) return fail(RGL_ERR_INVALID_ARGUMENT, "at most 2^31 - 1 intervals per call");
+    for (uint32_t i = 0; i < b->num_blocks; i++) {
+        if (b->block_offsets[i + 1] < b->block_offsets[i])
+            return fail(RGL_ERR_INVALID_ARGUMENT, "block offsets must be non-decreasing");
+        if (b->block_rows && b->block_rows[i] >= rows) return fail(RGL_ERR_INVALID_ARGUMENT, "block row >= num_rows");
+    }
+    if (!b->block_rows && b->num_blocks) return fail(RGL_ERR_INVALID_ARGUMENT, "batched p-values need block_rows");
+    if (!rows || !D) {
+        if (out_groups) *out_groups = 0;
+        return RGL_OK;
+    }
+    RGL_CUDA(cudaSetDevice(m->device));
+    cudaStream_t st = context_stream(ctx);
+    // slot table: compact_index(l) on the host with the reference's f64 ln, for every l below the
+    // largest chromosome's n_bins; slots past a chromosome's grid are rejected per group below
+    uint64_t lmax = 1;
+    for (uint32_t c = 0; c < C; c++) lmax = std::max(lmax, m->n_bins[c]);
+    if (m->slot_tab.cap < lmax * 4) {
+        std::vector<uint32_t> tab(lmax);
+        tab[0] = 0xFFFFFFFFu;
+        for (uint64_t l = 1; l < lmax; l++) tab[l] = (uint32_t)compact_index(l);
+        RGL_TRY(m->slot_tab.ensure(lmax * 4));
+        RGL_CUDA(cudaMemcpy(m->slot_tab.p, tab.data(), lmax * 4, cudaMemcpyHostToDevice));
+        RGL_TRY(m->coff.ensure(C * 8ull));
+        RGL_CUDA(cudaMemcpy(m->coff.p, m->chrom_off.data(), C * 8ull, cudaMemcpyHostToDevice));
+        RGL_TRY(m->nb.ensure(C * 8ull));
+        RGL_CUDA(cudaMemcpy(m->nb.p, m->n_bins.data(), C * 8ull, cudaMemcpyHostToDevice));
+    }
+    const uint32_t nblk = b->num_blocks;
+    std::vector<uint64_t> off(nblk + 1);
+    for (uint32_t i = 0; i <= nblk; i++) off[i] = b->block_offsets[i] - b->block_offsets[0];
+    std::vector<uint32_t> tabs(2ull * nblk + num_shards + 1, 0);
+    for (uint32_t i = 0; i < nblk; i++) {
+        tabs[i] = b->block_shards[i];
+        tabs[nblk + i] = b->block_rows[i];
+    }
+    for (uint32_t i = 0; i < num_shards; i++) tabs[2ull * nblk + i] = shard_chrom[i];
+    const uint64_t nn = std::max<uint64_t>(n, 1);
+    RGL_TRY(m->key_a.ensure(nn * 8));
+    RGL_TRY(m->key_b.ensure(nn * 8));
+    RGL_TRY(m->len_a.ensure(nn * 4));
+    RGL_TRY(m->len_b.ensure(nn * 4));
+    RGL_TRY(m->ukey.ensure(nn * 8));
+    RGL_TRY(m->agg.ensure(nn * sizeof(LenAgg)));
+    RGL_TRY(m->groups.ensure(nn * sizeof(QGroupDev)));
+    RGL_TRY(m->goff.ensure((rows + 1ull) * 8 + (nblk + 1ull) * 8 + tabs.size() * 4 + 64));
+    RGL_TRY(m->runs.ensure(64));
+    uint64_t* d_goff = m->goff.as<uint64_t>();
+    uint64_t* d_boff = d_goff + rows + 1;
+    uint32_t* d_tabs = reinterpret_cast<uint32_t*>(d_boff + nblk + 1);
+    RGL_CUDA(cudaMemcpyAsync(d_boff, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st));
+    RGL_CUDA(cudaMemcpyAsync(d_tabs, tabs.data(), tabs.size() * 4, cudaMemcpyHostToDevice, st));
+    // 2^segbits > rows * C: every valid key's high part is below all ones, so kNoGroup (all bits
+    // set) sorts strictly after every valid key within the sorted 32 + segbits bits
+    int segbits = 1;
+    while (segbits < 32 && (1ull << segbits) <= (uint64_t)rows * C) segbits++;
+    size_t need = 0, tb = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint64_t*)nullptr, (uint64_t*)nullptr, (uint32_t*)nullptr,
+                                    (uint32_t*)nullptr, (int)nn, 0, 64, st);
+    need = std::max(need, tb);
+    cub::TransformInputIterator<LenAgg, LenToAgg, const uint32_t*> vin(m->len_b.as<uint32_t>(), LenToAgg());
+    cub::DeviceReduce::ReduceByKey(nullptr, tb, m->key_b.as<uint64_t>(), m->ukey.as<uint64_t>(), vin,
+                                   m->agg.as<LenAgg>(), m->runs.as<uint32_t>(), LenAggOp(), (int)nn, st);
+    need = std::max(need, tb);
+    RGL_TRY(m->tmp.ensure(need + 256));
+    if (n) {
+        k_group_keys<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
+            n, b->d_intervals + b->block_offsets[0], d_boff, d_tabs, d_tabs + nblk, nblk + 1, d_tabs + 2ull * nblk,
+            num_shards, C, m->nb.as<uint64_t>(), (double)bin_size, m->key_a.as<uint64_t>(), m->len_a.as<uint32_t>());
+        tb = m->tmp.cap;
+        RGL_CUDA(cub::DeviceRadixSort::SortPairs(m->tmp.p, tb, m->key_a.as<uint64_t>(), m->key_b.as<uint64_t>(),
+                                                 m->len_a.as<uint32_t>(), m->len_b.as<uint32_t>(), (int)n, 0,
+                                                 std::min(64, 32 + segbits), st));
+        tb = m->tmp.cap;
+        RGL_CUDA(cub::DeviceReduce::ReduceByKey(m->tmp.p, tb, m->key_b.as<uint64_t>(), m->ukey.as<uint64_t>(), vin,
+                                                m->agg.as<LenAgg>(), m->runs.as<uint32_t>(), LenAggOp(), (int)n, st));
+    } else {
+        RGL_CUDA(cudaMemsetAsync(m->runs.p, 0, 4, st));
+    }
+    k_group_finish<<<(unsigned)((nn + 256) / 256), 256, 0, st>>>(
+        m->ukey.as<uint64_t>(), m->agg.as<LenAgg>(), m->runs.as<uint32_t>(), rows, C, (double)bin_size,
+        m->slot_tab.as<uint32_t>(), lmax, m->groups.as<QGroupDev>(), d_goff);
+    // the p-value kernel drops groups whose slot lies past the source's table (slot >= tab_len)
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+    const uint64_t cells = (uint64_t)rows * D;
+    const uint64_t warps = std::min<uint64_t>(cells, (uint64_t)nsm * 64);
+    k_pvalues<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(
+        rows, D, C, d_counts, reinterpret_cast<const unsigned long long*>(d_overlap_bp), (double)bin_size, d_goff,
+        m->groups.as<QGroupDev>(), m->d_mv, m->coff.as<uint64_t>(), m->stride, m->d_len, d_p, d_llr, d_log_p, d_flags);
+    RGL_CUDA(cudaGetLastError());
+    if (out_groups) {
+        uint32_t runs = 0;
+        uint64_t ng = 0;
+        RGL_CUDA(cudaMemcpyAsync(&runs, m->runs.p, 4, cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaMemcpyAsync(&ng, d_goff + rows, 8, cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaStreamSynchronize(st));
+        *out_groups = ng;
+    }
+    return RGL_OK;
 }
 
 }  // extern "C"

@@ -283,3 +283,60 @@ def test_host_batch_pipelined_copies_equal_device_batch():
     assert (c == oc).all() and (bp == obp).all()
     ctx.close()
     idx.close()
+
+
+@pytest.mark.parametrize("seed", [21, 22])
+def test_batch_pvalues_device_equal_host_stats_path(seed):
+    """The batch's stats stage on the device (length groups built from the batch's intervals) equals
+    the host path (rgl_query_chrom_groups per row and chromosome + rgl_query_pvalues), which the
+    p-value tests pin to the oracle."""
+    from riggle_b200 import api
+
+    rng = np.random.default_rng(seed)
+    layers, files, D, nsh = _random_batch(seed, nfiles=23, nshards=3, D=11)
+    nbins = [30_001, 25_000, 7]  # chromosome 2 is tiny: most of its groups have l_int >= n_bins
+    m = api.Moments(D, nbins)
+    for d in range(D):
+        for c in range(len(nbins)):
+            if rng.random() < 0.2:
+                continue
+            ns = m.slots(c)
+            mean = np.sort(rng.random(ns) * rng.uniform(0.01, 50))
+            var = mean * (rng.uniform(1.5, 30) if rng.random() < 0.6 else rng.uniform(0.1, 0.9))
+            mv = np.stack([mean, var], 1).astype(np.float32)
+            m.set(d, c, mv[: ns // 2] if rng.random() < 0.1 else mv)
+    shard_chrom = np.array([0, 1, 0xFFFFFFFF if seed % 2 else 2], np.uint32)
+    idx = rg.Index.from_layers(layers, D, [f"s{i}" for i in range(nsh)])
+    ctx = rg.Context(idx)
+    iv, shards, offs, rows = _file_major(files, nsh)
+    t, p = _dev(iv)
+    b = rg.DeviceBatch(len(files), shards, offs, p, rows)
+    R = len(files)
+    dc = torch.empty((R, D), dtype=torch.int32, device="cuda:0")
+    dbp = torch.empty((R, D), dtype=torch.int64, device="cuda:0")
+    ctx.query_batch_device(b, dc.data_ptr(), dbp.data_ptr(), sub_batch=3000)
+    out = {k: torch.empty((R, D), dtype=dt, device="cuda:0")
+           for k, dt in (("p", torch.float64), ("llr", torch.float64), ("lp", torch.float64), ("f", torch.uint8))}
+    ng = m.batch_pvalues_device(ctx, b, shard_chrom, dc.data_ptr(), dbp.data_ptr(), out["p"].data_ptr(),
+                                out["llr"].data_ptr(), out["lp"].data_ptr(), out["f"].data_ptr())
+    torch.cuda.synchronize()
+    assert ng > 0
+    counts = dc.cpu().numpy().view(np.uint32)
+    bp = dbp.cpu().numpy().view(np.uint64)
+    row_groups = []
+    for per in files:
+        chroms = []
+        for sh, a in per.items():
+            if shard_chrom[sh] != 0xFFFFFFFF:
+                chroms.append((int(shard_chrom[sh]), api.query_chrom_groups(a)))
+        row_groups.append(chroms)
+    hp, hl, hlp, hf = m.pvalues(row_groups, counts, bp)
+    dp, dl, dlp, df = (out[k].cpu().numpy() for k in ("p", "llr", "lp", "f"))
+    assert (df == hf).all()
+    assert (hf & 1).sum() > 10  # emitted cells exist
+    np.testing.assert_allclose(dl, hl, rtol=1e-11, atol=1e-13)
+    np.testing.assert_allclose(dp, hp, rtol=1e-11, atol=1e-300)
+    np.testing.assert_allclose(dlp, hlp, rtol=1e-11, atol=1e-13)
+    ctx.close()
+    m.close()
+    idx.close()
