@@ -497,6 +497,40 @@ def run_batched(args, dev):
     bc = dc.cpu().numpy().view(np.uint32)
     bb = dbp.cpu().numpy().view(np.uint64)
 
+    # the stats stage (FP64 p-value matrix): moments of every (source, chromosome) of the database
+    # built on the device at index time, then query length groups and p-values of the whole batch
+    from riggle_b200 import api
+
+    t0 = time.perf_counter()
+    mom = api.Moments(D, (np.asarray(cl, np.uint64) + 99) // 100, device=dev)
+    for f in range(dbspec.num_files):
+        for c in range(len(cl)):
+            blk = dbspec.block(f, c)
+            if len(blk):
+                mom.build(f, c, blk)
+    moments_s = time.perf_counter() - t0
+    shard_chrom = np.arange(len(cl), dtype=np.uint32)
+    pv = {k: torch.empty((F, D), dtype=dt, device=cuda)
+          for k, dt in (("p", torch.float64), ("llr", torch.float64), ("lp", torch.float64), ("f", torch.uint8))}
+
+    def stats_stage(count_groups=False):
+        return mom.batch_pvalues_device(ctx, batch, shard_chrom, dc.data_ptr(), dbp.data_ptr(), pv["p"].data_ptr(),
+                                        pv["llr"].data_ptr(), pv["lp"].data_ptr(), pv["f"].data_ptr(),
+                                        count_groups=count_groups)
+
+    ngroups = stats_stage(True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.batch_steps):
+        ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), graph=True, tuned=True, stats=False)
+        stats_stage()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ctx.check()
+    ms_pv = e0.elapsed_time(e1) / args.batch_steps
+    emitted = int((pv["f"] & 1).sum().item())
+    min_lp = float(pv["lp"].min().item())
+
     # the plain form on the same files: one rgl_query_counts_device call (one pipeline) per file
     t_plain = t_iv.clone()
     t_plain[:, 2] = 0
@@ -584,9 +618,14 @@ def run_batched(args, dev):
            "plain": {"value": plain_value, "ms_per_step": plain_ms,
                      "form": "one rgl_query_counts_device call per query file, same files, same units"},
            "batched_vs_plain": value / plain_value, "counts_exact_vs_plain": exact,
+           "with_pvalues": {"ms_per_step": ms_pv, "value": units / (ms_pv / 1e3), "query_length_groups": ngroups,
+                            "emitted_cells": emitted, "min_ln_p": min_lp, "moments_build_s": moments_s,
+                            "stage": "query length groups + FP64 p-values of every (file, source) cell on the "
+                                     "device (rgl_batch_pvalues_device) after the counts"},
            "e2e": {"value": units / e2e_s, "unit": UNIT, "ms_per_step": e2e_s * 1e3, "h2d_bytes_per_step": N * 12,
                    "d2h_bytes_per_step": F * D * 12, "api": "rgl_query_batch_host (page-locked host intervals)"},
            "cpu_baseline": cpu, "clocks": clk, "l2": "the batch's 5.6 GB of query intervals exceed L2"}
+    mom.close()
     ctx.close()
     return out, idx
 

@@ -549,16 +549,16 @@ class Moments:
         return p, llr, lp, fl
 
     def batch_pvalues_device(self, ctx, batch, shard_chrom, d_counts, d_bp, d_p, d_llr, d_log_p, d_flags,
-                             bin_size=BIN_SIZE):
-        """Stats stage of a device batch (pointers are device addresses, num_rows x D); returns the
-        number of query length groups."""
+                             bin_size=BIN_SIZE, count_groups=True):
+        """Stats stage of a device batch (pointers are device addresses, num_rows x D).  Returns the
+        number of query length groups (synchronising), or None with count_groups=False (asynchronous)."""
         sc = np.ascontiguousarray(shard_chrom, np.uint32)
         ng = C.c_uint64()
         check(load().rgl_batch_pvalues_device(ctx._h, self._h, C.byref(batch.c), _ptr(sc), len(sc), bin_size,
                                               C.c_void_p(d_counts), C.c_void_p(d_bp), C.c_void_p(d_p),
                                               C.c_void_p(d_llr), C.c_void_p(d_log_p) if d_log_p else None,
-                                              C.c_void_p(d_flags), C.byref(ng)))
-        return ng.value
+                                              C.c_void_p(d_flags), C.byref(ng) if count_groups else None))
+        return ng.value if count_groups else None
 
     def close(self):
         if self._h:
