@@ -129,6 +129,11 @@ int rgl_index_get_info(const rgl_index* index, rgl_index_info* out);
 int rgl_index_shard_id(const rgl_index* index, const char* name, uint32_t* out_id);
 const char* rgl_index_shard_name(const rgl_index* index, uint32_t shard);
 const char* rgl_index_source_name(const rgl_index* index, uint32_t sid);
+/* Column shard of an index (multi-GPU partition by database file, no counterpart in the reference):
+ * a new index on the same device holding only the intervals with sid in [sid_lo, sid_hi), sids
+ * rebased to 0, every layer still sorted by start.  Query results of the shard are the columns
+ * [sid_lo, sid_hi) of the full index's results. */
+int rgl_index_select_columns(const rgl_index* index, uint32_t sid_lo, uint32_t sid_hi, rgl_index** out);
 /* Number of intervals of (shard, layer) (0 when absent). */
 uint64_t rgl_index_layer_count(const rgl_index* index, uint32_t shard, uint32_t layer);
 /* Copies one (shard, layer) back to host arrays of its count (2*count pos words, count sids). */
@@ -205,6 +210,26 @@ int rgl_query_counts_device(rgl_context* ctx, uint32_t num_rows, uint32_t num_sh
                             const uint64_t* shard_offsets, const rgl_interval* d_intervals,
                             const rgl_query_opts* opts, uint32_t* d_counts, uint64_t* d_overlap_bp,
                             rgl_query_stats* stats);
+
+/* One overlapping pair of `--intervals` mode: IntervalHit (src/stats/mod.rs:4-15) with the query
+ * file as its row, the database file as its sid and the chromosome as its shard id. */
+typedef struct rgl_pair {
+    uint32_t query_start, query_end;
+    uint32_t db_start, db_end;
+    uint32_t row;             /* query file (Q_SID) */
+    uint32_t sid;             /* database source (D_SID) */
+    uint32_t shard;           /* index shard (chromosome) */
+    uint32_t intersection_bp; /* min(ends) - max(starts) */
+} rgl_pair;
+
+/* query_sweep_pairs (src/sweep/query.rs:11-41) driven as collect_interval_pairs
+ * (src/tasks/query/intervals.rs:16-112): every overlapping (query interval, database interval) pair
+ * of the batch with its exact intersection, in the order (layer, shard, row, query start, database
+ * start); the reference's order differs only in the shard order (a HashMap's) and in placing rows
+ * after start.  *out_count receives the number of pairs; with pairs == NULL nothing else is written,
+ * else capacity must hold them all (RGL_ERR_INVALID_ARGUMENT otherwise).  Synchronous. */
+int rgl_query_pairs(rgl_context* ctx, const rgl_query_batch* batch, uint64_t capacity, rgl_pair* pairs,
+                    uint64_t* out_count);
 
 /* ---- Batched form: many query files in one call -------------------------------------------------
  * Replaces query_database's loop over batches of query files (src/tasks/query/mod.rs:182-307) for a
@@ -406,6 +431,10 @@ int rgl_synth_chrom_layers_host(const rgl_synth_spec* spec, uint32_t chrom, uint
  * start all on the device).  Same content as bucketing the host blocks. */
 int rgl_index_synth(const rgl_synth_spec* spec, uint32_t min_size, uint32_t growth_factor, int device,
                     rgl_index** out);
+/* The same for files [file_lo, file_hi) only (each with its global stream; sid = sid_base + f -
+ * file_lo): one GPU's column shard of a database too large for one GPU. */
+int rgl_index_synth_columns(const rgl_synth_spec* spec, uint32_t min_size, uint32_t growth_factor, uint32_t file_lo,
+                            uint32_t file_hi, int device, rgl_index** out);
 /* File-major layout of a query batch drawn from a spec: block f * num_chroms + c holds the intervals
  * of (file f, chromosome c), sized as rgl_synth_file_chrom_counts.  block_offsets receives
  * num_files * num_chroms + 1 entries; block_shards (= c) and block_rows (= f) are optional. */

@@ -37,6 +37,7 @@ _SIGS = {
                                         C.c_uint32, C.c_uint32, C.c_uint32, _P, _P]),
     "orc_query_database": (C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P,
                                      C.c_uint32, C.c_int, C.c_int, _P, _P, _P, _P]),
+    "orc_query_pairs": (C.c_uint64, [C.c_uint32, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P, _P, C.c_uint64]),
     "orc_bruteforce_counts": (None, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                      _P, _P]),
     "orc_simd_cumsum_f32": (None, [_P, C.c_uint64]),
@@ -184,6 +185,19 @@ def bruteforce(layers, qshards, rows, num_sources, min_size=128, growth_factor=4
     lib().orc_bruteforce_counts(min_size, growth_factor, num_sources, len(layers), la, len(qshards), qa, rows,
                                 _p(counts), _p(bp))
     return counts, bp
+
+
+def query_pairs(layers, qshards, min_size=128, growth_factor=4):
+    """Restated `--intervals` mode: every overlapping pair as uint32[n, 8] records (q.start, q.end,
+    d.start, d.end, q.sid, d.sid, shard, intersection bp) in the reference's emission order
+    (shard, layer, query start, DB start)."""
+    la, k1 = _layer_structs(layers)
+    qa, k2 = _qshard_structs(qshards)
+    n = lib().orc_query_pairs(min_size, growth_factor, len(layers), la, len(qshards), qa, None, 0)
+    out = np.empty((n, 8), np.uint32)
+    if n:
+        lib().orc_query_pairs(min_size, growth_factor, len(layers), la, len(qshards), qa, _p(out), n)
+    return out
 
 
 def depth_signal(starts, ends, n_bins, bin_size=100):

@@ -708,6 +708,77 @@ void orc_bruteforce_counts(uint32_t min_size, uint32_t gf, uint32_t num_sources,
         }
 }
 
+// Restatement of `--intervals` mode: query_sweep_pairs (src/sweep/query.rs:11-41) driven as
+// collect_interval_pairs (src/tasks/query/intervals.rs:16-112): per shard (ascending index here;
+// a HashMap order in the reference), per layer in ascending index, the shard's queries sorted by
+// start (voracious_sort keys an Interval by its start, src/core/mod.rs:36-42), and for every query
+// the layer's positions from the jump-table seek + partition point while p.start < q.end, emitting
+// the pairs with p.end > q.start.  Record: q.start, q.end, d.start, d.end, q.sid (row), d.sid,
+// shard, intersection bp.  Returns the number of pairs; writes at most `cap`.
+uint64_t orc_query_pairs(uint32_t min_size, uint32_t gf, uint32_t n_layers, const orc_layer* layers,
+                         uint32_t n_qshards, const orc_qshard* qshards, uint32_t* out, uint64_t cap) {
+    uint64_t np = 0;
+    std::vector<const orc_qshard*> qs_sorted;
+    for (uint32_t i = 0; i < n_qshards; i++) qs_sorted.push_back(&qshards[i]);
+    std::stable_sort(qs_sorted.begin(), qs_sorted.end(), [](auto a, auto b) { return a->shard < b->shard; });
+    for (const orc_qshard* qsh : qs_sorted) {
+        if (qsh->count == 0) continue;
+        std::vector<uint64_t> order(qsh->count);
+        for (uint64_t i = 0; i < qsh->count; i++) order[i] = i;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](uint64_t a, uint64_t b) { return qsh->ivs[3 * a] < qsh->ivs[3 * b]; });
+        std::vector<const orc_layer*> ls;
+        for (uint32_t l = 0; l < n_layers; l++)
+            if (layers[l].shard == qsh->shard && layers[l].count) ls.push_back(&layers[l]);
+        std::stable_sort(ls.begin(), ls.end(), [](auto a, auto b) { return a->layer < b->layer; });
+        for (const orc_layer* L : ls) {
+            const uint32_t mx = layer_max_size(min_size, gf, L->layer);
+            const uint32_t tile = tile_size(min_size, gf, L->layer);
+            std::vector<uint64_t> own;
+            const uint64_t* jt = L->jump;
+            uint64_t jt_len = L->jump_len;
+            if (!jt) {
+                std::vector<uint32_t> st(L->count);
+                for (uint64_t i = 0; i < L->count; i++) st[i] = L->pos[2 * i];
+                own = build_jump_table(st.data(), L->count, tile);
+                jt = own.data();
+                jt_len = own.size();
+            }
+            const Pos* pos = reinterpret_cast<const Pos*>(L->pos);
+            for (uint64_t k : order) {
+                const uint32_t qs = qsh->ivs[3 * k], qe = qsh->ivs[3 * k + 1], qsid = qsh->ivs[3 * k + 2];
+                const uint32_t lo = qs >= mx ? qs - mx : 0;  // query.rs:23
+                uint64_t a = jump_lookup(jt, jt_len, tile, lo);
+                if (a > L->count) a = L->count;
+                uint64_t b = L->count;
+                while (a < b) {  // partition_point(|p| p.start < lo), query.rs:25
+                    const uint64_t m = a + (b - a) / 2;
+                    if (pos[m].start < lo) a = m + 1; else b = m;
+                }
+                for (uint64_t i = a; i < L->count; i++) {  // query.rs:28-39
+                    const Pos p = pos[i];
+                    if (p.start >= qe) break;
+                    if (p.end > qs) {
+                        if (np < cap && out) {
+                            uint32_t* r = out + 8 * np;
+                            r[0] = qs;
+                            r[1] = qe;
+                            r[2] = p.start;
+                            r[3] = p.end;
+                            r[4] = qsid;
+                            r[5] = L->sid[i];
+                            r[6] = qsh->shard;
+                            r[7] = std::min(qe, p.end) - std::max(qs, p.start);
+                        }
+                        np++;
+                    }
+                }
+            }
+        }
+    }
+    return np;
+}
+
 // ---- fourier ------------------------------------------------------------------------------
 void orc_simd_cumsum_f32(float* g, uint64_t n) { simd_cumsum_f32(g, n); }
 

@@ -176,6 +176,7 @@ _SIGS = {
                                    C.POINTER(QueryStats)]),
     "rgl_query_counts_device": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, _P, C.POINTER(QueryOpts), _P, _P,
                                           C.POINTER(QueryStats)]),
+    "rgl_query_pairs": (C.c_int, [_P, C.POINTER(QueryBatch), C.c_uint64, _P, C.POINTER(C.c_uint64)]),
     "rgl_query_batch_device": (C.c_int, [_P, C.POINTER(BatchDesc), C.POINTER(BatchOpts), _P, _P,
                                          C.POINTER(BatchStats)]),
     "rgl_query_batch_host": (C.c_int, [_P, C.POINTER(BatchDesc), _P, C.POINTER(BatchOpts), _P, _P,
@@ -217,6 +218,9 @@ _SIGS = {
     "rgl_synth_chrom_layers_host": (C.c_int, [C.POINTER(SynthSpec), C.c_uint32, C.c_uint32, C.c_uint32, _P,
                                               C.c_uint32, _P, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
     "rgl_index_synth": (C.c_int, [C.POINTER(SynthSpec), C.c_uint32, C.c_uint32, C.c_int, C.POINTER(_P)]),
+    "rgl_index_synth_columns": (C.c_int, [C.POINTER(SynthSpec), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
+                                          C.c_int, C.POINTER(_P)]),
+    "rgl_index_select_columns": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
     "rgl_synth_batch_layout": (C.c_int, [C.POINTER(SynthSpec), _P, _P, _P]),
     "rgl_synth_batch_device": (C.c_int, [C.POINTER(SynthSpec), C.c_int, _P, _P, _P]),
 }

@@ -87,6 +87,20 @@ class Index:
         check(load().rgl_index_synth(C.byref(spec.c), min_size, growth_factor, device, C.byref(h)))
         return cls(h)
 
+    @classmethod
+    def synth_columns(cls, spec, file_lo, file_hi, min_size=128, growth_factor=4, device=0):
+        """Files [file_lo, file_hi) of a synthetic database (a column shard), sids rebased to 0."""
+        h = C.c_void_p()
+        check(load().rgl_index_synth_columns(C.byref(spec.c), min_size, growth_factor, file_lo, file_hi, device,
+                                             C.byref(h)))
+        return cls(h)
+
+    def select_columns(self, sid_lo, sid_hi):
+        """A new index holding sources [sid_lo, sid_hi) of this one (sids rebased to 0)."""
+        h = C.c_void_p()
+        check(load().rgl_index_select_columns(self._h, sid_lo, sid_hi, C.byref(h)))
+        return Index(h)
+
     def shard_id(self, name):
         out = C.c_uint32()
         check(load().rgl_index_shard_id(self._h, name.encode(), C.byref(out)))
@@ -171,6 +185,31 @@ class Context:
         opts = self._opts(chunk, ctas_per_sm, not with_overlap, pair_ratio)
         check(load().rgl_query_counts(self._h, C.byref(batch), C.byref(opts), _ptr(counts), _ptr(bp), C.byref(st)))
         return counts, bp, st.as_dict()
+
+    @staticmethod
+    def _batch(shards, num_rows, keep):
+        arr = (_lib.QueryShard * max(1, len(shards)))()
+        for i, (k, ivs) in enumerate(shards.items()):
+            ivs = np.ascontiguousarray(ivs, dtype=np.uint32).reshape(-1, 3)
+            keep.append(ivs)
+            if isinstance(k, str):
+                arr[i] = _lib.QueryShard(k.encode(), 0, len(ivs), _ptr(ivs))
+            else:
+                arr[i] = _lib.QueryShard(None, int(k), len(ivs), _ptr(ivs))
+        keep.append(arr)
+        return _lib.QueryBatch(int(num_rows), len(shards), arr)
+
+    def query_pairs(self, shards, num_rows):
+        """`--intervals` mode: every overlapping pair as uint32[n, 8] records (query_start, query_end,
+        db_start, db_end, row, sid, shard, intersection_bp)."""
+        keep = []
+        batch = self._batch(shards, num_rows, keep)
+        n = C.c_uint64()
+        check(load().rgl_query_pairs(self._h, C.byref(batch), 0, None, C.byref(n)))
+        out = np.empty((n.value, 8), np.uint32)
+        if n.value:
+            check(load().rgl_query_pairs(self._h, C.byref(batch), n.value, _ptr(out), C.byref(n)))
+        return out
 
     def query_batch_device(self, batch, d_counts, d_bp=None, graph=False, tuned=False, sub_batch=0, chunk=0,
                            ctas_per_sm=0, pair_ratio=0, counts_only=False, stats=True):

@@ -7,6 +7,8 @@
 // (src/io/jump.rs) is size-checked at open for error parity but not uploaded: the device computes
 // exact partition points by binary search, which is what the reference's conservative lookup plus
 // partition_point yields (src/sweep/query.rs:141-143).
+#include <cub/cub.cuh>
+
 #include <algorithm>
 #include <cstring>
 
@@ -143,6 +145,24 @@ static int device_check(int device) {
     if (e != cudaSuccess || n == 0) return fail(RGL_ERR_NO_DEVICE, "no CUDA device visible");
     if (device < 0 || device >= n) return fail(RGL_ERR_INVALID_ARGUMENT, "device ordinal out of range");
     return RGL_OK;
+}
+
+// Column filter: flag[i] = sid in [lo, hi); after an exclusive scan, the kept elements move to
+// their compacted positions in order (so every layer stays sorted by start), sids rebased to 0.
+__global__ void k_col_flags(const uint32_t* __restrict__ sid, uint64_t n, uint32_t lo, uint32_t hi,
+                            uint32_t* __restrict__ flag) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= n; i += (uint64_t)gridDim.x * blockDim.x)
+        flag[i] = (i < n && sid[i] >= lo && sid[i] < hi) ? 1u : 0u;
+}
+
+__global__ void k_col_scatter(const uint2* __restrict__ pos, const uint32_t* __restrict__ sid, uint64_t n,
+                              const uint32_t* __restrict__ flag, const uint32_t* __restrict__ at, uint32_t lo,
+                              uint2* __restrict__ out_pos, uint32_t* __restrict__ out_sid) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (flag[i]) {
+            out_pos[at[i]] = pos[i];
+            out_sid[at[i]] = sid[i] - lo;
+        }
 }
 
 }  // namespace rgl
@@ -398,6 +418,83 @@ int rgl_index_export_layer(const rgl_index* index, uint32_t shard, uint32_t laye
     RGL_CUDA(cudaSetDevice(index->device));
     if (pos) RGL_CUDA(cudaMemcpy(pos, index->d_pos + l.off, l.n * 8, cudaMemcpyDeviceToHost));
     if (sid) RGL_CUDA(cudaMemcpy(sid, index->d_sid + l.off, l.n * 4, cudaMemcpyDeviceToHost));
+    return RGL_OK;
+}
+
+int rgl_index_select_columns(const rgl_index* src, uint32_t sid_lo, uint32_t sid_hi, rgl_index** out) {
+    clear_error();
+    if (!src || !out) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (sid_lo > sid_hi || sid_hi > src->num_sources) return fail(RGL_ERR_INVALID_ARGUMENT, "bad source range");
+    RGL_CUDA(cudaSetDevice(src->device));
+    uint64_t maxn = 1;
+    for (auto& l : src->layers) maxn = std::max(maxn, l.n);
+    DevBuf flag, at, tmp;
+    int s = flag.ensure((maxn + 1) * 4);
+    if (s == RGL_OK) s = at.ensure((maxn + 1) * 4);
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, (uint32_t*)nullptr, (uint32_t*)nullptr, (int)(maxn + 1));
+    if (s == RGL_OK) s = tmp.ensure(tb + 256);
+    if (s == RGL_OK && maxn + 1 >= (1ull << 31)) s = fail(RGL_ERR_UNSUPPORTED, "a layer of 2^31 or more intervals");
+    // pass 1: kept count of every layer
+    std::vector<uint64_t> kept(src->layers.size(), 0);
+    auto run_flags = [&](const LayerDev& l) -> int {
+        const unsigned blocks = (unsigned)std::min<uint64_t>((l.n + 256) / 256, 148ull * 16);
+        k_col_flags<<<blocks, 256>>>(src->d_sid + l.off, l.n, sid_lo, sid_hi, flag.as<uint32_t>());
+        size_t t = tmp.cap;
+        RGL_CUDA(cub::DeviceScan::ExclusiveSum(tmp.p, t, flag.as<uint32_t>(), at.as<uint32_t>(), (int)(l.n + 1)));
+        return RGL_OK;
+    };
+    for (size_t i = 0; i < src->layers.size() && s == RGL_OK; i++) {
+        s = run_flags(src->layers[i]);
+        uint32_t k = 0;
+        if (s == RGL_OK && cudaMemcpy(&k, at.as<uint32_t>() + src->layers[i].n, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+            s = fail(RGL_ERR_DEVICE, "column count");
+        kept[i] = k;
+    }
+    auto* idx = new rgl_index();
+    idx->device = src->device;
+    idx->min_size = src->min_size;
+    idx->gf = src->gf;
+    idx->num_sources = sid_hi - sid_lo;
+    idx->num_shards = src->num_shards;
+    idx->shard_names = src->shard_names;
+    idx->shard_ids = src->shard_ids;
+    for (uint32_t d = sid_lo; d < sid_hi; d++) idx->source_names.push_back(src->source_names[d]);
+    std::vector<size_t> from;
+    for (size_t i = 0; i < src->layers.size(); i++)
+        if (kept[i]) {
+            LayerDev l = src->layers[i];
+            l.n = kept[i];
+            l.flags = 0;
+            idx->layers.push_back(l);
+            idx->total += l.n;
+            from.push_back(i);
+        }
+    build_slots(idx);
+    if (s == RGL_OK) s = index_alloc(idx);
+    // pass 2: compaction into the new blocks
+    for (size_t j = 0; j < idx->layers.size() && s == RGL_OK; j++) {
+        const LayerDev& l = src->layers[from[j]];
+        s = run_flags(l);
+        if (s != RGL_OK) break;
+        const unsigned blocks = (unsigned)std::min<uint64_t>((l.n + 255) / 256, 148ull * 16);
+        k_col_scatter<<<blocks, 256>>>(src->d_pos + l.off, src->d_sid + l.off, l.n, flag.as<uint32_t>(),
+                                       at.as<uint32_t>(), sid_lo, idx->d_pos + idx->layers[j].off,
+                                       idx->d_sid + idx->layers[j].off);
+        if (cudaGetLastError() != cudaSuccess) s = fail(RGL_ERR_DEVICE, "column scatter");
+    }
+    if (s == RGL_OK && cudaDeviceSynchronize() != cudaSuccess) s = fail(RGL_ERR_DEVICE, "column filter");
+    flag.release();
+    at.release();
+    tmp.release();
+    if (s == RGL_OK) s = index_finalize(idx);
+    if (s != RGL_OK) {
+        index_free(idx);
+        delete idx;
+        return s;
+    }
+    *out = idx;
     return RGL_OK;
 }
 

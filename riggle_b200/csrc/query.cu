@@ -47,7 +47,7 @@ struct RangeDesc {
 // One query's candidate run for the pair sweep: DB elements [base, base + plen) of its layer.
 struct PairSeg {
     uint64_t base;
-    uint32_t qs, qe, qrow, pad;
+    uint32_t qs, qe, qrow, shard;
 };
 
 enum : uint8_t { M_RANK = 0, M_PAIR = 1 };
@@ -341,7 +341,7 @@ __global__ void k_pair_len(uint32_t n, uint32_t nslots, uint32_t rows, const uin
         const uint32_t r = ridx[t] + rflag[t] - 1;
         if (method[r] == M_PAIR) {
             len = hi[t] - lo[t];
-            psegs[t] = PairSeg{layers[li].off + lo[t], starts[i], qend[i], sg % rows, 0};
+            psegs[t] = PairSeg{layers[li].off + lo[t], starts[i], qend[i], sg % rows, sg / rows};
         }
     }
     plen[t] = len;
@@ -675,6 +675,70 @@ __global__ void __launch_bounds__(256, 4) k_pairs(SweepParams P) {
     }
 }
 
+// `--intervals` mode (query_sweep_pairs, src/sweep/query.rs:11-41): every overlapping pair of the
+// candidate runs, listed in the order of the pair work space (layer slot, shard, row, query start,
+// DB start).  Item i = positions [i * chunk, (i + 1) * chunk) is walked by one warp, 32 positions
+// per step: the count pass stores the item's hits, the emit pass writes them from the item's
+// offset (an exclusive scan of the counts) at their ballot ranks, so the list needs no atomics and
+// comes out in the same order every time.
+template <bool EMIT>
+__global__ void __launch_bounds__(256) k_pair_list(const uint64_t* __restrict__ ppos, uint64_t rcap,
+                                                   const PairSeg* __restrict__ psegs, const uint2* __restrict__ pos,
+                                                   const uint32_t* __restrict__ sid, uint64_t items, uint32_t chunk,
+                                                   uint64_t* __restrict__ item_hits,
+                                                   const uint64_t* __restrict__ item_base, rgl_pair* __restrict__ out) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t total = ppos[rcap];
+    for (uint64_t item = warp; item < items; item += nwarps) {
+        const uint64_t p0 = item * chunk, p1 = min(p0 + chunk, total);
+        uint64_t lo = 0, hi = rcap;  // last run t with ppos[t] <= p0
+        while (lo < hi) {
+            const uint64_t m = (lo + hi + 1) >> 1;
+            if (__ldg(ppos + m) <= p0) lo = m; else hi = m - 1;
+        }
+        uint32_t t = (uint32_t)lo;
+        uint64_t rhi = __ldg(ppos + t + 1), rlo = __ldg(ppos + t);
+        PairSeg ps = psegs[t];
+        const uint64_t base = EMIT ? item_base[item] : 0;
+        uint64_t done = 0;
+        for (uint64_t s = p0; s < p1; s += 32) {
+            const uint64_t p = s + lane;
+            bool hit = false;
+            uint2 d = make_uint2(0, 0);
+            uint64_t di = 0;
+            if (p < p1) {
+                if (p >= rhi) {
+                    t = range_advance(ppos, t, (uint32_t)rcap, p);
+                    rlo = __ldg(ppos + t);
+                    rhi = __ldg(ppos + t + 1);
+                    ps = psegs[t];
+                }
+                di = ps.base + (p - rlo);
+                d = __ldg(pos + di);
+                hit = d.y > ps.qs;
+            }
+            const uint32_t ballot = __ballot_sync(0xffffffffu, hit);
+            if (EMIT && hit) {
+                const uint32_t rank = __popc(ballot & ((1u << lane) - 1u));
+                rgl_pair r;
+                r.query_start = ps.qs;
+                r.query_end = ps.qe;
+                r.db_start = d.x;
+                r.db_end = d.y;
+                r.row = ps.qrow;
+                r.sid = __ldg(sid + di);
+                r.shard = ps.shard;
+                r.intersection_bp = min(ps.qe, d.y) - max(ps.qs, d.x);
+                out[base + done + rank] = r;
+            }
+            done += __popc(ballot);
+        }
+        if (!EMIT && lane == 0) item_hits[item] = done;
+    }
+}
+
 }  // namespace rgl
 
 using namespace rgl;
@@ -693,6 +757,7 @@ struct rgl_context {
     DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp, item_r0;
     DevBuf segtab, tab_len, tab_off, tab_s, tab_e, tab_xs, tab_xe;
     DevBuf cl, pc, method, ulen, plen, ppos, psegs, item_t0, seg_need;
+    DevBuf item_hits, item_base, pairs;  // intervals mode
     DevBuf bt_off, bt_shard, acc;  // batched form: sub-batch block tables (offsets; shards then rows), stats
     uint32_t* h_small = nullptr;  // pinned mirror of `small`
     unsigned long long* h_acc = nullptr;  // pinned mirror of `acc`
@@ -916,6 +981,7 @@ struct PipeMode {
     bool zero_out = true;
     bool reset_err = true;
     bool events = true;  // stats events and sweep timing (off inside a graph capture)
+    bool no_sweep = false;  // stop once the pair work space (ppos, psegs) is laid out
     unsigned long long* acc = nullptr;
 };
 
@@ -1071,6 +1137,13 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceReduce::Sum(c->cub_tmp.p, tb, c->ulen.as<uint64_t>(),
                                     reinterpret_cast<uint64_t*>(d_small + 4), (int)tot, st));
+    if (mode.no_sweep) {
+        c->last_tot = tot;
+        c->last_launches = launches;
+        c->last_n = n;
+        if (mode.reset_err) RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
+        return RGL_OK;
+    }
     k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(tot, c->rpos.as<uint64_t>(), L.chunk, kItemCap,
                                                                c->item_r0.as<uint32_t>());
     k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(tot, c->ppos.as<uint64_t>(), L.chunk, kItemCap,
@@ -1411,7 +1484,7 @@ int rgl_context_destroy(rgl_context* c) {
                       &c->out_counts, &c->out_bp, &c->item_r0,
                       &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe,
                       &c->cl, &c->pc, &c->method, &c->ulen, &c->plen, &c->ppos, &c->psegs, &c->item_t0,
-                      &c->seg_need, &c->bt_off, &c->bt_shard, &c->acc, &c->gc.t_off, &c->gc.t_shard};
+                      &c->seg_need, &c->item_hits, &c->item_base, &c->pairs, &c->bt_off, &c->bt_shard, &c->acc, &c->gc.t_off, &c->gc.t_shard};
     if (c->gc.exec) cudaGraphExecDestroy(c->gc.exec);
     if (c->gc.graph) cudaGraphDestroy(c->gc.graph);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
@@ -1796,6 +1869,79 @@ int rgl_batch_autotune(rgl_context* c, const rgl_batch* b, uint64_t sub_batch, r
     if (num_trials) *num_trials = nt;
     RGL_CUDA(cudaStreamSynchronize(st));
     return finish(c, L, nullptr);
+}
+
+int rgl_query_pairs(rgl_context* c, const rgl_query_batch* b, uint64_t capacity, rgl_pair* pairs,
+                    uint64_t* out_count) {
+    clear_error();
+    if (!c || !b || !out_count) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    RGL_CUDA(cudaSetDevice(c->idx->device));
+    *out_count = 0;
+    std::vector<uint32_t> ids;
+    std::vector<const rgl_query_shard*> blocks;
+    RGL_TRY(resolve_blocks(c, b, &ids, &blocks));
+    uint64_t n = 0;
+    std::vector<uint64_t> off(blocks.size() + 1, 0);
+    for (size_t i = 0; i < blocks.size(); i++) {
+        off[i] = n;
+        n += blocks[i]->count;
+    }
+    off[blocks.size()] = n;
+    RGL_TRY(ensure_workspace(c, n, 0, (uint32_t)blocks.size()));
+    cudaStream_t st = c->stream;
+    for (size_t i = 0; i < blocks.size(); i++)
+        RGL_CUDA(cudaMemcpyAsync(c->iv.as<rgl_interval>() + off[i], blocks[i]->intervals,
+                                 blocks[i]->count * sizeof(rgl_interval), cudaMemcpyHostToDevice, st));
+    if (!blocks.empty()) {
+        RGL_CUDA(cudaMemcpyAsync(c->blk_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st));
+        RGL_CUDA(cudaMemcpyAsync(c->blk_shard.p, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st));
+    }
+    // every candidate run becomes a pair run: a range is swept pair by pair when its candidates are
+    // at most pair_ratio x its union, which no range exceeds at this ratio
+    rgl_query_opts q{};
+    q.pair_ratio = 0xFFFFFFFFu;
+    PipeIn in{c->iv.as<rgl_interval>(), n, b->num_rows, 0, (uint32_t)blocks.size(), c->blk_off.as<uint64_t>(),
+              c->blk_shard.as<uint32_t>(), nullptr};
+    PipeMode m;
+    m.zero_out = false;
+    m.no_sweep = true;
+    RGL_TRY(run_pipeline(c, in, &q, nullptr, nullptr, nullptr, m));
+    RGL_CUDA(cudaStreamSynchronize(st));
+    RGL_TRY(finish(c, pick_launch(&q), nullptr));
+    if (!n || !c->idx->num_slots) return RGL_OK;
+    const uint64_t tot = c->last_tot;
+    uint64_t positions = 0;
+    RGL_CUDA(cudaMemcpy(&positions, c->ppos.as<uint64_t>() + tot, 8, cudaMemcpyDeviceToHost));
+    const uint32_t chunk = 2048;
+    const uint64_t items = (positions + chunk - 1) / chunk;
+    if (!items) return RGL_OK;
+    RGL_TRY(c->item_hits.ensure((items + 1) * 8));
+    RGL_TRY(c->item_base.ensure((items + 1) * 8));
+    size_t tb = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, tb, (uint64_t*)nullptr, (uint64_t*)nullptr, (int)(items + 1), st);
+    RGL_TRY(c->cub_tmp.ensure(tb + 256));
+    const unsigned grid = (unsigned)std::min<uint64_t>((items * 32 + 255) / 256, (uint64_t)c->num_sms * 16);
+    RGL_CUDA(cudaMemsetAsync(c->item_hits.as<uint64_t>() + items, 0, 8, st));
+    k_pair_list<false><<<grid, 256, 0, st>>>(c->ppos.as<uint64_t>(), tot, c->psegs.as<PairSeg>(), c->idx->d_pos,
+                                             c->idx->d_sid, items, chunk, c->item_hits.as<uint64_t>(), nullptr,
+                                             nullptr);
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->item_hits.as<uint64_t>(), c->item_base.as<uint64_t>(),
+                                           (int)(items + 1), st));
+    uint64_t hits = 0;
+    RGL_CUDA(cudaMemcpyAsync(&hits, c->item_base.as<uint64_t>() + items, 8, cudaMemcpyDeviceToHost, st));
+    RGL_CUDA(cudaStreamSynchronize(st));
+    *out_count = hits;
+    if (!pairs || !hits) return RGL_OK;
+    if (capacity < hits) return fail(RGL_ERR_INVALID_ARGUMENT, "pair capacity too small (needs " + std::to_string(hits) + ")");
+    RGL_TRY(c->pairs.ensure(hits * sizeof(rgl_pair)));
+    k_pair_list<true><<<grid, 256, 0, st>>>(c->ppos.as<uint64_t>(), tot, c->psegs.as<PairSeg>(), c->idx->d_pos,
+                                            c->idx->d_sid, items, chunk, nullptr, c->item_base.as<uint64_t>(),
+                                            c->pairs.as<rgl_pair>());
+    RGL_CUDA(cudaGetLastError());
+    RGL_CUDA(cudaMemcpyAsync(pairs, c->pairs.p, hits * sizeof(rgl_pair), cudaMemcpyDeviceToHost, st));
+    RGL_CUDA(cudaStreamSynchronize(st));
+    return RGL_OK;
 }
 
 int rgl_context_check(rgl_context* c) {

@@ -165,7 +165,7 @@ static int check_spec(const rgl_synth_spec* sp) {
 // ---- device generation of one chromosome --------------------------------------------------------
 __global__ void k_synth_chrom(GenParams g, const uint32_t* __restrict__ t_logn, const uint32_t* __restrict__ t_logu,
                               uint32_t chrom, uint32_t chrom_len, const uint64_t* __restrict__ file_off,
-                              uint32_t nfiles, uint64_t total, uint32_t min_size, uint32_t gf,
+                              uint32_t nfiles, uint32_t file_base, uint64_t total, uint32_t min_size, uint32_t gf,
                               uint64_t* __restrict__ key, uint64_t* __restrict__ val,
                               unsigned long long* __restrict__ layer_count, int count_only) {
     uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -176,7 +176,7 @@ __global__ void k_synth_chrom(GenParams g, const uint32_t* __restrict__ t_logn, 
         if (file_off[m] <= j) lo = m; else hi = m;
     }
     uint32_t s, e;
-    gen_interval(g, t_logn, t_logu, lo, chrom, chrom_len, j - file_off[lo], &s, &e);
+    gen_interval(g, t_logn, t_logu, file_base + lo, chrom, chrom_len, j - file_off[lo], &s, &e);
     // layer_for_size (src/io/meta.rs:33-58), power-of-two path or threshold loop
     uint32_t size = e - s, K;
     if (size < min_size) K = 0;
@@ -405,19 +405,26 @@ int rgl_synth_batch_device(const rgl_synth_spec* sp, int device, const uint64_t*
 }
 
 int rgl_index_synth(const rgl_synth_spec* sp, uint32_t min_size, uint32_t gf, int device, rgl_index** out) {
+    return rgl_index_synth_columns(sp, min_size, gf, 0, sp ? sp->num_files : 0, device, out);
+}
+
+int rgl_index_synth_columns(const rgl_synth_spec* sp, uint32_t min_size, uint32_t gf, uint32_t file_lo,
+                            uint32_t file_hi, int device, rgl_index** out) {
     clear_error();
     RGL_TRY(check_spec(sp));
     if (!out) return fail(RGL_ERR_INVALID_ARGUMENT, "null output");
     *out = nullptr;
     if (min_size == 0 || gf < 2) return fail(RGL_ERR_INVALID_ARGUMENT, "layer_config needs min_size >= 1, growth_factor >= 2");
+    if (file_lo > file_hi || file_hi > sp->num_files) return fail(RGL_ERR_INVALID_ARGUMENT, "bad file range");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(RGL_ERR_NO_DEVICE, "no CUDA device");
     RGL_CUDA(cudaSetDevice(device));
-    const uint32_t C = sp->num_chroms, F = sp->num_files;
+    // files [file_lo, file_hi) keep their global streams; their sids are sid_base + (f - file_lo)
+    const uint32_t C = sp->num_chroms, F = file_hi - file_lo;
     const uint32_t KMAX = 64;
     // per (file, chrom) counts and per-chromosome file offsets
     std::vector<uint64_t> fc((size_t)F * C);
-    for (uint32_t f = 0; f < F; f++) chrom_split(sp, sp->file_sizes[f], &fc[(size_t)f * C]);
+    for (uint32_t f = 0; f < F; f++) chrom_split(sp, sp->file_sizes[file_lo + f], &fc[(size_t)f * C]);
     std::vector<std::vector<uint64_t>> foff(C, std::vector<uint64_t>(F + 1, 0));
     for (uint32_t c = 0; c < C; c++)
         for (uint32_t f = 0; f < F; f++) foff[c][f + 1] = foff[c][f] + fc[(size_t)f * C + c];
@@ -441,8 +448,9 @@ int rgl_index_synth(const rgl_synth_spec* sp, uint32_t min_size, uint32_t gf, in
         uint64_t tot = foff[c][F];
         if (!tot) continue;
         RGL_CUDA(cudaMemcpy(d_foff, foff[c].data(), (F + 1) * 8ull, cudaMemcpyHostToDevice));
-        k_synth_chrom<<<(unsigned)((tot + 255) / 256), 256>>>(g, d_tn, d_tu, c, sp->chrom_len[c], d_foff, F, tot,
-                                                              min_size, gf, nullptr, nullptr, d_cnt + (size_t)c * KMAX, 1);
+        k_synth_chrom<<<(unsigned)((tot + 255) / 256), 256>>>(g, d_tn, d_tu, c, sp->chrom_len[c], d_foff, F, file_lo,
+                                                              tot, min_size, gf, nullptr, nullptr,
+                                                              d_cnt + (size_t)c * KMAX, 1);
     }
     RGL_CUDA(cudaGetLastError());
     std::vector<unsigned long long> cnt((size_t)C * KMAX);
@@ -462,7 +470,8 @@ int rgl_index_synth(const rgl_synth_spec* sp, uint32_t min_size, uint32_t gf, in
         idx->shard_names.push_back(nm);
         idx->shard_ids[nm] = c;
     }
-    for (uint32_t d = 0; d < idx->num_sources; d++) idx->source_names.push_back("source_" + std::to_string(d) + ".bed");
+    for (uint32_t d = 0; d < idx->num_sources; d++)
+        idx->source_names.push_back("source_" + std::to_string(d + file_lo) + ".bed");  // the global name
     for (uint32_t c = 0; c < C; c++)
         for (uint32_t K = 0; K < KMAX; K++)
             if (cnt[(size_t)c * KMAX + K]) {
@@ -514,8 +523,8 @@ int rgl_index_synth(const rgl_synth_spec* sp, uint32_t min_size, uint32_t gf, in
             s = fail(RGL_ERR_DEVICE, "synth upload");
             break;
         }
-        k_synth_chrom<<<(unsigned)((tot + 255) / 256), 256>>>(g, d_tn, d_tu, c, sp->chrom_len[c], d_foff, F, tot,
-                                                              min_size, gf, ka.as<uint64_t>(), va.as<uint64_t>(),
+        k_synth_chrom<<<(unsigned)((tot + 255) / 256), 256>>>(g, d_tn, d_tu, c, sp->chrom_len[c], d_foff, F, file_lo,
+                                                              tot, min_size, gf, ka.as<uint64_t>(), va.as<uint64_t>(),
                                                               nullptr, 0);
         size_t tbb = tmp.cap;
         if (cub::DeviceRadixSort::SortPairs(tmp.p, tbb, ka.as<uint64_t>(), kb.as<uint64_t>(), va.as<uint64_t>(),
