@@ -446,6 +446,32 @@ int rgl_synth_batch_device(const rgl_synth_spec* spec, int device, const uint64_
                            rgl_interval* d_out, void* stream);
 
 /* ------------------------------------------------------------------------------------------ */
+/* BED ingest: parse_bed_file (src/io/parse.rs:47-141) and parse_file_batch / enumerate_query_files */
+/* (src/tasks/query/files.rs:25-111), native and multi-threaded on the host.                    */
+/* ------------------------------------------------------------------------------------------ */
+typedef struct rgl_bed_batch rgl_bed_batch;
+
+/* The BED files under query_path sorted by path (*.bed, *.bed.gz), or query_path itself; parsed on
+ * `threads` host threads (0: all cores).  Files without intervals are dropped and the rest numbered
+ * 0.. in path order (compact Q_SIDs, written into every interval's sid).  Errors: RGL_ERR_INPUT_NOT_FOUND,
+ * RGL_ERR_IO, RGL_ERR_BED_INVALID_FORMAT / _RANGE with the file and 1-based line in rgl_last_error. */
+int rgl_bed_batch_load(const char* query_path, uint32_t threads, rgl_bed_batch** out);
+/* parse_bed_string (src/io/parse.rs:143-160): one row from text, kept even when empty. */
+int rgl_bed_parse_string(const char* text, uint64_t len, uint32_t sid, rgl_bed_batch** out);
+uint32_t rgl_bed_batch_rows(const rgl_bed_batch* batch);
+const char* rgl_bed_batch_row_name(const rgl_bed_batch* batch, uint32_t row);  /* the file name */
+uint64_t rgl_bed_batch_row_count(const rgl_bed_batch* batch, uint32_t row);
+uint32_t rgl_bed_batch_row_shards(const rgl_bed_batch* batch, uint32_t row);
+/* Shard k of a row (first-appearance order): its name and intervals (file order). */
+int rgl_bed_batch_block(const rgl_bed_batch* batch, uint32_t row, uint32_t k, const char** shard,
+                        const rgl_interval** intervals, uint64_t* count);
+/* query_database's counting path over a parsed batch: rgl_query_counts with one shard entry per
+ * (row, shard) block; shards absent from the index are skipped (src/tasks/query/mod.rs:194-196). */
+int rgl_bed_batch_query(rgl_context* ctx, const rgl_bed_batch* batch, const rgl_query_opts* opts, uint32_t* counts,
+                        uint64_t* overlap_bp, rgl_query_stats* stats);
+int rgl_bed_batch_free(rgl_bed_batch* batch);
+
+/* ------------------------------------------------------------------------------------------ */
 /* Request server (no counterpart in the reference, whose query_database answers one set of     */
 /* files per process run).  The index stays resident; query files arrive one at a time and are   */
 /* batched as they come: each worker owns a query context on its own stream and, whenever it is  */

@@ -5,6 +5,7 @@ The product is libriggle_b200.so (C ABI in include/riggle.h); this package is it
 from ._lib import RiggleError, load, LIB_PATH  # noqa: F401
 from .api import (  # noqa: F401
     CHROM_NAMES_24,
+    BedBatch,
     Context,
     DeviceBatch,
     Index,

@@ -183,6 +183,16 @@ _SIGS = {
                                        C.POINTER(BatchStats)]),
     "rgl_batch_autotune": (C.c_int, [_P, C.POINTER(BatchDesc), C.c_uint64, C.POINTER(QueryOpts),
                                      C.POINTER(TuneTrial), C.c_uint32, C.POINTER(C.c_uint32)]),
+    "rgl_bed_batch_load": (C.c_int, [C.c_char_p, C.c_uint32, C.POINTER(_P)]),
+    "rgl_bed_parse_string": (C.c_int, [C.c_char_p, C.c_uint64, C.c_uint32, C.POINTER(_P)]),
+    "rgl_bed_batch_rows": (C.c_uint32, [_P]),
+    "rgl_bed_batch_row_name": (C.c_char_p, [_P, C.c_uint32]),
+    "rgl_bed_batch_row_count": (C.c_uint64, [_P, C.c_uint32]),
+    "rgl_bed_batch_row_shards": (C.c_uint32, [_P, C.c_uint32]),
+    "rgl_bed_batch_block": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(C.c_char_p), C.POINTER(_P),
+                                      C.POINTER(C.c_uint64)]),
+    "rgl_bed_batch_query": (C.c_int, [_P, _P, C.POINTER(QueryOpts), _P, _P, C.POINTER(QueryStats)]),
+    "rgl_bed_batch_free": (C.c_int, [_P]),
     "rgl_server_create": (C.c_int, [_P, C.POINTER(ServerOpts), C.POINTER(_P)]),
     "rgl_server_submit": (C.c_int, [_P, C.POINTER(Request), C.POINTER(C.c_uint64)]),
     "rgl_server_wait": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.POINTER(RequestInfo)]),

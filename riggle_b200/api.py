@@ -270,6 +270,70 @@ class Context:
             pass
 
 
+class BedBatch:
+    """Parsed BED query files (rgl_bed_batch): rows = non-empty files in path order."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    @classmethod
+    def load(cls, query_path, threads=0):
+        """parse_file_batch over the *.bed / *.bed.gz files of a directory (or one file)."""
+        h = C.c_void_p()
+        check(load().rgl_bed_batch_load(str(query_path).encode(), threads, C.byref(h)))
+        return cls(h)
+
+    @classmethod
+    def parse_string(cls, text, sid=0):
+        data = text.encode() if isinstance(text, str) else bytes(text)
+        h = C.c_void_p()
+        check(load().rgl_bed_parse_string(data, len(data), sid, C.byref(h)))
+        return cls(h)
+
+    @property
+    def rows(self):
+        return load().rgl_bed_batch_rows(self._h)
+
+    def name(self, row):
+        r = load().rgl_bed_batch_row_name(self._h, row)
+        return r.decode() if r is not None else None
+
+    def count(self, row):
+        return load().rgl_bed_batch_row_count(self._h, row)
+
+    def shards(self, row):
+        """{shard name: uint32[n,3] (start, end, sid)} of one row, in first-appearance order."""
+        out = {}
+        for k in range(load().rgl_bed_batch_row_shards(self._h, row)):
+            name, ptr, n = C.c_char_p(), C.c_void_p(), C.c_uint64()
+            check(load().rgl_bed_batch_block(self._h, row, k, C.byref(name), C.byref(ptr), C.byref(n)))
+            a = np.ctypeslib.as_array((C.c_uint32 * (3 * n.value)).from_address(ptr.value)).reshape(-1, 3).copy() \
+                if n.value else np.zeros((0, 3), np.uint32)
+            out[name.value.decode()] = a
+        return out
+
+    def query(self, ctx, with_overlap=True):
+        """Counting path of query_database over the batch: (counts, overlap_bp, stats)."""
+        D = ctx.index.num_sources
+        counts = np.empty((self.rows, D), np.uint32)
+        bp = np.empty((self.rows, D), np.uint64) if with_overlap else None
+        st = _lib.QueryStats()
+        opts = Context._opts(counts_only=not with_overlap)
+        check(load().rgl_bed_batch_query(ctx._h, self._h, C.byref(opts), _ptr(counts), _ptr(bp), C.byref(st)))
+        return counts, bp, st.as_dict()
+
+    def close(self):
+        if self._h:
+            load().rgl_bed_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Server:
     """Request server over a resident Index (rgl_server_*): submit query files as they arrive, wait
     for their count / overlap rows; p50/p99/p99.9 latency in stats()."""
