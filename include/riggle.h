@@ -134,6 +134,20 @@ const char* rgl_index_source_name(const rgl_index* index, uint32_t sid);
  * rebased to 0, every layer still sorted by start.  Query results of the shard are the columns
  * [sid_lo, sid_hi) of the full index's results. */
 int rgl_index_select_columns(const rgl_index* index, uint32_t sid_lo, uint32_t sid_hi, rgl_index** out);
+/* add_to_database (src/tasks/build.rs:86-276) on the device: the BED files of input_path (*.bed,
+ * *.bed.gz sorted by path, or one such file; every file gets the next D_SID, empty files included)
+ * are parsed on `threads` host threads, bucketed by (shard, layer_for_size), sorted by start on the
+ * device (equal starts keep file and line order) and merged into `base`'s layers (NULL: a new
+ * index with layer config min_size / growth_factor) with new elements first on equal starts, as
+ * the reference's reverse co-merge (extend_layer, src/io/layer.rs:129-199) orders them.  The result
+ * is a new index on base's device (or `device`); base is unchanged.  RGL_ERR_INPUT_NOT_FOUND /
+ * RGL_ERR_NO_BED_FILES as AddError. */
+int rgl_index_add_beds(const rgl_index* base, const char* input_path, uint32_t min_size, uint32_t growth_factor,
+                       uint32_t threads, int device, rgl_index** out);
+/* Writes an index as a database directory in the reference's layout (meta.json and
+ * shards/<shard>/layer_K.{pos,sid,idx}; the .idx is build_jump_table of the layer,
+ * src/io/jump.rs:66-115), readable by rgl_index_open and by the reference's query. */
+int rgl_index_write(const rgl_index* index, const char* db_dir);
 /* Number of intervals of (shard, layer) (0 when absent). */
 uint64_t rgl_index_layer_count(const rgl_index* index, uint32_t shard, uint32_t layer);
 /* Copies one (shard, layer) back to host arrays of its count (2*count pos words, count sids). */

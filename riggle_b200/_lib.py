@@ -230,6 +230,8 @@ _SIGS = {
     "rgl_index_synth": (C.c_int, [C.POINTER(SynthSpec), C.c_uint32, C.c_uint32, C.c_int, C.POINTER(_P)]),
     "rgl_index_synth_columns": (C.c_int, [C.POINTER(SynthSpec), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32,
                                           C.c_int, C.POINTER(_P)]),
+    "rgl_index_add_beds": (C.c_int, [_P, C.c_char_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.POINTER(_P)]),
+    "rgl_index_write": (C.c_int, [_P, C.c_char_p]),
     "rgl_index_select_columns": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
     "rgl_synth_batch_layout": (C.c_int, [C.POINTER(SynthSpec), _P, _P, _P]),
     "rgl_synth_batch_device": (C.c_int, [C.POINTER(SynthSpec), C.c_int, _P, _P, _P]),

@@ -95,6 +95,24 @@ class Index:
                                              C.byref(h)))
         return cls(h)
 
+    @classmethod
+    def from_beds(cls, input_path, min_size=128, growth_factor=4, threads=0, device=0):
+        """add_to_database into a new device index from the BED files of a directory (or one file)."""
+        h = C.c_void_p()
+        check(load().rgl_index_add_beds(None, str(input_path).encode(), min_size, growth_factor, threads, device,
+                                        C.byref(h)))
+        return cls(h)
+
+    def add_beds(self, input_path, threads=0):
+        """A new index: this one with the BED files of input_path merged in (next D_SIDs)."""
+        h = C.c_void_p()
+        check(load().rgl_index_add_beds(self._h, str(input_path).encode(), 0, 0, threads, self.device, C.byref(h)))
+        return Index(h)
+
+    def write(self, db_dir):
+        """Writes the reference's database layout (meta.json, shards/<shard>/layer_K.{pos,sid,idx})."""
+        check(load().rgl_index_write(self._h, str(db_dir).encode()))
+
     def select_columns(self, sid_lo, sid_hi):
         """A new index holding sources [sid_lo, sid_hi) of this one (sids rebased to 0)."""
         h = C.c_void_p()

@@ -27,14 +27,9 @@
 
 #include "internal.h"
 
-namespace {
+using rgl::BedFile;
 
-struct BedFile {
-    std::string name;                 // file name (the reference's query name)
-    std::vector<std::string> shards;  // in first-appearance order
-    std::vector<std::vector<rgl_interval>> ivs;
-    uint64_t count = 0;
-};
+namespace {
 
 inline bool is_ws(char c) { return c == ' ' || c == '\t' || c == '\n' || c == '\r' || c == '\v' || c == '\f'; }
 
@@ -123,7 +118,11 @@ bool ends_with(const std::string& s, const char* suf) {
     return s.size() >= n && s.compare(s.size() - n, n, suf) == 0;
 }
 
-int read_bed(const std::string& path, uint32_t sid, BedFile* f) {
+}  // namespace
+
+namespace rgl {
+
+int bed_read(const std::string& path, uint32_t sid, BedFile* f) {
     std::vector<char> buf;
     if (ends_with(path, ".gz")) {
         gzFile g = gzopen(path.c_str(), "rb");
@@ -153,7 +152,53 @@ int read_bed(const std::string& path, uint32_t sid, BedFile* f) {
 
 bool is_bed_name(const std::string& n) { return ends_with(n, ".bed") || ends_with(n, ".bed.gz"); }
 
-}  // namespace
+int bed_list(const std::string& root, std::vector<std::string>* paths, bool* is_dir) {
+    struct stat stt;
+    if (stat(root.c_str(), &stt) != 0) return fail(RGL_ERR_INPUT_NOT_FOUND, "input path not found: " + root);
+    *is_dir = S_ISDIR(stt.st_mode);
+    if (*is_dir) {
+        DIR* d = opendir(root.c_str());
+        if (!d) return fail(RGL_ERR_IO, "cannot list " + root);
+        while (dirent* e = readdir(d)) {
+            std::string n = e->d_name;
+            if (!is_bed_name(n)) continue;
+            std::string p = root + (root.back() == '/' ? "" : "/") + n;
+            struct stat fs;
+            if (stat(p.c_str(), &fs) == 0 && S_ISREG(fs.st_mode)) paths->push_back(p);
+        }
+        closedir(d);
+        std::sort(paths->begin(), paths->end());
+    } else {
+        paths->push_back(root);
+    }
+    return RGL_OK;
+}
+
+int bed_read_all(const std::vector<std::string>& paths, uint32_t sid0, uint32_t threads, std::vector<BedFile>* out) {
+    out->assign(paths.size(), BedFile());
+    std::vector<int> status(paths.size(), RGL_OK);
+    std::vector<std::string> errs(paths.size());
+    std::atomic<size_t> next{0};
+    const uint32_t nt = std::max<uint32_t>(1, std::min<uint32_t>(threads ? threads : std::thread::hardware_concurrency(),
+                                                                 (uint32_t)std::max<size_t>(paths.size(), 1)));
+    auto work = [&]() {
+        for (size_t i; (i = next.fetch_add(1)) < paths.size();) {
+            status[i] = bed_read(paths[i], sid0 + (uint32_t)i, &(*out)[i]);
+            if (status[i] != RGL_OK) errs[i] = rgl_last_error();
+        }
+    };
+    std::vector<std::thread> pool;
+    for (uint32_t t = 1; t < nt; t++) pool.emplace_back(work);
+    work();
+    for (auto& t : pool) t.join();
+    for (size_t i = 0; i < paths.size(); i++)  // the first failing file in path order
+        if (status[i] != RGL_OK) return fail(status[i], paths[i] + ": " + errs[i]);
+    return RGL_OK;
+}
+
+}  // namespace rgl
+
+using namespace rgl;
 
 struct rgl_bed_batch {
     std::vector<BedFile> files;  // non-empty files, row = position
@@ -182,43 +227,11 @@ int rgl_bed_batch_load(const char* query_path, uint32_t threads, rgl_bed_batch**
     rgl::clear_error();
     if (!query_path || !out) return rgl::fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
     *out = nullptr;
-    std::string root(query_path);
-    struct stat stt;
-    if (stat(root.c_str(), &stt) != 0) return rgl::fail(RGL_ERR_INPUT_NOT_FOUND, "query path not found: " + root);
     std::vector<std::string> paths;
-    if (S_ISDIR(stt.st_mode)) {
-        DIR* d = opendir(root.c_str());
-        if (!d) return rgl::fail(RGL_ERR_IO, "cannot list " + root);
-        while (dirent* e = readdir(d)) {
-            std::string n = e->d_name;
-            if (!is_bed_name(n)) continue;
-            std::string p = root + (root.back() == '/' ? "" : "/") + n;
-            struct stat fs;
-            if (stat(p.c_str(), &fs) == 0 && S_ISREG(fs.st_mode)) paths.push_back(p);
-        }
-        closedir(d);
-        std::sort(paths.begin(), paths.end());  // files.sort() (files.rs:33)
-    } else {
-        paths.push_back(root);
-    }
-    std::vector<BedFile> parsed(paths.size());
-    std::vector<int> status(paths.size(), RGL_OK);
-    std::vector<std::string> errs(paths.size());
-    std::atomic<size_t> next{0};
-    const uint32_t nt = std::max<uint32_t>(1, std::min<uint32_t>(threads ? threads : std::thread::hardware_concurrency(),
-                                                                 (uint32_t)std::max<size_t>(paths.size(), 1)));
-    auto work = [&]() {
-        for (size_t i; (i = next.fetch_add(1)) < paths.size();) {
-            status[i] = read_bed(paths[i], (uint32_t)i, &parsed[i]);
-            if (status[i] != RGL_OK) errs[i] = rgl_last_error();
-        }
-    };
-    std::vector<std::thread> pool;
-    for (uint32_t t = 1; t < nt; t++) pool.emplace_back(work);
-    work();
-    for (auto& t : pool) t.join();
-    for (size_t i = 0; i < paths.size(); i++)  // the first failing file in path order, as collect()
-        if (status[i] != RGL_OK) return rgl::fail(status[i], paths[i] + ": " + errs[i]);
+    bool is_dir = false;
+    RGL_TRY(bed_list(query_path, &paths, &is_dir));  // files.sort() (files.rs:33)
+    std::vector<BedFile> parsed;
+    RGL_TRY(bed_read_all(paths, 0, threads, &parsed));
     auto* b = new rgl_bed_batch();
     for (size_t i = 0; i < paths.size(); i++) {
         if (!parsed[i].count) continue;  // empty files get no Q_SID (files.rs:80-82)

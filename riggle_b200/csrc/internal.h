@@ -115,6 +115,20 @@ struct SynthTables {
 };
 const SynthTables& synth_tables();
 
+// ---- BED files (bed.cpp) ------------------------------------------------------------------------
+struct BedFile {
+    std::string name;                 // file name
+    std::vector<std::string> shards;  // in first-appearance order
+    std::vector<std::vector<rgl_interval>> ivs;
+    uint64_t count = 0;
+};
+// parse_bed_file (src/io/parse.rs:117-141) of one .bed / .bed.gz file; every interval gets `sid`.
+int bed_read(const std::string& path, uint32_t sid, BedFile* f);
+// The *.bed / *.bed.gz files of a directory sorted by path, or the path itself.
+int bed_list(const std::string& root, std::vector<std::string>* paths, bool* is_dir);
+// Parses paths[i] with sid sid0 + i on `threads` threads (0: all cores).
+int bed_read_all(const std::vector<std::string>& paths, uint32_t sid0, uint32_t threads, std::vector<BedFile>* out);
+
 // ---- query contexts, for the request server --------------------------------------------------
 cudaStream_t context_stream(rgl_context* c);
 int context_reserve_rows(rgl_context* c, uint64_t max_intervals, uint32_t max_rows, uint32_t max_blocks);
