@@ -37,7 +37,7 @@ namespace rgl {
 
 struct RangeDesc {
     uint32_t db_lo, db_hi;      // DB index range within the layer
-    uint32_t i_first, i_last;   // queries whose candidate windows formed the range (sorted positions)
+    uint32_t c_first, c_last;   // live runs (compacted positions) whose windows formed the range
     uint32_t layer_idx;         // index into the layer table
     uint32_t qrow;              // query row (Q_SID)
     uint32_t seg;               // query segment (shard, row)
@@ -233,123 +233,210 @@ __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_
     hi_out[t] = hi;
 }
 
-// Range starts: first query of a segment, or a query whose lo is past every earlier hi.
-__global__ void k_range_flags(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ seg,
-                              const uint32_t* __restrict__ segflag, const int32_t* __restrict__ slot,
+// ---- scans whose length is a device count ------------------------------------------------------
+// After the compaction below, the number of entries (live candidate runs, ranges) is known only on
+// the device; these scans read it there, so the pipeline keeps no host synchronisation (and stays
+// graph-capturable) while its work follows the live count instead of the (query, slot) capacity.
+// Exclusive scan of in[0, n) into out[0, n], out[n] = total: per-tile sums, one block scanning the
+// tile sums, per-tile block scans offset by them.  Launched over the capacity; tiles past n exit.
+constexpr int kScanThreads = 256, kScanItems = 8, kScanTile = kScanThreads * kScanItems;
+
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const Tin* __restrict__ in,
+                                                              const uint32_t* __restrict__ n_ptr,
+                                                              Tout* __restrict__ tile_sums) {
+    const uint32_t n = *n_ptr;
+    const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+    if (base >= n) return;
+    Tout s = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) {
+        const uint64_t i = base + (uint64_t)k * kScanThreads + threadIdx.x;
+        if (i < n) s += (Tout)in[i];
+    }
+    using BR = cub::BlockReduce<Tout, kScanThreads>;
+    __shared__ typename BR::TempStorage tmp;
+    s = BR(tmp).Sum(s);
+    if (threadIdx.x == 0) tile_sums[blockIdx.x] = s;
+}
+
+template <typename Tout>
+__global__ void __launch_bounds__(1024) k_scan_tops(Tout* __restrict__ tile_sums, const uint32_t* __restrict__ n_ptr,
+                                                    Tout* __restrict__ out) {
+    const uint32_t n = *n_ptr;
+    const uint32_t nt = (uint32_t)((n + kScanTile - 1) / kScanTile);
+    using BS = cub::BlockScan<Tout, 1024>;
+    __shared__ typename BS::TempStorage tmp;
+    Tout run = 0;
+    for (uint32_t b0 = 0; b0 < nt; b0 += 1024) {
+        const uint32_t b = b0 + threadIdx.x;
+        Tout v = b < nt ? tile_sums[b] : (Tout)0, ex, agg;
+        BS(tmp).ExclusiveSum(v, ex, agg);
+        if (b < nt) tile_sums[b] = run + ex;
+        run += agg;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[n] = run;
+}
+
+template <typename Tin, typename Tout>
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(const Tin* __restrict__ in, Tout* __restrict__ out,
+                                                             const uint32_t* __restrict__ n_ptr,
+                                                             const Tout* __restrict__ tile_off) {
+    const uint32_t n = *n_ptr;
+    const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
+    if (base >= n) return;
+    const int valid = (int)((uint64_t)n - base < (uint64_t)kScanTile ? (uint64_t)n - base : (uint64_t)kScanTile);
+    using BL = cub::BlockLoad<Tout, kScanThreads, kScanItems, cub::BLOCK_LOAD_WARP_TRANSPOSE>;
+    using BSt = cub::BlockStore<Tout, kScanThreads, kScanItems, cub::BLOCK_STORE_WARP_TRANSPOSE>;
+    using BS = cub::BlockScan<Tout, kScanThreads>;
+    __shared__ union {
+        typename BL::TempStorage load;
+        typename BSt::TempStorage store;
+        typename BS::TempStorage scan;
+    } tmp;
+    Tout v[kScanItems];
+    BL(tmp.load).Load(in + base, v, valid, (Tout)0);
+    __syncthreads();
+    BS(tmp.scan).ExclusiveSum(v, v);
+    const Tout off = tile_off[blockIdx.x];
+#pragma unroll
+    for (int k = 0; k < kScanItems; k++) v[k] += off;
+    __syncthreads();
+    BSt(tmp.store).Store(out + base, v, valid);
+}
+
+// ---- 4b. live candidate runs -------------------------------------------------------------------
+// An entry (K, i) whose run [lo, hi) is empty takes part in nothing: with starts sorted, lo is
+// non-decreasing within a (K, segment) row, so an empty run's hi (= its lo) never exceeds a later
+// entry's lo and can neither merge nor split ranges.  The live entries are compacted (tl[c] = t,
+// c < L) and everything after this works on them.
+__global__ void k_live(uint64_t tot, const uint32_t* __restrict__ lo, const uint32_t* __restrict__ hi,
+                       uint32_t* __restrict__ flag) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t <= tot) flag[t] = (t < tot && hi[t] > lo[t]) ? 1u : 0u;
+}
+
+__global__ void k_compact(uint64_t tot, const uint32_t* __restrict__ lpos, uint32_t* __restrict__ tl,
+                          uint32_t* __restrict__ L_out) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t < tot && lpos[t + 1] != lpos[t]) tl[lpos[t]] = (uint32_t)t;
+    if (t == tot) *L_out = lpos[tot];
+}
+
+// Range starts among the live runs: the first live run of a (K, segment) row, or one whose lo is
+// past the running maximum of hi (maxhi over the row, which empty runs never raise past a later
+// lo); cl = the run's candidate count.
+__global__ void k_crange_flags(const uint32_t* __restrict__ Lp, uint32_t n, const uint32_t* __restrict__ tl,
+                               const uint32_t* __restrict__ segnum, const uint32_t* __restrict__ lo,
+                               const uint32_t* __restrict__ hi, const uint32_t* __restrict__ maxhi,
+                               uint32_t* __restrict__ cflag, uint64_t* __restrict__ ccl) {
+    const uint32_t L = *Lp;
+    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < L; c += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t t = tl[c];
+        bool start = c == 0;
+        if (!start) {
+            const uint32_t tp = tl[c - 1];
+            start = (tp / n != t / n) || (segnum[tp % n] != segnum[t % n]) || (lo[t] >= maxhi[t - 1]);
+        }
+        cflag[c] = start ? 1u : 0u;
+        ccl[c] = (uint64_t)(hi[t] - lo[t]);
+    }
+}
+
+__global__ void k_crange_emit(const uint32_t* __restrict__ Lp, uint32_t n, uint32_t nslots, uint32_t rows,
+                              const uint32_t* __restrict__ tl, const uint32_t* __restrict__ seg,
+                              const uint32_t* __restrict__ segnum, const int32_t* __restrict__ slot,
                               const uint32_t* __restrict__ lo, const uint32_t* __restrict__ maxhi,
-                              uint32_t* __restrict__ rflag) {
-    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    uint64_t total = (uint64_t)n * nslots;
-    if (t > total) return;
-    if (t == total) {
-        rflag[t] = 0;
-        return;
-    }
-    uint32_t K = (uint32_t)(t / n), i = (uint32_t)(t % n);
-    uint32_t shard = seg[i] / rows;
-    int32_t li = slot[(uint64_t)shard * nslots + K];
-    uint32_t f = 0;
-    if (li >= 0) f = (segflag[i] || lo[t] >= maxhi[t - 1]) ? 1u : 0u;
-    rflag[t] = f;
-}
-
-__global__ void k_range_emit(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ seg,
-                             const uint32_t* __restrict__ segflag, const uint32_t* __restrict__ segnum,
-                             const int32_t* __restrict__ slot,
-                             const uint32_t* __restrict__ lo, const uint32_t* __restrict__ maxhi,
-                             const uint32_t* __restrict__ rflag, const uint32_t* __restrict__ ridx,
-                             RangeDesc* __restrict__ ranges) {
-    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    uint64_t total = (uint64_t)n * nslots;
-    if (t >= total) return;
-    uint32_t K = (uint32_t)(t / n), i = (uint32_t)(t % n);
-    uint32_t sg = seg[i];
-    int32_t li = slot[(uint64_t)(sg / rows) * nslots + K];
-    if (li < 0) return;
-    uint32_t f = rflag[t];
-    if (!f && ridx[t] == 0) return;  // unreachable: every valid (K, segment) row starts with a flag
-    uint32_t r = ridx[t] + f - 1;  // inclusive range index of this element
-    if (f) {
-        ranges[r].db_lo = lo[t];
-        ranges[r].i_first = i;
-        ranges[r].layer_idx = (uint32_t)li;
-        ranges[r].qrow = sg % rows;
-        ranges[r].seg = segnum[i] - 1;
-        ranges[r].slot = K;
-    }
-    bool last = (i + 1 == n) || segflag[i + 1] || rflag[t + 1];
-    if (last) {
-        ranges[r].i_last = i;
-        ranges[r].db_hi = maxhi[t];
-    }
-}
-
-// Per range: the reference's candidate count (sum over its queries of hi - lo) against the size of
-// the union.  Where the two are close (narrow layers) the pair sweep reads each candidate once with
-// trivial per-pair work; where candidate windows overlap heavily (broad layers) the rank sweep reads
-// each union element once.  rlen = union length of rank ranges (the rank work space), ulen = union
-// length of every range (the swept count of the metric).
-__global__ void k_range_method(uint64_t cap, uint32_t n, const uint32_t* __restrict__ ridx_total_ptr,
-                               const RangeDesc* __restrict__ ranges, const uint64_t* __restrict__ pc,
-                               uint32_t pair_ratio, uint8_t* __restrict__ method, uint64_t* __restrict__ rlen,
-                               uint64_t* __restrict__ ulen, uint32_t* __restrict__ seg_need) {
-    const uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (r > cap) return;
-    const uint32_t R = *ridx_total_ptr;
-    if (r >= R) {
-        rlen[r] = 0;
-        ulen[r] = 0;
-        return;
-    }
-    const RangeDesc rd = ranges[r];
-    const uint64_t len = rd.db_hi - rd.db_lo;
-    const uint64_t t0 = (uint64_t)rd.slot * n + rd.i_first, t1 = (uint64_t)rd.slot * n + rd.i_last + 1;
-    const uint64_t cand = pc[t1] - pc[t0];
-    const uint8_t m = (cand <= (uint64_t)pair_ratio * len) ? M_PAIR : M_RANK;
-    method[r] = m;
-    if (m == M_RANK && len) seg_need[rd.seg] = 1u;
-    rlen[r] = m == M_RANK ? len : 0;
-    ulen[r] = len;
-}
-
-__global__ void k_cand_len(uint64_t tot, const uint32_t* __restrict__ lo, const uint32_t* __restrict__ hi,
-                           uint64_t* __restrict__ cl) {
-    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (t > tot) return;
-    cl[t] = t < tot ? (uint64_t)(hi[t] - lo[t]) : 0;
-}
-
-// Pair work space: each query of a pair range contributes its candidate run.
-__global__ void k_pair_len(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ seg,
-                           const int32_t* __restrict__ slot, const LayerDev* __restrict__ layers,
-                           const uint32_t* __restrict__ lo, const uint32_t* __restrict__ hi,
-                           const uint32_t* __restrict__ rflag, const uint32_t* __restrict__ ridx,
-                           const uint8_t* __restrict__ method, const uint32_t* __restrict__ starts,
-                           const uint32_t* __restrict__ qend, uint64_t* __restrict__ plen, PairSeg* __restrict__ psegs) {
-    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    const uint64_t tot = (uint64_t)n * nslots;
-    if (t > tot) return;
-    if (t == tot) {
-        plen[t] = 0;
-        return;
-    }
-    const uint32_t K = (uint32_t)(t / n), i = (uint32_t)(t % n);
-    const uint32_t sg = seg[i];
-    const int32_t li = slot[(uint64_t)(sg / rows) * nslots + K];
-    uint64_t len = 0;
-    if (li >= 0) {
-        const uint32_t r = ridx[t] + rflag[t] - 1;
-        if (method[r] == M_PAIR) {
-            len = hi[t] - lo[t];
-            psegs[t] = PairSeg{layers[li].off + lo[t], starts[i], qend[i], sg % rows, sg / rows};
+                              const uint32_t* __restrict__ cflag, const uint32_t* __restrict__ cridx,
+                              RangeDesc* __restrict__ ranges) {
+    const uint32_t L = *Lp;
+    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < L; c += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t t = tl[c], K = t / n, i = t % n;
+        const uint32_t f = cflag[c];
+        const uint32_t r = cridx[c] + f - 1;  // inclusive range index
+        if (f) {
+            const uint32_t sg = seg[i];
+            ranges[r].db_lo = lo[t];
+            ranges[r].c_first = (uint32_t)c;
+            ranges[r].layer_idx = (uint32_t)slot[(uint64_t)(sg / rows) * nslots + K];
+            ranges[r].qrow = sg % rows;
+            ranges[r].seg = segnum[i] - 1;
+            ranges[r].slot = K;
+        }
+        if (c + 1 == L || cflag[c + 1]) {
+            ranges[r].c_last = (uint32_t)c;
+            ranges[r].db_hi = maxhi[t];
         }
     }
-    plen[t] = len;
+}
+
+// Per range: the reference's candidate count (sum over its runs of hi - lo) against the size of the
+// union.  Where the two are close (narrow layers) the pair sweep reads each candidate once with
+// trivial per-pair work; where candidate windows overlap heavily (broad layers) the rank sweep reads
+// each union element once.  rlen = union length of rank ranges (the rank work space); the union of
+// every range is summed into *union_total (the swept count of the metric).
+__global__ void k_crange_method(const uint32_t* __restrict__ Lp, const uint32_t* __restrict__ cridx,
+                                const RangeDesc* __restrict__ ranges, const uint64_t* __restrict__ cpc,
+                                uint32_t pair_ratio, uint8_t* __restrict__ method, uint64_t* __restrict__ rlen,
+                                uint32_t* __restrict__ seg_need, uint32_t* __restrict__ R_out,
+                                unsigned long long* __restrict__ union_total) {
+    const uint32_t R = cridx[*Lp];
+    const uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (g == 0) *R_out = R;
+    unsigned long long acc = 0;
+    for (uint64_t r = g; r < R; r += (uint64_t)gridDim.x * blockDim.x) {
+        const RangeDesc rd = ranges[r];
+        const uint64_t len = rd.db_hi - rd.db_lo;
+        const uint64_t cand = cpc[rd.c_last + 1] - cpc[rd.c_first];
+        const uint8_t m = (cand <= (uint64_t)pair_ratio * len) ? M_PAIR : M_RANK;
+        method[r] = m;
+        if (m == M_RANK && len) seg_need[rd.seg] = 1u;
+        rlen[r] = m == M_RANK ? len : 0;
+        acc += len;
+    }
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31u) == 0 && acc) atomicAdd(union_total, acc);
+}
+
+// Pair work space: each live run of a pair range contributes its candidates.
+__global__ void k_cpair_len(const uint32_t* __restrict__ Lp, uint32_t n, uint32_t nslots, uint32_t rows,
+                            const uint32_t* __restrict__ tl, const uint32_t* __restrict__ seg,
+                            const int32_t* __restrict__ slot, const LayerDev* __restrict__ layers,
+                            const uint32_t* __restrict__ lo, const uint32_t* __restrict__ hi,
+                            const uint32_t* __restrict__ cflag, const uint32_t* __restrict__ cridx,
+                            const uint8_t* __restrict__ method, const uint32_t* __restrict__ starts,
+                            const uint32_t* __restrict__ qend, uint64_t* __restrict__ plen,
+                            PairSeg* __restrict__ psegs) {
+    const uint32_t L = *Lp;
+    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < L; c += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t t = tl[c], K = t / n, i = t % n;
+        const uint32_t r = cridx[c] + cflag[c] - 1;
+        uint64_t len = 0;
+        if (method[r] == M_PAIR) {
+            const uint32_t sg = seg[i];
+            const int32_t li = slot[(uint64_t)(sg / rows) * nslots + K];
+            len = hi[t] - lo[t];
+            psegs[c] = PairSeg{layers[li].off + lo[t], starts[i], qend[i], sg % rows, sg / rows};
+        }
+        plen[c] = len;
+    }
+}
+
+// Totals of the rank and pair work spaces (stats): small[10..11] = rpos[R], small[12..13] = ppos[L].
+__global__ void k_totals(uint32_t* __restrict__ small, const uint64_t* __restrict__ rpos,
+                         const uint64_t* __restrict__ ppos) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        unsigned long long* s64 = reinterpret_cast<unsigned long long*>(small);
+        s64[5] = rpos[small[9]];
+        s64[6] = ppos[small[8]];
+    }
 }
 
 struct SweepParams {
-    const uint64_t* rpos;   // exclusive scan of range lengths, cap+1 entries; rpos[cap] = total
-    uint64_t rcap;          // range capacity (entries of rpos minus one)
+    const uint64_t* rpos;   // exclusive scan of rank-range lengths, R + 1 entries; rpos[R] = total
+    const uint32_t* rcount; // R (device): ranges
+    const uint32_t* pcount; // L (device): live candidate runs
     const RangeDesc* ranges;
     const LayerDev* layers;
     const uint2* pos;
@@ -362,7 +449,7 @@ struct SweepParams {
     unsigned long long* bp;  // rows x D (may be null)
     uint32_t* queue;         // work counter
     const uint32_t* item_r0; // first range of each work item (items < item_cap)
-    const uint64_t* ppos;    // pair work space: exclusive scan of candidate runs, rcap + 1 entries
+    const uint64_t* ppos;    // pair work space: exclusive scan of candidate runs, L + 1 entries
     const PairSeg* psegs;
     const uint32_t* item_t0; // first run of each pair work item
     const SegTab* segtabs;   // per query segment
@@ -424,8 +511,10 @@ __device__ __forceinline__ uint32_t range_advance(const uint64_t* __restrict__ r
 // Work-item partition: item i covers positions [i * chunk, (i + 1) * chunk) of the concatenated
 // ranges; item_r0[i] = the range holding its first position (last r with rpos[r] <= i * chunk),
 // found by binary search over the range offsets (grid-stride over items).
-__global__ void k_item_ranges(uint64_t rcap, const uint64_t* __restrict__ rpos, uint32_t chunk, uint64_t item_cap,
+__global__ void k_item_ranges(const uint32_t* __restrict__ rcount, const uint64_t* __restrict__ rpos, uint32_t chunk,
+                              uint64_t item_cap,
                               uint32_t* __restrict__ item_r0) {
+    const uint32_t rcap = *rcount;
     const uint64_t total = rpos[rcap];
     const uint64_t items = min((total + chunk - 1) / chunk, item_cap);
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < items; i += (uint64_t)gridDim.x * blockDim.x) {
@@ -471,8 +560,8 @@ __device__ __forceinline__ uint32_t rank_end(const SweepParams& P, const SegTab&
     return lo == hi ? lo : ub_u32(P.ends, lo, hi, x);
 }
 
-__device__ __forceinline__ void cursor_seek(const SweepParams& P, Cursor& c, uint64_t p) {
-    if (p >= c.rhi) cursor_load(P, c, range_advance(P.rpos, c.r, (uint32_t)P.rcap, p));
+__device__ __forceinline__ void cursor_seek(const SweepParams& P, Cursor& c, uint64_t p, uint32_t rcap) {
+    if (p >= c.rhi) cursor_load(P, c, range_advance(P.rpos, c.r, rcap, p));
 }
 
 // Base pairs and tally of one DB interval d with a non-zero count (el_s, sl_e already known).
@@ -521,7 +610,8 @@ __global__ void __launch_bounds__(256, 3) k_sweep(SweepParams P) {
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
     const uint32_t lane = threadIdx.x & 31u;
 
-    const uint64_t total = P.rpos[P.rcap];
+    const uint32_t rcap = *P.rcount;
+    const uint64_t total = P.rpos[rcap];
     if (P.smem_tally) {
         for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
             s_cnt[k] = 0;
@@ -546,7 +636,7 @@ __global__ void __launch_bounds__(256, 3) k_sweep(SweepParams P) {
         if (item < P.item_cap) {
             r0 = __ldg(P.item_r0 + item);
         } else {
-            uint64_t lo = 0, hi = P.rcap;
+            uint64_t lo = 0, hi = rcap;
             while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (__ldg(P.rpos + m) <= p0) lo = m; else hi = m - 1; }
             r0 = (uint32_t)lo;
         }
@@ -554,7 +644,7 @@ __global__ void __launch_bounds__(256, 3) k_sweep(SweepParams P) {
         cursor_load(P, c, r0);
         for (uint64_t pb = p0 + lane; pb < p1; pb += 32 * kUnroll) {
             const uint64_t plast = min(pb + 32 * (kUnroll - 1), p1 - 1 - ((p1 - 1 - pb) & 31));
-            cursor_seek(P, c, pb);
+            cursor_seek(P, c, pb, rcap);
             if (plast < c.rhi) {
                 // all of this lane's positions of the step lie in one range: batch the loads
                 const SegTab t = c.tab;
@@ -589,7 +679,7 @@ __global__ void __launch_bounds__(256, 3) k_sweep(SweepParams P) {
             } else {
                 // the step crosses a range boundary: one position at a time
                 for (uint64_t pj = pb; pj < p1 && pj <= pb + 32 * (kUnroll - 1); pj += 32) {
-                    cursor_seek(P, c, pj);
+                    cursor_seek(P, c, pj, rcap);
                     const uint64_t di = c.base + (pj - c.rlo);
                     const uint2 d = __ldg(P.pos + di);
                     const uint32_t el_s = rank_end(P, c.tab, d.x);
@@ -620,7 +710,8 @@ __global__ void __launch_bounds__(256, 4) k_pairs(SweepParams P) {
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
     const uint32_t lane = threadIdx.x & 31u;
-    const uint64_t total = P.ppos[P.rcap];
+    const uint32_t rcap = *P.pcount;
+    const uint64_t total = P.ppos[rcap];
     if (P.smem_tally)
         for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
             s_cnt[k] = 0;
@@ -638,7 +729,7 @@ __global__ void __launch_bounds__(256, 4) k_pairs(SweepParams P) {
         if (item < P.item_cap) {
             t = __ldg(P.item_t0 + item);
         } else {
-            uint64_t lo = 0, hi = P.rcap;
+            uint64_t lo = 0, hi = rcap;
             while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (__ldg(P.ppos + m) <= p0) lo = m; else hi = m - 1; }
             t = (uint32_t)lo;
         }
@@ -646,7 +737,7 @@ __global__ void __launch_bounds__(256, 4) k_pairs(SweepParams P) {
         PairSeg ps = P.psegs[t];
         for (uint64_t p = p0 + lane; p < p1; p += 32) {
             if (p >= rhi) {
-                t = range_advance(P.ppos, t, (uint32_t)P.rcap, p);
+                t = range_advance(P.ppos, t, rcap, p);
                 rlo = __ldg(P.ppos + t);
                 rhi = __ldg(P.ppos + t + 1);
                 ps = P.psegs[t];
@@ -682,7 +773,8 @@ __global__ void __launch_bounds__(256, 4) k_pairs(SweepParams P) {
 // offset (an exclusive scan of the counts) at their ballot ranks, so the list needs no atomics and
 // comes out in the same order every time.
 template <bool EMIT>
-__global__ void __launch_bounds__(256) k_pair_list(const uint64_t* __restrict__ ppos, uint64_t rcap,
+__global__ void __launch_bounds__(256) k_pair_list(const uint64_t* __restrict__ ppos,
+                                                   const uint32_t* __restrict__ pcount,
                                                    const PairSeg* __restrict__ psegs, const uint2* __restrict__ pos,
                                                    const uint32_t* __restrict__ sid, uint64_t items, uint32_t chunk,
                                                    uint64_t* __restrict__ item_hits,
@@ -690,6 +782,7 @@ __global__ void __launch_bounds__(256) k_pair_list(const uint64_t* __restrict__ 
     const uint32_t lane = threadIdx.x & 31u;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint32_t rcap = *pcount;
     const uint64_t total = ppos[rcap];
     for (uint64_t item = warp; item < items; item += nwarps) {
         const uint64_t p0 = item * chunk, p1 = min(p0 + chunk, total);
@@ -710,7 +803,7 @@ __global__ void __launch_bounds__(256) k_pair_list(const uint64_t* __restrict__ 
             uint64_t di = 0;
             if (p < p1) {
                 if (p >= rhi) {
-                    t = range_advance(ppos, t, (uint32_t)rcap, p);
+                    t = range_advance(ppos, t, rcap, p);
                     rlo = __ldg(ppos + t);
                     rhi = __ldg(ppos + t + 1);
                     ps = psegs[t];
@@ -756,7 +849,7 @@ struct rgl_context {
     DevBuf starts, ends, seg, segflag, segnum, seg_begin, ps_in, pe_in, ps, pe;
     DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp, item_r0;
     DevBuf segtab, tab_len, tab_off, tab_s, tab_e, tab_xs, tab_xe;
-    DevBuf cl, pc, method, ulen, plen, ppos, psegs, item_t0, seg_need;
+    DevBuf cl, pc, method, plen, ppos, psegs, item_t0, seg_need, lpos, tl, scan_sums;
     DevBuf item_hits, item_base, pairs;  // intervals mode
     DevBuf bt_off, bt_shard, acc;  // batched form: sub-batch block tables (offsets; shards then rows), stats
     uint32_t* h_small = nullptr;  // pinned mirror of `small`
@@ -836,7 +929,9 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     RGL_TRY(c->cl.ensure(tot * 8 + 16));
     RGL_TRY(c->pc.ensure(tot * 8 + 16));
     RGL_TRY(c->method.ensure(tot + 16));
-    RGL_TRY(c->ulen.ensure(tot * 8 + 16));
+    RGL_TRY(c->lpos.ensure(tot * 4 + 8));
+    RGL_TRY(c->tl.ensure(tot * 4 + 8));
+    RGL_TRY(c->scan_sums.ensure((tot / kScanTile + 4) * 8));
     RGL_TRY(c->plen.ensure(tot * 8 + 16));
     RGL_TRY(c->ppos.ensure(tot * 8 + 16));
     RGL_TRY(c->psegs.ensure(tot * sizeof(PairSeg) + sizeof(PairSeg)));
@@ -886,7 +981,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
                       &c->ends, &c->seg, &c->segflag, &c->segnum, &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps,
                       &c->pe, &c->lo, &c->hi, &c->maxhi, &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos,
                       &c->cub_tmp, &c->small, &c->item_r0, &c->item_t0, &c->segtab, &c->tab_len, &c->tab_off,
-                      &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->cl, &c->pc, &c->method, &c->ulen, &c->plen, &c->ppos, &c->psegs,
+                      &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs,
                       &c->seg_need, &c->acc})
         sig = (sig ^ (uint64_t)(uintptr_t)b->p ^ ((uint64_t)b->cap << 17)) * 1099511628211ull;
     c->ws_sig = sig;
@@ -938,14 +1033,16 @@ int finish(rgl_context* c, const Launch& L, rgl_query_stats* stats) {
             RGL_CUDA(cudaEventElapsedTime(&t_all, c->ev[0], c->ev[2]));
         }
         stats->query_intervals = c->last_n;
-        stats->ranges = c->last_n ? c->h_small[2] : 0;
+        // the pipeline's device counters (small[4..5] union, [9] ranges, [10..11] / [12..13] rank /
+        // pair work) were copied to h_small after the run
+        stats->ranges = c->last_n ? c->h_small[9] : 0;
         uint64_t T = 0;
         if (c->last_n) std::memcpy(&T, c->h_small + 4, 8);
         stats->db_swept = T;
         uint64_t TR = 0, TP = 0;
         if (c->last_n) {
-            std::memcpy(&TR, c->h_small + 6, 8);
-            std::memcpy(&TP, c->h_small + 8, 8);
+            std::memcpy(&TR, c->h_small + 10, 8);
+            std::memcpy(&TP, c->h_small + 12, 8);
         }
         stats->rank_positions = TR;
         stats->pair_candidates = TP;
@@ -960,6 +1057,17 @@ int finish(rgl_context* c, const Launch& L, rgl_query_stats* stats) {
     if (c->h_small[0] & ERR_BAD_INTERVAL) return fail(RGL_ERR_INVALID_ARGUMENT, "a query interval has start >= end");
     if (c->h_small[0] & ERR_BAD_ROW) return fail(RGL_ERR_INVALID_ARGUMENT, "a query interval's sid >= num_rows");
     return RGL_OK;
+}
+
+// Exclusive scan of in[0, *n_ptr) into out (with out[n] = total), n <= cap; returns the launches.
+template <typename Tin, typename Tout>
+uint32_t scan_dev(rgl_context* c, const Tin* in, Tout* out, const uint32_t* n_ptr, uint64_t cap, cudaStream_t st) {
+    const unsigned tiles = (unsigned)(cap / kScanTile + 1);
+    Tout* sums = c->scan_sums.as<Tout>();
+    k_scan_reduce<Tin, Tout><<<tiles, kScanThreads, 0, st>>>(in, n_ptr, sums);
+    k_scan_tops<Tout><<<1, 1024, 0, st>>>(sums, n_ptr, out);
+    k_scan_apply<Tin, Tout><<<tiles, kScanThreads, 0, st>>>(in, out, n_ptr, sums);
+    return 3;
 }
 
 // Input of one pipeline run: n intervals at `iv` (device), block b = [blk_off[b], blk_off[b+1]) on
@@ -1063,6 +1171,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     launches++;
     RGL_CUDA(cudaMemsetAsync(c->seg_need.p, 0, (size_t)(n + 1) * 4, st));
     const uint64_t tot = (uint64_t)n * ns;
+    if (tot + 1 >= (1ull << 31)) return fail(RGL_ERR_INVALID_ARGUMENT, "query intervals x layer slots must be < 2^31 per run");
     k_lohi<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, rows, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
                                                 c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, idx->d_pos,
                                                 c->lo.as<uint32_t>(), c->hi.as<uint32_t>());
@@ -1074,30 +1183,33 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                                      c->maxhi.as<uint32_t>() + (uint64_t)K * n, MaxOp(), (int)n,
                                                      cub::Equality(), st));
     }
-    k_range_flags<<<grid_for(tot + 1, 256), 256, 0, st>>>(n, ns, rows, c->seg.as<uint32_t>(),
-                                                          c->segflag.as<uint32_t>(), idx->d_slot,
-                                                          c->lo.as<uint32_t>(), c->maxhi.as<uint32_t>(),
-                                                          c->rflag.as<uint32_t>());
-    launches++;
+    // live runs: compaction of the (K, query) entries with a non-empty candidate run
+    k_live<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
+                                                   c->rflag.as<uint32_t>());
     tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->rflag.as<uint32_t>(), c->lpos.as<uint32_t>(),
                                            (int)(tot + 1), st));
-    k_range_emit<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, rows, c->seg.as<uint32_t>(), c->segflag.as<uint32_t>(),
-                                                     c->segnum.as<uint32_t>(), idx->d_slot, c->lo.as<uint32_t>(), c->maxhi.as<uint32_t>(),
-                                                     c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
-                                                     c->ranges.as<RangeDesc>());
+    uint32_t* Lp = d_small + 8;  // live runs L
+    uint32_t* Rp = d_small + 9;  // ranges R
+    k_compact<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, c->lpos.as<uint32_t>(), c->tl.as<uint32_t>(), Lp);
+    launches += 2;
+    // ranges over the live runs, their candidate counts and methods
+    const unsigned gc = (unsigned)std::min<uint64_t>(grid_for(tot, 256), (uint64_t)c->num_sms * 32);
+    k_crange_flags<<<gc, 256, 0, st>>>(Lp, n, c->tl.as<uint32_t>(), c->segnum.as<uint32_t>(), c->lo.as<uint32_t>(),
+                                       c->hi.as<uint32_t>(), c->maxhi.as<uint32_t>(), c->rflag.as<uint32_t>(),
+                                       c->cl.as<uint64_t>());
     launches++;
-    // candidate counts per (K, query) -> per-range method; rank and pair work spaces
-    k_cand_len<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
-                                                       c->cl.as<uint64_t>());
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->cl.as<uint64_t>(), c->pc.as<uint64_t>(),
-                                           (int)(tot + 1), st));
-    k_range_method<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, n, c->ridx.as<uint32_t>() + tot,
-                                                           c->ranges.as<RangeDesc>(), c->pc.as<uint64_t>(),
-                                                           L.pair_ratio, c->method.as<uint8_t>(),
-                                                           c->rlen.as<uint64_t>(), c->ulen.as<uint64_t>(),
-                                                           c->seg_need.as<uint32_t>());
+    launches += scan_dev(c, c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(), Lp, tot, st);
+    launches += scan_dev(c, c->cl.as<uint64_t>(), c->pc.as<uint64_t>(), Lp, tot, st);
+    k_crange_emit<<<gc, 256, 0, st>>>(Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(),
+                                      c->segnum.as<uint32_t>(), idx->d_slot, c->lo.as<uint32_t>(),
+                                      c->maxhi.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
+                                      c->ranges.as<RangeDesc>());
+    k_crange_method<<<gc, 256, 0, st>>>(Lp, c->ridx.as<uint32_t>(), c->ranges.as<RangeDesc>(), c->pc.as<uint64_t>(),
+                                        L.pair_ratio, c->method.as<uint8_t>(), c->rlen.as<uint64_t>(),
+                                        c->seg_need.as<uint32_t>(), Rp,
+                                        reinterpret_cast<unsigned long long*>(d_small + 4));
+    launches += 2;
     // rank tables of the query segments that have a rank-difference range
     k_seg_tabsize<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->seg_begin.as<uint32_t>(),
                                                         c->seg_need.as<uint32_t>(), c->ends.as<uint32_t>(),
@@ -1121,22 +1233,15 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     RGL_CUDA(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tb, c->tab_xe.as<uint32_t>(), c->tab_e.as<uint32_t>(),
                                            (int)tab_cap, st));
     launches += 3;
-    k_pair_len<<<grid_for(tot + 1, 256), 256, 0, st>>>(n, ns, rows, c->seg.as<uint32_t>(), idx->d_slot,
-                                                       idx->d_layers, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
-                                                       c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
-                                                       c->method.as<uint8_t>(), c->starts.as<uint32_t>(),
-                                                       c->val_b.as<uint32_t>(), c->plen.as<uint64_t>(),
-                                                       c->psegs.as<PairSeg>());
-    launches += 3;
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(),
-                                           (int)(tot + 1), st));
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->plen.as<uint64_t>(), c->ppos.as<uint64_t>(),
-                                           (int)(tot + 1), st));
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceReduce::Sum(c->cub_tmp.p, tb, c->ulen.as<uint64_t>(),
-                                    reinterpret_cast<uint64_t*>(d_small + 4), (int)tot, st));
+    k_cpair_len<<<gc, 256, 0, st>>>(Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), idx->d_slot,
+                                    idx->d_layers, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(), c->rflag.as<uint32_t>(),
+                                    c->ridx.as<uint32_t>(), c->method.as<uint8_t>(), c->starts.as<uint32_t>(),
+                                    c->val_b.as<uint32_t>(), c->plen.as<uint64_t>(), c->psegs.as<PairSeg>());
+    launches++;
+    launches += scan_dev(c, c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(), Rp, tot, st);
+    launches += scan_dev(c, c->plen.as<uint64_t>(), c->ppos.as<uint64_t>(), Lp, tot, st);
+    k_totals<<<1, 32, 0, st>>>(d_small, c->rpos.as<uint64_t>(), c->ppos.as<uint64_t>());
+    launches++;
     if (mode.no_sweep) {
         c->last_tot = tot;
         c->last_launches = launches;
@@ -1144,9 +1249,9 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
         if (mode.reset_err) RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
         return RGL_OK;
     }
-    k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(tot, c->rpos.as<uint64_t>(), L.chunk, kItemCap,
+    k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(Rp, c->rpos.as<uint64_t>(), L.chunk, kItemCap,
                                                                c->item_r0.as<uint32_t>());
-    k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(tot, c->ppos.as<uint64_t>(), L.chunk, kItemCap,
+    k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(Lp, c->ppos.as<uint64_t>(), L.chunk, kItemCap,
                                                                c->item_t0.as<uint32_t>());
     launches += 2;
     SweepParams P;
@@ -1159,7 +1264,8 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     P.tab_e = c->tab_e.as<uint32_t>();
     P.item_cap = kItemCap;
     P.rpos = c->rpos.as<uint64_t>();
-    P.rcap = tot;
+    P.rcount = Rp;
+    P.pcount = Lp;
     P.ranges = c->ranges.as<RangeDesc>();
     P.layers = idx->d_layers;
     P.pos = idx->d_pos;
@@ -1190,10 +1296,9 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     RGL_CUDA(cudaGetLastError());
     if (c->timing && mode.events) RGL_TRY(timing_record(c, false));
     if (mode.acc) {
-        k_acc_stats<<<1, 32, 0, st>>>(mode.acc, c->ridx.as<uint32_t>() + tot,
-                                      reinterpret_cast<unsigned long long*>(d_small + 4),
-                                      c->rpos.as<unsigned long long>() + tot, c->ppos.as<unsigned long long>() + tot,
-                                      n);
+        k_acc_stats<<<1, 32, 0, st>>>(mode.acc, d_small + 9, reinterpret_cast<unsigned long long*>(d_small + 4),
+                                      reinterpret_cast<unsigned long long*>(d_small + 10),
+                                      reinterpret_cast<unsigned long long*>(d_small + 12), n);
         launches++;
     }
     c->last_tot = tot;
@@ -1201,10 +1306,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     c->last_n = n;
     if (ev) {
         RGL_CUDA(cudaEventRecord(c->ev[2], st));
-        RGL_CUDA(cudaMemcpyAsync(c->h_small + 2, c->ridx.as<uint32_t>() + tot, 4, cudaMemcpyDeviceToHost, st));
-        RGL_CUDA(cudaMemcpyAsync(c->h_small + 4, d_small + 4, 8, cudaMemcpyDeviceToHost, st));
-        RGL_CUDA(cudaMemcpyAsync(c->h_small + 6, c->rpos.as<uint64_t>() + tot, 8, cudaMemcpyDeviceToHost, st));
-        RGL_CUDA(cudaMemcpyAsync(c->h_small + 8, c->ppos.as<uint64_t>() + tot, 8, cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaMemcpyAsync(c->h_small + 4, d_small + 4, 48, cudaMemcpyDeviceToHost, st));
     }
     if (mode.reset_err) RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
     return RGL_OK;
@@ -1483,7 +1585,7 @@ int rgl_context_destroy(rgl_context* c) {
                       &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos, &c->cub_tmp, &c->small,
                       &c->out_counts, &c->out_bp, &c->item_r0,
                       &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe,
-                      &c->cl, &c->pc, &c->method, &c->ulen, &c->plen, &c->ppos, &c->psegs, &c->item_t0,
+                      &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs, &c->item_t0,
                       &c->seg_need, &c->item_hits, &c->item_base, &c->pairs, &c->bt_off, &c->bt_shard, &c->acc, &c->gc.t_off, &c->gc.t_shard};
     if (c->gc.exec) cudaGraphExecDestroy(c->gc.exec);
     if (c->gc.graph) cudaGraphDestroy(c->gc.graph);
@@ -1909,9 +2011,9 @@ int rgl_query_pairs(rgl_context* c, const rgl_query_batch* b, uint64_t capacity,
     RGL_CUDA(cudaStreamSynchronize(st));
     RGL_TRY(finish(c, pick_launch(&q), nullptr));
     if (!n || !c->idx->num_slots) return RGL_OK;
-    const uint64_t tot = c->last_tot;
-    uint64_t positions = 0;
-    RGL_CUDA(cudaMemcpy(&positions, c->ppos.as<uint64_t>() + tot, 8, cudaMemcpyDeviceToHost));
+    uint64_t positions = 0;  // the pair work space total, small[12..13]
+    RGL_CUDA(cudaMemcpy(&positions, c->small.as<uint32_t>() + 12, 8, cudaMemcpyDeviceToHost));
+    const uint32_t* Lp = c->small.as<uint32_t>() + 8;
     const uint32_t chunk = 2048;
     const uint64_t items = (positions + chunk - 1) / chunk;
     if (!items) return RGL_OK;
@@ -1922,7 +2024,7 @@ int rgl_query_pairs(rgl_context* c, const rgl_query_batch* b, uint64_t capacity,
     RGL_TRY(c->cub_tmp.ensure(tb + 256));
     const unsigned grid = (unsigned)std::min<uint64_t>((items * 32 + 255) / 256, (uint64_t)c->num_sms * 16);
     RGL_CUDA(cudaMemsetAsync(c->item_hits.as<uint64_t>() + items, 0, 8, st));
-    k_pair_list<false><<<grid, 256, 0, st>>>(c->ppos.as<uint64_t>(), tot, c->psegs.as<PairSeg>(), c->idx->d_pos,
+    k_pair_list<false><<<grid, 256, 0, st>>>(c->ppos.as<uint64_t>(), Lp, c->psegs.as<PairSeg>(), c->idx->d_pos,
                                              c->idx->d_sid, items, chunk, c->item_hits.as<uint64_t>(), nullptr,
                                              nullptr);
     tb = c->cub_tmp.cap;
@@ -1935,7 +2037,7 @@ int rgl_query_pairs(rgl_context* c, const rgl_query_batch* b, uint64_t capacity,
     if (!pairs || !hits) return RGL_OK;
     if (capacity < hits) return fail(RGL_ERR_INVALID_ARGUMENT, "pair capacity too small (needs " + std::to_string(hits) + ")");
     RGL_TRY(c->pairs.ensure(hits * sizeof(rgl_pair)));
-    k_pair_list<true><<<grid, 256, 0, st>>>(c->ppos.as<uint64_t>(), tot, c->psegs.as<PairSeg>(), c->idx->d_pos,
+    k_pair_list<true><<<grid, 256, 0, st>>>(c->ppos.as<uint64_t>(), Lp, c->psegs.as<PairSeg>(), c->idx->d_pos,
                                             c->idx->d_sid, items, chunk, nullptr, c->item_base.as<uint64_t>(),
                                             c->pairs.as<rgl_pair>());
     RGL_CUDA(cudaGetLastError());
