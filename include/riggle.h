@@ -263,7 +263,7 @@ typedef struct rgl_batch {
 
 typedef struct rgl_batch_opts {
     rgl_query_opts query; /* launch shape of every sub-batch (zeros: tuned shape or defaults) */
-    uint64_t sub_batch;   /* query intervals per sub-batch, the unit of device workspace (0: 2^24) */
+    uint64_t sub_batch;   /* query intervals per sub-batch, the unit of device workspace (0: 2^25) */
     uint32_t flags;       /* RGL_BF_* */
 } rgl_batch_opts;
 

@@ -51,6 +51,17 @@ __global__ void k_validate_layer(const uint2* __restrict__ pos, const uint32_t* 
     if (f && (threadIdx.x & 31) == 0) atomicOr(flags, f);
 }
 
+// Bucket table of one sorted layer: thread j writes j into the buckets after element j-1's bucket
+// up to its own (j == n: up to the last entry), so tab[b] = first j with start_j >= b << s.
+__global__ void k_bucket_fill(const uint2* __restrict__ pos, uint64_t n, uint32_t s, uint32_t nb,
+                              uint32_t* __restrict__ tab) {
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j <= n; j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t lo_b = j == 0 ? 0u : (pos[j - 1].x >> s) + 1u;
+        const uint32_t hi_b = j == n ? nb - 1u : (pos[j].x >> s);
+        for (uint32_t b = lo_b; b <= hi_b && b < nb; b++) tab[b] = (uint32_t)j;
+    }
+}
+
 int index_alloc(rgl_index* idx) {
     uint64_t off = 0;
     for (auto& l : idx->layers)
@@ -104,6 +115,30 @@ int index_finalize(rgl_index* idx) {
                         where + ": an interval has start >= end or a size outside its layer's class "
                                 "(the reference's add never writes one)");
     }
+    // bucket tables: widths 2^s >= (max start + 1) / n, so about one interval per bucket and at most
+    // n + 2 entries (4 bytes per interval)
+    uint64_t btot = 0;
+    for (LayerDev& l : idx->layers) {
+        uint32_t maxstart = 0;
+        if (l.n) RGL_CUDA(cudaMemcpy(&maxstart, &idx->d_pos[l.off + l.n - 1].x, 4, cudaMemcpyDeviceToHost));
+        const uint64_t ratio = l.n ? ((uint64_t)maxstart + 1 + l.n - 1) / l.n : 1;
+        uint32_t sh = 0;
+        while (sh < 31 && (1ull << sh) < ratio) sh++;
+        l.bshift = sh;
+        l.nb = (maxstart >> sh) + 2;
+        l.boff = btot;
+        btot += l.nb;
+    }
+    if (idx->d_btab) cudaFree(idx->d_btab);
+    idx->d_btab = nullptr;
+    RGL_CUDA(cudaMalloc(&idx->d_btab, std::max<uint64_t>(btot, 1) * 4));
+    idx->device_bytes += std::max<uint64_t>(btot, 1) * 4;
+    for (const LayerDev& l : idx->layers) {
+        const unsigned blocks = (unsigned)std::min<uint64_t>((l.n + 256) / 256, 148ull * 32);
+        k_bucket_fill<<<blocks, 256>>>(idx->d_pos + l.off, l.n, l.bshift, l.nb, idx->d_btab + l.boff);
+    }
+    RGL_CUDA(cudaGetLastError());
+    RGL_CUDA(cudaDeviceSynchronize());
     if (!idx->layers.empty())
         RGL_CUDA(cudaMemcpy(idx->d_layers, idx->layers.data(), idx->layers.size() * sizeof(LayerDev),
                             cudaMemcpyHostToDevice));
@@ -125,6 +160,8 @@ void index_free(rgl_index* idx) {
     if (idx->d_pos) cudaFree(idx->d_pos);
     if (idx->d_sid) cudaFree(idx->d_sid);
     if (idx->d_layers) cudaFree(idx->d_layers);
+    if (idx->d_btab) cudaFree(idx->d_btab);
+    idx->d_btab = nullptr;
     if (idx->d_slot) cudaFree(idx->d_slot);
     idx->d_pos = nullptr;
     idx->d_sid = nullptr;

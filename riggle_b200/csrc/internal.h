@@ -48,6 +48,10 @@ struct LayerDev {
     uint32_t shard;
     uint32_t layer;
     uint32_t flags;  // LF_* bits from validation
+    // bucket table (built by index_finalize): d_btab[boff + b] = #(start < b << bshift) for b < nb,
+    // buckets of 2^bshift bp holding about one interval each; d_btab[boff + nb - 1] = n
+    uint64_t boff;
+    uint32_t bshift, nb;
 };
 enum : uint32_t { LF_UNSORTED = 1u, LF_BAD_SID = 2u, LF_EMPTY_IV = 4u, LF_OVERSIZE = 8u };
 
@@ -78,6 +82,7 @@ struct rgl_index {
     uint2* d_pos = nullptr;
     uint32_t* d_sid = nullptr;
     rgl::LayerDev* d_layers = nullptr;
+    uint32_t* d_btab = nullptr;         // bucket tables of all layers
     int32_t* d_slot = nullptr;
     uint64_t device_bytes = 0;
     // one reference for the handle returned to the caller plus one per live context; the device

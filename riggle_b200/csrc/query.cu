@@ -85,9 +85,13 @@ __device__ __forceinline__ uint32_t ub_u32(const uint32_t* __restrict__ a, uint3
     }
     return lo;
 }
-__device__ __forceinline__ uint32_t pp_layer(const uint2* __restrict__ pos, uint32_t n, uint32_t x) {
-    // partition point of (start < x) over a layer sorted by start
-    uint32_t lo = 0, hi = n;
+__device__ __forceinline__ uint32_t pp_layer(const uint2* __restrict__ pos, const uint32_t* __restrict__ btab,
+                                             const LayerDev& L, uint32_t x) {
+    // partition point of (start < x) over a layer sorted by start: the bucket table gives the
+    // elements whose starts share x's bucket, searched by bisection
+    const uint32_t b = x >> L.bshift;
+    if (b >= L.nb - 1) return (uint32_t)L.n;
+    uint32_t lo = __ldg(btab + b), hi = __ldg(btab + b + 1);
     while (lo < hi) {
         uint32_t m = lo + ((hi - lo) >> 1);
         if (__ldg(&pos[m].x) < x) lo = m + 1; else hi = m;
@@ -184,6 +188,19 @@ __global__ void k_seg_tabsize(uint32_t n, const uint32_t* __restrict__ segnum, c
 // With the per-bin counts placed one entry to the right (bin b at entry b + 1) and every other
 // segment's single entry holding its element count, an inclusive scan over all segments' entries
 // yields exactly that: everything before a segment's first entry sums to its `beg`.
+// Zeroes the count arrays over the tables' actual size (tab_off[number of segments]) and records
+// that size in *count for the scans.
+__global__ void k_tab_zero(uint32_t n, const uint32_t* __restrict__ segnum, const uint32_t* __restrict__ tab_off,
+                           uint32_t* __restrict__ xs, uint32_t* __restrict__ xe, uint32_t* __restrict__ count) {
+    const uint32_t total = tab_off[segnum[n - 1]];
+    const uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (g == 0) *count = total;
+    for (uint64_t i = g; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+        xs[i] = 0;
+        xe[i] = 0;
+    }
+}
+
 __global__ void k_tab_place(uint32_t n, const uint32_t* __restrict__ segnum, SegTab* __restrict__ tabs,
                             const uint32_t* __restrict__ tab_off, uint32_t* __restrict__ xs, uint32_t* __restrict__ xe) {
     const uint32_t sgi = blockIdx.x * blockDim.x + threadIdx.x;
@@ -213,7 +230,8 @@ __global__ void k_tab_count(uint32_t n, const uint32_t* __restrict__ segnum, con
 __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ starts,
                        const uint32_t* __restrict__ qend, const uint32_t* __restrict__ seg,
                        const int32_t* __restrict__ slot, const LayerDev* __restrict__ layers,
-                       const uint2* __restrict__ pos, uint32_t* __restrict__ lo_out, uint32_t* __restrict__ hi_out) {
+                       const uint2* __restrict__ pos, const uint32_t* __restrict__ btab,
+                       uint32_t* __restrict__ lo_out, uint32_t* __restrict__ hi_out) {
     uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (t >= (uint64_t)n * nslots) return;
     uint32_t K = (uint32_t)(t / n), i = (uint32_t)(t % n);
@@ -225,8 +243,9 @@ __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_
         const uint2* p = pos + L.off;
         uint32_t s = starts[i];
         uint32_t back = s >= L.max_size ? s - L.max_size : 0u;  // saturating_sub, query.rs:141
-        lo = pp_layer(p, (uint32_t)L.n, back);
-        hi = pp_layer(p, (uint32_t)L.n, qend[i]);
+        const uint32_t* bt = btab + L.boff;
+        lo = pp_layer(p, bt, L, back);
+        hi = pp_layer(p, bt, L, qend[i]);
         if (hi < lo) hi = lo;
     }
     lo_out[t] = lo;
@@ -931,15 +950,15 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     RGL_TRY(c->method.ensure(tot + 16));
     RGL_TRY(c->lpos.ensure(tot * 4 + 8));
     RGL_TRY(c->tl.ensure(tot * 4 + 8));
-    RGL_TRY(c->scan_sums.ensure((tot / kScanTile + 4) * 8));
+    RGL_TRY(c->scan_sums.ensure((std::max<uint64_t>(tot, 10 * n + 16) / kScanTile + 4) * 8));
     RGL_TRY(c->plen.ensure(tot * 8 + 16));
     RGL_TRY(c->ppos.ensure(tot * 8 + 16));
     RGL_TRY(c->psegs.ensure(tot * sizeof(PairSeg) + sizeof(PairSeg)));
     RGL_TRY(c->segtab.ensure((n + 1) * sizeof(SegTab)));
     RGL_TRY(c->tab_len.ensure((n + 2) * 4));
     RGL_TRY(c->tab_off.ensure((n + 2) * 4));
-    RGL_TRY(c->tab_s.ensure((10 * n + 16) * 4));
-    RGL_TRY(c->tab_e.ensure((10 * n + 16) * 4));
+    RGL_TRY(c->tab_s.ensure((10 * n + 18) * 4));
+    RGL_TRY(c->tab_e.ensure((10 * n + 18) * 4));
     RGL_TRY(c->tab_xs.ensure((10 * n + 16) * 4));
     RGL_TRY(c->tab_xe.ensure((10 * n + 16) * 4));
     RGL_TRY(c->acc.ensure(64));
@@ -1174,7 +1193,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     if (tot + 1 >= (1ull << 31)) return fail(RGL_ERR_INVALID_ARGUMENT, "query intervals x layer slots must be < 2^31 per run");
     k_lohi<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, rows, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
                                                 c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, idx->d_pos,
-                                                c->lo.as<uint32_t>(), c->hi.as<uint32_t>());
+                                                idx->d_btab, c->lo.as<uint32_t>(), c->hi.as<uint32_t>());
     launches++;
     for (uint32_t K = 0; K < ns; K++) {
         tb = c->cub_tmp.cap;
@@ -1218,21 +1237,21 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->tab_len.as<uint32_t>(), c->tab_off.as<uint32_t>(),
                                            (int)n + 1, st));
     const uint64_t tab_cap = 10ull * n + 16;
-    RGL_CUDA(cudaMemsetAsync(c->tab_xs.p, 0, tab_cap * 4, st));
-    RGL_CUDA(cudaMemsetAsync(c->tab_xe.p, 0, tab_cap * 4, st));
+    uint32_t* tab_count = d_small + 14;
+    k_tab_zero<<<(unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, st>>>(
+        n, c->segnum.as<uint32_t>(), c->tab_off.as<uint32_t>(), c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>(),
+        tab_count);
     k_tab_place<<<grid_for(n, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
                                                   c->tab_off.as<uint32_t>(), c->tab_xs.as<uint32_t>(),
                                                   c->tab_xe.as<uint32_t>());
     k_tab_count<<<grid_for(n, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
                                                   c->starts.as<uint32_t>(), c->ends.as<uint32_t>(),
                                                   c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>());
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tb, c->tab_xs.as<uint32_t>(), c->tab_s.as<uint32_t>(),
-                                           (int)tab_cap, st));
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tb, c->tab_xe.as<uint32_t>(), c->tab_e.as<uint32_t>(),
-                                           (int)tab_cap, st));
-    launches += 3;
+    // inclusive scans written one entry ahead: exclusive scan into tab_* whose entry k + 1 is the
+    // inclusive sum through k (the tables are read from tab_* + 1)
+    launches += scan_dev(c, c->tab_xs.as<uint32_t>(), c->tab_s.as<uint32_t>(), tab_count, tab_cap, st);
+    launches += scan_dev(c, c->tab_xe.as<uint32_t>(), c->tab_e.as<uint32_t>(), tab_count, tab_cap, st);
+    launches += 4;
     k_cpair_len<<<gc, 256, 0, st>>>(Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), idx->d_slot,
                                     idx->d_layers, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(), c->rflag.as<uint32_t>(),
                                     c->ridx.as<uint32_t>(), c->method.as<uint8_t>(), c->starts.as<uint32_t>(),
@@ -1260,8 +1279,8 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     P.ppos = c->ppos.as<uint64_t>();
     P.psegs = c->psegs.as<PairSeg>();
     P.segtabs = c->segtab.as<SegTab>();
-    P.tab_s = c->tab_s.as<uint32_t>();
-    P.tab_e = c->tab_e.as<uint32_t>();
+    P.tab_s = c->tab_s.as<uint32_t>() + 1;
+    P.tab_e = c->tab_e.as<uint32_t>() + 1;
     P.item_cap = kItemCap;
     P.rpos = c->rpos.as<uint64_t>();
     P.rcount = Rp;
@@ -1699,7 +1718,7 @@ int rgl_query_batch_device(rgl_context* c, const rgl_batch* b, const rgl_batch_o
     if (b->num_blocks && (!b->block_offsets || !b->block_shards || !b->d_intervals))
         return fail(RGL_ERR_INVALID_ARGUMENT, "incomplete batch");
     RGL_CUDA(cudaSetDevice(c->idx->device));
-    const uint64_t sub = (o && o->sub_batch) ? std::min<uint64_t>(o->sub_batch, kMaxRunIntervals) : (1ull << 24);
+    const uint64_t sub = (o && o->sub_batch) ? std::min<uint64_t>(o->sub_batch, kMaxRunIntervals) : (1ull << 25);
     rgl_query_opts q;
     const Launch L = batch_launch(c, o, &q);
     const bool graph = o && (o->flags & RGL_BF_GRAPH);
@@ -1799,7 +1818,7 @@ int rgl_query_batch_host(rgl_context* c, const rgl_batch* b, const rgl_interval*
     if (b->num_blocks && (!b->block_offsets || !b->block_shards || !h_intervals))
         return fail(RGL_ERR_INVALID_ARGUMENT, "incomplete batch");
     RGL_CUDA(cudaSetDevice(c->idx->device));
-    const uint64_t sub = (o && o->sub_batch) ? std::min<uint64_t>(o->sub_batch, kMaxRunIntervals) : (1ull << 24);
+    const uint64_t sub = (o && o->sub_batch) ? std::min<uint64_t>(o->sub_batch, kMaxRunIntervals) : (1ull << 25);
     rgl_query_opts q;
     const Launch L = batch_launch(c, o, &q);
     const bool want_bp = overlap_bp && !(q.flags & RGL_QF_NO_OVERLAP);
@@ -1890,7 +1909,7 @@ int rgl_batch_autotune(rgl_context* c, const rgl_batch* b, uint64_t sub_batch, r
     if (!c || !b || !best) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
     RGL_CUDA(cudaSetDevice(c->idx->device));
     BatchPlan P;
-    const uint64_t sub = sub_batch ? std::min<uint64_t>(sub_batch, kMaxRunIntervals) : (1ull << 24);
+    const uint64_t sub = sub_batch ? std::min<uint64_t>(sub_batch, kMaxRunIntervals) : (1ull << 25);
     RGL_TRY(plan_batch(c, b, sub, &P));
     if (P.subs.empty()) return fail(RGL_ERR_INVALID_ARGUMENT, "empty batch");
     size_t big = 0;
