@@ -15,7 +15,8 @@ One JSON line with three parts:
     plain form on the same files (one call per file), with the results compared cell by cell.
   "serving": Poisson arrivals at 200 query files/s (log-uniform [1e3, 1e6] intervals) against the
     resident 64-file database through the request server: p50/p99/p99.9 latency and sustained rate,
-    continuous batching vs one query file per launch.
+    continuous batching vs one query file per launch; "high_load" repeats it at 1,000 files/s, where
+    one file per launch can no longer keep up.
 
 "intervals swept" = query intervals + database intervals in the union of the reference's candidate
 ranges [q.start - layer_max_K, q.end) over all (shard, layer), per query file (computed by the
@@ -646,6 +647,14 @@ def serve_trace(srv, reqs, arrivals, hp):
 
 
 def run_serving(args, dev, idx):
+    """Serving at the configured rate, then at five times it (for a shorter trace): continuous batching
+    against one query file per launch on the same arrivals."""
+    base = serve_once(args, dev, idx, args.serve_rate, args.serve_seconds, 77)
+    high = serve_once(args, dev, idx, 5 * args.serve_rate, max(1.0, args.serve_seconds / 2.5), 78)
+    return dict(base, high_load=high)
+
+
+def serve_once(args, dev, idx, lam, T, seed):
     import torch
 
     import riggle_b200 as rg
@@ -653,13 +662,12 @@ def run_serving(args, dev, idx):
 
     lib = rg.load()
     cl = rg.synth_chrom_lengths(1, 24)
-    rng = np.random.default_rng(77)
-    lam, T = args.serve_rate, args.serve_seconds
+    rng = np.random.default_rng(seed)
     arr = np.cumsum(rng.exponential(1.0 / lam, size=int(lam * T * 2) + 64))
     arr = arr[arr < T]
     nreq = len(arr)
-    sizes = rg.synth_loguniform_sizes(777, nreq, 1000, 1_000_000)
-    spec = rg.SynthSpec(7000, cl, sizes)
+    sizes = rg.synth_loguniform_sizes(700 + seed, nreq, 1000, 1_000_000)
+    spec = rg.SynthSpec(7000 + seed, cl, sizes)
     off, sh, _ = rg.synth_batch_layout(spec)
     N = int(off[-1])
     t_iv = torch.empty((max(N, 1), 3), dtype=torch.int32, device=f"cuda:{dev}")
