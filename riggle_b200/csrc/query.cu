@@ -623,7 +623,7 @@ __device__ __forceinline__ uint2 bin_bounds(const uint32_t* __restrict__ tab, co
 constexpr uint32_t kUnroll = 4;  // DB intervals per lane per step
 
 template <bool WITH_BP>
-__global__ void __launch_bounds__(256, 3) k_sweep(SweepParams P) {
+__global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
@@ -1014,7 +1014,7 @@ struct Launch {
 };
 
 Launch pick_launch(const rgl_query_opts* o) {
-    Launch l{2048, 4, 256, 2};
+    Launch l{2048, 8, 256, 2};
     if (o) {
         if (o->chunk) l.chunk = o->chunk;
         if (o->ctas_per_sm) l.ctas_per_sm = o->ctas_per_sm;
