@@ -327,11 +327,13 @@ def run_riggle(args, rank, world, local_rank, dist):
     torch.cuda.synchronize()
     lib.rgl_context_set_timing(ctx._h, 1)
     tc0 = time.perf_counter()
+    torch.cuda.profiler.start()  # the profiled range under `ncu --profile-from-start off`
     e0.record(stream)
     for i in range(args.warmup, nfiles):
         dev_step(i)
     e1.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     tc1 = time.perf_counter()
     sweep_ms = C.c_float()
     launches = C.c_uint32()
@@ -397,7 +399,7 @@ def run_riggle(args, rank, world, local_rank, dist):
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": profiled_traffic(), "kernel": "k_sweep", "peak_source": peak_kind,
+                "traffic": profiled_traffic(), "kernel": "k_sweep + k_pairs (sweep stage)", "peak_source": peak_kind,
                 "sweep_ms_per_launch": per_launch_ms, "algorithmic_bytes_per_launch": alg_bytes}
 
     cpu = None
