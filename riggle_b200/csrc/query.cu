@@ -724,7 +724,7 @@ __global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
 // coalesce).  A candidate d of query q overlaps when d.end > q.start (d.start < q.end and the
 // look-back bound hold by construction of the run); it adds 1 and min(ends) - max(starts).
 template <bool WITH_BP>
-__global__ void __launch_bounds__(256, 4) k_pairs(SweepParams P) {
+__global__ void __launch_bounds__(256, 8) k_pairs(SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
@@ -754,24 +754,56 @@ __global__ void __launch_bounds__(256, 4) k_pairs(SweepParams P) {
         }
         uint64_t rlo = __ldg(P.ppos + t), rhi = __ldg(P.ppos + t + 1);
         PairSeg ps = P.psegs[t];
-        for (uint64_t p = p0 + lane; p < p1; p += 32) {
-            if (p >= rhi) {
-                t = range_advance(P.ppos, t, rcap, p);
+        auto tally = [&](const PairSeg& q, uint2 d, uint32_t sid) {
+            if (d.y <= q.qs) return;
+            if (P.smem_tally) {
+                atomicAdd(&s_cnt[sid], 1u);
+                if (WITH_BP) atomicAdd(&s_bp[sid], (unsigned long long)(min(q.qe, d.y) - max(q.qs, d.x)));
+            } else {
+                const uint64_t cell = (uint64_t)q.qrow * P.D + sid;
+                atomicAdd(&P.counts[cell], 1u);
+                if (WITH_BP) atomicAdd(&P.bp[cell], (unsigned long long)(min(q.qe, d.y) - max(q.qs, d.x)));
+            }
+        };
+        // A step covers 32 * kUnroll consecutive positions, lane l taking pb + l + 32 j.  When a
+        // lane's positions of the step lie in one run (runs hold hundreds of candidates in narrow
+        // layers), all their DB intervals and sids are requested before any is used.
+        for (uint64_t pb = p0 + lane; pb < p1; pb += 32 * kUnroll) {
+            const uint64_t plast = min(pb + 32 * (kUnroll - 1), p1 - 1 - ((p1 - 1 - pb) & 31));
+            if (pb >= rhi) {
+                t = range_advance(P.ppos, t, rcap, pb);
                 rlo = __ldg(P.ppos + t);
                 rhi = __ldg(P.ppos + t + 1);
                 ps = P.psegs[t];
             }
-            const uint64_t di = ps.base + (p - rlo);
-            const uint2 d = __ldg(P.pos + di);
-            if (d.y > ps.qs) {
-                const uint32_t sid = __ldg(P.sid + di);
-                if (P.smem_tally) {
-                    atomicAdd(&s_cnt[sid], 1u);
-                    if (WITH_BP) atomicAdd(&s_bp[sid], (unsigned long long)(min(ps.qe, d.y) - max(ps.qs, d.x)));
-                } else {
-                    const uint64_t cell = (uint64_t)ps.qrow * P.D + sid;
-                    atomicAdd(&P.counts[cell], 1u);
-                    if (WITH_BP) atomicAdd(&P.bp[cell], (unsigned long long)(min(ps.qe, d.y) - max(ps.qs, d.x)));
+            if (plast < rhi) {
+                const uint64_t off = ps.base - rlo;
+                uint2 d[kUnroll];
+                uint32_t sid[kUnroll];
+#pragma unroll
+                for (uint32_t j = 0; j < kUnroll; j++) {
+                    const uint64_t pj = pb + 32 * j;
+                    if (pj < p1) {
+                        d[j] = __ldg(P.pos + off + pj);
+                        sid[j] = __ldg(P.sid + off + pj);
+                    } else {
+                        d[j] = make_uint2(0, 0);  // never a hit: d.y = 0 <= qs
+                        sid[j] = 0;
+                    }
+                }
+#pragma unroll
+                for (uint32_t j = 0; j < kUnroll; j++) tally(ps, d[j], sid[j]);
+            } else {
+                // the step crosses a run boundary: one position at a time
+                for (uint64_t pj = pb; pj < p1 && pj <= pb + 32 * (kUnroll - 1); pj += 32) {
+                    if (pj >= rhi) {
+                        t = range_advance(P.ppos, t, rcap, pj);
+                        rlo = __ldg(P.ppos + t);
+                        rhi = __ldg(P.ppos + t + 1);
+                        ps = P.psegs[t];
+                    }
+                    const uint64_t di = ps.base + (pj - rlo);
+                    tally(ps, __ldg(P.pos + di), __ldg(P.sid + di));
                 }
             }
         }
