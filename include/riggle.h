@@ -185,12 +185,12 @@ typedef struct rgl_query_batch {
 
 /* Launch shape.  0 = default / autotuned. */
 typedef struct rgl_query_opts {
-    uint32_t chunk;       /* positions per work item */
-    uint32_t ctas_per_sm; /* persistent CTAs per SM */
+    uint32_t chunk;       /* positions per work item (default 1024) */
+    uint32_t ctas_per_sm; /* persistent CTAs per SM (default 8) */
     uint32_t block;       /* threads per CTA */
     uint32_t flags;       /* RGL_QF_* */
     uint32_t pair_ratio;  /* a candidate range is swept pair by pair when its candidates are at most
-                             pair_ratio x its union size, else by rank differences (default 2) */
+                             pair_ratio x its union size, else by rank differences (default 4) */
 } rgl_query_opts;
 
 #define RGL_QF_NO_OVERLAP 1u /* skip base-pair accumulation (counts only) */

@@ -1046,7 +1046,7 @@ struct Launch {
 };
 
 Launch pick_launch(const rgl_query_opts* o) {
-    Launch l{2048, 8, 256, 2};
+    Launch l{1024, 8, 256, 4};
     if (o) {
         if (o->chunk) l.chunk = o->chunk;
         if (o->ctas_per_sm) l.ctas_per_sm = o->ctas_per_sm;
