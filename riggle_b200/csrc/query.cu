@@ -62,6 +62,15 @@ struct SegTab {
     uint32_t pad;
 };
 
+// Key of entry t = K * n + i of the [K][n] arrays: (K, segment of query i).
+struct RowKey {
+    const uint32_t* segnum;
+    uint32_t n;
+    __host__ __device__ __forceinline__ uint64_t operator()(uint32_t t) const {
+        return ((uint64_t)(t / n) << 32) | segnum[t % n];
+    }
+};
+
 struct MaxOp {
     __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
 };
@@ -1009,8 +1018,12 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nn + 1, c->stream);
     need = std::max(need, b);
-    cub::DeviceScan::InclusiveScanByKey(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, (uint32_t*)nullptr,
-                                        MaxOp(), nn, cub::Equality(), c->stream);
+    {
+        cub::CountingInputIterator<uint32_t> ti(0);
+        cub::TransformInputIterator<uint64_t, RowKey, cub::CountingInputIterator<uint32_t>> keys(ti, RowKey{nullptr, 1});
+        cub::DeviceScan::InclusiveScanByKey(nullptr, b, keys, (uint32_t*)nullptr, (uint32_t*)nullptr, MaxOp(), nt,
+                                            cub::Equality(), c->stream);
+    }
     need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, nt, c->stream);
     need = std::max(need, b);
@@ -1227,12 +1240,14 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                                 c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, idx->d_pos,
                                                 idx->d_btab, c->lo.as<uint32_t>(), c->hi.as<uint32_t>());
     launches++;
-    for (uint32_t K = 0; K < ns; K++) {
+    {  // running max of hi along every (slot, segment) row: one scan keyed by (slot, segment)
+        cub::CountingInputIterator<uint32_t> ti(0);
+        cub::TransformInputIterator<uint64_t, RowKey, cub::CountingInputIterator<uint32_t>> keys(
+            ti, RowKey{c->segnum.as<uint32_t>(), n});
         tb = c->cub_tmp.cap;
-        RGL_CUDA(cub::DeviceScan::InclusiveScanByKey(c->cub_tmp.p, tb, c->segnum.as<uint32_t>(),
-                                                     c->hi.as<uint32_t>() + (uint64_t)K * n,
-                                                     c->maxhi.as<uint32_t>() + (uint64_t)K * n, MaxOp(), (int)n,
-                                                     cub::Equality(), st));
+        RGL_CUDA(cub::DeviceScan::InclusiveScanByKey(c->cub_tmp.p, tb, keys, c->hi.as<uint32_t>(),
+                                                     c->maxhi.as<uint32_t>(), MaxOp(), (int)tot, cub::Equality(),
+                                                     st));
     }
     // live runs: compaction of the (K, query) entries with a non-empty candidate run
     k_live<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
