@@ -629,10 +629,11 @@ __device__ __forceinline__ uint2 bin_bounds(const uint32_t* __restrict__ tab, co
     return make_uint2(__ldg(tab + t.off + b), __ldg(tab + t.off + b + 1));
 }
 
-constexpr uint32_t kUnroll = 4;  // DB intervals per lane per step
+constexpr uint32_t kUnroll = 2;      // DB intervals per lane per step of the rank sweep
+constexpr uint32_t kPairUnroll = 4;  // candidates per lane per step of the pair sweep
 
 template <bool WITH_BP>
-__global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
+__global__ void __launch_bounds__(256, 6) k_sweep(SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
@@ -774,11 +775,11 @@ __global__ void __launch_bounds__(256, 8) k_pairs(SweepParams P) {
                 if (WITH_BP) atomicAdd(&P.bp[cell], (unsigned long long)(min(q.qe, d.y) - max(q.qs, d.x)));
             }
         };
-        // A step covers 32 * kUnroll consecutive positions, lane l taking pb + l + 32 j.  When a
+        // A step covers 32 * kPairUnroll consecutive positions, lane l taking pb + l + 32 j.  When a
         // lane's positions of the step lie in one run (runs hold hundreds of candidates in narrow
         // layers), all their DB intervals and sids are requested before any is used.
-        for (uint64_t pb = p0 + lane; pb < p1; pb += 32 * kUnroll) {
-            const uint64_t plast = min(pb + 32 * (kUnroll - 1), p1 - 1 - ((p1 - 1 - pb) & 31));
+        for (uint64_t pb = p0 + lane; pb < p1; pb += 32 * kPairUnroll) {
+            const uint64_t plast = min(pb + 32 * (kPairUnroll - 1), p1 - 1 - ((p1 - 1 - pb) & 31));
             if (pb >= rhi) {
                 t = range_advance(P.ppos, t, rcap, pb);
                 rlo = __ldg(P.ppos + t);
@@ -787,10 +788,10 @@ __global__ void __launch_bounds__(256, 8) k_pairs(SweepParams P) {
             }
             if (plast < rhi) {
                 const uint64_t off = ps.base - rlo;
-                uint2 d[kUnroll];
-                uint32_t sid[kUnroll];
+                uint2 d[kPairUnroll];
+                uint32_t sid[kPairUnroll];
 #pragma unroll
-                for (uint32_t j = 0; j < kUnroll; j++) {
+                for (uint32_t j = 0; j < kPairUnroll; j++) {
                     const uint64_t pj = pb + 32 * j;
                     if (pj < p1) {
                         d[j] = __ldg(P.pos + off + pj);
@@ -801,10 +802,10 @@ __global__ void __launch_bounds__(256, 8) k_pairs(SweepParams P) {
                     }
                 }
 #pragma unroll
-                for (uint32_t j = 0; j < kUnroll; j++) tally(ps, d[j], sid[j]);
+                for (uint32_t j = 0; j < kPairUnroll; j++) tally(ps, d[j], sid[j]);
             } else {
                 // the step crosses a run boundary: one position at a time
-                for (uint64_t pj = pb; pj < p1 && pj <= pb + 32 * (kUnroll - 1); pj += 32) {
+                for (uint64_t pj = pb; pj < p1 && pj <= pb + 32 * (kPairUnroll - 1); pj += 32) {
                     if (pj >= rhi) {
                         t = range_advance(P.ppos, t, rcap, pj);
                         rlo = __ldg(P.ppos + t);
