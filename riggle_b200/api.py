@@ -184,15 +184,7 @@ class Context:
         Returns (counts uint32[num_rows, D], overlap_bp uint64[num_rows, D] or None, stats dict).
         """
         keep = []
-        arr = (_lib.QueryShard * max(1, len(shards)))()
-        for i, (k, ivs) in enumerate(shards.items()):
-            ivs = np.ascontiguousarray(ivs, dtype=np.uint32).reshape(-1, 3)
-            keep.append(ivs)
-            if isinstance(k, str):
-                arr[i] = _lib.QueryShard(k.encode(), 0, len(ivs), _ptr(ivs))
-            else:
-                arr[i] = _lib.QueryShard(None, int(k), len(ivs), _ptr(ivs))
-        batch = _lib.QueryBatch(int(num_rows), len(shards), arr)
+        batch = self._batch(shards, num_rows, keep)
         D = self.index.num_sources
         if out is None:
             counts = np.empty((num_rows, D), np.uint32)
