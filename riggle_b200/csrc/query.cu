@@ -52,9 +52,10 @@ struct PairSeg {
 
 enum : uint8_t { M_RANK = 0, M_PAIR = 1 };
 
-// Rank table of one query segment: bin b (width 2^shift bp) holds, at tab[off + b], the number of
-// the segment's sorted starts (tab_s) or ends (tab_e) below b << shift, as absolute positions in
-// the sorted arrays.  A rank is then one table read plus a search over at most one bin.
+// Rank table of one query segment: bin b (width 2^shift bp) holds, at tab2[off + b], the numbers
+// of the segment's sorted starts and ends below b << shift, as absolute positions in the sorted
+// arrays.  A rank is then one table read plus a search over at most one bin, and the two entries
+// of a bin serve the start rank and the end rank of any x in it.
 struct SegTab {
     uint32_t beg, end;  // the segment's positions in the sorted arrays
     uint32_t shift, nbins;
@@ -232,6 +233,15 @@ __global__ void k_tab_count(uint32_t n, const uint32_t* __restrict__ segnum, con
     if (t.nbins == 0) return;
     atomicAdd(xs + t.off + (starts[j] >> t.shift) + 1, 1u);
     atomicAdd(xe + t.off + (ends_s[j] >> t.shift) + 1, 1u);
+}
+
+// Interleaves the two scanned count arrays into (#starts, #ends) pairs: entry k of the tables is
+// entry k + 1 of the exclusive scans (the inclusive sums through k).
+__global__ void k_tab_interleave(const uint32_t* __restrict__ count, const uint32_t* __restrict__ xs_scan,
+                                 const uint32_t* __restrict__ xe_scan, uint2* __restrict__ tab2) {
+    const uint32_t total = *count;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x)
+        tab2[k] = make_uint2(xs_scan[k + 1], xe_scan[k + 1]);
 }
 
 // ---- 4. K1 partition -----------------------------------------------------------------------------
@@ -481,8 +491,7 @@ struct SweepParams {
     const PairSeg* psegs;
     const uint32_t* item_t0; // first run of each pair work item
     const SegTab* segtabs;   // per query segment
-    const uint32_t* tab_s;   // rank tables of sorted starts / ends
-    const uint32_t* tab_e;
+    const uint2* tab2;       // rank tables, bin b = (#starts, #ends) below b << shift
     uint64_t item_cap;
     uint32_t rows, D, chunk;
     int smem_tally;          // 1: one row, shared-memory histograms
@@ -578,13 +587,13 @@ __device__ __forceinline__ void cursor_load(const SweepParams& P, Cursor& c, uin
 __device__ __forceinline__ uint32_t rank_start(const SweepParams& P, const SegTab& t, uint32_t x) {
     const uint32_t b = x >> t.shift;
     if (b >= t.nbins) return t.end;
-    const uint32_t lo = __ldg(P.tab_s + t.off + b), hi = __ldg(P.tab_s + t.off + b + 1);
+    const uint32_t lo = __ldg(&P.tab2[t.off + b].x), hi = __ldg(&P.tab2[t.off + b + 1].x);
     return lo == hi ? lo : lb_u32(P.starts, lo, hi, x);
 }
 __device__ __forceinline__ uint32_t rank_end(const SweepParams& P, const SegTab& t, uint32_t x) {
     const uint32_t b = x >> t.shift;
     if (b >= t.nbins) return t.end;
-    const uint32_t lo = __ldg(P.tab_e + t.off + b), hi = __ldg(P.tab_e + t.off + b + 1);
+    const uint32_t lo = __ldg(&P.tab2[t.off + b].y), hi = __ldg(&P.tab2[t.off + b + 1].y);
     return lo == hi ? lo : ub_u32(P.ends, lo, hi, x);
 }
 
@@ -592,15 +601,39 @@ __device__ __forceinline__ void cursor_seek(const SweepParams& P, Cursor& c, uin
     if (p >= c.rhi) cursor_load(P, c, range_advance(P.rpos, c.r, rcap, p));
 }
 
-// Base pairs and tally of one DB interval d with a non-zero count (el_s, sl_e already known).
+// Bin entries (#starts, #ends) b and b + 1 for the bin of x, or (end, end) twice past the table.
+__device__ __forceinline__ void bin_pair(const SweepParams& P, const SegTab& t, uint32_t x, uint2& lo, uint2& hi) {
+    const uint32_t b = x >> t.shift;
+    if (b >= t.nbins) {
+        lo = hi = make_uint2(t.end, t.end);
+        return;
+    }
+    lo = __ldg(P.tab2 + t.off + b);
+    hi = __ldg(P.tab2 + t.off + b + 1);
+}
+// Ranks inside one bin: #starts < x given the bin's start counts, #ends <= x given its end counts.
+__device__ __forceinline__ uint32_t starts_in(const SweepParams& P, uint32_t lo, uint32_t hi, uint32_t x) {
+    return lo == hi ? lo : lb_u32(P.starts, lo, hi, x);
+}
+__device__ __forceinline__ uint32_t ends_in(const SweepParams& P, uint32_t lo, uint32_t hi, uint32_t x) {
+    return lo == hi ? lo : ub_u32(P.ends, lo, hi, x);
+}
+
+// One DB interval d with the table entries of its start's bin (a0, a1) and its end's bin (b0, b1):
+// count(d) = #{q.start < d.end} - #{q.end <= d.start}, and for a non-zero count the overlap
+// Cov(d.end) - Cov(d.start) and the tally.
 template <bool WITH_BP>
-__device__ __forceinline__ void finish_hit(const SweepParams& P, const SegTab& t, uint32_t qrow, uint2 d,
-                                          uint32_t sid, uint32_t cnt, uint32_t el_s, uint32_t sl_e,
-                                          uint32_t* s_cnt, unsigned long long* s_bp) {
+__device__ __forceinline__ void sweep_one(const SweepParams& P, uint32_t qrow, uint2 d, uint32_t sid, uint2 a0,
+                                          uint2 a1, uint2 b0, uint2 b1, uint32_t* s_cnt,
+                                          unsigned long long* s_bp) {
+    const uint32_t el_s = ends_in(P, a0.y, a1.y, d.x);
+    const uint32_t sl_e = starts_in(P, b0.x, b1.x, d.y);
+    const uint32_t cnt = sl_e - el_s;
+    if (!cnt) return;
     unsigned long long bpv = 0;
     if (WITH_BP) {
-        const uint32_t sl_s = rank_start(P, t, d.x);
-        const uint32_t el_e = rank_end(P, t, d.y);
+        const uint32_t sl_s = starts_in(P, a0.x, a1.x, d.x);
+        const uint32_t el_e = ends_in(P, b0.y, b1.y, d.y);
         if (sl_e == sl_s && el_e == el_s) {
             // no query starts or ends inside d: every overlapping query covers all of d
             bpv = (unsigned long long)(d.y - d.x) * cnt;
@@ -622,18 +655,11 @@ __device__ __forceinline__ void finish_hit(const SweepParams& P, const SegTab& t
     }
 }
 
-// Two table entries tab[b], tab[b + 1] (b < nbins) for the bin of x, or (end, end) past the table.
-__device__ __forceinline__ uint2 bin_bounds(const uint32_t* __restrict__ tab, const SegTab& t, uint32_t x) {
-    const uint32_t b = x >> t.shift;
-    if (b >= t.nbins) return make_uint2(t.end, t.end);
-    return make_uint2(__ldg(tab + t.off + b), __ldg(tab + t.off + b + 1));
-}
-
 constexpr uint32_t kUnroll = 2;      // DB intervals per lane per step of the rank sweep
 constexpr uint32_t kPairUnroll = 4;  // candidates per lane per step of the pair sweep
 
 template <bool WITH_BP>
-__global__ void __launch_bounds__(256, 6) k_sweep(SweepParams P) {
+__global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
@@ -691,30 +717,26 @@ __global__ void __launch_bounds__(256, 6) k_sweep(SweepParams P) {
                         sid[j] = 0;
                     }
                 }
-                uint2 be[kUnroll], bs[kUnroll];
+                uint2 a0[kUnroll], a1[kUnroll], b0[kUnroll], b1[kUnroll];
 #pragma unroll
                 for (uint32_t j = 0; j < kUnroll; j++) {
-                    be[j] = bin_bounds(P.tab_e, t, d[j].x);
-                    bs[j] = bin_bounds(P.tab_s, t, d[j].y);
+                    bin_pair(P, t, d[j].x, a0[j], a1[j]);
+                    bin_pair(P, t, d[j].y, b0[j], b1[j]);
                 }
 #pragma unroll
-                for (uint32_t j = 0; j < kUnroll; j++) {
-                    if (pb + 32 * j >= p1) continue;
-                    const uint32_t el_s = be[j].x == be[j].y ? be[j].x : ub_u32(P.ends, be[j].x, be[j].y, d[j].x);
-                    const uint32_t sl_e = bs[j].x == bs[j].y ? bs[j].x : lb_u32(P.starts, bs[j].x, bs[j].y, d[j].y);
-                    const uint32_t cnt = sl_e - el_s;
-                    if (cnt) finish_hit<WITH_BP>(P, t, c.rd.qrow, d[j], sid[j], cnt, el_s, sl_e, s_cnt, s_bp);
-                }
+                for (uint32_t j = 0; j < kUnroll; j++)
+                    if (pb + 32 * j < p1)
+                        sweep_one<WITH_BP>(P, c.rd.qrow, d[j], sid[j], a0[j], a1[j], b0[j], b1[j], s_cnt, s_bp);
             } else {
                 // the step crosses a range boundary: one position at a time
                 for (uint64_t pj = pb; pj < p1 && pj <= pb + 32 * (kUnroll - 1); pj += 32) {
                     cursor_seek(P, c, pj, rcap);
                     const uint64_t di = c.base + (pj - c.rlo);
                     const uint2 d = __ldg(P.pos + di);
-                    const uint32_t el_s = rank_end(P, c.tab, d.x);
-                    const uint32_t sl_e = rank_start(P, c.tab, d.y);
-                    const uint32_t cnt = sl_e - el_s;
-                    if (cnt) finish_hit<WITH_BP>(P, c.tab, c.rd.qrow, d, __ldg(P.sid + di), cnt, el_s, sl_e, s_cnt, s_bp);
+                    uint2 a0, a1, b0, b1;
+                    bin_pair(P, c.tab, d.x, a0, a1);
+                    bin_pair(P, c.tab, d.y, b0, b1);
+                    sweep_one<WITH_BP>(P, c.rd.qrow, d, __ldg(P.sid + di), a0, a1, b0, b1, s_cnt, s_bp);
                 }
             }
         }
@@ -909,7 +931,7 @@ struct rgl_context {
     DevBuf iv, blk_off, blk_shard, key_a, key_b, val_a, val_b, ekey_a, ekey_b;
     DevBuf starts, ends, seg, segflag, segnum, seg_begin, ps_in, pe_in, ps, pe;
     DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp, item_r0;
-    DevBuf segtab, tab_len, tab_off, tab_s, tab_e, tab_xs, tab_xe;
+    DevBuf segtab, tab_len, tab_off, tab_s, tab_e, tab_xs, tab_xe, tab2;
     DevBuf cl, pc, method, plen, ppos, psegs, item_t0, seg_need, lpos, tl, scan_sums;
     DevBuf item_hits, item_base, pairs;  // intervals mode
     DevBuf bt_off, bt_shard, acc;  // batched form: sub-batch block tables (offsets; shards then rows), stats
@@ -1001,6 +1023,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     RGL_TRY(c->tab_off.ensure((n + 2) * 4));
     RGL_TRY(c->tab_s.ensure((10 * n + 18) * 4));
     RGL_TRY(c->tab_e.ensure((10 * n + 18) * 4));
+    RGL_TRY(c->tab2.ensure((10 * n + 18) * 8));
     RGL_TRY(c->tab_xs.ensure((10 * n + 16) * 4));
     RGL_TRY(c->tab_xe.ensure((10 * n + 16) * 4));
     RGL_TRY(c->acc.ensure(64));
@@ -1046,7 +1069,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
                       &c->ends, &c->seg, &c->segflag, &c->segnum, &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps,
                       &c->pe, &c->lo, &c->hi, &c->maxhi, &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos,
                       &c->cub_tmp, &c->small, &c->item_r0, &c->item_t0, &c->segtab, &c->tab_len, &c->tab_off,
-                      &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs,
+                      &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->tab2, &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs,
                       &c->seg_need, &c->acc})
         sig = (sig ^ (uint64_t)(uintptr_t)b->p ^ ((uint64_t)b->cap << 17)) * 1099511628211ull;
     c->ws_sig = sig;
@@ -1299,6 +1322,9 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     // inclusive sum through k (the tables are read from tab_* + 1)
     launches += scan_dev(c, c->tab_xs.as<uint32_t>(), c->tab_s.as<uint32_t>(), tab_count, tab_cap, st);
     launches += scan_dev(c, c->tab_xe.as<uint32_t>(), c->tab_e.as<uint32_t>(), tab_count, tab_cap, st);
+    k_tab_interleave<<<(unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, st>>>(
+        tab_count, c->tab_s.as<uint32_t>(), c->tab_e.as<uint32_t>(), c->tab2.as<uint2>());
+    launches++;
     launches += 4;
     k_cpair_len<<<gc, 256, 0, st>>>(Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), idx->d_slot,
                                     idx->d_layers, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(), c->rflag.as<uint32_t>(),
@@ -1327,8 +1353,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     P.ppos = c->ppos.as<uint64_t>();
     P.psegs = c->psegs.as<PairSeg>();
     P.segtabs = c->segtab.as<SegTab>();
-    P.tab_s = c->tab_s.as<uint32_t>() + 1;
-    P.tab_e = c->tab_e.as<uint32_t>() + 1;
+    P.tab2 = c->tab2.as<uint2>();
     P.item_cap = kItemCap;
     P.rpos = c->rpos.as<uint64_t>();
     P.rcount = Rp;
@@ -1651,7 +1676,7 @@ int rgl_context_destroy(rgl_context* c) {
                       &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps, &c->pe, &c->lo, &c->hi, &c->maxhi,
                       &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos, &c->cub_tmp, &c->small,
                       &c->out_counts, &c->out_bp, &c->item_r0,
-                      &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe,
+                      &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->tab2,
                       &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs, &c->item_t0,
                       &c->seg_need, &c->item_hits, &c->item_base, &c->pairs, &c->bt_off, &c->bt_shard, &c->acc, &c->gc.t_off, &c->gc.t_shard};
     if (c->gc.exec) cudaGraphExecDestroy(c->gc.exec);
