@@ -235,6 +235,14 @@ __global__ void k_tab_count(uint32_t n, const uint32_t* __restrict__ segnum, con
     atomicAdd(xe + t.off + (ends_s[j] >> t.shift) + 1, 1u);
 }
 
+// Adds a 32-bit value to a 64-bit shared-memory counter with 32-bit atomics: the low word, and the
+// high word only when the low word wraps (one pair's overlap always fits 32 bits).
+__device__ __forceinline__ void add_u64_lo(unsigned long long* c, uint32_t v) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(c);  // little-endian: w[0] low, w[1] high
+    const uint32_t old = atomicAdd(w, v);
+    if (old + v < old) atomicAdd(w + 1, 1u);
+}
+
 // Interleaves the two scanned count arrays into (#starts, #ends) pairs: entry k of the tables is
 // entry k + 1 of the exclusive scans (the inclusive sums through k).
 __global__ void k_tab_interleave(const uint32_t* __restrict__ count, const uint32_t* __restrict__ xs_scan,
@@ -790,7 +798,7 @@ __global__ void __launch_bounds__(256, 8) k_pairs(SweepParams P) {
             if (d.y <= q.qs) return;
             if (P.smem_tally) {
                 atomicAdd(&s_cnt[sid], 1u);
-                if (WITH_BP) atomicAdd(&s_bp[sid], (unsigned long long)(min(q.qe, d.y) - max(q.qs, d.x)));
+                if (WITH_BP) add_u64_lo(&s_bp[sid], min(q.qe, d.y) - max(q.qs, d.x));
             } else {
                 const uint64_t cell = (uint64_t)q.qrow * P.D + sid;
                 atomicAdd(&P.counts[cell], 1u);
