@@ -243,6 +243,14 @@ __device__ __forceinline__ void add_u64_lo(unsigned long long* c, uint32_t v) {
     if (old + v < old) atomicAdd(w + 1, 1u);
 }
 
+// The same for a 64-bit value: low word, then the high word plus the carry when either is non-zero.
+__device__ __forceinline__ void add_u64(unsigned long long* c, unsigned long long v) {
+    uint32_t* w = reinterpret_cast<uint32_t*>(c);
+    const uint32_t lo = (uint32_t)v, old = atomicAdd(w, lo);
+    const uint32_t hi = (uint32_t)(v >> 32) + (old + lo < old ? 1u : 0u);
+    if (hi) atomicAdd(w + 1, hi);
+}
+
 // Interleaves the two scanned count arrays into (#starts, #ends) pairs: entry k of the tables is
 // entry k + 1 of the exclusive scans (the inclusive sums through k).
 __global__ void k_tab_interleave(const uint32_t* __restrict__ count, const uint32_t* __restrict__ xs_scan,
@@ -655,7 +663,7 @@ __device__ __forceinline__ void sweep_one(const SweepParams& P, uint32_t qrow, u
     }
     if (P.smem_tally) {
         atomicAdd(&s_cnt[sid], cnt);
-        if (WITH_BP) atomicAdd(&s_bp[sid], bpv);
+        if (WITH_BP) add_u64(&s_bp[sid], bpv);
     } else {
         const uint64_t cell = (uint64_t)qrow * P.D + sid;
         atomicAdd(&P.counts[cell], cnt);
