@@ -766,12 +766,67 @@ __global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
     }
 }
 
+// A pair candidate d of the run with query interval [qs, qe) and Q_SID qrow: when d.end > qs it
+// adds 1 and min(ends) - max(starts) to cell (qrow, sid) — in the block's shared histograms (SMEM,
+// one query row) or in the output matrix.
+template <bool WITH_BP, bool SMEM>
+__device__ __forceinline__ void pair_tally(const SweepParams& P, uint32_t qs, uint32_t qe, uint32_t qrow, uint2 d,
+                                           uint32_t sid, uint32_t* s_cnt, unsigned long long* s_bp) {
+    if (d.y <= qs) return;
+    if (SMEM) {
+        atomicAdd(&s_cnt[sid], 1u);
+        if (WITH_BP) add_u64_lo(&s_bp[sid], min(qe, d.y) - max(qs, d.x));
+    } else {
+        const uint64_t cell = (uint64_t)qrow * P.D + sid;
+        atomicAdd(&P.counts[cell], 1u);
+        if (WITH_BP) atomicAdd(&P.bp[cell], (unsigned long long)(min(qe, d.y) - max(qs, d.x)));
+    }
+}
+
+// One step of the pair sweep position by position, each position's run found on its own by a
+// galloping search from t.  Kept out of line: it runs only when a step holds 32 or more run
+// boundaries (a stretch of empty runs), and inlined its registers would count against the whole
+// kernel.
+template <bool WITH_BP, bool SMEM>
+__device__ __noinline__ void pairs_step_slow(const uint64_t* __restrict__ ppos, const PairSeg* __restrict__ psegs,
+                                             const uint2* __restrict__ pos, const uint32_t* __restrict__ sidv,
+                                             uint32_t* counts, unsigned long long* bp, uint32_t D, uint32_t t,
+                                             uint32_t rcap, uint64_t pb, uint32_t span, uint32_t lane,
+                                             uint32_t* s_cnt, unsigned long long* s_bp) {
+    for (uint32_t o = lane; o <= span; o += 32) {
+        const uint64_t pj = pb + o;
+        const uint32_t tt = range_advance(ppos, t, rcap, pj);
+        const PairSeg q = psegs[tt];
+        const uint64_t di = q.base + (pj - __ldg(ppos + tt));
+        const uint2 d = __ldg(pos + di);
+        const uint32_t sid = __ldg(sidv + di);
+        if (d.y <= q.qs) continue;
+        if (SMEM) {
+            atomicAdd(&s_cnt[sid], 1u);
+            if (WITH_BP) add_u64_lo(&s_bp[sid], min(q.qe, d.y) - max(q.qs, d.x));
+        } else {
+            const uint64_t cell = (uint64_t)q.qrow * D + sid;
+            atomicAdd(&counts[cell], 1u);
+            if (WITH_BP) atomicAdd(&bp[cell], (unsigned long long)(min(q.qe, d.y) - max(q.qs, d.x)));
+        }
+    }
+}
+
 // The pair sweep: the reference's scan (src/sweep/query.rs:147-158) over the candidate runs of the
-// queries of pair ranges, every candidate read once by one lane (lane l of a warp takes positions
-// p0 + l, p0 + l + 32, ...; consecutive positions of a run are consecutive DB elements, so the loads
-// coalesce).  A candidate d of query q overlaps when d.end > q.start (d.start < q.end and the
-// look-back bound hold by construction of the run); it adds 1 and min(ends) - max(starts).
-template <bool WITH_BP>
+// queries of pair ranges, every candidate read once by one lane (consecutive positions of a run are
+// consecutive DB elements, so the loads coalesce).  A candidate d of query q overlaps when
+// d.end > q.start (d.start < q.end and the look-back bound hold by construction of the run); it
+// adds 1 and min(ends) - max(starts).
+//
+// A warp takes work items of `chunk` positions from the queue and walks each in steps of the
+// 32 * kPairUnroll consecutive positions [pb, pend], lane l taking pb + l + 32 j.  The warp keeps
+// the run t of the step's first position (uniform), so the choice between the forms below never
+// splits the warp.  When the step lies in run t, every lane requests all its DB intervals and sids
+// before using any.  When it spans several runs (about a quarter of the steps at hundreds of
+// candidates per run), lane l holds the boundary ppos[t + 1 + l] of the following runs: a
+// position's run is t plus the number of boundaries at or below it, counted over the few
+// boundaries inside the step, and the run descriptors come from L1.
+template <bool WITH_BP, bool SMEM>
 __global__ void __launch_bounds__(256, 8) k_pairs(SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
@@ -779,7 +834,7 @@ __global__ void __launch_bounds__(256, 8) k_pairs(SweepParams P) {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t rcap = *P.pcount;
     const uint64_t total = P.ppos[rcap];
-    if (P.smem_tally)
+    if (SMEM)
         for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
             s_cnt[k] = 0;
             if (WITH_BP) s_bp[k] = 0;
@@ -802,61 +857,87 @@ __global__ void __launch_bounds__(256, 8) k_pairs(SweepParams P) {
         }
         uint64_t rlo = __ldg(P.ppos + t), rhi = __ldg(P.ppos + t + 1);
         PairSeg ps = P.psegs[t];
-        auto tally = [&](const PairSeg& q, uint2 d, uint32_t sid) {
-            if (d.y <= q.qs) return;
-            if (P.smem_tally) {
-                atomicAdd(&s_cnt[sid], 1u);
-                if (WITH_BP) add_u64_lo(&s_bp[sid], min(q.qe, d.y) - max(q.qs, d.x));
-            } else {
-                const uint64_t cell = (uint64_t)q.qrow * P.D + sid;
-                atomicAdd(&P.counts[cell], 1u);
-                if (WITH_BP) atomicAdd(&P.bp[cell], (unsigned long long)(min(q.qe, d.y) - max(q.qs, d.x)));
-            }
-        };
-        // A step covers 32 * kPairUnroll consecutive positions, lane l taking pb + l + 32 j.  When a
-        // lane's positions of the step lie in one run (runs hold hundreds of candidates in narrow
-        // layers), all their DB intervals and sids are requested before any is used.
-        for (uint64_t pb = p0 + lane; pb < p1; pb += 32 * kPairUnroll) {
-            const uint64_t plast = min(pb + 32 * (kPairUnroll - 1), p1 - 1 - ((p1 - 1 - pb) & 31));
+        for (uint64_t pb = p0; pb < p1; pb += 32 * kPairUnroll) {
+            const uint64_t pend = min(pb + 32 * kPairUnroll, p1) - 1;
+            const uint32_t span = (uint32_t)(pend - pb);
             if (pb >= rhi) {
                 t = range_advance(P.ppos, t, rcap, pb);
                 rlo = __ldg(P.ppos + t);
                 rhi = __ldg(P.ppos + t + 1);
                 ps = P.psegs[t];
             }
-            if (plast < rhi) {
-                const uint64_t off = ps.base - rlo;
+            const uint64_t base0 = ps.base - rlo + pb;  // element of offset 0 when it lies in run t
+            if (pend < rhi) {
                 uint2 d[kPairUnroll];
                 uint32_t sid[kPairUnroll];
 #pragma unroll
                 for (uint32_t j = 0; j < kPairUnroll; j++) {
-                    const uint64_t pj = pb + 32 * j;
-                    if (pj < p1) {
-                        d[j] = __ldg(P.pos + off + pj);
-                        sid[j] = __ldg(P.sid + off + pj);
+                    const uint32_t o = lane + 32 * j;
+                    if (o <= span) {
+                        d[j] = __ldg(P.pos + base0 + o);
+                        sid[j] = __ldg(P.sid + base0 + o);
                     } else {
                         d[j] = make_uint2(0, 0);  // never a hit: d.y = 0 <= qs
                         sid[j] = 0;
                     }
                 }
 #pragma unroll
-                for (uint32_t j = 0; j < kPairUnroll; j++) tally(ps, d[j], sid[j]);
-            } else {
-                // the step crosses a run boundary: one position at a time
-                for (uint64_t pj = pb; pj < p1 && pj <= pb + 32 * (kPairUnroll - 1); pj += 32) {
-                    if (pj >= rhi) {
-                        t = range_advance(P.ppos, t, rcap, pj);
-                        rlo = __ldg(P.ppos + t);
-                        rhi = __ldg(P.ppos + t + 1);
-                        ps = P.psegs[t];
-                    }
-                    const uint64_t di = ps.base + (pj - rlo);
-                    tally(ps, __ldg(P.pos + di), __ldg(P.sid + di));
+                for (uint32_t j = 0; j < kPairUnroll; j++)
+                    pair_tally<WITH_BP, SMEM>(P, ps.qs, ps.qe, ps.qrow, d[j], sid[j], s_cnt, s_bp);
+                continue;
+            }
+            // lane l: boundary ppos[t + 1 + l] as an offset from pb (> 0, since run t holds pb);
+            // offsets inside the step fit 32 bits
+            const uint64_t B = (uint64_t)t + 1 + lane <= rcap ? __ldg(P.ppos + t + 1 + lane) : ~0ull;
+            const uint32_t rel = B - pb < 0xffffffffull ? (uint32_t)(B - pb) : 0xffffffffu;
+            const uint32_t nb = __popc(__ballot_sync(0xffffffffu, rel <= span));
+            if (nb == 32) {
+                pairs_step_slow<WITH_BP, SMEM>(P.ppos, P.psegs, P.pos, P.sid, P.counts, P.bp, P.D, t, rcap, pb, span,
+                                               lane, s_cnt, s_bp);
+                continue;  // the next step starts past rhi: range_advance finds its run
+            }
+            uint32_t k[kPairUnroll];  // position lane + 32 j lies in run t + k[j]
+#pragma unroll
+            for (uint32_t j = 0; j < kPairUnroll; j++) k[j] = 0;
+            for (uint32_t i = 0; i < nb; i++) {  // rel[0..nb) are the boundaries inside the step
+                const uint32_t bv = __shfl_sync(0xffffffffu, rel, i);
+#pragma unroll
+                for (uint32_t j = 0; j < kPairUnroll; j++) k[j] += bv <= lane + 32 * j ? 1u : 0u;
+            }
+            uint2 d[kPairUnroll];
+            uint32_t sid[kPairUnroll];
+#pragma unroll
+            for (uint32_t j = 0; j < kPairUnroll; j++) {
+                // run t + k (k > 0) starts at offset rel[k - 1]; t + k < rcap since ppos[rcap] = total > pend
+                const uint32_t o = lane + 32 * j;
+                const uint32_t rb = __shfl_sync(0xffffffffu, rel, k[j] ? k[j] - 1 : 0);
+                if (o <= span) {
+                    const uint64_t di = k[j] ? __ldg(&P.psegs[t + k[j]].base) + (o - rb) : base0 + o;
+                    d[j] = __ldg(P.pos + di);
+                    sid[j] = __ldg(P.sid + di);
+                } else {
+                    d[j] = make_uint2(0, 0);
+                    sid[j] = 0;
                 }
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kPairUnroll; j++) {
+                const PairSeg* q = P.psegs + t + k[j];
+                pair_tally<WITH_BP, SMEM>(P, __ldg(&q->qs), __ldg(&q->qe), SMEM ? 0u : __ldg(&q->qrow), d[j], sid[j],
+                                          s_cnt, s_bp);
+            }
+            // the run of the next step's first position pend + 1, from the boundaries in hand (at
+            // least one boundary, ppos[t + 1] <= pend, lies at or below it)
+            const uint32_t kn = __popc(__ballot_sync(0xffffffffu, rel <= span + 1));
+            if (pend + 1 < p1 && kn < 32) {
+                t += kn;
+                rlo = __ldg(P.ppos + t);
+                rhi = __ldg(P.ppos + t + 1);
+                ps = P.psegs[t];
             }
         }
     }
-    if (P.smem_tally) {
+    if (SMEM) {
         __syncthreads();
         for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
             if (s_cnt[k]) atomicAdd(&P.counts[k], s_cnt[k]);
@@ -1397,8 +1478,13 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     if (with_bp) k_sweep<true><<<grid, 256, smem, st>>>(P);
     else k_sweep<false><<<grid, 256, smem, st>>>(P);
     P.queue = d_small + 2;  // the pair sweep pulls from its own counter
-    if (with_bp) k_pairs<true><<<grid, 256, smem, st>>>(P);
-    else k_pairs<false><<<grid, 256, smem, st>>>(P);
+    if (P.smem_tally) {
+        if (with_bp) k_pairs<true, true><<<grid, 256, smem, st>>>(P);
+        else k_pairs<false, true><<<grid, 256, smem, st>>>(P);
+    } else {
+        if (with_bp) k_pairs<true, false><<<grid, 256, smem, st>>>(P);
+        else k_pairs<false, false><<<grid, 256, smem, st>>>(P);
+    }
     launches++;
     launches++;
     RGL_CUDA(cudaGetLastError());
@@ -1665,8 +1751,8 @@ int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
         const int mx = 160 * 1024;
         if (cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
             cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-            cudaFuncSetAttribute(k_pairs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-            cudaFuncSetAttribute(k_pairs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess)
+            cudaFuncSetAttribute(k_pairs<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+            cudaFuncSetAttribute(k_pairs<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess)
             s = fail(RGL_ERR_DEVICE, "cudaFuncSetAttribute");
     }
     for (int i = 0; i < 4 && s == RGL_OK; i++)
