@@ -1024,12 +1024,17 @@ struct rgl_context {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // second stream for the independent chains of a run (the end-key sort, the prefix sums of the
+    // starts and ends, the rank tables), forked from and joined back into `stream`
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int num_sms = 148;
     DevBuf iv, blk_off, blk_shard, key_a, key_b, val_a, val_b, ekey_a, ekey_b;
     DevBuf starts, ends, seg, segflag, segnum, seg_begin, ps_in, pe_in, ps, pe;
     DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp, item_r0;
     DevBuf segtab, tab_len, tab_off, tab_s, tab_e, tab_xs, tab_xe, tab2;
     DevBuf cl, pc, method, plen, ppos, psegs, item_t0, seg_need, lpos, tl, scan_sums;
+    DevBuf cub_tmp2, scan_sums2;  // the side stream's own scratch
     DevBuf item_hits, item_base, pairs;  // intervals mode
     DevBuf bt_off, bt_shard, acc;  // batched form: sub-batch block tables (offsets; shards then rows), stats
     uint32_t* h_small = nullptr;  // pinned mirror of `small`
@@ -1112,6 +1117,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     RGL_TRY(c->lpos.ensure(tot * 4 + 8));
     RGL_TRY(c->tl.ensure(tot * 4 + 8));
     RGL_TRY(c->scan_sums.ensure((std::max<uint64_t>(tot, 10 * n + 16) / kScanTile + 4) * 8));
+    RGL_TRY(c->scan_sums2.ensure((10 * n + 16) / kScanTile * 8 + 32));
     RGL_TRY(c->plen.ensure(tot * 8 + 16));
     RGL_TRY(c->ppos.ensure(tot * 8 + 16));
     RGL_TRY(c->psegs.ensure(tot * sizeof(PairSeg) + sizeof(PairSeg)));
@@ -1155,6 +1161,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nt, c->stream);
     need = std::max(need, b);
     RGL_TRY(c->cub_tmp.ensure(need + 256));
+    RGL_TRY(c->cub_tmp2.ensure(need + 256));
     if (rows) {
         RGL_TRY(c->out_counts.ensure((uint64_t)rows * idx->num_sources * 4 + 16));
         RGL_TRY(c->out_bp.ensure((uint64_t)rows * idx->num_sources * 8 + 16));
@@ -1167,7 +1174,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
                       &c->pe, &c->lo, &c->hi, &c->maxhi, &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos,
                       &c->cub_tmp, &c->small, &c->item_r0, &c->item_t0, &c->segtab, &c->tab_len, &c->tab_off,
                       &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->tab2, &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs,
-                      &c->seg_need, &c->acc})
+                      &c->seg_need, &c->acc, &c->cub_tmp2, &c->scan_sums2})
         sig = (sig ^ (uint64_t)(uintptr_t)b->p ^ ((uint64_t)b->cap << 17)) * 1099511628211ull;
     c->ws_sig = sig;
     return RGL_OK;
@@ -1245,14 +1252,21 @@ int finish(rgl_context* c, const Launch& L, rgl_query_stats* stats) {
 }
 
 // Exclusive scan of in[0, *n_ptr) into out (with out[n] = total), n <= cap; returns the launches.
+// `sums` holds cap / kScanTile + 1 tile sums (one buffer per stream that scans concurrently).
 template <typename Tin, typename Tout>
-uint32_t scan_dev(rgl_context* c, const Tin* in, Tout* out, const uint32_t* n_ptr, uint64_t cap, cudaStream_t st) {
+uint32_t scan_dev(Tout* sums, const Tin* in, Tout* out, const uint32_t* n_ptr, uint64_t cap, cudaStream_t st) {
     const unsigned tiles = (unsigned)(cap / kScanTile + 1);
-    Tout* sums = c->scan_sums.as<Tout>();
     k_scan_reduce<Tin, Tout><<<tiles, kScanThreads, 0, st>>>(in, n_ptr, sums);
     k_scan_tops<Tout><<<1, 1024, 0, st>>>(sums, n_ptr, out);
     k_scan_apply<Tin, Tout><<<tiles, kScanThreads, 0, st>>>(in, out, n_ptr, sums);
     return 3;
+}
+
+// `to` waits for everything enqueued on `from` so far.
+int stream_after(cudaStream_t to, cudaStream_t from, cudaEvent_t e) {
+    RGL_CUDA(cudaEventRecord(e, from));
+    RGL_CUDA(cudaStreamWaitEvent(to, e, 0));
+    return RGL_OK;
 }
 
 // Input of one pipeline run: n intervals at `iv` (device), block b = [blk_off[b], blk_off[b+1]) on
@@ -1324,39 +1338,49 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     if (nseg >= (1ull << 32)) return fail(RGL_ERR_INVALID_ARGUMENT, "num_shards * num_rows must be < 2^32");
 
     if (ev) RGL_CUDA(cudaEventRecord(c->ev[0], st));
+    // Two streams: `st` carries the chain from the sorted starts to the sweeps, `sd` the chains that
+    // only the rank sweep needs (the end-key sort, the prefix sums of starts and ends, the rank
+    // tables), so that the small kernels of both overlap; `sd` is joined back before the sweeps.
+    cudaStream_t sd = c->side;
     uint32_t launches = 0;
     k_expand_keys<<<grid_for(n, 256), 256, 0, st>>>(n, in.iv, in.blk_off, in.blk_shard, in.blk_row,
                                                     in.row_from_block, in.nblk, rows, in.row_base,
                                                     c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
                                                     c->ekey_a.as<uint64_t>(), d_small);
     launches++;
-    size_t tb = c->cub_tmp.cap;
+    RGL_TRY(stream_after(sd, st, c->ev_fork));
+    size_t tb = c->cub_tmp2.cap;
+    RGL_CUDA(cub::DeviceRadixSort::SortKeys(c->cub_tmp2.p, tb, c->ekey_a.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
+                                            (int)n, 0, 32 + segbits, sd));
+    tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tb, c->key_a.as<uint64_t>(), c->key_b.as<uint64_t>(),
                                              c->val_a.as<uint32_t>(), c->val_b.as<uint32_t>(), (int)n, 0,
                                              32 + segbits, st));
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceRadixSort::SortKeys(c->cub_tmp.p, tb, c->ekey_a.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
-                                            (int)n, 0, 32 + segbits, st));
+    RGL_TRY(stream_after(st, sd, c->ev_join));
     k_unpack<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->key_b.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
                                                    c->starts.as<uint32_t>(), c->ends.as<uint32_t>(),
                                                    c->seg.as<uint32_t>(), c->segflag.as<uint32_t>(),
                                                    c->ps_in.as<uint64_t>(), c->pe_in.as<uint64_t>());
     launches++;
+    RGL_TRY(stream_after(sd, st, c->ev_fork));
+    tb = c->cub_tmp2.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp2.p, tb, c->ps_in.as<uint64_t>(), c->ps.as<uint64_t>(),
+                                           (int)n + 1, sd));
+    tb = c->cub_tmp2.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp2.p, tb, c->pe_in.as<uint64_t>(), c->pe.as<uint64_t>(),
+                                           (int)n + 1, sd));
     tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tb, c->segflag.as<uint32_t>(), c->segnum.as<uint32_t>(),
                                            (int)n, st));
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->ps_in.as<uint64_t>(), c->ps.as<uint64_t>(),
-                                           (int)n + 1, st));
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->pe_in.as<uint64_t>(), c->pe.as<uint64_t>(),
-                                           (int)n + 1, st));
     k_seg_begin<<<grid_for(n, 256), 256, 0, st>>>(n, c->segflag.as<uint32_t>(), c->segnum.as<uint32_t>(),
                                                   c->seg_begin.as<uint32_t>());
     launches++;
     RGL_CUDA(cudaMemsetAsync(c->seg_need.p, 0, (size_t)(n + 1) * 4, st));
     const uint64_t tot = (uint64_t)n * ns;
-    if (tot + 1 >= (1ull << 31)) return fail(RGL_ERR_INVALID_ARGUMENT, "query intervals x layer slots must be < 2^31 per run");
+    if (tot + 1 >= (1ull << 31)) {
+        RGL_TRY(stream_after(st, sd, c->ev_join));
+        return fail(RGL_ERR_INVALID_ARGUMENT, "query intervals x layer slots must be < 2^31 per run");
+    }
     k_lohi<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, rows, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
                                                 c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, idx->d_pos,
                                                 idx->d_btab, c->lo.as<uint32_t>(), c->hi.as<uint32_t>());
@@ -1386,8 +1410,8 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                        c->hi.as<uint32_t>(), c->maxhi.as<uint32_t>(), c->rflag.as<uint32_t>(),
                                        c->cl.as<uint64_t>());
     launches++;
-    launches += scan_dev(c, c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(), Lp, tot, st);
-    launches += scan_dev(c, c->cl.as<uint64_t>(), c->pc.as<uint64_t>(), Lp, tot, st);
+    launches += scan_dev(c->scan_sums.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(), Lp, tot, st);
+    launches += scan_dev(c->scan_sums.as<uint64_t>(), c->cl.as<uint64_t>(), c->pc.as<uint64_t>(), Lp, tot, st);
     k_crange_emit<<<gc, 256, 0, st>>>(Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(),
                                       c->segnum.as<uint32_t>(), idx->d_slot, c->lo.as<uint32_t>(),
                                       c->maxhi.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
@@ -1397,42 +1421,46 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                         c->seg_need.as<uint32_t>(), Rp,
                                         reinterpret_cast<unsigned long long*>(d_small + 4));
     launches += 2;
-    // rank tables of the query segments that have a rank-difference range
-    k_seg_tabsize<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->seg_begin.as<uint32_t>(),
+    // side stream: rank tables of the query segments that have a rank-difference range
+    RGL_TRY(stream_after(sd, st, c->ev_fork));
+    k_seg_tabsize<<<grid_for(n + 1, 256), 256, 0, sd>>>(n, c->segnum.as<uint32_t>(), c->seg_begin.as<uint32_t>(),
                                                         c->seg_need.as<uint32_t>(), c->ends.as<uint32_t>(),
                                                         c->segtab.as<SegTab>(), c->tab_len.as<uint32_t>());
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->tab_len.as<uint32_t>(), c->tab_off.as<uint32_t>(),
-                                           (int)n + 1, st));
+    tb = c->cub_tmp2.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp2.p, tb, c->tab_len.as<uint32_t>(), c->tab_off.as<uint32_t>(),
+                                           (int)n + 1, sd));
     const uint64_t tab_cap = 10ull * n + 16;
     uint32_t* tab_count = d_small + 14;
-    k_tab_zero<<<(unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, st>>>(
+    k_tab_zero<<<(unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, sd>>>(
         n, c->segnum.as<uint32_t>(), c->tab_off.as<uint32_t>(), c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>(),
         tab_count);
-    k_tab_place<<<grid_for(n, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
+    k_tab_place<<<grid_for(n, 256), 256, 0, sd>>>(n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
                                                   c->tab_off.as<uint32_t>(), c->tab_xs.as<uint32_t>(),
                                                   c->tab_xe.as<uint32_t>());
-    k_tab_count<<<grid_for(n, 256), 256, 0, st>>>(n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
+    k_tab_count<<<grid_for(n, 256), 256, 0, sd>>>(n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
                                                   c->starts.as<uint32_t>(), c->ends.as<uint32_t>(),
                                                   c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>());
     // inclusive scans written one entry ahead: exclusive scan into tab_* whose entry k + 1 is the
     // inclusive sum through k (the tables are read from tab_* + 1)
-    launches += scan_dev(c, c->tab_xs.as<uint32_t>(), c->tab_s.as<uint32_t>(), tab_count, tab_cap, st);
-    launches += scan_dev(c, c->tab_xe.as<uint32_t>(), c->tab_e.as<uint32_t>(), tab_count, tab_cap, st);
-    k_tab_interleave<<<(unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, st>>>(
+    uint32_t* sums2 = c->scan_sums2.as<uint32_t>();
+    launches += scan_dev(sums2, c->tab_xs.as<uint32_t>(), c->tab_s.as<uint32_t>(), tab_count, tab_cap, sd);
+    launches += scan_dev(sums2, c->tab_xe.as<uint32_t>(), c->tab_e.as<uint32_t>(), tab_count, tab_cap, sd);
+    k_tab_interleave<<<(unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, sd>>>(
         tab_count, c->tab_s.as<uint32_t>(), c->tab_e.as<uint32_t>(), c->tab2.as<uint2>());
     launches++;
     launches += 4;
+    // main stream: the pair work space and the rank ranges' positions
     k_cpair_len<<<gc, 256, 0, st>>>(Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), idx->d_slot,
                                     idx->d_layers, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(), c->rflag.as<uint32_t>(),
                                     c->ridx.as<uint32_t>(), c->method.as<uint8_t>(), c->starts.as<uint32_t>(),
                                     c->val_b.as<uint32_t>(), c->plen.as<uint64_t>(), c->psegs.as<PairSeg>());
     launches++;
-    launches += scan_dev(c, c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(), Rp, tot, st);
-    launches += scan_dev(c, c->plen.as<uint64_t>(), c->ppos.as<uint64_t>(), Lp, tot, st);
+    launches += scan_dev(c->scan_sums.as<uint64_t>(), c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(), Rp, tot, st);
+    launches += scan_dev(c->scan_sums.as<uint64_t>(), c->plen.as<uint64_t>(), c->ppos.as<uint64_t>(), Lp, tot, st);
     k_totals<<<1, 32, 0, st>>>(d_small, c->rpos.as<uint64_t>(), c->ppos.as<uint64_t>());
     launches++;
     if (mode.no_sweep) {
+        RGL_TRY(stream_after(st, sd, c->ev_join));
         c->last_tot = tot;
         c->last_launches = launches;
         c->last_n = n;
@@ -1473,6 +1501,9 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     P.smem_tally = (rows == 1 && smem <= 160 * 1024) ? 1 : 0;
     if (!P.smem_tally) smem = 0;
     unsigned grid = (unsigned)(c->num_sms * L.ctas_per_sm);
+    // the rank tables are joined before the sweeps; the two sweeps run one after the other on
+    // `st` (each fills every SM with persistent blocks; run side by side they were slower)
+    RGL_TRY(stream_after(st, sd, c->ev_join));
     if (ev) RGL_CUDA(cudaEventRecord(c->ev[1], st));
     if (c->timing && mode.events) RGL_TRY(timing_record(c, true));
     if (with_bp) k_sweep<true><<<grid, 256, smem, st>>>(P);
@@ -1744,6 +1775,10 @@ int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
         else
             c->own_stream = true;
     }
+    if (s == RGL_OK && (cudaStreamCreateWithFlags(&c->side, cudaStreamNonBlocking) != cudaSuccess ||
+                        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+                        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess))
+        s = fail(RGL_ERR_DEVICE, "side stream");
     if (s == RGL_OK) cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, index->device);
     // shared-memory tallies of up to 160 KB (one row, D x 12 B); set once here so that no launch
     // path changes function attributes (graph capture included)
@@ -1773,6 +1808,7 @@ int rgl_context_destroy(rgl_context* c) {
     if (!c) return RGL_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->side) cudaStreamSynchronize(c->side);
     DevBuf* bufs[] = {&c->iv, &c->blk_off, &c->blk_shard, &c->key_a, &c->key_b, &c->val_a, &c->val_b,
                       &c->ekey_a, &c->ekey_b, &c->starts, &c->ends, &c->seg, &c->segflag, &c->segnum,
                       &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps, &c->pe, &c->lo, &c->hi, &c->maxhi,
@@ -1780,7 +1816,8 @@ int rgl_context_destroy(rgl_context* c) {
                       &c->out_counts, &c->out_bp, &c->item_r0,
                       &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->tab2,
                       &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs, &c->item_t0,
-                      &c->seg_need, &c->item_hits, &c->item_base, &c->pairs, &c->bt_off, &c->bt_shard, &c->acc, &c->gc.t_off, &c->gc.t_shard};
+                      &c->seg_need, &c->item_hits, &c->item_base, &c->pairs, &c->bt_off, &c->bt_shard, &c->acc, &c->gc.t_off, &c->gc.t_shard,
+                      &c->cub_tmp2, &c->scan_sums2};
     if (c->gc.exec) cudaGraphExecDestroy(c->gc.exec);
     if (c->gc.graph) cudaGraphDestroy(c->gc.graph);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
@@ -1797,6 +1834,9 @@ int rgl_context_destroy(rgl_context* c) {
     if (c->h_small) cudaFreeHost(c->h_small);
     if (c->h_acc) cudaFreeHost(c->h_acc);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    if (c->side) cudaStreamDestroy(c->side);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     index_release(c->idx);
     delete c;
     (void)cudaGetLastError();
