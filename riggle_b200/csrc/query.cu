@@ -563,21 +563,34 @@ __device__ __forceinline__ uint32_t range_advance(const uint64_t* __restrict__ r
 
 // Work-item partition: item i covers positions [i * chunk, (i + 1) * chunk) of the concatenated
 // ranges; item_r0[i] = the range holding its first position (last r with rpos[r] <= i * chunk),
-// found by binary search over the range offsets (grid-stride over items).
-__global__ void k_item_ranges(const uint32_t* __restrict__ rcount, const uint64_t* __restrict__ rpos, uint32_t chunk,
-                              uint64_t item_cap,
-                              uint32_t* __restrict__ item_r0) {
-    const uint32_t rcap = *rcount;
-    const uint64_t total = rpos[rcap];
-    const uint64_t items = min((total + chunk - 1) / chunk, item_cap);
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < items; i += (uint64_t)gridDim.x * blockDim.x) {
+// found by binary search over the range offsets.  One launch serves the rank ranges (rpos, *Rp
+// ranges) and the pair runs (ppos, *Lp runs), grid-stride over the items of both, and records the
+// two position totals in the counter block (64-bit words 5 and 6).
+__global__ void k_item_ranges(uint32_t* __restrict__ small, const uint32_t* __restrict__ Rp,
+                              const uint64_t* __restrict__ rpos, const uint32_t* __restrict__ Lp,
+                              const uint64_t* __restrict__ ppos, uint32_t chunk, uint64_t item_cap,
+                              uint32_t* __restrict__ item_r0, uint32_t* __restrict__ item_t0) {
+    const uint32_t R = *Rp, L = *Lp;
+    const uint64_t rtot = rpos[R], ptot = ppos[L];
+    const uint64_t g0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (g0 == 0) {
+        unsigned long long* s64 = reinterpret_cast<unsigned long long*>(small);
+        s64[5] = rtot;
+        s64[6] = ptot;
+    }
+    const uint64_t ri = min((rtot + chunk - 1) / chunk, item_cap);
+    const uint64_t pi = min((ptot + chunk - 1) / chunk, item_cap);
+    for (uint64_t g = g0; g < ri + pi; g += (uint64_t)gridDim.x * blockDim.x) {
+        const bool rank = g < ri;
+        const uint64_t* a = rank ? rpos : ppos;
+        const uint64_t i = rank ? g : g - ri;
         const uint64_t p = i * chunk;
-        uint64_t lo = 0, hi = rcap;
+        uint64_t lo = 0, hi = rank ? R : L;
         while (lo < hi) {
             uint64_t m = (lo + hi + 1) >> 1;
-            if (__ldg(rpos + m) <= p) lo = m; else hi = m - 1;
+            if (__ldg(a + m) <= p) lo = m; else hi = m - 1;
         }
-        item_r0[i] = (uint32_t)lo;
+        (rank ? item_r0 : item_t0)[i] = (uint32_t)lo;
     }
 }
 
@@ -597,20 +610,6 @@ __device__ __forceinline__ void cursor_load(const SweepParams& P, Cursor& c, uin
     c.rd = P.ranges[r];
     c.base = P.layers[c.rd.layer_idx].off + c.rd.db_lo;
     c.tab = P.segtabs[c.rd.seg];
-}
-
-// #starts < x and #ends <= x within the cursor's segment, as absolute sorted positions.
-__device__ __forceinline__ uint32_t rank_start(const SweepParams& P, const SegTab& t, uint32_t x) {
-    const uint32_t b = x >> t.shift;
-    if (b >= t.nbins) return t.end;
-    const uint32_t lo = __ldg(&P.tab2[t.off + b].x), hi = __ldg(&P.tab2[t.off + b + 1].x);
-    return lo == hi ? lo : lb_u32(P.starts, lo, hi, x);
-}
-__device__ __forceinline__ uint32_t rank_end(const SweepParams& P, const SegTab& t, uint32_t x) {
-    const uint32_t b = x >> t.shift;
-    if (b >= t.nbins) return t.end;
-    const uint32_t lo = __ldg(&P.tab2[t.off + b].y), hi = __ldg(&P.tab2[t.off + b + 1].y);
-    return lo == hi ? lo : ub_u32(P.ends, lo, hi, x);
 }
 
 __device__ __forceinline__ void cursor_seek(const SweepParams& P, Cursor& c, uint64_t p, uint32_t rcap) {
@@ -1457,9 +1456,9 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     launches++;
     launches += scan_dev(c->scan_sums.as<uint64_t>(), c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(), Rp, tot, st);
     launches += scan_dev(c->scan_sums.as<uint64_t>(), c->plen.as<uint64_t>(), c->ppos.as<uint64_t>(), Lp, tot, st);
-    k_totals<<<1, 32, 0, st>>>(d_small, c->rpos.as<uint64_t>(), c->ppos.as<uint64_t>());
-    launches++;
     if (mode.no_sweep) {
+        k_totals<<<1, 32, 0, st>>>(d_small, c->rpos.as<uint64_t>(), c->ppos.as<uint64_t>());
+        launches++;
         RGL_TRY(stream_after(st, sd, c->ev_join));
         c->last_tot = tot;
         c->last_launches = launches;
@@ -1467,11 +1466,10 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
         if (mode.reset_err) RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
         return RGL_OK;
     }
-    k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(Rp, c->rpos.as<uint64_t>(), L.chunk, kItemCap,
-                                                               c->item_r0.as<uint32_t>());
-    k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(Lp, c->ppos.as<uint64_t>(), L.chunk, kItemCap,
-                                                               c->item_t0.as<uint32_t>());
-    launches += 2;
+    k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(d_small, Rp, c->rpos.as<uint64_t>(), Lp,
+                                                               c->ppos.as<uint64_t>(), L.chunk, kItemCap,
+                                                               c->item_r0.as<uint32_t>(), c->item_t0.as<uint32_t>());
+    launches++;
     SweepParams P;
     P.item_r0 = c->item_r0.as<uint32_t>();
     P.item_t0 = c->item_t0.as<uint32_t>();
