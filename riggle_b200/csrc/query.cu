@@ -292,7 +292,9 @@ __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_
 // the device; these scans read it there, so the pipeline keeps no host synchronisation (and stays
 // graph-capturable) while its work follows the live count instead of the (query, slot) capacity.
 // Exclusive scan of in[0, n) into out[0, n], out[n] = total: per-tile sums, one block scanning the
-// tile sums, per-tile block scans offset by them.  Launched over the capacity; tiles past n exit.
+// tile sums, per-tile block scans offset by them.  The tile kernels are launched with a grid sized
+// for the SMs and walk the tiles below n grid-stride, so a capacity far above the live count costs
+// no empty blocks.
 constexpr int kScanThreads = 256, kScanItems = 8, kScanTile = kScanThreads * kScanItems;
 
 template <typename Tin, typename Tout>
@@ -300,18 +302,20 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const Tin* __restr
                                                               const uint32_t* __restrict__ n_ptr,
                                                               Tout* __restrict__ tile_sums) {
     const uint32_t n = *n_ptr;
-    const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
-    if (base >= n) return;
-    Tout s = 0;
-#pragma unroll
-    for (int k = 0; k < kScanItems; k++) {
-        const uint64_t i = base + (uint64_t)k * kScanThreads + threadIdx.x;
-        if (i < n) s += (Tout)in[i];
-    }
     using BR = cub::BlockReduce<Tout, kScanThreads>;
     __shared__ typename BR::TempStorage tmp;
-    s = BR(tmp).Sum(s);
-    if (threadIdx.x == 0) tile_sums[blockIdx.x] = s;
+    for (uint64_t tile = blockIdx.x; tile * kScanTile < n; tile += gridDim.x) {
+        const uint64_t base = tile * kScanTile;
+        Tout s = 0;
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++) {
+            const uint64_t i = base + (uint64_t)k * kScanThreads + threadIdx.x;
+            if (i < n) s += (Tout)in[i];
+        }
+        s = BR(tmp).Sum(s);
+        if (threadIdx.x == 0) tile_sums[tile] = s;
+        __syncthreads();  // tmp is reused by the next tile
+    }
 }
 
 template <typename Tout>
@@ -338,9 +342,6 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const Tin* __restri
                                                              const uint32_t* __restrict__ n_ptr,
                                                              const Tout* __restrict__ tile_off) {
     const uint32_t n = *n_ptr;
-    const uint64_t base = (uint64_t)blockIdx.x * kScanTile;
-    if (base >= n) return;
-    const int valid = (int)((uint64_t)n - base < (uint64_t)kScanTile ? (uint64_t)n - base : (uint64_t)kScanTile);
     using BL = cub::BlockLoad<Tout, kScanThreads, kScanItems, cub::BLOCK_LOAD_WARP_TRANSPOSE>;
     using BSt = cub::BlockStore<Tout, kScanThreads, kScanItems, cub::BLOCK_STORE_WARP_TRANSPOSE>;
     using BS = cub::BlockScan<Tout, kScanThreads>;
@@ -349,15 +350,20 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const Tin* __restri
         typename BSt::TempStorage store;
         typename BS::TempStorage scan;
     } tmp;
-    Tout v[kScanItems];
-    BL(tmp.load).Load(in + base, v, valid, (Tout)0);
-    __syncthreads();
-    BS(tmp.scan).ExclusiveSum(v, v);
-    const Tout off = tile_off[blockIdx.x];
+    for (uint64_t tile = blockIdx.x; tile * kScanTile < n; tile += gridDim.x) {
+        const uint64_t base = tile * kScanTile;
+        const int valid = (int)((uint64_t)n - base < (uint64_t)kScanTile ? (uint64_t)n - base : (uint64_t)kScanTile);
+        Tout v[kScanItems];
+        BL(tmp.load).Load(in + base, v, valid, (Tout)0);
+        __syncthreads();
+        BS(tmp.scan).ExclusiveSum(v, v);
+        const Tout off = tile_off[tile];
 #pragma unroll
-    for (int k = 0; k < kScanItems; k++) v[k] += off;
-    __syncthreads();
-    BSt(tmp.store).Store(out + base, v, valid);
+        for (int k = 0; k < kScanItems; k++) v[k] += off;
+        __syncthreads();
+        BSt(tmp.store).Store(out + base, v, valid);
+        __syncthreads();  // tmp is reused by the next tile
+    }
 }
 
 // ---- 4b. live candidate runs -------------------------------------------------------------------
@@ -1254,10 +1260,10 @@ int finish(rgl_context* c, const Launch& L, rgl_query_stats* stats) {
 // `sums` holds cap / kScanTile + 1 tile sums (one buffer per stream that scans concurrently).
 template <typename Tin, typename Tout>
 uint32_t scan_dev(Tout* sums, const Tin* in, Tout* out, const uint32_t* n_ptr, uint64_t cap, cudaStream_t st) {
-    const unsigned tiles = (unsigned)(cap / kScanTile + 1);
-    k_scan_reduce<Tin, Tout><<<tiles, kScanThreads, 0, st>>>(in, n_ptr, sums);
+    const unsigned grid = (unsigned)std::min<uint64_t>(cap / kScanTile + 1, 148ull * 8);
+    k_scan_reduce<Tin, Tout><<<grid, kScanThreads, 0, st>>>(in, n_ptr, sums);
     k_scan_tops<Tout><<<1, 1024, 0, st>>>(sums, n_ptr, out);
-    k_scan_apply<Tin, Tout><<<tiles, kScanThreads, 0, st>>>(in, out, n_ptr, sums);
+    k_scan_apply<Tin, Tout><<<grid, kScanThreads, 0, st>>>(in, out, n_ptr, sums);
     return 3;
 }
 
