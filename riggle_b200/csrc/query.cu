@@ -95,18 +95,36 @@ __device__ __forceinline__ uint32_t ub_u32(const uint32_t* __restrict__ a, uint3
     }
     return lo;
 }
-__device__ __forceinline__ uint32_t pp_layer(const uint2* __restrict__ pos, const uint32_t* __restrict__ btab,
-                                             const LayerDev& L, uint32_t x) {
-    // partition point of (start < x) over a layer sorted by start: the bucket table gives the
-    // elements whose starts share x's bucket, searched by bisection
-    const uint32_t b = x >> L.bshift;
-    if (b >= L.nb - 1) return (uint32_t)L.n;
-    uint32_t lo = __ldg(btab + b), hi = __ldg(btab + b + 1);
-    while (lo < hi) {
-        uint32_t m = lo + ((hi - lo) >> 1);
-        if (__ldg(&pos[m].x) < x) lo = m + 1; else hi = m;
+// Partition points of (start < x) over a layer sorted by start, for x0 -> r0 and x1 -> r1: the
+// bucket table gives the elements whose starts share x's bucket, searched by bisection.  The two
+// run in lockstep (both bucket reads issued together, then one probe of each bisection per round),
+// so their chains of dependent random reads overlap instead of following one another.
+__device__ __forceinline__ void pp_layer2(const uint2* __restrict__ pos, const uint32_t* __restrict__ btab,
+                                          const LayerDev& L, uint32_t x0, uint32_t x1, uint32_t& r0, uint32_t& r1) {
+    const uint32_t last = L.nb - 1;
+    const uint32_t b0 = x0 >> L.bshift, b1 = x1 >> L.bshift;
+    uint32_t lo0 = (uint32_t)L.n, hi0 = (uint32_t)L.n, lo1 = (uint32_t)L.n, hi1 = (uint32_t)L.n;
+    if (b0 < last) {
+        lo0 = __ldg(btab + b0);
+        hi0 = __ldg(btab + b0 + 1);
     }
-    return lo;
+    if (b1 < last) {
+        lo1 = __ldg(btab + b1);
+        hi1 = __ldg(btab + b1 + 1);
+    }
+    while (lo0 < hi0 || lo1 < hi1) {
+        const bool a0 = lo0 < hi0, a1 = lo1 < hi1;
+        const uint32_t m0 = lo0 + ((hi0 - lo0) >> 1), m1 = lo1 + ((hi1 - lo1) >> 1);
+        const uint32_t v0 = a0 ? __ldg(&pos[m0].x) : 0u, v1 = a1 ? __ldg(&pos[m1].x) : 0u;
+        if (a0) {
+            if (v0 < x0) lo0 = m0 + 1; else hi0 = m0;
+        }
+        if (a1) {
+            if (v1 < x1) lo1 = m1 + 1; else hi1 = m1;
+        }
+    }
+    r0 = lo0;
+    r1 = lo1;
 }
 
 // ---- 1. keys ------------------------------------------------------------------------------------
@@ -279,8 +297,7 @@ __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_
         uint32_t s = starts[i];
         uint32_t back = s >= L.max_size ? s - L.max_size : 0u;  // saturating_sub, query.rs:141
         const uint32_t* bt = btab + L.boff;
-        lo = pp_layer(p, bt, L, back);
-        hi = pp_layer(p, bt, L, qend[i]);
+        pp_layer2(p, bt, L, back, qend[i], lo, hi);
         if (hi < lo) hi = lo;
     }
     lo_out[t] = lo;
