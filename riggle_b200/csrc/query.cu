@@ -30,6 +30,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <type_traits>
 
 #include "internal.h"
 
@@ -155,6 +156,77 @@ __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, c
 }
 
 // ---- 2/3. unpack sorted keys ---------------------------------------------------------------------
+// Block-local sort of the query keys, for runs in which every input block holds one segment
+// ((shard, row)) and no two blocks share one: the segment-major order of the device-wide radix
+// sort is then the blocks' own order, each block sorted by position.  One thread block per input
+// block of at most kBlockSortCap intervals: with VALUES the start keys with their ends as values
+// (key_a / val_a -> key_b / val_b), else the end keys alone (ekey_a -> ekey_b).  A block that is
+// already in order (the usual case for sorted BED input) is copied through; otherwise a shared-memory
+// radix sort over the bits the block's positions use.  Both forms are stable, like the radix sort.
+constexpr int kBsThreads = 1024, kBsItems = 16;
+constexpr uint64_t kBlockSortCap = (uint64_t)kBsThreads * kBsItems;
+
+template <bool VALUES>
+struct BlockSortTypes {
+    using Sort = cub::BlockRadixSort<uint32_t, kBsThreads, kBsItems, typename std::conditional<VALUES, uint32_t, cub::NullType>::type>;
+    union Smem {
+        typename Sort::TempStorage sort;
+        uint32_t last[kBsThreads];
+    };
+};
+
+template <bool VALUES>
+__global__ void __launch_bounds__(kBsThreads, 1) k_block_sort(const uint64_t* __restrict__ blk_off,
+                                                             const uint64_t* __restrict__ kin,
+                                                             const uint32_t* __restrict__ vin,
+                                                             uint64_t* __restrict__ kout, uint32_t* __restrict__ vout) {
+    using T = BlockSortTypes<VALUES>;
+    extern __shared__ __align__(16) unsigned char bs_smem[];
+    typename T::Smem& sm = *reinterpret_cast<typename T::Smem*>(bs_smem);
+    const uint64_t base = blk_off[blockIdx.x];
+    const uint32_t cnt = (uint32_t)(blk_off[blockIdx.x + 1] - base);
+    if (cnt == 0) return;
+    const uint64_t hi = kin[base] & 0xFFFFFFFF00000000ull;  // the block's segment, in the high word
+    uint32_t k[kBsItems], v[kBsItems];
+    uint32_t any = 0;
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < kBsItems; j++) {
+        const uint32_t i = threadIdx.x * kBsItems + j;  // blocked: thread t holds [16 t, 16 t + 16)
+        k[j] = i < cnt ? (uint32_t)kin[base + i] : 0xFFFFFFFFu;  // padding sorts last
+        v[j] = (VALUES && i < cnt) ? vin[base + i] : 0u;
+        any |= i < cnt ? k[j] : 0u;
+        if (j) ok = ok && k[j - 1] <= k[j];
+    }
+    __shared__ uint32_t s_bits;  // bitwise OR of the block's keys
+    sm.last[threadIdx.x] = k[kBsItems - 1];
+    if (threadIdx.x == 0) s_bits = 0;
+    __syncthreads();
+    if (threadIdx.x) ok = ok && sm.last[threadIdx.x - 1] <= k[0];
+    any = __reduce_or_sync(0xffffffffu, any);
+    if ((threadIdx.x & 31u) == 0) atomicOr(&s_bits, any);
+    const bool sorted = __syncthreads_and(ok);  // also orders the atomicOr before the read below
+    const uint32_t bits = s_bits;
+    if (!sorted) {
+        const int end_bit = bits ? 32 - __clz(bits) : 1;
+        if constexpr (VALUES)
+            typename T::Sort(sm.sort).Sort(k, v, 0, end_bit);
+        else
+            typename T::Sort(sm.sort).Sort(k, 0, end_bit);
+    }
+#pragma unroll
+    for (int j = 0; j < kBsItems; j++) {
+        const uint32_t i = threadIdx.x * kBsItems + j;
+        if (i < cnt) {
+            kout[base + i] = hi | k[j];
+            if (VALUES) vout[base + i] = v[j];
+        }
+    }
+}
+
+template <bool VALUES>
+constexpr size_t block_sort_smem() { return sizeof(typename BlockSortTypes<VALUES>::Smem); }
+
 __global__ void k_unpack(uint32_t n, const uint64_t* __restrict__ key, const uint64_t* __restrict__ ekey,
                          uint32_t* __restrict__ starts, uint32_t* __restrict__ ends_s, uint32_t* __restrict__ seg,
                          uint32_t* __restrict__ segflag, uint64_t* __restrict__ ps_in, uint64_t* __restrict__ pe_in) {
@@ -1301,7 +1373,25 @@ struct PipeIn {
     const uint32_t* blk_shard;
     const uint32_t* blk_row;  // optional: the row every interval of the block must carry
     int row_from_block = 0;   // 1: rows come from blk_row, interval sids are ignored
+    int block_local = 0;      // 1: one segment per block, no segment in two blocks, blocks <= kBlockSortCap
 };
+
+// Whether a run's blocks allow the block-local key sort: with one row, or rows taken from the
+// blocks, every block is one segment; they must be distinct and each at most kBlockSortCap
+// intervals.  off: nblk + 1 host offsets; row: the blocks' rows (null: row 0 of one row).
+bool blocks_local(uint32_t nblk, const uint64_t* off, const uint32_t* shard, const uint32_t* row, uint32_t rows,
+                  uint32_t row_base) {
+    if (!row && rows != 1) return false;
+    std::vector<uint64_t> segs;
+    segs.reserve(nblk);
+    for (uint32_t b = 0; b < nblk; b++) {
+        const uint64_t cnt = off[b + 1] - off[b];
+        if (cnt > kBlockSortCap) return false;
+        if (cnt) segs.push_back((uint64_t)shard[b] * rows + (row ? row[b] - row_base : 0u));
+    }
+    std::sort(segs.begin(), segs.end());
+    return std::adjacent_find(segs.begin(), segs.end()) == segs.end();
+}
 
 // What a run does besides the sweep: the single-call entry points zero their rows, reset the error
 // word and record stats events; the sub-batches of a batched call leave all of that to the caller
@@ -1372,12 +1462,21 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     launches++;
     RGL_TRY(stream_after(sd, st, c->ev_fork));
     size_t tb = c->cub_tmp2.cap;
-    RGL_CUDA(cub::DeviceRadixSort::SortKeys(c->cub_tmp2.p, tb, c->ekey_a.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
-                                            (int)n, 0, 32 + segbits, sd));
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tb, c->key_a.as<uint64_t>(), c->key_b.as<uint64_t>(),
-                                             c->val_a.as<uint32_t>(), c->val_b.as<uint32_t>(), (int)n, 0,
-                                             32 + segbits, st));
+    if (in.block_local) {
+        k_block_sort<false><<<in.nblk, kBsThreads, block_sort_smem<false>(), sd>>>(
+            in.blk_off, c->ekey_a.as<uint64_t>(), nullptr, c->ekey_b.as<uint64_t>(), nullptr);
+        k_block_sort<true><<<in.nblk, kBsThreads, block_sort_smem<true>(), st>>>(
+            in.blk_off, c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(), c->key_b.as<uint64_t>(),
+            c->val_b.as<uint32_t>());
+        launches += 2;
+    } else {
+        RGL_CUDA(cub::DeviceRadixSort::SortKeys(c->cub_tmp2.p, tb, c->ekey_a.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
+                                                (int)n, 0, 32 + segbits, sd));
+        tb = c->cub_tmp.cap;
+        RGL_CUDA(cub::DeviceRadixSort::SortPairs(c->cub_tmp.p, tb, c->key_a.as<uint64_t>(), c->key_b.as<uint64_t>(),
+                                                 c->val_a.as<uint32_t>(), c->val_b.as<uint32_t>(), (int)n, 0,
+                                                 32 + segbits, st));
+    }
     RGL_TRY(stream_after(st, sd, c->ev_join));
     k_unpack<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->key_b.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
                                                    c->starts.as<uint32_t>(), c->ends.as<uint32_t>(),
@@ -1597,6 +1696,10 @@ struct BatchPlan {
     std::vector<uint32_t> row;   // per sub-batch: nblk block rows (same layout; unused without block_rows)
     uint64_t max_n = 0;
     uint32_t max_rows = 0, max_blk = 0;
+    bool local(const SubBatch& sb, bool block_rows) const {  // block-local key sort allowed
+        return blocks_local(sb.nblk, &off[sb.tab_at], &shard[sb.tab_at], block_rows ? &row[sb.tab_at] : nullptr,
+                            sb.rows, sb.row_lo);
+    }
     std::vector<uint32_t> shard_rows() const {  // the device table: shards, then rows
         std::vector<uint32_t> v(shard);
         v.insert(v.end(), row.begin(), row.end());
@@ -1686,6 +1789,7 @@ int enqueue_batch(rgl_context* c, const rgl_batch* b, const BatchPlan& P, const 
     for (const SubBatch& sb : P.subs) {
         PipeIn in{b->d_intervals + sb.begin, sb.n, sb.rows, sb.row_lo, sb.nblk, d_off + sb.tab_at,
                   d_sr + sb.tab_at, b->block_rows ? d_sr + P.shard.size() + sb.tab_at : nullptr};
+        in.block_local = P.local(sb, b->block_rows != nullptr);
         RGL_TRY(run_pipeline(c, in, q, d_counts + (uint64_t)sb.row_lo * D,
                              d_bp ? d_bp + (uint64_t)sb.row_lo * D : nullptr, nullptr, m));
         nl += c->last_launches;
@@ -1764,6 +1868,7 @@ int enqueue_block_rows(rgl_context* c, uint32_t num_rows, uint32_t nblk, const u
     if (d_bp) RGL_CUDA(cudaMemsetAsync(d_bp, 0, (size_t)num_rows * D * 8, st));
     PipeIn in{d_iv + off[0], n, num_rows, 0, nblk, c->bt_off.as<uint64_t>(), c->bt_shard.as<uint32_t>(),
               c->bt_shard.as<uint32_t>() + nblk + 1, 1};
+    in.block_local = blocks_local(nblk, rel.data(), shards, rows, num_rows, 0);
     PipeMode m;
     m.zero_out = false;
     // the table uploads read pageable vectors that die here: an asynchronous copy from pageable
@@ -1808,7 +1913,11 @@ int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
         if (cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
             cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
             cudaFuncSetAttribute(k_pairs<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-            cudaFuncSetAttribute(k_pairs<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess)
+            cudaFuncSetAttribute(k_pairs<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+            cudaFuncSetAttribute(k_block_sort<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)block_sort_smem<true>()) != cudaSuccess ||
+            cudaFuncSetAttribute(k_block_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)block_sort_smem<false>()) != cudaSuccess)
             s = fail(RGL_ERR_DEVICE, "cudaFuncSetAttribute");
     }
     for (int i = 0; i < 4 && s == RGL_OK; i++)
@@ -1902,6 +2011,7 @@ int rgl_query_counts_device(rgl_context* c, uint32_t num_rows, uint32_t num_shar
     }
     PipeIn in{c->iv.as<rgl_interval>(), n, num_rows, 0, num_shards, c->blk_off.as<uint64_t>(),
               c->blk_shard.as<uint32_t>(), nullptr};
+    in.block_local = blocks_local(num_shards, off.data(), shard_ids, nullptr, num_rows, 0);
     RGL_TRY(run_pipeline(c, in, opts, d_counts, reinterpret_cast<unsigned long long*>(d_overlap_bp), stats));
     if (!stats) return RGL_OK;
     RGL_CUDA(cudaStreamSynchronize(c->stream));
@@ -1937,6 +2047,7 @@ int rgl_query_counts(rgl_context* c, const rgl_query_batch* b, const rgl_query_o
     }
     PipeIn in{c->iv.as<rgl_interval>(), n, rows, 0, (uint32_t)blocks.size(), c->blk_off.as<uint64_t>(),
               c->blk_shard.as<uint32_t>(), nullptr};
+    in.block_local = blocks_local((uint32_t)blocks.size(), off.data(), ids.data(), nullptr, rows, 0);
     RGL_TRY(run_pipeline(c, in, opts, c->out_counts.as<uint32_t>(),
                          overlap_bp ? c->out_bp.as<unsigned long long>() : nullptr, stats));
     if (cells) {
@@ -2101,6 +2212,7 @@ int rgl_query_batch_host(rgl_context* c, const rgl_batch* b, const rgl_interval*
         RGL_CUDA(cudaStreamWaitEvent(st, c->ev_copied[slot], 0));
         PipeIn in{stage, sb.n, sb.rows, sb.row_lo, sb.nblk, d_off + sb.tab_at, d_sr + sb.tab_at,
                   b->block_rows ? d_sr + P.shard.size() + sb.tab_at : nullptr};
+        in.block_local = P.local(sb, b->block_rows != nullptr);
         RGL_TRY(run_pipeline(c, in, &q, d_counts + (uint64_t)sb.row_lo * D, d_bp ? d_bp + (uint64_t)sb.row_lo * D : nullptr,
                              nullptr, m));
         RGL_CUDA(cudaEventRecord(c->ev_used[slot], st));
@@ -2162,6 +2274,7 @@ int rgl_batch_autotune(rgl_context* c, const rgl_batch* b, uint64_t sub_batch, r
     PipeIn in{b->d_intervals + sb.begin, sb.n, sb.rows, sb.row_lo, sb.nblk, c->bt_off.as<uint64_t>() + sb.tab_at,
               c->bt_shard.as<uint32_t>() + sb.tab_at,
               b->block_rows ? c->bt_shard.as<uint32_t>() + P.shard.size() + sb.tab_at : nullptr};
+    in.block_local = P.local(sb, b->block_rows != nullptr);
     const bool was_timing = c->timing;
     *best = rgl_query_opts{};
     uint32_t nt = 0;

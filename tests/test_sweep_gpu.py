@@ -168,3 +168,35 @@ def test_config1_parity_with_oracle():
     assert st["db_swept"] == ost["db_swept"]
     # the reference's f32 bins agree with exact bp / 100 to f32 accumulation error
     np.testing.assert_allclose(of32, obp / 100.0, rtol=1e-4)
+
+
+def test_block_local_sort_equals_radix_sort():
+    """With one row and one block per chromosome of at most 16,384 query intervals, the keys are
+    sorted block by block in shared memory (copied through when a block is already in order);
+    otherwise by the device-wide radix sort.  Both must give the oracle's counts and overlaps, on
+    unsorted blocks, an already sorted block, a block at the cap and one just above it."""
+    rng = np.random.default_rng(11)
+    D = 23
+    blocks = [(sh, helpers.random_db(rng, 30000, 2_000_000, D)) for sh in range(2)]
+    layers = rg.bucket_layers(blocks)
+
+    def queries(b, n):
+        q = np.concatenate([helpers.queries_touching(rng, b, n // 2, 1), helpers.random_db(rng, n - n // 2, 2_000_000, 1)])
+        q[:, 2] = 0
+        q[: n // 8] = q[n // 8: 2 * (n // 8)]  # equal starts (and whole duplicates)
+        return q[rng.permutation(n)]
+
+    idx = rg.Index.from_layers(layers, D, ["s0", "s1"])
+    ctx = rg.Context(idx)
+    for n0, n1, presorted in ((5000, 700, False), (16384, 3000, True), (16384, 16385, False)):
+        q0, q1 = queries(blocks[0][1], n0), queries(blocks[1][1], n1)
+        if presorted:
+            q0 = q0[np.lexsort((q0[:, 1], q0[:, 0]))]
+        oc, _, obp, _ = O.query_database(layers, {0: q0.copy(), 1: q1.copy()}, 1, D, threads=4)
+        local = ctx.query_counts({"s0": q0, "s1": q1}, 1)  # one block per chromosome
+        k = n0 // 3
+        split = ctx.query_counts({"s0": q0[:k], 0: q0[k:], "s1": q1}, 1)  # chromosome 0 in two blocks
+        for c, bp, _ in (local, split):
+            assert (c == oc).all() and (bp == obp).all(), (n0, n1, presorted)
+    ctx.close()
+    idx.close()
