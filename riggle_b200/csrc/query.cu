@@ -525,7 +525,7 @@ __global__ void k_crange_emit(const uint32_t* __restrict__ Lp, uint32_t n, uint3
 // trivial per-pair work; where candidate windows overlap heavily (broad layers) the rank sweep reads
 // each union element once.  rlen = union length of rank ranges (the rank work space); the union of
 // every range is summed into *union_total (the swept count of the metric).
-__global__ void k_crange_method(const uint32_t* __restrict__ Lp, const uint32_t* __restrict__ cridx,
+__global__ void __launch_bounds__(256) k_crange_method(const uint32_t* __restrict__ Lp, const uint32_t* __restrict__ cridx,
                                 const RangeDesc* __restrict__ ranges, const uint64_t* __restrict__ cpc,
                                 uint32_t pair_ratio, uint8_t* __restrict__ method, uint64_t* __restrict__ rlen,
                                 uint32_t* __restrict__ seg_need, uint32_t* __restrict__ R_out,
@@ -544,8 +544,11 @@ __global__ void k_crange_method(const uint32_t* __restrict__ Lp, const uint32_t*
         rlen[r] = m == M_RANK ? len : 0;
         acc += len;
     }
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
-    if ((threadIdx.x & 31u) == 0 && acc) atomicAdd(union_total, acc);
+    // one atomic per block on the shared total
+    using BR = cub::BlockReduce<unsigned long long, 256>;
+    __shared__ typename BR::TempStorage tmp;
+    acc = BR(tmp).Sum(acc);
+    if (threadIdx.x == 0 && acc) atomicAdd(union_total, acc);
 }
 
 // Pair work space: each live run of a pair range contributes its candidates.
