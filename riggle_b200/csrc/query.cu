@@ -227,24 +227,34 @@ __global__ void __launch_bounds__(kBsThreads, 1) k_block_sort(const uint64_t* __
 template <bool VALUES>
 constexpr size_t block_sort_smem() { return sizeof(typename BlockSortTypes<VALUES>::Smem); }
 
-__global__ void k_unpack(uint32_t n, const uint64_t* __restrict__ key, const uint64_t* __restrict__ ekey,
-                         uint32_t* __restrict__ starts, uint32_t* __restrict__ ends_s, uint32_t* __restrict__ seg,
-                         uint32_t* __restrict__ segflag, uint64_t* __restrict__ ps_in, uint64_t* __restrict__ pe_in) {
+// The sorted start keys into starts, segment ids, segment-start flags and the starts' prefix-sum
+// input (entry n = 0); the sorted end keys into ends and the ends' prefix-sum input.
+__global__ void k_unpack_starts(uint32_t n, const uint64_t* __restrict__ key, uint32_t* __restrict__ starts,
+                                uint32_t* __restrict__ seg, uint32_t* __restrict__ segflag,
+                                uint64_t* __restrict__ ps_in) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i > n) return;
     if (i == n) {
         ps_in[n] = 0;
-        pe_in[n] = 0;
         return;
     }
-    uint64_t k = key[i], ek = ekey[i];
-    uint32_t s = (uint32_t)k, e = (uint32_t)ek;
-    uint32_t sg = (uint32_t)(k >> 32);
+    const uint64_t k = key[i];
+    const uint32_t s = (uint32_t)k, sg = (uint32_t)(k >> 32);
     starts[i] = s;
-    ends_s[i] = e;
     seg[i] = sg;
     segflag[i] = (i == 0 || (uint32_t)(key[i - 1] >> 32) != sg) ? 1u : 0u;
     ps_in[i] = s;
+}
+__global__ void k_unpack_ends(uint32_t n, const uint64_t* __restrict__ ekey, uint32_t* __restrict__ ends_s,
+                              uint64_t* __restrict__ pe_in) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    if (i == n) {
+        pe_in[n] = 0;
+        return;
+    }
+    const uint32_t e = (uint32_t)ekey[i];
+    ends_s[i] = e;
     pe_in[i] = e;
 }
 
@@ -1454,8 +1464,9 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
 
     if (ev) RGL_CUDA(cudaEventRecord(c->ev[0], st));
     // Two streams: `st` carries the chain from the sorted starts to the sweeps, `sd` the chains that
-    // only the rank sweep needs (the end-key sort, the prefix sums of starts and ends, the rank
-    // tables), so that the small kernels of both overlap; `sd` is joined back before the sweeps.
+    // only the rank sweep needs (the end-key sort and unpack, the prefix sums of starts and ends,
+    // the rank tables), so that the small kernels of both overlap; `sd` is joined back before the
+    // sweeps.
     cudaStream_t sd = c->side;
     uint32_t launches = 0;
     k_expand_keys<<<grid_for(n, 256), 256, 0, st>>>(n, in.iv, in.blk_off, in.blk_shard, in.blk_row,
@@ -1480,18 +1491,19 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                                  c->val_a.as<uint32_t>(), c->val_b.as<uint32_t>(), (int)n, 0,
                                                  32 + segbits, st));
     }
-    RGL_TRY(stream_after(st, sd, c->ev_join));
-    k_unpack<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->key_b.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
-                                                   c->starts.as<uint32_t>(), c->ends.as<uint32_t>(),
-                                                   c->seg.as<uint32_t>(), c->segflag.as<uint32_t>(),
-                                                   c->ps_in.as<uint64_t>(), c->pe_in.as<uint64_t>());
-    launches++;
+    // the side stream goes on with the ends (their prefix sums), the main one with the starts
+    k_unpack_ends<<<grid_for(n + 1, 256), 256, 0, sd>>>(n, c->ekey_b.as<uint64_t>(), c->ends.as<uint32_t>(),
+                                                        c->pe_in.as<uint64_t>());
+    tb = c->cub_tmp2.cap;
+    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp2.p, tb, c->pe_in.as<uint64_t>(), c->pe.as<uint64_t>(),
+                                           (int)n + 1, sd));
+    k_unpack_starts<<<grid_for(n + 1, 256), 256, 0, st>>>(n, c->key_b.as<uint64_t>(), c->starts.as<uint32_t>(),
+                                                          c->seg.as<uint32_t>(), c->segflag.as<uint32_t>(),
+                                                          c->ps_in.as<uint64_t>());
+    launches += 2;
     RGL_TRY(stream_after(sd, st, c->ev_fork));
     tb = c->cub_tmp2.cap;
     RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp2.p, tb, c->ps_in.as<uint64_t>(), c->ps.as<uint64_t>(),
-                                           (int)n + 1, sd));
-    tb = c->cub_tmp2.cap;
-    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp2.p, tb, c->pe_in.as<uint64_t>(), c->pe.as<uint64_t>(),
                                            (int)n + 1, sd));
     tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceScan::InclusiveSum(c->cub_tmp.p, tb, c->segflag.as<uint32_t>(), c->segnum.as<uint32_t>(),
