@@ -1695,6 +1695,20 @@ int resolve_blocks(rgl_context* c, const rgl_query_batch* b, std::vector<uint32_
     return RGL_OK;
 }
 
+// Copies the blocks' host intervals into the context's interval buffer at offsets off, one copy per
+// run of blocks that lie back to back in host memory (a file read into one buffer).
+int copy_blocks(rgl_context* c, const std::vector<const rgl_query_shard*>& blocks, const std::vector<uint64_t>& off,
+                cudaStream_t st) {
+    for (size_t i = 0; i < blocks.size();) {
+        size_t j = i + 1;
+        while (j < blocks.size() && blocks[j]->intervals == blocks[j - 1]->intervals + blocks[j - 1]->count) j++;
+        RGL_CUDA(cudaMemcpyAsync(c->iv.as<rgl_interval>() + off[i], blocks[i]->intervals,
+                                 (off[j] - off[i]) * sizeof(rgl_interval), cudaMemcpyHostToDevice, st));
+        i = j;
+    }
+    return RGL_OK;
+}
+
 // ---- batched form ------------------------------------------------------------------------------
 // A batch is cut into sub-batches of at most `sub` intervals (cutting blocks where needed: counts and
 // base pairs are sums over pairs, so a row split across sub-batches adds up to the same cells).
@@ -2053,9 +2067,7 @@ int rgl_query_counts(rgl_context* c, const rgl_query_batch* b, const rgl_query_o
     const uint64_t cells = (uint64_t)rows * c->idx->num_sources;
     RGL_TRY(ensure_workspace(c, n, rows, (uint32_t)blocks.size()));
     cudaStream_t st = c->stream;
-    for (size_t i = 0; i < blocks.size(); i++)
-        RGL_CUDA(cudaMemcpyAsync(c->iv.as<rgl_interval>() + off[i], blocks[i]->intervals,
-                                 blocks[i]->count * sizeof(rgl_interval), cudaMemcpyHostToDevice, st));
+    RGL_TRY(copy_blocks(c, blocks, off, st));
     if (!blocks.empty()) {
         RGL_CUDA(cudaMemcpyAsync(c->blk_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st));
         RGL_CUDA(cudaMemcpyAsync(c->blk_shard.p, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st));
@@ -2374,9 +2386,7 @@ int rgl_query_pairs(rgl_context* c, const rgl_query_batch* b, uint64_t capacity,
     off[blocks.size()] = n;
     RGL_TRY(ensure_workspace(c, n, 0, (uint32_t)blocks.size()));
     cudaStream_t st = c->stream;
-    for (size_t i = 0; i < blocks.size(); i++)
-        RGL_CUDA(cudaMemcpyAsync(c->iv.as<rgl_interval>() + off[i], blocks[i]->intervals,
-                                 blocks[i]->count * sizeof(rgl_interval), cudaMemcpyHostToDevice, st));
+    RGL_TRY(copy_blocks(c, blocks, off, st));
     if (!blocks.empty()) {
         RGL_CUDA(cudaMemcpyAsync(c->blk_off.p, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st));
         RGL_CUDA(cudaMemcpyAsync(c->blk_shard.p, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice, st));

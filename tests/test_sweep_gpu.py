@@ -200,3 +200,28 @@ def test_block_local_sort_equals_radix_sort():
             assert (c == oc).all() and (bp == obp).all(), (n0, n1, presorted)
     ctx.close()
     idx.close()
+
+
+def test_blocks_adjacent_in_host_memory():
+    """Chromosome blocks that are consecutive slices of one host buffer travel in one copy; the
+    result equals that of separately allocated blocks (and the oracle's)."""
+    rng = np.random.default_rng(12)
+    D, nsh = 17, 4
+    blocks = [(sh, helpers.random_db(rng, 8000, 2_000_000, D)) for sh in range(nsh)]
+    layers = rg.bucket_layers(blocks)
+    parts = [helpers.queries_touching(rng, b, 900, 2) for _, b in blocks]
+    buf = np.concatenate(parts)
+    views, at = {}, 0
+    for sh, p in enumerate(parts):
+        views[f"s{sh}"] = buf[at:at + len(p)]  # views into one buffer, back to back
+        at += len(p)
+    oc, _, obp, _ = O.query_database(layers, {sh: p.copy() for sh, p in enumerate(parts)}, 2, D, threads=4)
+    idx = rg.Index.from_layers(layers, D, [f"s{i}" for i in range(nsh)])
+    ctx = rg.Context(idx)
+    a = ctx.query_counts(views, 2)
+    b = ctx.query_counts({f"s{sh}": p.copy() for sh, p in enumerate(parts)}, 2)
+    rev = ctx.query_counts({k: views[k] for k in reversed(list(views))}, 2)  # adjacent, but in reverse order
+    for c, bp, _ in (a, b, rev):
+        assert (c == oc).all() and (bp == obp).all()
+    ctx.close()
+    idx.close()
