@@ -79,6 +79,15 @@ struct MaxOp {
 
 enum : uint32_t { ERR_BAD_INTERVAL = 1u, ERR_BAD_ROW = 2u };
 
+// Programmatic dependent launch.  The short kernels of the pipeline's chains have a PDL variant
+// (template flag PDL) that starts with pdl_wait(): it returns once the grid launched before it on
+// the stream has completed and its memory is visible, so nothing is read or written before it.
+// pdl_release() lets the next grid of the stream be scheduled before this one finishes; that grid
+// still waits in pdl_wait() for this one to complete.  Large runs launch the variants without
+// either instruction.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_release() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
 // ---- small device helpers ----------------------------------------------------------------------
 __device__ __forceinline__ uint32_t lb_u32(const uint32_t* __restrict__ a, uint32_t lo, uint32_t hi, uint32_t x) {
     // first index in [lo, hi) with a[i] >= x
@@ -311,8 +320,13 @@ __global__ void k_tab_zero(uint32_t n, const uint32_t* __restrict__ segnum, cons
     }
 }
 
+template <bool PDL>
 __global__ void k_tab_place(uint32_t n, const uint32_t* __restrict__ segnum, SegTab* __restrict__ tabs,
                             const uint32_t* __restrict__ tab_off, uint32_t* __restrict__ xs, uint32_t* __restrict__ xe) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t sgi = blockIdx.x * blockDim.x + threadIdx.x;
     if (sgi >= segnum[n - 1]) return;
     const uint32_t off = tab_off[sgi];
@@ -324,9 +338,14 @@ __global__ void k_tab_place(uint32_t n, const uint32_t* __restrict__ segnum, Seg
     }
 }
 
+template <bool PDL>
 __global__ void k_tab_count(uint32_t n, const uint32_t* __restrict__ segnum, const SegTab* __restrict__ tabs,
                             const uint32_t* __restrict__ starts, const uint32_t* __restrict__ ends_s,
                             uint32_t* __restrict__ xs, uint32_t* __restrict__ xe) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     const SegTab t = tabs[segnum[j] - 1];
@@ -353,8 +372,13 @@ __device__ __forceinline__ void add_u64(unsigned long long* c, unsigned long lon
 
 // Interleaves the two scanned count arrays into (#starts, #ends) pairs: entry k of the tables is
 // entry k + 1 of the exclusive scans (the inclusive sums through k).
+template <bool PDL>
 __global__ void k_tab_interleave(const uint32_t* __restrict__ count, const uint32_t* __restrict__ xs_scan,
                                  const uint32_t* __restrict__ xe_scan, uint2* __restrict__ tab2) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t total = *count;
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < total; k += (uint64_t)gridDim.x * blockDim.x)
         tab2[k] = make_uint2(xs_scan[k + 1], xe_scan[k + 1]);
@@ -396,10 +420,14 @@ __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_
 // no empty blocks.
 constexpr int kScanThreads = 256, kScanItems = 8, kScanTile = kScanThreads * kScanItems;
 
-template <typename Tin, typename Tout>
+template <typename Tin, typename Tout, bool PDL>
 __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const Tin* __restrict__ in,
                                                               const uint32_t* __restrict__ n_ptr,
                                                               Tout* __restrict__ tile_sums) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t n = *n_ptr;
     using BR = cub::BlockReduce<Tout, kScanThreads>;
     __shared__ typename BR::TempStorage tmp;
@@ -417,9 +445,13 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const Tin* __restr
     }
 }
 
-template <typename Tout>
+template <typename Tout, bool PDL>
 __global__ void __launch_bounds__(1024) k_scan_tops(Tout* __restrict__ tile_sums, const uint32_t* __restrict__ n_ptr,
                                                     Tout* __restrict__ out) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t n = *n_ptr;
     const uint32_t nt = (uint32_t)((n + kScanTile - 1) / kScanTile);
     using BS = cub::BlockScan<Tout, 1024>;
@@ -436,10 +468,14 @@ __global__ void __launch_bounds__(1024) k_scan_tops(Tout* __restrict__ tile_sums
     if (threadIdx.x == 0) out[n] = run;
 }
 
-template <typename Tin, typename Tout>
+template <typename Tin, typename Tout, bool PDL>
 __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const Tin* __restrict__ in, Tout* __restrict__ out,
                                                              const uint32_t* __restrict__ n_ptr,
                                                              const Tout* __restrict__ tile_off) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t n = *n_ptr;
     using BL = cub::BlockLoad<Tout, kScanThreads, kScanItems, cub::BLOCK_LOAD_WARP_TRANSPOSE>;
     using BSt = cub::BlockStore<Tout, kScanThreads, kScanItems, cub::BLOCK_STORE_WARP_TRANSPOSE>;
@@ -476,8 +512,13 @@ __global__ void k_live(uint64_t tot, const uint32_t* __restrict__ lo, const uint
     if (t <= tot) flag[t] = (t < tot && hi[t] > lo[t]) ? 1u : 0u;
 }
 
+template <bool PDL>
 __global__ void k_compact(uint64_t tot, const uint32_t* __restrict__ lpos, uint32_t* __restrict__ tl,
                           uint32_t* __restrict__ L_out) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (t < tot && lpos[t + 1] != lpos[t]) tl[lpos[t]] = (uint32_t)t;
     if (t == tot) *L_out = lpos[tot];
@@ -486,10 +527,15 @@ __global__ void k_compact(uint64_t tot, const uint32_t* __restrict__ lpos, uint3
 // Range starts among the live runs: the first live run of a (K, segment) row, or one whose lo is
 // past the running maximum of hi (maxhi over the row, which empty runs never raise past a later
 // lo); cl = the run's candidate count.
+template <bool PDL>
 __global__ void k_crange_flags(const uint32_t* __restrict__ Lp, uint32_t n, const uint32_t* __restrict__ tl,
                                const uint32_t* __restrict__ segnum, const uint32_t* __restrict__ lo,
                                const uint32_t* __restrict__ hi, const uint32_t* __restrict__ maxhi,
                                uint32_t* __restrict__ cflag, uint64_t* __restrict__ ccl) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t L = *Lp;
     for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < L; c += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t t = tl[c];
@@ -503,12 +549,17 @@ __global__ void k_crange_flags(const uint32_t* __restrict__ Lp, uint32_t n, cons
     }
 }
 
+template <bool PDL>
 __global__ void k_crange_emit(const uint32_t* __restrict__ Lp, uint32_t n, uint32_t nslots, uint32_t rows,
                               const uint32_t* __restrict__ tl, const uint32_t* __restrict__ seg,
                               const uint32_t* __restrict__ segnum, const int32_t* __restrict__ slot,
                               const uint32_t* __restrict__ lo, const uint32_t* __restrict__ maxhi,
                               const uint32_t* __restrict__ cflag, const uint32_t* __restrict__ cridx,
                               RangeDesc* __restrict__ ranges) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t L = *Lp;
     for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < L; c += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t t = tl[c], K = t / n, i = t % n;
@@ -535,11 +586,16 @@ __global__ void k_crange_emit(const uint32_t* __restrict__ Lp, uint32_t n, uint3
 // trivial per-pair work; where candidate windows overlap heavily (broad layers) the rank sweep reads
 // each union element once.  rlen = union length of rank ranges (the rank work space); the union of
 // every range is summed into *union_total (the swept count of the metric).
+template <bool PDL>
 __global__ void __launch_bounds__(256) k_crange_method(const uint32_t* __restrict__ Lp, const uint32_t* __restrict__ cridx,
                                 const RangeDesc* __restrict__ ranges, const uint64_t* __restrict__ cpc,
                                 uint32_t pair_ratio, uint8_t* __restrict__ method, uint64_t* __restrict__ rlen,
                                 uint32_t* __restrict__ seg_need, uint32_t* __restrict__ R_out,
                                 unsigned long long* __restrict__ union_total) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t R = cridx[*Lp];
     const uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (g == 0) *R_out = R;
@@ -562,6 +618,7 @@ __global__ void __launch_bounds__(256) k_crange_method(const uint32_t* __restric
 }
 
 // Pair work space: each live run of a pair range contributes its candidates.
+template <bool PDL>
 __global__ void k_cpair_len(const uint32_t* __restrict__ Lp, uint32_t n, uint32_t nslots, uint32_t rows,
                             const uint32_t* __restrict__ tl, const uint32_t* __restrict__ seg,
                             const int32_t* __restrict__ slot, const LayerDev* __restrict__ layers,
@@ -570,6 +627,10 @@ __global__ void k_cpair_len(const uint32_t* __restrict__ Lp, uint32_t n, uint32_
                             const uint8_t* __restrict__ method, const uint32_t* __restrict__ starts,
                             const uint32_t* __restrict__ qend, uint64_t* __restrict__ plen,
                             PairSeg* __restrict__ psegs) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t L = *Lp;
     for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < L; c += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t t = tl[c], K = t / n, i = t % n;
@@ -674,10 +735,15 @@ __device__ __forceinline__ uint32_t range_advance(const uint64_t* __restrict__ r
 // found by binary search over the range offsets.  One launch serves the rank ranges (rpos, *Rp
 // ranges) and the pair runs (ppos, *Lp runs), grid-stride over the items of both, and records the
 // two position totals in the counter block (64-bit words 5 and 6).
+template <bool PDL>
 __global__ void k_item_ranges(uint32_t* __restrict__ small, const uint32_t* __restrict__ Rp,
                               const uint64_t* __restrict__ rpos, const uint32_t* __restrict__ Lp,
                               const uint64_t* __restrict__ ppos, uint32_t chunk, uint64_t item_cap,
                               uint32_t* __restrict__ item_r0, uint32_t* __restrict__ item_t0) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
     const uint32_t R = *Rp, L = *Lp;
     const uint64_t rtot = rpos[R], ptot = ppos[L];
     const uint64_t g0 = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
@@ -1179,6 +1245,9 @@ namespace {
 // Work items whose first range is precomputed; items beyond it search the range list themselves.
 constexpr uint64_t kItemCap = 1ull << 22;
 
+// Runs up to this many query intervals chain their kernels with programmatic dependent launch.
+constexpr uint64_t kPdlMaxIntervals = 1ull << 21;
+
 // Query intervals per pipeline run: the rank tables (up to 10 entries per interval) use 31-bit offsets.
 constexpr uint64_t kMaxRunIntervals = 200000000ull;
 
@@ -1359,13 +1428,38 @@ int finish(rgl_context* c, const Launch& L, rgl_query_stats* stats) {
 }
 
 // Exclusive scan of in[0, *n_ptr) into out (with out[n] = total), n <= cap; returns the launches.
+// Launches a kernel of a chain; with `pdl` (its PDL variant, which begins with pdl_wait()) it may be
+// scheduled while the previous grid of the stream is finishing.  Used for small runs, where the launch latency between the short
+// kernels of a chain is a visible share of the run; in large runs the early-scheduled blocks of
+// the next grid only take SM slots from the current one.
+template <typename... K, typename... A>
+cudaError_t launch_pdl(bool pdl, void (*kernel)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
+                       A&&... args) {
+    if (!pdl) {
+        kernel<<<grid, block, smem, st>>>(std::forward<A>(args)...);  // errors surface at the next check
+        return cudaSuccess;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+}
+
 // `sums` holds cap / kScanTile + 1 tile sums (one buffer per stream that scans concurrently).
 template <typename Tin, typename Tout>
-uint32_t scan_dev(Tout* sums, const Tin* in, Tout* out, const uint32_t* n_ptr, uint64_t cap, cudaStream_t st) {
+uint32_t scan_dev(Tout* sums, const Tin* in, Tout* out, const uint32_t* n_ptr, uint64_t cap, cudaStream_t st,
+                  bool pdl) {
     const unsigned grid = (unsigned)std::min<uint64_t>(cap / kScanTile + 1, 148ull * 8);
-    k_scan_reduce<Tin, Tout><<<grid, kScanThreads, 0, st>>>(in, n_ptr, sums);
-    k_scan_tops<Tout><<<1, 1024, 0, st>>>(sums, n_ptr, out);
-    k_scan_apply<Tin, Tout><<<grid, kScanThreads, 0, st>>>(in, out, n_ptr, sums);
+    (void)launch_pdl(pdl, pdl ? k_scan_reduce<Tin, Tout, true> : k_scan_reduce<Tin, Tout, false>, grid, kScanThreads, 0, st, in, n_ptr, sums);
+    (void)launch_pdl(pdl, pdl ? k_scan_tops<Tout, true> : k_scan_tops<Tout, false>, 1, 1024, 0, st, sums, n_ptr, out);
+    (void)launch_pdl(pdl, pdl ? k_scan_apply<Tin, Tout, true> : k_scan_apply<Tin, Tout, false>, grid, kScanThreads, 0, st, in, out, n_ptr, sums);
     return 3;
 }
 
@@ -1440,6 +1534,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     Launch L = pick_launch(opts);
     const bool with_bp = d_bp != nullptr && !(opts && (opts->flags & RGL_QF_NO_OVERLAP));
     const bool ev = mode.events && stats;
+    const bool pdl = in.n <= kPdlMaxIntervals;
 
     uint32_t* d_small = c->small.as<uint32_t>();  // [0] error bits, [1] queue, [2..] scratch
     if (mode.reset_err) RGL_CUDA(cudaMemsetAsync(d_small, 0, 64, st));
@@ -1538,21 +1633,21 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                            (int)(tot + 1), st));
     uint32_t* Lp = d_small + 8;  // live runs L
     uint32_t* Rp = d_small + 9;  // ranges R
-    k_compact<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, c->lpos.as<uint32_t>(), c->tl.as<uint32_t>(), Lp);
+    (void)launch_pdl(pdl, pdl ? k_compact<true> : k_compact<false>, grid_for(tot + 1, 256), 256, 0, st, tot, c->lpos.as<uint32_t>(), c->tl.as<uint32_t>(), Lp);
     launches += 2;
     // ranges over the live runs, their candidate counts and methods
     const unsigned gc = (unsigned)std::min<uint64_t>(grid_for(tot, 256), (uint64_t)c->num_sms * 32);
-    k_crange_flags<<<gc, 256, 0, st>>>(Lp, n, c->tl.as<uint32_t>(), c->segnum.as<uint32_t>(), c->lo.as<uint32_t>(),
+    (void)launch_pdl(pdl, pdl ? k_crange_flags<true> : k_crange_flags<false>, gc, 256, 0, st, Lp, n, c->tl.as<uint32_t>(), c->segnum.as<uint32_t>(), c->lo.as<uint32_t>(),
                                        c->hi.as<uint32_t>(), c->maxhi.as<uint32_t>(), c->rflag.as<uint32_t>(),
                                        c->cl.as<uint64_t>());
     launches++;
-    launches += scan_dev(c->scan_sums.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(), Lp, tot, st);
-    launches += scan_dev(c->scan_sums.as<uint64_t>(), c->cl.as<uint64_t>(), c->pc.as<uint64_t>(), Lp, tot, st);
-    k_crange_emit<<<gc, 256, 0, st>>>(Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(),
+    launches += scan_dev(c->scan_sums.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(), Lp, tot, st, pdl);
+    launches += scan_dev(c->scan_sums.as<uint64_t>(), c->cl.as<uint64_t>(), c->pc.as<uint64_t>(), Lp, tot, st, pdl);
+    (void)launch_pdl(pdl, pdl ? k_crange_emit<true> : k_crange_emit<false>, gc, 256, 0, st, Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(),
                                       c->segnum.as<uint32_t>(), idx->d_slot, c->lo.as<uint32_t>(),
                                       c->maxhi.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
                                       c->ranges.as<RangeDesc>());
-    k_crange_method<<<gc, 256, 0, st>>>(Lp, c->ridx.as<uint32_t>(), c->ranges.as<RangeDesc>(), c->pc.as<uint64_t>(),
+    (void)launch_pdl(pdl, pdl ? k_crange_method<true> : k_crange_method<false>, gc, 256, 0, st, Lp, c->ridx.as<uint32_t>(), c->ranges.as<RangeDesc>(), c->pc.as<uint64_t>(),
                                         L.pair_ratio, c->method.as<uint8_t>(), c->rlen.as<uint64_t>(),
                                         c->seg_need.as<uint32_t>(), Rp,
                                         reinterpret_cast<unsigned long long*>(d_small + 4));
@@ -1570,29 +1665,29 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     k_tab_zero<<<(unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, sd>>>(
         n, c->segnum.as<uint32_t>(), c->tab_off.as<uint32_t>(), c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>(),
         tab_count);
-    k_tab_place<<<grid_for(n, 256), 256, 0, sd>>>(n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
+    (void)launch_pdl(pdl, pdl ? k_tab_place<true> : k_tab_place<false>, grid_for(n, 256), 256, 0, sd, n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
                                                   c->tab_off.as<uint32_t>(), c->tab_xs.as<uint32_t>(),
                                                   c->tab_xe.as<uint32_t>());
-    k_tab_count<<<grid_for(n, 256), 256, 0, sd>>>(n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
+    (void)launch_pdl(pdl, pdl ? k_tab_count<true> : k_tab_count<false>, grid_for(n, 256), 256, 0, sd, n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
                                                   c->starts.as<uint32_t>(), c->ends.as<uint32_t>(),
                                                   c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>());
     // inclusive scans written one entry ahead: exclusive scan into tab_* whose entry k + 1 is the
     // inclusive sum through k (the tables are read from tab_* + 1)
     uint32_t* sums2 = c->scan_sums2.as<uint32_t>();
-    launches += scan_dev(sums2, c->tab_xs.as<uint32_t>(), c->tab_s.as<uint32_t>(), tab_count, tab_cap, sd);
-    launches += scan_dev(sums2, c->tab_xe.as<uint32_t>(), c->tab_e.as<uint32_t>(), tab_count, tab_cap, sd);
-    k_tab_interleave<<<(unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, sd>>>(
+    launches += scan_dev(sums2, c->tab_xs.as<uint32_t>(), c->tab_s.as<uint32_t>(), tab_count, tab_cap, sd, pdl);
+    launches += scan_dev(sums2, c->tab_xe.as<uint32_t>(), c->tab_e.as<uint32_t>(), tab_count, tab_cap, sd, pdl);
+    (void)launch_pdl(pdl, pdl ? k_tab_interleave<true> : k_tab_interleave<false>, (unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, sd, 
         tab_count, c->tab_s.as<uint32_t>(), c->tab_e.as<uint32_t>(), c->tab2.as<uint2>());
     launches++;
     launches += 4;
     // main stream: the pair work space and the rank ranges' positions
-    k_cpair_len<<<gc, 256, 0, st>>>(Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), idx->d_slot,
+    (void)launch_pdl(pdl, pdl ? k_cpair_len<true> : k_cpair_len<false>, gc, 256, 0, st, Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), idx->d_slot,
                                     idx->d_layers, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(), c->rflag.as<uint32_t>(),
                                     c->ridx.as<uint32_t>(), c->method.as<uint8_t>(), c->starts.as<uint32_t>(),
                                     c->val_b.as<uint32_t>(), c->plen.as<uint64_t>(), c->psegs.as<PairSeg>());
     launches++;
-    launches += scan_dev(c->scan_sums.as<uint64_t>(), c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(), Rp, tot, st);
-    launches += scan_dev(c->scan_sums.as<uint64_t>(), c->plen.as<uint64_t>(), c->ppos.as<uint64_t>(), Lp, tot, st);
+    launches += scan_dev(c->scan_sums.as<uint64_t>(), c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(), Rp, tot, st, pdl);
+    launches += scan_dev(c->scan_sums.as<uint64_t>(), c->plen.as<uint64_t>(), c->ppos.as<uint64_t>(), Lp, tot, st, pdl);
     if (mode.no_sweep) {
         k_totals<<<1, 32, 0, st>>>(d_small, c->rpos.as<uint64_t>(), c->ppos.as<uint64_t>());
         launches++;
@@ -1603,7 +1698,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
         if (mode.reset_err) RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
         return RGL_OK;
     }
-    k_item_ranges<<<(unsigned)(c->num_sms * 8), 256, 0, st>>>(d_small, Rp, c->rpos.as<uint64_t>(), Lp,
+    (void)launch_pdl(pdl, pdl ? k_item_ranges<true> : k_item_ranges<false>, (unsigned)(c->num_sms * 8), 256, 0, st, d_small, Rp, c->rpos.as<uint64_t>(), Lp,
                                                                c->ppos.as<uint64_t>(), L.chunk, kItemCap,
                                                                c->item_r0.as<uint32_t>(), c->item_t0.as<uint32_t>());
     launches++;
