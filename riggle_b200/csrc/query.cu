@@ -275,10 +275,14 @@ __global__ void k_seg_begin(uint32_t n, const uint32_t* __restrict__ segflag, co
     if (i == n - 1) seg_begin[segnum[i]] = n;
 }
 
-// Bin width per segment: about four bins per query, at least 64 bp.  A segment with a rank-
-// difference range gets nbins + 1 table entries, any other segment a single entry (see k_tab_place).
+// Bin width per segment: about four bins per query, at least 64 bp, but no more than one bin per 8
+// DB intervals the segment's rank-difference ranges sweep (need[]): each swept interval reads the
+// table a few times, so a table much larger than its sweep costs more to build than its finer bins
+// save (large query files against a small database).  A coarser bin only lengthens the search
+// inside it.  A segment with a rank-difference range gets nbins + 1 table entries, any other
+// segment a single entry (see k_tab_place).
 __global__ void k_seg_tabsize(uint32_t n, const uint32_t* __restrict__ segnum, const uint32_t* __restrict__ seg_begin,
-                              const uint32_t* __restrict__ need, const uint32_t* __restrict__ ends_s,
+                              const unsigned long long* __restrict__ need, const uint32_t* __restrict__ ends_s,
                               SegTab* __restrict__ tabs, uint32_t* __restrict__ tab_len) {
     uint32_t sgi = blockIdx.x * blockDim.x + threadIdx.x;
     if (sgi > n) return;
@@ -294,7 +298,8 @@ __global__ void k_seg_tabsize(uint32_t n, const uint32_t* __restrict__ segnum, c
         return;
     }
     const uint64_t extent = (uint64_t)ends_s[end - 1] + 1;  // covers every start and end of the segment
-    const uint64_t want = extent / (4ull * (end - beg));
+    const uint64_t bins = max(1ull, min(4ull * (end - beg), need[sgi] / 8));
+    const uint64_t want = extent / bins;
     uint32_t shift = want > 1 ? 63u - __clzll(want) : 0u;
     if (shift < 6) shift = 6;
     if (shift > 31) shift = 31;
@@ -590,7 +595,7 @@ template <bool PDL>
 __global__ void __launch_bounds__(256) k_crange_method(const uint32_t* __restrict__ Lp, const uint32_t* __restrict__ cridx,
                                 const RangeDesc* __restrict__ ranges, const uint64_t* __restrict__ cpc,
                                 uint32_t pair_ratio, uint8_t* __restrict__ method, uint64_t* __restrict__ rlen,
-                                uint32_t* __restrict__ seg_need, uint32_t* __restrict__ R_out,
+                                unsigned long long* __restrict__ seg_need, uint32_t* __restrict__ R_out,
                                 unsigned long long* __restrict__ union_total) {
     if constexpr (PDL) {
         pdl_wait();
@@ -606,7 +611,7 @@ __global__ void __launch_bounds__(256) k_crange_method(const uint32_t* __restric
         const uint64_t cand = cpc[rd.c_last + 1] - cpc[rd.c_first];
         const uint8_t m = (cand <= (uint64_t)pair_ratio * len) ? M_PAIR : M_RANK;
         method[r] = m;
-        if (m == M_RANK && len) seg_need[rd.seg] = 1u;
+        if (m == M_RANK && len) atomicAdd(&seg_need[rd.seg], (unsigned long long)len);  // rank-swept positions
         rlen[r] = m == M_RANK ? len : 0;
         acc += len;
     }
@@ -1271,7 +1276,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     RGL_TRY(c->segflag.ensure(n * 4 + 4));
     RGL_TRY(c->segnum.ensure(n * 4 + 4));
     RGL_TRY(c->seg_begin.ensure(n * 4 + 4));
-    RGL_TRY(c->seg_need.ensure(n * 4 + 4));
+    RGL_TRY(c->seg_need.ensure(n * 8 + 8));
     RGL_TRY(c->ps_in.ensure(n * 8 + 16));
     RGL_TRY(c->pe_in.ensure(n * 8 + 16));
     RGL_TRY(c->ps.ensure(n * 8 + 16));
@@ -1606,7 +1611,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     k_seg_begin<<<grid_for(n, 256), 256, 0, st>>>(n, c->segflag.as<uint32_t>(), c->segnum.as<uint32_t>(),
                                                   c->seg_begin.as<uint32_t>());
     launches++;
-    RGL_CUDA(cudaMemsetAsync(c->seg_need.p, 0, (size_t)(n + 1) * 4, st));
+    RGL_CUDA(cudaMemsetAsync(c->seg_need.p, 0, (size_t)(n + 1) * 8, st));
     const uint64_t tot = (uint64_t)n * ns;
     if (tot + 1 >= (1ull << 31)) {
         RGL_TRY(stream_after(st, sd, c->ev_join));
@@ -1649,13 +1654,13 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                       c->ranges.as<RangeDesc>());
     (void)launch_pdl(pdl, pdl ? k_crange_method<true> : k_crange_method<false>, gc, 256, 0, st, Lp, c->ridx.as<uint32_t>(), c->ranges.as<RangeDesc>(), c->pc.as<uint64_t>(),
                                         L.pair_ratio, c->method.as<uint8_t>(), c->rlen.as<uint64_t>(),
-                                        c->seg_need.as<uint32_t>(), Rp,
+                                        c->seg_need.as<unsigned long long>(), Rp,
                                         reinterpret_cast<unsigned long long*>(d_small + 4));
     launches += 2;
     // side stream: rank tables of the query segments that have a rank-difference range
     RGL_TRY(stream_after(sd, st, c->ev_fork));
     k_seg_tabsize<<<grid_for(n + 1, 256), 256, 0, sd>>>(n, c->segnum.as<uint32_t>(), c->seg_begin.as<uint32_t>(),
-                                                        c->seg_need.as<uint32_t>(), c->ends.as<uint32_t>(),
+                                                        c->seg_need.as<unsigned long long>(), c->ends.as<uint32_t>(),
                                                         c->segtab.as<SegTab>(), c->tab_len.as<uint32_t>());
     tb = c->cub_tmp2.cap;
     RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp2.p, tb, c->tab_len.as<uint32_t>(), c->tab_off.as<uint32_t>(),
