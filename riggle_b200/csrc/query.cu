@@ -1433,15 +1433,15 @@ int finish(rgl_context* c, const Launch& L, rgl_query_stats* stats) {
 }
 
 // Exclusive scan of in[0, *n_ptr) into out (with out[n] = total), n <= cap; returns the launches.
-// Launches a kernel of a chain; with `pdl` (its PDL variant, which begins with pdl_wait()) it may be
-// scheduled while the previous grid of the stream is finishing.  Used for small runs, where the launch latency between the short
-// kernels of a chain is a visible share of the run; in large runs the early-scheduled blocks of
-// the next grid only take SM slots from the current one.
+// Launches a short kernel of a pipeline chain: with `pdl` its PDL variant (which begins with
+// pdl_wait()) with programmatic stream serialization, so that it may be scheduled while the previous
+// grid of the stream is finishing; else its plain variant.  PDL is used for small runs, where the
+// launch latency between the short kernels of a chain is a visible share of the run.
 template <typename... K, typename... A>
-cudaError_t launch_pdl(bool pdl, void (*kernel)(K...), dim3 grid, dim3 block, size_t smem, cudaStream_t st,
-                       A&&... args) {
+cudaError_t launch_chain(bool pdl, void (*with_pdl)(K...), void (*plain)(K...), dim3 grid, dim3 block, size_t smem,
+                         cudaStream_t st, A&&... args) {
     if (!pdl) {
-        kernel<<<grid, block, smem, st>>>(std::forward<A>(args)...);  // errors surface at the next check
+        plain<<<grid, block, smem, st>>>(std::forward<A>(args)...);  // errors surface at the next check
         return cudaSuccess;
     }
     cudaLaunchConfig_t cfg = {};
@@ -1454,7 +1454,7 @@ cudaError_t launch_pdl(bool pdl, void (*kernel)(K...), dim3 grid, dim3 block, si
     attr[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kernel, std::forward<A>(args)...);
+    return cudaLaunchKernelEx(&cfg, with_pdl, std::forward<A>(args)...);
 }
 
 // `sums` holds cap / kScanTile + 1 tile sums (one buffer per stream that scans concurrently).
@@ -1462,9 +1462,11 @@ template <typename Tin, typename Tout>
 uint32_t scan_dev(Tout* sums, const Tin* in, Tout* out, const uint32_t* n_ptr, uint64_t cap, cudaStream_t st,
                   bool pdl) {
     const unsigned grid = (unsigned)std::min<uint64_t>(cap / kScanTile + 1, 148ull * 8);
-    (void)launch_pdl(pdl, pdl ? k_scan_reduce<Tin, Tout, true> : k_scan_reduce<Tin, Tout, false>, grid, kScanThreads, 0, st, in, n_ptr, sums);
-    (void)launch_pdl(pdl, pdl ? k_scan_tops<Tout, true> : k_scan_tops<Tout, false>, 1, 1024, 0, st, sums, n_ptr, out);
-    (void)launch_pdl(pdl, pdl ? k_scan_apply<Tin, Tout, true> : k_scan_apply<Tin, Tout, false>, grid, kScanThreads, 0, st, in, out, n_ptr, sums);
+    (void)launch_chain(pdl, k_scan_reduce<Tin, Tout, true>, k_scan_reduce<Tin, Tout, false>, grid, kScanThreads, 0,
+                     st, in, n_ptr, sums);
+    (void)launch_chain(pdl, k_scan_tops<Tout, true>, k_scan_tops<Tout, false>, 1, 1024, 0, st, sums, n_ptr, out);
+    (void)launch_chain(pdl, k_scan_apply<Tin, Tout, true>, k_scan_apply<Tin, Tout, false>, grid, kScanThreads, 0, st,
+                     in, out, n_ptr, sums);
     return 3;
 }
 
@@ -1638,24 +1640,25 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                            (int)(tot + 1), st));
     uint32_t* Lp = d_small + 8;  // live runs L
     uint32_t* Rp = d_small + 9;  // ranges R
-    (void)launch_pdl(pdl, pdl ? k_compact<true> : k_compact<false>, grid_for(tot + 1, 256), 256, 0, st, tot, c->lpos.as<uint32_t>(), c->tl.as<uint32_t>(), Lp);
+    (void)launch_chain(pdl, k_compact<true>, k_compact<false>, grid_for(tot + 1, 256), 256, 0, st, tot,
+                     c->lpos.as<uint32_t>(), c->tl.as<uint32_t>(), Lp);
     launches += 2;
     // ranges over the live runs, their candidate counts and methods
     const unsigned gc = (unsigned)std::min<uint64_t>(grid_for(tot, 256), (uint64_t)c->num_sms * 32);
-    (void)launch_pdl(pdl, pdl ? k_crange_flags<true> : k_crange_flags<false>, gc, 256, 0, st, Lp, n, c->tl.as<uint32_t>(), c->segnum.as<uint32_t>(), c->lo.as<uint32_t>(),
-                                       c->hi.as<uint32_t>(), c->maxhi.as<uint32_t>(), c->rflag.as<uint32_t>(),
-                                       c->cl.as<uint64_t>());
+    (void)launch_chain(pdl, k_crange_flags<true>, k_crange_flags<false>, gc, 256, 0, st, Lp, n, c->tl.as<uint32_t>(),
+                     c->segnum.as<uint32_t>(), c->lo.as<uint32_t>(), c->hi.as<uint32_t>(), c->maxhi.as<uint32_t>(),
+                     c->rflag.as<uint32_t>(), c->cl.as<uint64_t>());
     launches++;
     launches += scan_dev(c->scan_sums.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(), Lp, tot, st, pdl);
     launches += scan_dev(c->scan_sums.as<uint64_t>(), c->cl.as<uint64_t>(), c->pc.as<uint64_t>(), Lp, tot, st, pdl);
-    (void)launch_pdl(pdl, pdl ? k_crange_emit<true> : k_crange_emit<false>, gc, 256, 0, st, Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(),
-                                      c->segnum.as<uint32_t>(), idx->d_slot, c->lo.as<uint32_t>(),
-                                      c->maxhi.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
-                                      c->ranges.as<RangeDesc>());
-    (void)launch_pdl(pdl, pdl ? k_crange_method<true> : k_crange_method<false>, gc, 256, 0, st, Lp, c->ridx.as<uint32_t>(), c->ranges.as<RangeDesc>(), c->pc.as<uint64_t>(),
-                                        L.pair_ratio, c->method.as<uint8_t>(), c->rlen.as<uint64_t>(),
-                                        c->seg_need.as<unsigned long long>(), Rp,
-                                        reinterpret_cast<unsigned long long*>(d_small + 4));
+    (void)launch_chain(pdl, k_crange_emit<true>, k_crange_emit<false>, gc, 256, 0, st, Lp, n, ns, rows,
+                     c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), c->segnum.as<uint32_t>(), idx->d_slot,
+                     c->lo.as<uint32_t>(), c->maxhi.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
+                     c->ranges.as<RangeDesc>());
+    (void)launch_chain(pdl, k_crange_method<true>, k_crange_method<false>, gc, 256, 0, st, Lp, c->ridx.as<uint32_t>(),
+                     c->ranges.as<RangeDesc>(), c->pc.as<uint64_t>(), L.pair_ratio, c->method.as<uint8_t>(),
+                     c->rlen.as<uint64_t>(), c->seg_need.as<unsigned long long>(), Rp,
+                     reinterpret_cast<unsigned long long*>(d_small + 4));
     launches += 2;
     // side stream: rank tables of the query segments that have a rank-difference range
     RGL_TRY(stream_after(sd, st, c->ev_fork));
@@ -1670,26 +1673,28 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     k_tab_zero<<<(unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, sd>>>(
         n, c->segnum.as<uint32_t>(), c->tab_off.as<uint32_t>(), c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>(),
         tab_count);
-    (void)launch_pdl(pdl, pdl ? k_tab_place<true> : k_tab_place<false>, grid_for(n, 256), 256, 0, sd, n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
-                                                  c->tab_off.as<uint32_t>(), c->tab_xs.as<uint32_t>(),
-                                                  c->tab_xe.as<uint32_t>());
-    (void)launch_pdl(pdl, pdl ? k_tab_count<true> : k_tab_count<false>, grid_for(n, 256), 256, 0, sd, n, c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(),
-                                                  c->starts.as<uint32_t>(), c->ends.as<uint32_t>(),
-                                                  c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>());
+    (void)launch_chain(pdl, k_tab_place<true>, k_tab_place<false>, grid_for(n, 256), 256, 0, sd, n,
+                     c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(), c->tab_off.as<uint32_t>(),
+                     c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>());
+    (void)launch_chain(pdl, k_tab_count<true>, k_tab_count<false>, grid_for(n, 256), 256, 0, sd, n,
+                     c->segnum.as<uint32_t>(), c->segtab.as<SegTab>(), c->starts.as<uint32_t>(),
+                     c->ends.as<uint32_t>(), c->tab_xs.as<uint32_t>(), c->tab_xe.as<uint32_t>());
     // inclusive scans written one entry ahead: exclusive scan into tab_* whose entry k + 1 is the
     // inclusive sum through k (the tables are read from tab_* + 1)
     uint32_t* sums2 = c->scan_sums2.as<uint32_t>();
     launches += scan_dev(sums2, c->tab_xs.as<uint32_t>(), c->tab_s.as<uint32_t>(), tab_count, tab_cap, sd, pdl);
     launches += scan_dev(sums2, c->tab_xe.as<uint32_t>(), c->tab_e.as<uint32_t>(), tab_count, tab_cap, sd, pdl);
-    (void)launch_pdl(pdl, pdl ? k_tab_interleave<true> : k_tab_interleave<false>, (unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, sd, 
-        tab_count, c->tab_s.as<uint32_t>(), c->tab_e.as<uint32_t>(), c->tab2.as<uint2>());
+    (void)launch_chain(pdl, k_tab_interleave<true>, k_tab_interleave<false>,
+                     (unsigned)std::min<uint64_t>(grid_for(tab_cap, 256), (uint64_t)c->num_sms * 32), 256, 0, sd,
+                     tab_count, c->tab_s.as<uint32_t>(), c->tab_e.as<uint32_t>(), c->tab2.as<uint2>());
     launches++;
     launches += 4;
     // main stream: the pair work space and the rank ranges' positions
-    (void)launch_pdl(pdl, pdl ? k_cpair_len<true> : k_cpair_len<false>, gc, 256, 0, st, Lp, n, ns, rows, c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), idx->d_slot,
-                                    idx->d_layers, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(), c->rflag.as<uint32_t>(),
-                                    c->ridx.as<uint32_t>(), c->method.as<uint8_t>(), c->starts.as<uint32_t>(),
-                                    c->val_b.as<uint32_t>(), c->plen.as<uint64_t>(), c->psegs.as<PairSeg>());
+    (void)launch_chain(pdl, k_cpair_len<true>, k_cpair_len<false>, gc, 256, 0, st, Lp, n, ns, rows,
+                     c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, c->lo.as<uint32_t>(),
+                     c->hi.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(), c->method.as<uint8_t>(),
+                     c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(), c->plen.as<uint64_t>(),
+                     c->psegs.as<PairSeg>());
     launches++;
     launches += scan_dev(c->scan_sums.as<uint64_t>(), c->rlen.as<uint64_t>(), c->rpos.as<uint64_t>(), Rp, tot, st, pdl);
     launches += scan_dev(c->scan_sums.as<uint64_t>(), c->plen.as<uint64_t>(), c->ppos.as<uint64_t>(), Lp, tot, st, pdl);
@@ -1703,9 +1708,9 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
         if (mode.reset_err) RGL_CUDA(cudaMemcpyAsync(c->h_small, d_small, 4, cudaMemcpyDeviceToHost, st));
         return RGL_OK;
     }
-    (void)launch_pdl(pdl, pdl ? k_item_ranges<true> : k_item_ranges<false>, (unsigned)(c->num_sms * 8), 256, 0, st, d_small, Rp, c->rpos.as<uint64_t>(), Lp,
-                                                               c->ppos.as<uint64_t>(), L.chunk, kItemCap,
-                                                               c->item_r0.as<uint32_t>(), c->item_t0.as<uint32_t>());
+    (void)launch_chain(pdl, k_item_ranges<true>, k_item_ranges<false>, (unsigned)(c->num_sms * 8), 256, 0, st,
+                     d_small, Rp, c->rpos.as<uint64_t>(), Lp, c->ppos.as<uint64_t>(), L.chunk, kItemCap,
+                     c->item_r0.as<uint32_t>(), c->item_t0.as<uint32_t>());
     launches++;
     SweepParams P;
     P.item_r0 = c->item_r0.as<uint32_t>();
