@@ -261,6 +261,30 @@ def test_config1_database_batch_equals_one_file_per_call():
     db.close()
 
 
+def test_large_and_small_runs_agree():
+    """Runs above 2^21 query intervals launch the pipeline's short kernels without programmatic
+    dependent launch, smaller runs with it; one batch of ~6M intervals as one run and as runs of
+    2^20 must agree on every cell (and the large run must take the block-local sort for no block:
+    these files have blocks above 16,384 intervals)."""
+    cl = rg.synth_chrom_lengths(1, 24)
+    db = rg.Index.synth(rg.SynthSpec(2, cl, np.full(64, 50_000, np.uint64)))
+    sizes = rg.synth_loguniform_sizes(17, 12, 100_000, 1_000_000)
+    spec = rg.SynthSpec(3000, cl, sizes, hotspot_fraction=0.1, num_hotspots=8)
+    off, sh, rw = rg.synth_batch_layout(spec)
+    assert int(off[-1]) > (1 << 21) and int(np.diff(off).max()) > 16384
+    t = torch.empty((int(off[-1]), 3), dtype=torch.int32, device="cuda:0")
+    rg.synth_batch_device(spec, off, t.data_ptr())
+    ctx = rg.Context(db)
+    b = rg.DeviceBatch(spec.num_files, sh, off, t.data_ptr(), rw)
+    c1, bp1, st1 = _run(ctx, b, 64, sub_batch=int(off[-1]))
+    c2, bp2, st2 = _run(ctx, b, 64, sub_batch=1 << 20)
+    assert st1["sub_batches"] == 1 and st2["sub_batches"] > 1
+    assert (c1 == c2).all() and (bp1 == bp2).all()
+    assert c1.sum() > 0
+    ctx.close()
+    db.close()
+
+
 def test_host_batch_pipelined_copies_equal_device_batch():
     layers, files, D, nsh = _random_batch(13, nfiles=29)
     oc, obp = _oracle(layers, files, D, nsh)
