@@ -15,6 +15,7 @@
 // 0..=max_start / tile_size, the partition point of start < t * tile_size — the table
 // build_jump_table (src/io/jump.rs:66-115) computes for a freshly written layer.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
 #include <cerrno>
@@ -280,7 +281,7 @@ int rgl_index_add_beds(const rgl_index* base, const char* input_path, uint32_t m
             k_new_starts<<<grid(sc.new_n), 256>>>(sc.new_n, nidx, d_iv.as<rgl_interval>(), k1.as<uint32_t>());
             k_base_starts<<<grid(BL->n), 256>>>(BL->n, base->d_pos + BL->off, k2.as<uint32_t>());
             // new first on equal starts: the first input wins ties
-            cub::CountingInputIterator<uint32_t> v1(0), v2((uint32_t)sc.new_n);
+            thrust::counting_iterator<uint32_t> v1(0), v2((uint32_t)sc.new_n);
             size_t t3 = 0;
             cub::DeviceMerge::MergePairs(nullptr, t3, k1.as<uint32_t>(), v1, (int)sc.new_n, k2.as<uint32_t>(), v2,
                                          (int)BL->n, mk.as<uint32_t>(), mv.as<uint32_t>());

@@ -20,6 +20,7 @@
 //     signal, so the cancellation that the reference's d*-autocorrelation suffers (~1e10,
 //     docs/todo.md) does not arise; all prefix sums are double-double (compensated two-sum).
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include <algorithm>
 #include <cmath>
@@ -370,11 +371,11 @@ int depth_signal_dev(MomentWs& w, const rgl_interval* h_iv, uint64_t n, uint64_t
     RGL_CUDA(cudaMemsetAsync(w.cnt.p, 0, 16, st));
     if (full) {
         size_t tb = 0;
-        cub::DeviceSelect::Flagged(nullptr, tb, cub::CountingInputIterator<uint32_t>(0), w.nz.as<uint8_t>(),
+        cub::DeviceSelect::Flagged(nullptr, tb, thrust::counting_iterator<uint32_t>(0), w.nz.as<uint8_t>(),
                                    w.idx.as<uint32_t>(), w.cnt.as<int>(), (int)full, st);
         RGL_TRY(w.tmp.ensure(tb + 256));
         tb = w.tmp.cap;
-        RGL_CUDA(cub::DeviceSelect::Flagged(w.tmp.p, tb, cub::CountingInputIterator<uint32_t>(0), w.nz.as<uint8_t>(),
+        RGL_CUDA(cub::DeviceSelect::Flagged(w.tmp.p, tb, thrust::counting_iterator<uint32_t>(0), w.nz.as<uint8_t>(),
                                             w.idx.as<uint32_t>(), w.cnt.as<int>(), (int)full, st));
     }
     k_carry_chain<<<1, 1, 0, st>>>(w.cnt.as<int>(), w.idx.as<uint32_t>(), w.totals.as<float>(), w.cum.as<float>(),
@@ -603,7 +604,7 @@ int noalloc_setup(int device, unsigned char** out) {
         size_t sort_b = 0, sel_b = 0;
         cub::DeviceRadixSort::SortPairs(nullptr, sort_b, (uint64_t*)nullptr, (uint64_t*)nullptr, (float*)nullptr,
                                         (float*)nullptr, (int)(4 * kNaMaxIv), 0, 64);
-        cub::DeviceSelect::Flagged(nullptr, sel_b, cub::CountingInputIterator<uint32_t>(0), (uint8_t*)nullptr,
+        cub::DeviceSelect::Flagged(nullptr, sel_b, thrust::counting_iterator<uint32_t>(0), (uint8_t*)nullptr,
                                    (uint32_t*)nullptr, (int*)nullptr, (int)kNaChunks);
         if (std::max(sort_b, sel_b) > kNaTmpBytes)
             return fail(RGL_ERR_UNSUPPORTED, "CUB temporary storage exceeds the reserved scratch");
@@ -662,7 +663,7 @@ extern "C" int rgl_depth_signal_noalloc(int device, const rgl_interval* d_interv
         if (full) {
             k_chunk_local<<<blocks_for(full), 256, 0, st>>>(full, d_g, totals, nz);
             size_t tb = kNaTmpBytes;
-            RGL_CUDA(cub::DeviceSelect::Flagged(tmp, tb, cub::CountingInputIterator<uint32_t>(0), nz, idx, cnt,
+            RGL_CUDA(cub::DeviceSelect::Flagged(tmp, tb, thrust::counting_iterator<uint32_t>(0), nz, idx, cnt,
                                                 (int)full, st));
         }
         k_carry_chain<<<1, 1, 0, st>>>(cnt, idx, totals, cum, d_g, n_bins, full);

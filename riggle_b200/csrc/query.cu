@@ -27,6 +27,8 @@
 //      Counts and base pairs are tallied per (row, source) in shared memory when a chunk belongs to
 //      one row, else with global atomics.
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
 
 #include <algorithm>
 #include <cstring>
@@ -72,6 +74,9 @@ struct RowKey {
         return ((uint64_t)(t / n) << 32) | segnum[t % n];
     }
 };
+
+// (slot, segment) key of every (slot, query) entry, as an iterator over the entries.
+using RowKeyIter = thrust::transform_iterator<RowKey, thrust::counting_iterator<uint32_t>>;
 
 struct MaxOp {
     __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
@@ -1327,8 +1332,7 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nn + 1, c->stream);
     need = std::max(need, b);
     {
-        cub::CountingInputIterator<uint32_t> ti(0);
-        cub::TransformInputIterator<uint64_t, RowKey, cub::CountingInputIterator<uint32_t>> keys(ti, RowKey{nullptr, 1});
+        RowKeyIter keys(thrust::counting_iterator<uint32_t>(0), RowKey{nullptr, 1});
         cub::DeviceScan::InclusiveScanByKey(nullptr, b, keys, (uint32_t*)nullptr, (uint32_t*)nullptr, MaxOp(), nt,
                                             cub::Equality(), c->stream);
     }
@@ -1624,9 +1628,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                                 idx->d_btab, c->lo.as<uint32_t>(), c->hi.as<uint32_t>());
     launches++;
     {  // running max of hi along every (slot, segment) row: one scan keyed by (slot, segment)
-        cub::CountingInputIterator<uint32_t> ti(0);
-        cub::TransformInputIterator<uint64_t, RowKey, cub::CountingInputIterator<uint32_t>> keys(
-            ti, RowKey{c->segnum.as<uint32_t>(), n});
+        RowKeyIter keys(thrust::counting_iterator<uint32_t>(0), RowKey{c->segnum.as<uint32_t>(), n});
         tb = c->cub_tmp.cap;
         RGL_CUDA(cub::DeviceScan::InclusiveScanByKey(c->cub_tmp.p, tb, keys, c->hi.as<uint32_t>(),
                                                      c->maxhi.as<uint32_t>(), MaxOp(), (int)tot, cub::Equality(),

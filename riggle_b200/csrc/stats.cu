@@ -12,6 +12,7 @@
 // 0 dispatches NB / Poisson, evaluates the LLR and the A&S 7.1.26 tail exactly as the reference
 // writes it (src/fourier/stats.rs:65-126).
 #include <cub/cub.cuh>
+#include <thrust/iterator/transform_iterator.h>
 
 #include <algorithm>
 #include <cmath>
@@ -178,7 +179,7 @@ struct LenAggOp {
     }
 };
 struct LenToAgg {
-    __device__ __forceinline__ LenAgg operator()(uint32_t len) const {
+    __host__ __device__ __forceinline__ LenAgg operator()(uint32_t len) const {
         const unsigned long long l = len;
         return LenAgg{1ull, l, l * l, 0ull};  // len < 2^32: len^2 fits 64 bits
     }
@@ -561,7 +562,7 @@ int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* m, const rgl_batch* 
     cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint64_t*)nullptr, (uint64_t*)nullptr, (uint32_t*)nullptr,
                                     (uint32_t*)nullptr, (int)nn, 0, 64, st);
     need = std::max(need, tb);
-    cub::TransformInputIterator<LenAgg, LenToAgg, const uint32_t*> vin(m->len_b.as<uint32_t>(), LenToAgg());
+    thrust::transform_iterator<LenToAgg, const uint32_t*, LenAgg> vin(m->len_b.as<uint32_t>(), LenToAgg());
     cub::DeviceReduce::ReduceByKey(nullptr, tb, m->key_b.as<uint64_t>(), m->ukey.as<uint64_t>(), vin,
                                    m->agg.as<LenAgg>(), m->runs.as<uint32_t>(), LenAggOp(), (int)nn, st);
     need = std::max(need, tb);
