@@ -10,10 +10,10 @@
  * Semantics kept from the reference:
  *   - a query interval q and a database interval d overlap when
  *       q.start - layer_max_size(K) (saturating) <= d.start < q.end  and  d.end > q.start
- *     (src/sweep/query.rs:141-152, half-open intervals: touching ends do not overlap);
+ *     (src/sweep/query.rs:98-108, half-open intervals: touching ends do not overlap);
  *   - counts are u32 per (query row, database source) and wrap modulo 2^32 as the reference's
  *     release build does (src/matrix/dense.rs:42-45);
- *   - the reference's f32 "overlap bins" (src/sweep/query.rs:154-156) are returned as exact u64
+ *   - the reference's f32 "overlap bins" (src/sweep/query.rs:111-113) are returned as exact u64
  *     base pairs; bins = bp / bin_size.
  */
 #ifndef RIGGLE_B200_H
@@ -60,6 +60,15 @@ const char* rgl_status_str(int status);
 const char* rgl_last_error(void);
 /* ABI version: major*10000 + minor*100 + patch. */
 int rgl_version(void);
+
+/* Layout of the public structs below as compiled into this library (no counterpart in the
+ * reference; it lets a binding in another language check its declarations against the ABI).
+ * rgl_abi_struct_name(i) names struct i (NULL past the last).  rgl_abi_layout fills sizeof,
+ * alignof and the field count of the named struct, and for the first `capacity` fields in
+ * declaration order their names, offsets and sizes (any output may be NULL). */
+const char* rgl_abi_struct_name(uint32_t i);
+int rgl_abi_layout(const char* name, uint64_t* size, uint64_t* align, uint32_t* num_fields,
+                   const char** field_names, uint64_t* offsets, uint64_t* sizes, uint32_t capacity);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Layer configuration — LayerConfig (src/io/meta.rs:23-90).  Pure host functions.             */
@@ -116,7 +125,7 @@ typedef struct rgl_index_info {
 
 /* Opens `db_dir` written by the reference's `add` (src/tasks/build.rs:86-128): meta.json
  * (src/io/meta.rs:124-127) and shards/<shard>/layer_K.{pos,sid,idx} (src/io/layer.rs:51-78,
- * src/io/jump.rs:225-237), with the reference's size checks, and uploads the layers to HBM.
+ * src/io/jump.rs:27-44), with the reference's size checks, and uploads the layers to HBM.
  * Replaces Meta::load + MappedLayer::open + MappedJumpTable::open in query_database
  * (src/tasks/query/mod.rs:124-129, 205-233). */
 int rgl_index_open(const char* db_dir, int device, rgl_index** out);
@@ -208,7 +217,7 @@ typedef struct rgl_query_stats {
 } rgl_query_stats;
 
 /* Replaces the counting path of query_database (src/tasks/query/mod.rs:182-307): the per-shard,
- * per-64-row-window, per-layer calls to query_sweep_windowed (src/sweep/query.rs:127-160) and the
+ * per-64-row-window, per-layer calls to query_sweep_windowed (src/sweep/query.rs:84-117) and the
  * window merge (add_submatrix_rows, src/matrix/dense.rs:75-86).  Host buffers: the batch is copied
  * to HBM, `counts` (num_rows x num_sources u32, row-major) and `overlap_bp` (same shape, u64; may
  * be NULL) are written on return.  Query intervals need start < end (the parser guarantees it,
@@ -354,8 +363,11 @@ int rgl_depth_signal(int device, const rgl_interval* intervals, uint64_t n, uint
  * `stream` (a cudaStream_t, NULL = legacy default stream) without synchronising.  Its scratch is a
  * static device array of RGL_NOALLOC_SCRATCH_BYTES (17 MiB) that every GPU loading the library
  * holds until exit; inputs above RGL_NOALLOC_MAX_INTERVALS intervals or RGL_NOALLOC_MAX_BINS bins
- * are rejected with RGL_ERR_INVALID_ARGUMENT.  The first call on a device looks up the array's
- * device address (make it before any stream capture).  All calls share the array: calls that may
+ * are rejected with RGL_ERR_INVALID_ARGUMENT, and so are a d_g that is not 16-byte aligned (it is
+ * read and written as float4) and d_intervals that are not 4-byte aligned.  The first call on a
+ * device looks up the array's device address (make it before any stream capture); the address is
+ * looked up again when the device's context has been replaced since (cudaDeviceReset), so make the
+ * first call after such a reset before any capture too.  All calls share the array: calls that may
  * overlap on the GPU (different streams, or threads) race and must be serialised by the caller. */
 #define RGL_NOALLOC_MAX_INTERVALS 65536u
 #define RGL_NOALLOC_MAX_BINS 4194304u

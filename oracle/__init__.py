@@ -116,7 +116,7 @@ def extend_layer(old_pos, old_sid, new_ivs):
 
 
 def query_sweep(db, layer_max, queries, nrows, ncols, bin_size=100):
-    """Reference unit-test helper `sweep` (src/sweep/query.rs:187-200): db/queries are (start,end,sid)."""
+    """Reference unit-test helper `sweep` (src/sweep/query.rs:144-157): db/queries are (start,end,sid)."""
     db = np.asarray(db, np.uint32).reshape(-1, 3)
     q = np.ascontiguousarray(np.asarray(queries, np.uint32).reshape(-1, 3))
     tile = max(layer_max // 2, 1)

@@ -76,7 +76,7 @@ uint32_t tile_size(uint32_t min_size, uint32_t gf, uint32_t layer) {
 // --------------------------------------------------------------------------------------------
 std::vector<uint64_t> build_jump_table(const uint32_t* starts, uint64_t n, uint32_t tile) {
     // jump.rs:66-113.  table[t] = number of intervals with start < t*tile; the reference's
-    // sparse-checkpoint/densify construction yields exactly this (its own test at jump.rs:238-252
+    // sparse-checkpoint/densify construction yields exactly this (its own test at src/io/jump.rs:220-237
     // checks it against partition_point); it is restated here as one sequential pass.
     if (n == 0) return {0};
     uint64_t max_tile = starts[n - 1] / tile;
@@ -98,7 +98,7 @@ uint64_t jump_lookup(const uint64_t* table, uint64_t num_tiles, uint32_t tile, u
 }
 
 // --------------------------------------------------------------------------------------------
-// src/sweep/query.rs:127-160 — query_sweep_windowed (identical scan to query_sweep :87-120)
+// src/sweep/query.rs:84-117 — query_sweep_windowed (identical scan to query_sweep :44-77)
 // --------------------------------------------------------------------------------------------
 struct Pos {
     uint32_t start, end;
@@ -114,7 +114,7 @@ void query_sweep_windowed(const Pos* pos, const uint32_t* sids, uint64_t n, uint
                           const uint32_t* q /*start,end,sid triples*/, uint64_t nq, uint32_t q_sid_base,
                           uint32_t cols, uint32_t bin_size, uint32_t* counts, float* overlap,
                           uint64_t* overlap_bp, SweepStats* st) {
-    if (nq == 0 || n == 0) return;  // query.rs:137-139
+    if (nq == 0 || n == 0) return;  // src/sweep/query.rs:94-96
     for (uint64_t k = 0; k < nq; k++) {
         uint32_t qs = q[3 * k], qe = q[3 * k + 1], qsid = q[3 * k + 2];
         uint32_t lo = qs >= layer_max ? qs - layer_max : 0;  // saturating_sub  :141
@@ -470,7 +470,7 @@ void orc_extend_layer(const uint32_t* old_pos, const uint32_t* old_sid, uint64_t
     std::memcpy(out_sid, s.data(), 4 * total);
 }
 
-// query.rs:127-160 on one layer.  counts/overlap are rows x cols row-major, row = qsid - base.
+// src/sweep/query.rs:84-117 on one layer.  counts/overlap are rows x cols row-major, row = qsid - base.
 void orc_query_sweep_windowed(const uint32_t* pos, const uint32_t* sids, uint64_t n, uint32_t layer_max,
                               const uint64_t* jt, uint64_t jt_len, uint32_t tile, const uint32_t* q, uint64_t nq,
                               uint32_t q_sid_base, uint32_t cols, uint32_t bin_size, uint32_t* counts,
@@ -682,7 +682,7 @@ int orc_query_database(uint32_t min_size, uint32_t gf, uint32_t num_sources, uin
     return 0;
 }
 
-// Brute-force O(Nq * Nd) pair oracle of the same predicate (query.rs:141-152 with the layer
+// Brute-force O(Nq * Nd) pair oracle of the same predicate (src/sweep/query.rs:98-108 with the layer
 // look-back bound) — independent of jump tables and scans; small cases only.
 void orc_bruteforce_counts(uint32_t min_size, uint32_t gf, uint32_t num_sources, uint32_t n_layers,
                            const orc_layer* layers, uint32_t n_qshards, const orc_qshard* qshards, uint32_t rows,

@@ -78,6 +78,12 @@ class QueryStats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class Pair(C.Structure):
+    _fields_ = [("query_start", C.c_uint32), ("query_end", C.c_uint32), ("db_start", C.c_uint32),
+                ("db_end", C.c_uint32), ("row", C.c_uint32), ("sid", C.c_uint32), ("shard", C.c_uint32),
+                ("intersection_bp", C.c_uint32)]
+
+
 class BatchDesc(C.Structure):
     _fields_ = [("num_rows", C.c_uint32), ("num_blocks", C.c_uint32), ("block_shards", C.c_void_p),
                 ("block_rows", C.c_void_p), ("block_offsets", C.c_void_p), ("d_intervals", C.c_void_p)]
@@ -235,6 +241,19 @@ _SIGS = {
     "rgl_index_select_columns": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
     "rgl_synth_batch_layout": (C.c_int, [C.POINTER(SynthSpec), _P, _P, _P]),
     "rgl_synth_batch_device": (C.c_int, [C.POINTER(SynthSpec), C.c_int, _P, _P, _P]),
+    "rgl_abi_struct_name": (C.c_char_p, [C.c_uint32]),
+    "rgl_abi_layout": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
+                                 C.POINTER(C.c_char_p), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_uint32]),
+}
+
+# The ctypes mirror of every public struct of include/riggle.h, by its C name.
+MIRRORS = {
+    "rgl_interval": Interval, "rgl_layer_desc": LayerDesc, "rgl_index_desc": IndexDesc,
+    "rgl_index_info": IndexInfo, "rgl_query_shard": QueryShard, "rgl_query_batch": QueryBatch,
+    "rgl_query_opts": QueryOpts, "rgl_query_stats": QueryStats, "rgl_pair": Pair, "rgl_batch": BatchDesc,
+    "rgl_batch_opts": BatchOpts, "rgl_batch_stats": BatchStats, "rgl_tune_trial": TuneTrial,
+    "rgl_pvalue_batch": PValueBatch, "rgl_synth_spec": SynthSpec, "rgl_server_opts": ServerOpts,
+    "rgl_request": Request, "rgl_request_info": RequestInfo, "rgl_server_stats": ServerStats,
 }
 
 EXPORTED = tuple(_SIGS)

@@ -11,7 +11,7 @@
 //
 // write: meta.json (serde field names of Meta, src/io/meta.rs:99-110), and per layer
 // shards/<shard>/layer_K.{pos,sid,idx}: raw little-endian (start, end) u32 pairs, u32 sids, and the
-// jump table as a flat u64 array (write_jump_table, src/io/jump.rs:225-237) holding, for tile t in
+// jump table as a flat u64 array (write_jump_table, src/io/jump.rs:116-133) holding, for tile t in
 // 0..=max_start / tile_size, the partition point of start < t * tile_size — the table
 // build_jump_table (src/io/jump.rs:66-115) computes for a freshly written layer.
 #include <cub/cub.cuh>

@@ -6,7 +6,7 @@
 // (16-byte aligned sid blocks, 32-byte aligned pos blocks).  The reference's `.idx` jump table
 // (src/io/jump.rs) is size-checked at open for error parity but not uploaded: the device computes
 // exact partition points by binary search, which is what the reference's conservative lookup plus
-// partition_point yields (src/sweep/query.rs:141-143).
+// partition_point yields (src/sweep/query.rs:98-100).
 #include <cub/cub.cuh>
 
 #include <algorithm>
@@ -318,7 +318,7 @@ int rgl_index_open(const char* db_dir, int device, rgl_index** out) {
     std::vector<Pending> files;
     int s = RGL_OK;
     // Same file checks and order as query_database's layer loading (src/tasks/query/mod.rs:205-233)
-    // and MappedLayer::open / MappedJumpTable::open (src/io/layer.rs:51-78, src/io/jump.rs:225-237).
+    // and MappedLayer::open / MappedJumpTable::open (src/io/layer.rs:51-78, src/io/jump.rs:27-44).
     for (uint32_t sh = 0; sh < idx->num_shards && s == RGL_OK; sh++) {
         for (uint64_t k = 0; k < meta.num_layers && s == RGL_OK; k++) {
             std::string base = dir + "/shards/" + meta.shards[sh] + "/layer_" + std::to_string(k);

@@ -33,6 +33,20 @@ void clear_error();
         if (s_ != RGL_OK) return s_;      \
     } while (0)
 
+// Makes `device` current for the scope and gives the calling thread its previous device back on
+// exit, so an entry point leaves the caller's device selection as it found it.
+struct DeviceScope {
+    int prev = -1;
+    int enter(int device) {
+        RGL_CUDA(cudaGetDevice(&prev));
+        RGL_CUDA(cudaSetDevice(device));
+        return RGL_OK;
+    }
+    ~DeviceScope() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 // ---- layer configuration (src/io/meta.rs:33-81) ---------------------------------------------
 uint32_t layer_for_size(uint32_t min_size, uint32_t gf, uint32_t size);
 uint32_t layer_max_size(uint32_t min_size, uint32_t gf, uint32_t layer);

@@ -441,8 +441,9 @@ int rgl_depth_signal(int device, const rgl_interval* intervals, uint64_t n, uint
     if (n_bins * (uint64_t)bin_size > 0xFFFFFFFFull) return fail(RGL_ERR_INVALID_ARGUMENT, "n_bins * bin_size overflows u32");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(RGL_ERR_NO_DEVICE, "no CUDA device");
-    RGL_CUDA(cudaSetDevice(device));
-    if (device < 0 || device >= 16) return fail(RGL_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    if (device < 0 || device >= 16 || device >= ndev) return fail(RGL_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    DeviceScope scope;
+    RGL_TRY(scope.enter(device));
     std::lock_guard<std::mutex> lk(g_ws_mu);
     RGL_TRY(depth_signal_dev(g_ws[device], intervals, n, n_bins, bin_size, 0));
     RGL_CUDA(cudaMemcpy(g_out, g_ws[device].g.p, n_bins * 4, cudaMemcpyDeviceToHost));
@@ -458,9 +459,10 @@ int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_in
     int device = 0;
     RGL_TRY(moments_table_ptr(m, sid, chrom, &table, &slots, &N, &device));
     if (N * (uint64_t)bin_size > 0xFFFFFFFFull) return fail(RGL_ERR_INVALID_ARGUMENT, "n_bins * bin_size overflows u32");
-    RGL_CUDA(cudaSetDevice(device));
-    if (N <= 1) return moments_mark(m, sid, chrom, 0);  // moments_from_signal returns no entries
     if (device < 0 || device >= 16) return fail(RGL_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    if (N <= 1) return moments_mark(m, sid, chrom, 0);  // moments_from_signal returns no entries
+    DeviceScope scope;
+    RGL_TRY(scope.enter(device));
     std::lock_guard<std::mutex> lk(g_ws_mu);
     MomentWs& w = g_ws[device];
     cudaStream_t st = 0;
@@ -590,13 +592,46 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[RGL_NOALLOC_SCR
 
 namespace {
 std::mutex g_na_mu;
-unsigned char* g_na_ptr[64] = {nullptr};  // device address of g_noalloc_scratch, per device
+struct NoallocSlot {
+    unsigned long long ctx_id = 0;  // the context the address belongs to (0: not looked up yet)
+    unsigned char* ptr = nullptr;   // device address of g_noalloc_scratch in that context
+};
+NoallocSlot g_na[64];
 
-// Once per device, with that device current: the array's device address (the symbol itself is only
-// a host-side stand-in), and a check that CUB's temporary storage for the largest inputs fits.
+// The unique id of the calling thread's current context (cuCtxGetId, unique for the life of the
+// process, so a context destroyed by cudaDeviceReset and made again gets a new one), through the
+// runtime's driver entry points so that the library needs no link against libcuda.
+typedef int (*CtxGetCurrentFn)(void**);
+typedef int (*CtxGetIdFn)(void*, unsigned long long*);
+int current_context_id(unsigned long long* id) {
+    static CtxGetCurrentFn get_current = nullptr;
+    static CtxGetIdFn get_id = nullptr;
+    if (!get_current || !get_id) {
+        void* f1 = nullptr;
+        void* f2 = nullptr;
+        cudaDriverEntryPointQueryResult q1{}, q2{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f1, cudaEnableDefault, &q1) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &f2, cudaEnableDefault, &q2) != cudaSuccess || !f1 || !f2)
+            return fail(RGL_ERR_DEVICE, "driver entry points cuCtxGetCurrent / cuCtxGetId are unavailable");
+        get_current = reinterpret_cast<CtxGetCurrentFn>(f1);
+        get_id = reinterpret_cast<CtxGetIdFn>(f2);
+    }
+    void* ctx = nullptr;
+    if (get_current(&ctx) != 0 || !ctx) return fail(RGL_ERR_DEVICE, "no current CUDA context");
+    if (get_id(ctx, id) != 0) return fail(RGL_ERR_DEVICE, "cuCtxGetId failed");
+    return RGL_OK;
+}
+
+// With `device` current: the array's device address in the current context (the symbol itself is
+// only a host-side stand-in), looked up on the first call and again whenever the device's context
+// has changed since (after cudaDeviceReset the module is loaded anew, possibly elsewhere), and a
+// check that CUB's temporary storage for the largest inputs fits.
 int noalloc_setup(int device, unsigned char** out) {
     std::lock_guard<std::mutex> lk(g_na_mu);
-    if (!g_na_ptr[device]) {
+    unsigned long long id = 0;
+    RGL_TRY(current_context_id(&id));
+    NoallocSlot& slot = g_na[device];
+    if (slot.ctx_id != id || !slot.ptr) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess)
@@ -608,9 +643,10 @@ int noalloc_setup(int device, unsigned char** out) {
                                    (uint32_t*)nullptr, (int*)nullptr, (int)kNaChunks);
         if (std::max(sort_b, sel_b) > kNaTmpBytes)
             return fail(RGL_ERR_UNSUPPORTED, "CUB temporary storage exceeds the reserved scratch");
-        g_na_ptr[device] = static_cast<unsigned char*>(p);
+        slot.ptr = static_cast<unsigned char*>(p);
+        slot.ctx_id = id;
     }
-    *out = g_na_ptr[device];
+    *out = slot.ptr;
     return RGL_OK;
 }
 }  // namespace
@@ -626,14 +662,14 @@ extern "C" int rgl_depth_signal_noalloc(int device, const rgl_interval* d_interv
         return fail(RGL_ERR_INVALID_ARGUMENT, "rgl_depth_signal_noalloc takes at most " +
                                                   std::to_string(kNaMaxBins) + " bins (got " + std::to_string(n_bins) + ")");
     if (n_bins * (uint64_t)bin_size > 0xFFFFFFFFull) return fail(RGL_ERR_INVALID_ARGUMENT, "n_bins * bin_size overflows u32");
+    // the chunk pass reads and writes d_g as float4, the spike pass reads the intervals as u32 words
+    if (reinterpret_cast<uintptr_t>(d_g) % 16 != 0)
+        return fail(RGL_ERR_INVALID_ARGUMENT, "d_g must be 16-byte aligned");
+    if (reinterpret_cast<uintptr_t>(d_intervals) % 4 != 0)
+        return fail(RGL_ERR_INVALID_ARGUMENT, "d_intervals must be 4-byte aligned");
     if (device < 0 || device >= 64) return fail(RGL_ERR_INVALID_ARGUMENT, "device ordinal out of range");
-    int prev = 0;
-    RGL_CUDA(cudaGetDevice(&prev));
-    RGL_CUDA(cudaSetDevice(device));
-    struct Restore {
-        int d;
-        ~Restore() { cudaSetDevice(d); }
-    } restore{prev};
+    DeviceScope scope;
+    RGL_TRY(scope.enter(device));
     unsigned char* base = nullptr;
     RGL_TRY(noalloc_setup(device, &base));
     cudaStream_t st = reinterpret_cast<cudaStream_t>(stream);

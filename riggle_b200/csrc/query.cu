@@ -1,5 +1,5 @@
 // The sweep: query_database's counting path (src/tasks/query/mod.rs:182-307) and
-// query_sweep_windowed (src/sweep/query.rs:127-160) as one device pipeline.
+// query_sweep_windowed (src/sweep/query.rs:84-117) as one device pipeline.
 //
 // Per batch (all on the context stream, no host synchronisation, graph-capturable once the
 // workspace is reserved):
@@ -11,7 +11,7 @@
 //   3. exclusive u64 prefix sums of the sorted starts and sorted ends (PS, PE).
 //   4. K1 partition: for every (layer slot K, query i) the candidate range of the reference's scan,
 //      [pp(start - max_K), pp(end)) with pp = partition point of the layer's starts
-//      (src/sweep/query.rs:141-148); a segmented max-scan merges them into disjoint ranges per
+//      (src/sweep/query.rs:98-105); a segmented max-scan merges them into disjoint ranges per
 //      (K, segment); an exclusive scan of the range lengths lays all ranges end to end.
 //   5. K2 sweep (k_sweep): a persistent kernel pulls fixed-size chunks of that concatenated range
 //      space from a device counter.  Each thread takes one DB interval d and computes, against the
@@ -411,7 +411,7 @@ __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_
         LayerDev L = layers[li];
         const uint2* p = pos + L.off;
         uint32_t s = starts[i];
-        uint32_t back = s >= L.max_size ? s - L.max_size : 0u;  // saturating_sub, query.rs:141
+        uint32_t back = s >= L.max_size ? s - L.max_size : 0u;  // saturating_sub, src/sweep/query.rs:98
         const uint32_t* bt = btab + L.boff;
         pp_layer2(p, bt, L, back, qend[i], lo, hi);
         if (hi < lo) hi = lo;
@@ -995,7 +995,7 @@ __device__ __noinline__ void pairs_step_slow(const uint64_t* __restrict__ ppos, 
     }
 }
 
-// The pair sweep: the reference's scan (src/sweep/query.rs:147-158) over the candidate runs of the
+// The pair sweep: the reference's scan (src/sweep/query.rs:104-115) over the candidate runs of the
 // queries of pair ranges, every candidate read once by one lane (consecutive positions of a run are
 // consecutive DB elements, so the loads coalesce).  A candidate d of query q overlaps when
 // d.end > q.start (d.start < q.end and the look-back bound hold by construction of the run); it

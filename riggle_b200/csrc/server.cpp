@@ -32,6 +32,8 @@ struct Req {
     double t_submit = 0, t_start = 0, t_done = 0;
     int status = RGL_OK;
     bool done = false;
+    bool released = false;  // taken out of the ticket table by a completed wait
+    uint32_t waiters = 0;   // threads inside rgl_server_wait on this request
     uint32_t batch_requests = 0;
     uint64_t batch_intervals = 0;
 };
@@ -293,8 +295,12 @@ int rgl_server_wait(rgl_server* S, uint64_t ticket, uint32_t timeout_ms, rgl_req
     auto it = S->reqs.find(ticket);
     if (it == S->reqs.end()) return fail(RGL_ERR_INVALID_ARGUMENT, "unknown ticket");
     Req* q = it->second;
-    if (!S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return q->done; }))
-        return fail(RGL_ERR_TIMEOUT, "request not done yet");
+    // Several threads may wait on one ticket: the request is freed only by the last of them to
+    // leave, so no waiter reads it after the delete.
+    q->waiters++;
+    const bool done = S->cv_done.wait_for(lk, std::chrono::milliseconds(timeout_ms), [&] { return q->done; });
+    q->waiters--;
+    if (!done) return fail(RGL_ERR_TIMEOUT, "request not done yet");
     if (info) {
         info->status = q->status;
         info->batch_requests = q->batch_requests;
@@ -304,8 +310,11 @@ int rgl_server_wait(rgl_server* S, uint64_t ticket, uint32_t timeout_ms, rgl_req
         info->start_s = q->t_start;
         info->done_s = q->t_done;
     }
-    S->reqs.erase(it);
-    delete q;
+    if (!q->released) {
+        S->reqs.erase(q->ticket);
+        q->released = true;
+    }
+    if (q->waiters == 0) delete q;
     return RGL_OK;
 }
 

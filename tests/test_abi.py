@@ -1,5 +1,6 @@
 """C-ABI checks that need no GPU: the library loads, exports every entry point include/riggle.h
 declares, and its host-side arithmetic matches the oracle."""
+import ctypes as C
 import os
 import re
 
@@ -81,3 +82,139 @@ def test_bad_meta_json_is_meta_error(tmp_path):
     with pytest.raises(rg.RiggleError) as e:
         rg.Index.open(tmp_path)
     assert e.value.status == _lib.RGL_ERR_META_JSON
+
+
+def compiled_layout(name):
+    lib = rg.load()
+    size, align, nf = C.c_uint64(), C.c_uint64(), C.c_uint32()
+    cap = 64
+    names = (C.c_char_p * cap)()
+    offs = (C.c_uint64 * cap)()
+    sizes = (C.c_uint64 * cap)()
+    _lib.check(lib.rgl_abi_layout(name.encode(), C.byref(size), C.byref(align), C.byref(nf), names, offs, sizes,
+                                  cap))
+    fields = [(names[k].decode(), offs[k], sizes[k]) for k in range(nf.value)]
+    return size.value, align.value, fields
+
+
+def public_structs():
+    lib = rg.load()
+    out, i = [], 0
+    while True:
+        n = lib.rgl_abi_struct_name(i)
+        if n is None:
+            return out
+        out.append(n.decode())
+        i += 1
+
+
+def header_structs():
+    src = open(os.path.join(ROOT, "include", "riggle.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(re.findall(r"typedef struct (\w+) \{", src))
+
+
+def test_every_header_struct_has_a_compiled_layout():
+    assert sorted(public_structs()) == header_structs()
+
+
+def test_ctypes_mirrors_match_the_compiled_layout():
+    """Every ctypes mirror in riggle_b200/_lib.py has the compiled struct's size, field names and
+    offsets (a field added to riggle.h and not to the mirror fails here)."""
+    for name in public_structs():
+        mirror = _lib.MIRRORS[name]
+        size, _, fields = compiled_layout(name)
+        assert C.sizeof(mirror) == size, name
+        got = [(f, getattr(mirror, f).offset, getattr(mirror, f).size) for f, _ in mirror._fields_]
+        assert got == fields, name
+
+
+_RUST_SCALARS = {"u8": 1, "u16": 2, "u32": 4, "u64": 8, "i32": 4, "i64": 8, "f32": 4, "f64": 8, "c_int": 4,
+                 "usize": 8}
+
+
+def _rust_block():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    m = re.search(r"```rust\n(.*?)```", text, flags=re.S)
+    assert m, "INTEGRATION.md has no rust block"
+    return re.sub(r"//[^\n]*", "", m.group(1))
+
+
+def _rust_structs(block):
+    out = {}
+    for m in re.finditer(r"#\[repr\(C\)\](?:\s*#\[derive\([^)]*\)\])?\s*pub struct (\w+)\s*\{(.*?)\}", block,
+                         flags=re.S):
+        fields = []
+        for decl in m.group(2).split(","):
+            decl = decl.strip()
+            if not decl:
+                continue
+            fm = re.match(r"pub (\w+):\s*(.+)$", decl, flags=re.S)
+            assert fm, decl
+            fields.append((fm.group(1), " ".join(fm.group(2).split())))
+        out[m.group(1)] = fields
+    return out
+
+
+def _c_name(rust_name):
+    return "rgl_" + re.sub(r"(?<!^)([A-Z])", r"_\1", rust_name[3:]).lower()
+
+
+def _rust_layout(structs, name, memo):
+    """sizeof / alignof / field offsets of a #[repr(C)] Rust struct, by the C layout rules."""
+    if name in memo:
+        return memo[name]
+    off, align, fields = 0, 1, []
+    for f, t in structs[name]:
+        if t.startswith("*"):
+            fs = fa = 8
+        elif t in _RUST_SCALARS:
+            fs = fa = _RUST_SCALARS[t]
+        else:
+            fs, fa, _ = _rust_layout(structs, t, memo)
+        off = (off + fa - 1) // fa * fa
+        fields.append((f, off, fs))
+        off += fs
+        align = max(align, fa)
+    size = (off + align - 1) // align * align
+    memo[name] = (size, align, fields)
+    return memo[name]
+
+
+def test_integration_rust_binding_matches_the_compiled_layout():
+    """The #[repr(C)] structs of INTEGRATION.md's Rust binding lay out like the compiled structs, and
+    its extern block declares only exported functions, with the header's parameter counts."""
+    block = _rust_block()
+    structs = _rust_structs(block)
+    assert {"RglQueryOpts", "RglBatchOpts", "RglServerOpts", "RglRequest", "RglPvalueBatch"} <= set(structs)
+    memo = {}
+    for rname in structs:
+        cname = _c_name(rname)
+        size, align, fields = compiled_layout(cname)
+        rsize, ralign, rfields = _rust_layout(structs, rname, memo)
+        assert (rsize, ralign) == (size, align), rname
+        assert rfields == fields, rname
+    # every struct named in a function signature is declared in the block (or opaque)
+    opaque = set(re.findall(r"pub enum (\w+) \{\}", block))
+    for t in set(re.findall(r"\b(Rgl\w+)\b", block)):
+        assert t in structs or t in opaque, f"{t} is used but not declared"
+    src = open(os.path.join(ROOT, "include", "riggle.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    for m in re.finditer(r"pub fn (rgl_\w+)\((.*?)\)\s*->", block, flags=re.S):
+        fn, args = m.group(1), m.group(2).strip()
+        hm = re.search(r"\b" + fn + r"\s*\((.*?)\);", src, flags=re.S)
+        assert hm, f"{fn} is not declared in riggle.h"
+        nc = 0 if hm.group(1).strip() in ("", "void") else hm.group(1).count(",") + 1
+        nr = 0 if not args else args.rstrip(",").count(",") + 1
+        assert nr == nc, f"{fn}: {nr} parameters in the binding, {nc} in riggle.h"
+
+
+def test_noalloc_depth_signal_refuses_misaligned_buffers():
+    """rgl_depth_signal_noalloc reads and writes d_g as float4 and reads the intervals as u32 words:
+    a d_g off a 16-byte boundary or intervals off a 4-byte boundary are refused before anything is
+    enqueued (so this runs without a GPU; the pointers are never dereferenced)."""
+    lib = rg.load()
+    for iv, g in ((0x10000, 0x20004), (0x10000, 0x20008), (0x10002, 0x20000)):
+        st = lib.rgl_depth_signal_noalloc(0, C.c_void_p(iv), 10, 1000, 100, C.c_void_p(g), None)
+        assert st == _lib.RGL_ERR_INVALID_ARGUMENT
+        assert b"aligned" in lib.rgl_last_error()

@@ -54,3 +54,18 @@ def test_noalloc_rejects_sizes_beyond_its_scratch():
     with pytest.raises(rg.RiggleError) as e:
         _noalloc(iv[:10], 4_194_305)
     assert e.value.status == _lib.RGL_ERR_INVALID_ARGUMENT
+
+
+def test_noalloc_refuses_an_output_off_a_16_byte_boundary():
+    import torch
+
+    lib = rg.load()
+    iv = np.array([[100, 900, 0]], np.uint32)
+    d_iv = torch.from_numpy(iv.view(np.int32)).cuda()
+    d_g = torch.zeros(1001, dtype=torch.float32, device="cuda")
+    st = lib.rgl_depth_signal_noalloc(0, C.c_void_p(d_iv.data_ptr()), 1, 1000, 100, C.c_void_p(d_g.data_ptr() + 4),
+                                      None)
+    assert st == _lib.RGL_ERR_INVALID_ARGUMENT
+    # the aligned buffer still works after the refusal
+    got = _noalloc(iv, 1000)
+    assert np.array_equal(got, api.depth_signal(iv, 1000))
