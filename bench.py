@@ -78,16 +78,27 @@ def parse():
 # ---------------------------------------------------------------------------------------------
 # workload definitions
 # ---------------------------------------------------------------------------------------------
-def workload_spec(name, db_intervals=2_000_000_000, chroms=24):
+def generator(cpu=False):
+    """The seeded workload generator: the library's, or (cpu=True) the oracle's restatement of it,
+    which gives the same bits without loading the GPU library (the CPU reference arm)."""
+    if cpu:
+        import oracle as O
+
+        return O, O.SynthWorkload
     import riggle_b200 as rg
 
-    cl = rg.synth_chrom_lengths(1, 24)
+    return rg, rg.SynthSpec
+
+
+def workload_spec(name, db_intervals=2_000_000_000, chroms=24, cpu=False):
+    gen, Spec = generator(cpu)
+    cl = gen.synth_chrom_lengths(1, 24)
     share = float(cl[:chroms].sum()) / float(cl.sum())
     cl = cl[:chroms]
     if name == "plain":
-        sizes = rg.synth_zipf_sizes(1000, 1.1, max(1, int(1000 * share)), max(1, int(10_000_000 * share)),
-                                    int(db_intervals * share))
-        db = rg.SynthSpec(2, cl, sizes, broad_fraction=0.05)
+        sizes = gen.synth_zipf_sizes(1000, 1.1, max(1, int(1000 * share)), max(1, int(10_000_000 * share)),
+                                     int(db_intervals * share))
+        db = Spec(2, cl, sizes, broad_fraction=0.05)
         qsize = int(round(100_000 * share))
         desc = {"workload": f"plain GPU-scale sweep: 1,000-file Zipf(1.1) database, {db_intervals:.3g} intervals "
                             "(5% broad 10k-1M bp), one 1e5-interval query file per launch",
@@ -95,20 +106,21 @@ def workload_spec(name, db_intervals=2_000_000_000, chroms=24):
                 "chromosomes": len(cl), "bin_size": 100, "layer_config": "min_size 128, growth_factor 4"}
     else:
         sizes = np.full(64, int(round(50_000 * share)), np.uint64)
-        db = rg.SynthSpec(2, cl, sizes)
+        db = Spec(2, cl, sizes)
         qsize = int(round(10_000 * share))
         desc = {"workload": "plain CPU-runnable sweep: 64-file database x 50k intervals, one 1e4-interval "
                             "query file per launch",
                 "db_files": 64, "db_intervals": int(sizes.sum()), "query_intervals_per_step": qsize,
                 "chromosomes": len(cl), "bin_size": 100, "layer_config": "min_size 128, growth_factor 4"}
+    desc["reference_arm_sample"] = ("the shortest chromosome of each step's query file against all database files "
+                                    "(the CPU reference arm and cpu_baseline time this bounded sample)")
     return cl, db, qsize, desc
 
 
-def query_file(cl, seed, qsize):
+def query_file(cl, seed, qsize, cpu=False):
     """One seeded query file as AoS (start, end, row=0) grouped by chromosome + shard offsets."""
-    import riggle_b200 as rg
-
-    q = rg.SynthSpec(seed, cl, [qsize])
+    _, Spec = generator(cpu)
+    q = Spec(seed, cl, [qsize])
     blocks = [q.block(0, c) for c in range(len(cl))]
     offs = np.zeros(len(cl) + 1, np.uint64)
     for c, b in enumerate(blocks):
@@ -244,21 +256,22 @@ def run_reference(args, rank, world):
     this image) on the host cores, on a bounded sample of the same workload."""
     if rank != 0:
         return
-    import riggle_b200 as rg
+    import oracle as O
 
-    cl, db, qsize, desc = workload_spec(args.workload, args.db_intervals, args.chroms)
+    # inputs from the oracle's generator: this arm never loads the GPU library
+    cl, db, qsize, desc = workload_spec(args.workload, args.db_intervals, args.chroms, cpu=True)
     qsize = args.query_size or qsize
     cores = os.cpu_count() or 1
     chroms = pick_sample(cl, args.workload)
     sl = sample_layers(db, chroms)
     vals = []
     for step in range(args.warmup + args.steps):
-        _, _, blocks = query_file(cl, 1000 + step, qsize)
+        _, _, blocks = query_file(cl, 1000 + step, qsize, cpu=True)
         n, t = cpu_sample(db, sl, blocks, cores, 1)
         if step >= args.warmup:
             vals.append(n / t)
     v = float(np.mean(vals))
-    sample = (f"chromosome(s) {[rg.CHROM_NAMES_24[c] for c in chroms]} of each step's query file against all "
+    sample = (f"chromosome(s) {[O.CHROM_NAMES_24[c] for c in chroms]} of each step's query file against all "
               f"database files, query-block parallel restatement of src/sweep/query.rs on {cores} threads")
     out = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",

@@ -418,6 +418,19 @@ int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* moments, const rgl_b
                              const uint32_t* d_counts, const uint64_t* d_overlap_bp, double* d_p, double* d_llr,
                              double* d_log_p, uint8_t* d_flags, uint64_t* out_groups);
 
+/* The query length groups that rgl_batch_pvalues_device builds on the device from the batch's own
+ * intervals (build_query_chrom_data, src/fourier/moments.rs:138-177, for every (row, chromosome)),
+ * copied to host memory: row q owns groups [row_group_offsets[q], row_group_offsets[q+1])
+ * (num_rows + 1 entries), ascending by (chromosome, l_int).  Groups whose l_int reaches the
+ * chromosome's n_bins are not materialised: the reference's store lookup returns None for them
+ * (src/io/momentstore.rs:66-79).  *out_groups receives the count; with every group array NULL only
+ * the offsets are written, else capacity must hold all groups.  Synchronous. */
+int rgl_batch_query_groups(rgl_context* ctx, rgl_moments* moments, const rgl_batch* batch,
+                           const uint32_t* shard_chrom, uint32_t num_shards, uint32_t bin_size,
+                           uint64_t* row_group_offsets, uint32_t* group_chrom, uint64_t* group_l_int,
+                           double* group_sum_scale, double* group_sum_scale2, uint64_t* group_count,
+                           uint64_t capacity, uint64_t* out_groups);
+
 /* ------------------------------------------------------------------------------------------ */
 /* Seeded synthetic workloads (no counterpart in the reference; used by tests and benchmarks).  */
 /* SplitMix64 counter streams (Steele, Lea & Flood 2014) drive identical host and device        */

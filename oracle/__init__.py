@@ -58,6 +58,13 @@ _SIGS = {
     "orc_analytic_stats": (C.c_int, [C.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_double,
                                      C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int)]),
     "orc_log_p": (C.c_double, [C.c_double, C.c_int, C.c_double, C.c_double]),
+    "orc_synth_chrom_lengths": (None, [C.c_uint64, C.c_uint32, _P]),
+    "orc_synth_zipf_sizes": (None, [C.c_uint32, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, _P]),
+    "orc_synth_loguniform_sizes": (None, [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, _P]),
+    "orc_synth_block": (C.c_uint64, [C.c_uint64, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_double, C.c_double,
+                                     C.c_uint32, C.c_uint32, _P]),
+    "orc_synth_chrom_layers": (C.c_uint64, [C.c_uint64, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32, C.c_double,
+                                            C.c_uint32, C.c_uint32, C.c_uint32, _P, C.c_uint32, _P, _P]),
 }
 
 _lib = None
@@ -66,8 +73,8 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        src = os.path.join(ORACLE_DIR, "oracle.cpp")
-        if not os.path.exists(ORACLE_LIB) or os.path.getmtime(ORACLE_LIB) < os.path.getmtime(src):
+        srcs = [os.path.join(ORACLE_DIR, f) for f in ("oracle.cpp", "synth.cpp")]
+        if not os.path.exists(ORACLE_LIB) or any(os.path.getmtime(ORACLE_LIB) < os.path.getmtime(f) for f in srcs):
             subprocess.run(["make", "-s", "-C", ORACLE_DIR], check=True)
         L = C.CDLL(ORACLE_LIB)
         for k, (r, a) in _SIGS.items():
@@ -232,6 +239,9 @@ def moments_from_signal(g):
 
 
 def moments_exact(g, ls, threads=4):
+    """Exact window moments of g for the window lengths ls; threads <= 0 uses every host core."""
+    if threads <= 0:
+        threads = os.cpu_count() or 1
     g = np.ascontiguousarray(g, np.float32)
     ls = np.ascontiguousarray(ls, np.uint64)
     m = np.empty(len(ls), np.float64)
@@ -329,3 +339,67 @@ def analytic_stats(q_chroms, db, observed):
     if not ok:
         return None
     return p.value, (llr.value if has.value else None)
+
+
+# ---- seeded synthetic workloads (the same bits as the library's generator, without loading it) ----
+CHROM_NAMES_24 = [f"chr{i}" for i in range(1, 23)] + ["chrX", "chrY"]
+
+
+def synth_chrom_lengths(seed=1, num_chroms=24):
+    out = np.empty(num_chroms, np.uint32)
+    lib().orc_synth_chrom_lengths(seed, num_chroms, _p(out))
+    return out
+
+
+def synth_zipf_sizes(num_files, s=1.1, lo=1000, hi=10_000_000, target=2_000_000_000):
+    out = np.empty(num_files, np.uint64)
+    lib().orc_synth_zipf_sizes(num_files, s, lo, hi, target, _p(out))
+    return out
+
+
+def synth_loguniform_sizes(seed, num_files, lo, hi):
+    out = np.empty(num_files, np.uint64)
+    lib().orc_synth_loguniform_sizes(seed, num_files, lo, hi, _p(out))
+    return out
+
+
+class SynthWorkload:
+    """A seeded dataset description (seed, chromosome lengths, file sizes, broad / hot-spot shares)
+    whose blocks and layers are generated on the CPU."""
+
+    def __init__(self, seed, chrom_len, file_sizes, broad_fraction=0.0, hotspot_fraction=0.0, num_hotspots=0,
+                 sid_base=0):
+        self.seed = int(seed)
+        self.chrom_len = np.ascontiguousarray(chrom_len, np.uint32)
+        self.file_sizes = np.ascontiguousarray(file_sizes, np.uint64)
+        self.broad, self.hot, self.nhot, self.sid_base = float(broad_fraction), float(hotspot_fraction), \
+            int(num_hotspots), int(sid_base)
+
+    @property
+    def num_files(self):
+        return len(self.file_sizes)
+
+    def block(self, file, chrom):
+        args = (self.seed, _p(self.chrom_len), len(self.chrom_len), _p(self.file_sizes), file, chrom, self.broad,
+                self.hot, self.nhot, self.sid_base)
+        n = lib().orc_synth_block(*args, None)
+        out = np.empty((n, 3), np.uint32)
+        lib().orc_synth_block(*args, _p(out))
+        return out
+
+    def chrom_layers(self, chrom, min_size=128, growth_factor=4):
+        """{(chrom, K): (pos uint32[n,2], sid uint32[n])} of every file's intervals on one chromosome."""
+        cnt = np.zeros(64, np.uint64)
+        args = (self.seed, _p(self.chrom_len), len(self.chrom_len), _p(self.file_sizes), self.num_files, chrom,
+                self.broad, self.sid_base, min_size, growth_factor, _p(cnt), 64)
+        n = lib().orc_synth_chrom_layers(*args, None, None)
+        pos = np.empty((n, 2), np.uint32)
+        sid = np.empty(n, np.uint32)
+        lib().orc_synth_chrom_layers(*args, _p(pos), _p(sid))
+        out, acc = {}, 0
+        for k in range(64):
+            m = int(cnt[k])
+            if m:
+                out[(chrom, k)] = (pos[acc:acc + m], sid[acc:acc + m])
+                acc += m
+        return out

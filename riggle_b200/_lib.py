@@ -225,6 +225,8 @@ _SIGS = {
     "rgl_query_pvalues": (C.c_int, [_P, C.POINTER(PValueBatch), C.c_uint32, _P, _P, _P, _P, _P, _P]),
     "rgl_batch_pvalues_device": (C.c_int, [_P, _P, C.POINTER(BatchDesc), _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P,
                                            _P, _P, C.POINTER(C.c_uint64)]),
+    "rgl_batch_query_groups": (C.c_int, [_P, _P, C.POINTER(BatchDesc), _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P,
+                                         _P, _P, C.c_uint64, C.POINTER(C.c_uint64)]),
     "rgl_synth_chrom_lengths": (C.c_int, [C.c_uint64, C.c_uint32, _P]),
     "rgl_synth_zipf_sizes": (C.c_int, [C.c_uint32, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64, _P]),
     "rgl_synth_loguniform_sizes": (C.c_int, [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint64, _P]),

@@ -673,6 +673,31 @@ class Moments:
                                               C.c_void_p(d_flags), C.byref(ng) if count_groups else None))
         return ng.value if count_groups else None
 
+    def batch_query_groups(self, ctx, batch, shard_chrom, bin_size=BIN_SIZE):
+        """The device-built query length groups of a DeviceBatch (rgl_batch_query_groups): per row a
+        list of (chrom, (l_int, sum_scale, sum_scale2, count)), ascending by chromosome."""
+        sc = np.ascontiguousarray(shard_chrom, np.uint32)
+        rows = batch.num_rows
+        offs = np.zeros(rows + 1, np.uint64)
+        ng = C.c_uint64()
+        args = (ctx._h, self._h, C.byref(batch.c), _ptr(sc), len(sc), bin_size)
+        check(load().rgl_batch_query_groups(*args, _ptr(offs), None, None, None, None, None, 0, C.byref(ng)))
+        n = ng.value
+        ch = np.empty(n, np.uint32)
+        li, ss, ss2, cnt = (np.empty(n, np.uint64), np.empty(n, np.float64), np.empty(n, np.float64),
+                            np.empty(n, np.uint64))
+        check(load().rgl_batch_query_groups(*args, _ptr(offs), _ptr(ch), _ptr(li), _ptr(ss), _ptr(ss2), _ptr(cnt), n,
+                                            C.byref(ng)))
+        out = []
+        for q in range(rows):
+            a, b = int(offs[q]), int(offs[q + 1])
+            per = []
+            for c in np.unique(ch[a:b]):
+                k = np.nonzero(ch[a:b] == c)[0] + a
+                per.append((int(c), (li[k], ss[k], ss2[k], cnt[k])))
+            out.append(per)
+        return out
+
     def close(self):
         if self._h:
             load().rgl_moments_destroy(self._h)

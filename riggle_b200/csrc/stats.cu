@@ -489,14 +489,16 @@ int rgl_query_pvalues(rgl_moments* m, const rgl_pvalue_batch* b, uint32_t bin_si
     return s;
 }
 
-int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* m, const rgl_batch* b, const uint32_t* shard_chrom,
-                             uint32_t num_shards, uint32_t bin_size, const uint32_t* d_counts,
-                             const uint64_t* d_overlap_bp, double* d_p, double* d_llr, double* d_log_p,
-                             uint8_t* d_flags, uint64_t* out_groups) {
-    clear_error();
-    if (!ctx || !m || !b || !d_counts || !d_overlap_bp || !d_p || !d_llr || !d_flags || !bin_size ||
-        (num_shards && !shard_chrom))
+}  // extern "C"
+
+// Enqueues the query length groups of a device batch on the context stream: m->groups holds them
+// (row-major, ascending (chromosome, l_int) within a row) and d_goff[0..rows] the per-row group
+// offsets.  *empty is set when there is nothing to do (no rows or no sources).
+static int enqueue_batch_groups(rgl_context* ctx, rgl_moments* m, const rgl_batch* b, const uint32_t* shard_chrom,
+                                uint32_t num_shards, uint32_t bin_size, bool* empty, uint64_t** goff_out) {
+    if (!ctx || !m || !b || !bin_size || (num_shards && !shard_chrom))
         return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    *empty = false;
     if (b->num_blocks && (!b->block_offsets || !b->block_shards || !b->d_intervals))
         return fail(RGL_ERR_INVALID_ARGUMENT, "incomplete batch");
     const uint32_t rows = b->num_rows, D = m->num_sources, C = m->num_chroms;
@@ -510,7 +512,7 @@ int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* m, const rgl_batch* 
     }
     if (!b->block_rows && b->num_blocks) return fail(RGL_ERR_INVALID_ARGUMENT, "batched p-values need block_rows");
     if (!rows || !D) {
-        if (out_groups) *out_groups = 0;
+        *empty = true;
         return RGL_OK;
     }
     RGL_CUDA(cudaSetDevice(m->device));
@@ -584,6 +586,30 @@ int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* m, const rgl_batch* 
     k_group_finish<<<(unsigned)((nn + 256) / 256), 256, 0, st>>>(
         m->ukey.as<uint64_t>(), m->agg.as<LenAgg>(), m->runs.as<uint32_t>(), rows, C, (double)bin_size,
         m->slot_tab.as<uint32_t>(), lmax, m->groups.as<QGroupDev>(), d_goff);
+    RGL_CUDA(cudaGetLastError());
+    *goff_out = d_goff;
+    return RGL_OK;
+}
+
+extern "C" {
+
+int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* m, const rgl_batch* b, const uint32_t* shard_chrom,
+                             uint32_t num_shards, uint32_t bin_size, const uint32_t* d_counts,
+                             const uint64_t* d_overlap_bp, double* d_p, double* d_llr, double* d_log_p,
+                             uint8_t* d_flags, uint64_t* out_groups) {
+    clear_error();
+    if (!ctx || !m || !b || !d_counts || !d_overlap_bp || !d_p || !d_llr || !d_flags || !bin_size ||
+        (num_shards && !shard_chrom))
+        return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    bool empty = false;
+    uint64_t* d_goff = nullptr;
+    RGL_TRY(enqueue_batch_groups(ctx, m, b, shard_chrom, num_shards, bin_size, &empty, &d_goff));
+    if (empty) {
+        if (out_groups) *out_groups = 0;
+        return RGL_OK;
+    }
+    const uint32_t rows = b->num_rows, D = m->num_sources, C = m->num_chroms;
+    cudaStream_t st = context_stream(ctx);
     // the p-value kernel drops groups whose slot lies past the source's table (slot >= tab_len)
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
@@ -600,6 +626,42 @@ int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* m, const rgl_batch* 
         RGL_CUDA(cudaMemcpyAsync(&ng, d_goff + rows, 8, cudaMemcpyDeviceToHost, st));
         RGL_CUDA(cudaStreamSynchronize(st));
         *out_groups = ng;
+    }
+    return RGL_OK;
+}
+
+int rgl_batch_query_groups(rgl_context* ctx, rgl_moments* m, const rgl_batch* b, const uint32_t* shard_chrom,
+                           uint32_t num_shards, uint32_t bin_size, uint64_t* row_group_offsets, uint32_t* group_chrom,
+                           uint64_t* group_l_int, double* group_sum_scale, double* group_sum_scale2,
+                           uint64_t* group_count, uint64_t capacity, uint64_t* out_groups) {
+    clear_error();
+    if (!out_groups) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    bool empty = false;
+    uint64_t* d_goff = nullptr;
+    RGL_TRY(enqueue_batch_groups(ctx, m, b, shard_chrom, num_shards, bin_size, &empty, &d_goff));
+    const uint32_t rows = b->num_rows;
+    if (empty) {
+        if (row_group_offsets) std::fill(row_group_offsets, row_group_offsets + rows + 1, 0ull);
+        *out_groups = 0;
+        return RGL_OK;
+    }
+    cudaStream_t st = context_stream(ctx);
+    std::vector<uint64_t> goff(rows + 1ull);
+    RGL_CUDA(cudaMemcpyAsync(goff.data(), d_goff, goff.size() * 8, cudaMemcpyDeviceToHost, st));
+    RGL_CUDA(cudaStreamSynchronize(st));
+    const uint64_t ng = goff[rows];
+    *out_groups = ng;
+    if (row_group_offsets) std::copy(goff.begin(), goff.end(), row_group_offsets);
+    if (!group_chrom && !group_l_int && !group_sum_scale && !group_sum_scale2 && !group_count) return RGL_OK;
+    if (ng > capacity) return fail(RGL_ERR_INVALID_ARGUMENT, "group capacity too small");
+    std::vector<QGroupDev> g(ng);
+    if (ng) RGL_CUDA(cudaMemcpy(g.data(), m->groups.p, ng * sizeof(QGroupDev), cudaMemcpyDeviceToHost));
+    for (uint64_t k = 0; k < ng; k++) {
+        if (group_chrom) group_chrom[k] = g[k].chrom;
+        if (group_l_int) group_l_int[k] = (uint64_t)g[k].l_int;
+        if (group_sum_scale) group_sum_scale[k] = g[k].ss;
+        if (group_sum_scale2) group_sum_scale2[k] = g[k].ss2;
+        if (group_count) group_count[k] = (uint64_t)g[k].count;
     }
     return RGL_OK;
 }

@@ -320,6 +320,7 @@ def test_batch_pvalues_device_equal_host_stats_path(seed):
     layers, files, D, nsh = _random_batch(seed, nfiles=23, nshards=3, D=11)
     nbins = [30_001, 25_000, 7]  # chromosome 2 is tiny: most of its groups have l_int >= n_bins
     m = api.Moments(D, nbins)
+    tables = {}
     for d in range(D):
         for c in range(len(nbins)):
             if rng.random() < 0.2:
@@ -328,7 +329,9 @@ def test_batch_pvalues_device_equal_host_stats_path(seed):
             mean = np.sort(rng.random(ns) * rng.uniform(0.01, 50))
             var = mean * (rng.uniform(1.5, 30) if rng.random() < 0.6 else rng.uniform(0.1, 0.9))
             mv = np.stack([mean, var], 1).astype(np.float32)
-            m.set(d, c, mv[: ns // 2] if rng.random() < 0.1 else mv)
+            mv = mv[: ns // 2] if rng.random() < 0.1 else mv
+            m.set(d, c, mv)
+            tables[(d, c)] = mv
     shard_chrom = np.array([0, 1, 0xFFFFFFFF if seed % 2 else 2], np.uint32)
     idx = rg.Index.from_layers(layers, D, [f"s{i}" for i in range(nsh)])
     ctx = rg.Context(idx)
@@ -347,12 +350,13 @@ def test_batch_pvalues_device_equal_host_stats_path(seed):
     assert ng > 0
     counts = dc.cpu().numpy().view(np.uint32)
     bp = dbp.cpu().numpy().view(np.uint64)
+    # the oracle's own groups (its restatement of build_query_chrom_data) on the reference side
     row_groups = []
     for per in files:
         chroms = []
-        for sh, a in per.items():
+        for sh, a in sorted(per.items()):
             if shard_chrom[sh] != 0xFFFFFFFF:
-                chroms.append((int(shard_chrom[sh]), api.query_chrom_groups(a)))
+                chroms.append((int(shard_chrom[sh]), O.query_groups(a[:, 0], a[:, 1])))
         row_groups.append(chroms)
     hp, hl, hlp, hf = m.pvalues(row_groups, counts, bp)
     dp, dl, dlp, df = (out[k].cpu().numpy() for k in ("p", "llr", "lp", "f"))
@@ -361,6 +365,24 @@ def test_batch_pvalues_device_equal_host_stats_path(seed):
     np.testing.assert_allclose(dl, hl, rtol=1e-11, atol=1e-13)
     np.testing.assert_allclose(dp, hp, rtol=1e-11, atol=1e-300)
     np.testing.assert_allclose(dlp, hlp, rtol=1e-11, atol=1e-13)
+    # and every emitted cell against the oracle's compute_analytic_stats directly
+    checked = 0
+    for q in range(R):
+        for d in range(D):
+            if not counts[q, d]:
+                continue
+            db = {c: (nbins[c], tables[(d, c)]) for c in range(len(nbins)) if (d, c) in tables}
+            want = O.analytic_stats(row_groups[q], db, float(bp[q, d]) / 100.0)
+            if want is None:
+                assert df[q, d] == 0
+                continue
+            wp, wl = want
+            assert df[q, d] & 1 and bool(df[q, d] & 2) == (wl is not None)
+            if wl is not None:
+                assert dl[q, d] == pytest.approx(wl, rel=1e-9, abs=1e-12)
+            assert dp[q, d] == pytest.approx(wp, rel=1e-9, abs=1e-300)
+            checked += 1
+    assert checked > 10
     ctx.close()
     m.close()
     idx.close()

@@ -112,3 +112,43 @@ def test_moments_feed_pvalues_like_the_reference_integration_test():
     p, llr, lp, fl = m.pvalues(groups, counts, bp)
     assert fl[0, 0] & 1 and fl[0, 1] & 1
     assert p[0, 0] < p[0, 1] and p[0, 0] < 1e-10
+
+
+def _grid_subset(n_bins, stride):
+    """Grid indices with L in [2^8, 2^16] (every `stride`-th) plus the grid's first, last and a few
+    L below 2^8, so that every size class of window is covered."""
+    grid = O.moment_grid(n_bins)
+    mid = np.nonzero((grid >= 256) & (grid <= 65_536))[0][::stride]
+    edge = np.array([0, 1, 50, 99, 150, len(grid) - 1])
+    return grid, np.unique(np.concatenate([mid, edge[edge < len(grid)]]))
+
+
+@pytest.mark.parametrize("n_bins,bin_size,n,stride", [
+    (1 << 20, 100, 60_000, 1),      # every grid L
+    (1 << 20, 64, 60_000, 1),
+    (1 << 22, 64, 200_000, 3),
+    (1 << 22, 100, 200_000, 3),
+    (1 << 23, 64, 300_000, 6),
+])
+def test_moments_at_precision_sizes(n_bins, bin_size, n, stride):
+    """Config-3 sizes (2^20-2^23 bins, 64 and 100 bp bins, FFT lengths up to 2^25): the device's
+    FP64 moments against the oracle's exact (double-double, direct) window moments; mean within
+    1e-9 and variance within 1e-6 relative, for L in [2^8, 2^16] and the grid's edges."""
+    rng = np.random.default_rng(n_bins + bin_size)
+    span = n_bins * bin_size
+    spec = rg.SynthSpec(int(rng.integers(1, 1 << 30)), np.array([min(span, 2**32 - 1)], np.uint32), [n],
+                        broad_fraction=0.05)
+    iv = spec.block(0, 0)
+    m = api.Moments(1, [n_bins])
+    mean, var = m.build(0, 0, iv, bin_size=bin_size, report=True)
+    g = O.depth_signal(iv[:, 0], iv[:, 1], n_bins, bin_size)
+    grid, sel = _grid_subset(n_bins, stride)
+    em, ev = O.moments_exact(g, grid[sel], threads=0)
+    scale = np.maximum(np.abs(ev), 1e-12 * em * em + 1e-300)
+    err_var = np.abs(var[sel] - ev) / scale
+    err_mean = np.abs(mean[sel] - em) / np.maximum(np.abs(em), 1e-300)
+    mid = (grid[sel] >= 256) & (grid[sel] <= 65_536)
+    print(f"n_bins=2^{int(np.log2(n_bins))} bin={bin_size}: {len(sel)} L; max rel err mean {err_mean.max():.2e}, "
+          f"var {err_var.max():.2e} (L in [2^8, 2^16]: mean {err_mean[mid].max():.2e}, var {err_var[mid].max():.2e})")
+    assert err_mean.max() < 1e-9
+    assert err_var.max() < 1e-6

@@ -231,3 +231,29 @@ def test_batched_query_matches_unbatched():
         sub[:, 2] = 0
         one, _, bpo, _ = O.query_database(layers, {0: sub}, 1, 4)
         assert (one[0] == full[r]).all() and (bpo[0] == bpf[r]).all()
+
+
+def test_oracle_workload_generator_equals_the_library_generator():
+    """The CPU reference arm builds its inputs with the oracle's restatement of the seeded workload
+    generator (so it never loads the GPU library); it must produce the library generator's bits."""
+    import riggle_b200 as rg
+
+    assert np.array_equal(O.synth_chrom_lengths(1, 24), rg.synth_chrom_lengths(1, 24))
+    assert np.array_equal(O.synth_zipf_sizes(1000, 1.1, 1000, 10_000_000, 2_000_000_000),
+                          rg.synth_zipf_sizes(1000, 1.1, 1000, 10_000_000, 2_000_000_000))
+    assert np.array_equal(O.synth_loguniform_sizes(4242, 300, 100, 1_000_000),
+                          rg.synth_loguniform_sizes(4242, 300, 100, 1_000_000))
+    cl = O.synth_chrom_lengths(1, 24)
+    sizes = O.synth_zipf_sizes(40, 1.1, 100, 20_000, 200_000)
+    o = O.SynthWorkload(2, cl, sizes, broad_fraction=0.05)
+    r = rg.SynthSpec(2, cl, sizes, broad_fraction=0.05)
+    for c in (0, 7, 23):
+        ol, rl = o.chrom_layers(c), r.chrom_layers(c)
+        assert ol.keys() == rl.keys()
+        for k in ol:
+            assert np.array_equal(ol[k][0], rl[k][0]) and np.array_equal(ol[k][1], rl[k][1])
+    oq = O.SynthWorkload(5000, cl, [3000, 800], hotspot_fraction=0.1, num_hotspots=8)
+    rq = rg.SynthSpec(5000, cl, [3000, 800], hotspot_fraction=0.1, num_hotspots=8)
+    for f in range(2):
+        for c in (0, 3, 23):
+            assert np.array_equal(oq.block(f, c), rq.block(f, c))

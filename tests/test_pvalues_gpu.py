@@ -37,9 +37,9 @@ def random_case(rng, rows, D):
                 mv = mv[: ns // 2]  # a shorter table: lookups past it return None
             m.set(d, c, mv)
             tables[(d, c)] = mv
-    row_groups = []
+    row_groups, oracle_groups = [], []
     for q in range(rows):
-        chroms = []
+        chroms, ochroms = [], []
         for c in range(len(nbins)):
             if rng.random() < 0.3:
                 continue
@@ -47,24 +47,26 @@ def random_case(rng, rows, D):
             lens = np.concatenate([rng.integers(1, 3000, n), rng.integers(1, 300_000, 5)])
             ivs = np.stack([np.zeros(len(lens)), lens, np.zeros(len(lens))], 1).astype(np.uint32)
             chroms.append((c, api.query_chrom_groups(ivs)))
+            ochroms.append((c, O.query_groups(ivs[:, 0], ivs[:, 1])))
         row_groups.append(chroms)
+        oracle_groups.append(ochroms)
     counts = rng.integers(0, 3, (rows, D)).astype(np.uint32)
     bp = (rng.random((rows, D)) * rng.choice([10, 1e4, 1e7], (rows, D))).astype(np.uint64)
-    return m, tables, row_groups, counts, bp
+    return m, tables, row_groups, oracle_groups, counts, bp
 
 
 @pytest.mark.parametrize("seed", [1, 2, 3])
 def test_pvalues_match_oracle(seed):
     rng = np.random.default_rng(seed)
     rows, D = 9, 13
-    m, tables, row_groups, counts, bp = random_case(rng, rows, D)
+    m, tables, row_groups, oracle_groups, counts, bp = random_case(rng, rows, D)
     p, llr, lp, fl = m.pvalues(row_groups, counts, bp)
     n_emit = 0
     for q in range(rows):
         for d in range(D):
             want = None
             if counts[q, d]:
-                want = oracle_cell(row_groups[q], tables, d, float(bp[q, d]) / 100.0)
+                want = oracle_cell(oracle_groups[q], tables, d, float(bp[q, d]) / 100.0)
             if want is None:
                 assert fl[q, d] == 0 and p[q, d] == 1.0
                 continue
@@ -133,12 +135,14 @@ def test_end_to_end_counts_moments_pvalues():
             m.set(f, c, mv)
             tables[(f, c)] = mv
     row_groups = [[(c, api.query_chrom_groups(qs.block(f, c))) for c in range(2)] for f in range(2)]
+    oracle_groups = [[(c, O.query_groups(qs.block(f, c)[:, 0], qs.block(f, c)[:, 1])) for c in range(2)]
+                     for f in range(2)]
     p, llr, lp, fl = m.pvalues(row_groups, counts, bp)
     for q in range(2):
         for d in range(6):
             if not counts[q, d]:
                 continue
-            wp, wl = oracle_cell(row_groups[q], tables, d, float(bp[q, d]) / 100.0)
+            wp, wl = oracle_cell(oracle_groups[q], tables, d, float(bp[q, d]) / 100.0)
             assert p[q, d] == pytest.approx(wp, rel=1e-9, abs=1e-300)
             if wl is not None:
                 assert llr[q, d] == pytest.approx(wl, rel=1e-9)
