@@ -380,6 +380,18 @@ int rgl_depth_signal_noalloc(int device, const rgl_interval* d_intervals, uint64
  * mean_out / var_out (optional, host, grid length) receive the FP64 values. */
 int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_interval* intervals, uint64_t n,
                       uint32_t bin_size, double* mean_out, double* var_out);
+/* rgl_moments_build with a choice of arithmetic for the FFT autocorrelation and the prefix sums
+ * (the reference computes them in f64 with rustfft, src/fourier/moments.rs:421-466):
+ *   RGL_MOM_FP64  - FP64 Stockham FFT and double-double prefix sums (rgl_moments_build);
+ *   RGL_MOM_FP32C - compensated FP32: the centred signal scaled by a power of two per chromosome,
+ *                   a float-float (two-sum / FMA two-product) Stockham FFT, power spectrum and
+ *                   prefix sums, FP64 only in the final per-L reduction and the variance
+ *                   subtraction.  About 48 significant bits per value.
+ * The depth signal is the reference's f32 signal bit for bit in both. */
+#define RGL_MOM_FP64 0u
+#define RGL_MOM_FP32C 1u
+int rgl_moments_build_ex(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_interval* intervals, uint64_t n,
+                         uint32_t bin_size, uint32_t precision, double* mean_out, double* var_out);
 
 /* Query length groups of a batch: row q owns groups [row_group_offsets[q], row_group_offsets[q+1]),
  * each on chromosome group_chrom[g] of the moment store. */
@@ -430,6 +442,41 @@ int rgl_batch_query_groups(rgl_context* ctx, rgl_moments* moments, const rgl_bat
                            uint64_t* row_group_offsets, uint32_t* group_chrom, uint64_t* group_l_int,
                            double* group_sum_scale, double* group_sum_scale2, uint64_t* group_count,
                            uint64_t capacity, uint64_t* out_groups);
+
+/* ------------------------------------------------------------------------------------------ */
+/* Results: sparse counts and the reference's JSON output.                                       */
+/* ------------------------------------------------------------------------------------------ */
+/* K9 on the device: the non-zero cells of a dense num_rows x num_sources count matrix (device,
+ * e.g. rgl_query_batch_device's output) as CSR in (row, column) order, which is how query_database
+ * collects all_entries and builds its CsMat (src/tasks/query/mod.rs:288-307,
+ * build_csr_from_sorted_entries src/tasks/query/sweep.rs:4-23).  d_indptr (num_rows + 1, device)
+ * always receives the row pointers and *out_nnz the entry count (synchronises).  With d_indices
+ * non-NULL the column indices, and the counts (d_values) and overlap base pairs (d_bp_values, which
+ * needs d_overlap_bp) where given, are written for the first `capacity` entries;
+ * RGL_ERR_INVALID_ARGUMENT when nnz exceeds capacity.  Runs on the context's stream. */
+int rgl_dense_to_csr_device(rgl_context* ctx, uint32_t num_rows, uint32_t num_sources, const uint32_t* d_counts,
+                            const uint64_t* d_overlap_bp, uint64_t* d_indptr, uint32_t* d_indices,
+                            uint32_t* d_values, uint64_t* d_bp_values, uint64_t capacity, uint64_t* out_nnz);
+
+/* The StatsOutput JSON of `chuckle query` (src/main.rs:141-204; StatResult, src/stats/mod.rs:30-60,
+ * serde_json::to_string_pretty), byte for byte: one result per CSR entry (host arrays, e.g. copied
+ * from rgl_dense_to_csr_device) with its query / database names and overlap count.  With p_value
+ * non-NULL (stats mode; observed_bins, p_value, llr and flags are dense num_rows x num_sources host
+ * arrays as rgl_query_pvalues writes them) only cells flagged RGL_PV_EMITTED are written, with
+ * observed_bins, p_value and llr (when RGL_PV_HAS_LLR), sorted by ascending p-value (ties in
+ * (query, database) order; the reference's follow a HashMap); without, every entry, sorted by
+ * descending overlap count (stable, as the reference).  *out_len receives the byte length; with out
+ * NULL nothing else is written, else capacity must hold it (no terminating NUL is added). */
+int rgl_format_stats_json(uint32_t num_rows, uint32_t num_sources, const char* const* query_names,
+                          const char* const* db_names, const uint64_t* indptr, const uint32_t* indices,
+                          const uint32_t* counts, const double* observed_bins, const double* p_value,
+                          const double* llr, const uint8_t* flags, char* out, uint64_t capacity,
+                          uint64_t* out_len);
+/* The IntervalsOutput JSON of `chuckle query --intervals` (IntervalHit, src/stats/mod.rs:4-27): one
+ * hit per rgl_pair in the given order, names taken by row, sid and shard. */
+int rgl_format_intervals_json(const rgl_pair* pairs, uint64_t n, uint32_t num_rows, uint32_t num_sources,
+                              uint32_t num_shards, const char* const* query_names, const char* const* db_names,
+                              const char* const* shard_names, char* out, uint64_t capacity, uint64_t* out_len);
 
 /* ------------------------------------------------------------------------------------------ */
 /* Seeded synthetic workloads (no counterpart in the reference; used by tests and benchmarks).  */

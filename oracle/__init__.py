@@ -403,3 +403,68 @@ class SynthWorkload:
                 out[(chrom, k)] = (pos[acc:acc + m], sid[acc:acc + m])
                 acc += m
         return out
+
+
+# ---- results (test infrastructure) ---------------------------------------------------------------
+def dense_to_csr(counts):
+    """query_database's non-zero extraction (src/tasks/query/mod.rs:288-298: rows in order, columns
+    in order, val > 0) and build_csr_from_sorted_entries (src/tasks/query/sweep.rs:4-23)."""
+    counts = np.asarray(counts)
+    rows = counts.shape[0]
+    indptr = np.zeros(rows + 1, np.uint64)
+    indices, data = [], []
+    for r in range(rows):
+        cols = np.nonzero(counts[r] > 0)[0]
+        indices.extend(cols.tolist())
+        data.extend(counts[r, cols].tolist())
+        indptr[r + 1] = indptr[r] + len(cols)
+    return indptr, np.array(indices, np.uint32), np.array(data, np.uint32)
+
+
+def json_f64(v):
+    """An f64 as serde_json writes it (its shortest-round-trip float printer): plain decimal when
+    the decimal exponent kk (10^(kk-1) <= |v| < 10^kk) satisfies -5 < kk <= 16, with ".0" on
+    integers; else d.ddde<exp>.  Digits from Python's shortest repr."""
+    import decimal
+    import math
+
+    if not math.isfinite(v):
+        return "null"
+    if v == 0.0:
+        return "-0.0" if math.copysign(1.0, v) < 0 else "0.0"
+    t = decimal.Decimal(repr(v)).as_tuple()
+    digits = "".join(map(str, t.digits)).rstrip("0") or "0"
+    exp = t.exponent + (len(t.digits) - len(digits))  # v = digits x 10^exp
+    length = len(digits)
+    kk = length + exp
+    sign = "-" if t.sign else ""
+    if 0 <= exp and kk <= 16:
+        return sign + digits + "0" * exp + ".0"
+    if 0 < kk <= 16:
+        return sign + digits[:kk] + "." + digits[kk:]
+    if -5 < kk <= 0:
+        return sign + "0." + "0" * (-kk) + digits
+    return sign + digits[0] + ("." + digits[1:] if length > 1 else "") + "e" + str(kk - 1)
+
+
+def json_pretty(results_key, objects):
+    """serde_json::to_string_pretty of a struct with one Vec field of flat structs: objects is a list
+    of [(key, value)] with value str, int or float (StatsOutput / IntervalsOutput,
+    src/stats/mod.rs:1-60)."""
+    import json
+
+    if not objects:
+        return '{\n  "%s": []\n}' % results_key
+    parts = []
+    for obj in objects:
+        lines = []
+        for k, v in obj:
+            if isinstance(v, str):
+                val = json.dumps(v, ensure_ascii=False)
+            elif isinstance(v, float):
+                val = json_f64(v)
+            else:
+                val = str(int(v))
+            lines.append('      "%s": %s' % (k, val))
+        parts.append("    {\n" + ",\n".join(lines) + "\n    }")
+    return '{\n  "%s": [\n' % results_key + ",\n".join(parts) + "\n  ]\n}"

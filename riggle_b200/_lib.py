@@ -222,6 +222,7 @@ _SIGS = {
     "rgl_depth_signal": (C.c_int, [C.c_int, _P, C.c_uint64, C.c_uint64, C.c_uint32, _P]),
     "rgl_depth_signal_noalloc": (C.c_int, [C.c_int, _P, C.c_uint64, C.c_uint64, C.c_uint32, _P, _P]),
     "rgl_moments_build": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, C.c_uint64, C.c_uint32, _P, _P]),
+    "rgl_moments_build_ex": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, C.c_uint64, C.c_uint32, C.c_uint32, _P, _P]),
     "rgl_query_pvalues": (C.c_int, [_P, C.POINTER(PValueBatch), C.c_uint32, _P, _P, _P, _P, _P, _P]),
     "rgl_batch_pvalues_device": (C.c_int, [_P, _P, C.POINTER(BatchDesc), _P, C.c_uint32, C.c_uint32, _P, _P, _P, _P,
                                            _P, _P, C.POINTER(C.c_uint64)]),
@@ -243,6 +244,12 @@ _SIGS = {
     "rgl_index_select_columns": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
     "rgl_synth_batch_layout": (C.c_int, [C.POINTER(SynthSpec), _P, _P, _P]),
     "rgl_synth_batch_device": (C.c_int, [C.POINTER(SynthSpec), C.c_int, _P, _P, _P]),
+    "rgl_dense_to_csr_device": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, _P, _P, _P, _P, C.c_uint64,
+                                          C.POINTER(C.c_uint64)]),
+    "rgl_format_stats_json": (C.c_int, [C.c_uint32, C.c_uint32, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P, C.c_uint64,
+                                        C.POINTER(C.c_uint64)]),
+    "rgl_format_intervals_json": (C.c_int, [_P, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, _P, _P, _P, _P,
+                                            C.c_uint64, C.POINTER(C.c_uint64)]),
     "rgl_abi_struct_name": (C.c_char_p, [C.c_uint32]),
     "rgl_abi_layout": (C.c_int, [C.c_char_p, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint32),
                                  C.POINTER(C.c_char_p), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.c_uint32]),

@@ -616,13 +616,16 @@ class Moments:
         mv = np.ascontiguousarray(np.asarray(mean_var, np.float32).reshape(-1, 2))
         check(load().rgl_moments_set(self._h, sid, chrom, _ptr(mv), len(mv)))
 
-    def build(self, sid, chrom, intervals, bin_size=BIN_SIZE, report=False):
-        """Moments of one source's intervals (file order) on one chromosome, computed on the GPU."""
+    def build(self, sid, chrom, intervals, bin_size=BIN_SIZE, report=False, precision="fp64"):
+        """Moments of one source's intervals (file order) on one chromosome, computed on the GPU;
+        precision "fp64" (FP64 FFT) or "fp32c" (compensated FP32, FP64 only in the final reduction)."""
         iv = np.ascontiguousarray(np.asarray(intervals, np.uint32).reshape(-1, 3))
         n = self.slots(chrom)
         mean = np.empty(n, np.float64) if report else None
         var = np.empty(n, np.float64) if report else None
-        check(load().rgl_moments_build(self._h, sid, chrom, _ptr(iv), len(iv), bin_size, _ptr(mean), _ptr(var)))
+        mode = {"fp64": 0, "fp32c": 1}[precision]
+        check(load().rgl_moments_build_ex(self._h, sid, chrom, _ptr(iv), len(iv), bin_size, mode, _ptr(mean),
+                                          _ptr(var)))
         return (mean, var) if report else None
 
     def get(self, sid, chrom):
@@ -708,3 +711,69 @@ class Moments:
             self.close()
         except Exception:
             pass
+
+
+def _names(names):
+    if names is None:
+        return None, None
+    arr = (C.c_char_p * len(names))(*[str(n).encode() for n in names])
+    return arr, C.cast(arr, C.c_void_p)
+
+
+def stats_json(indptr, indices, counts, query_names, db_names, num_sources, observed_bins=None, p_value=None,
+               llr=None, flags=None):
+    """The reference's StatsOutput JSON (rgl_format_stats_json) of a CSR count matrix, optionally with the
+    dense p-value arrays of rgl_query_pvalues (stats mode).  Returns the JSON text."""
+    indptr = np.ascontiguousarray(indptr, np.uint64)
+    indices = np.ascontiguousarray(indices, np.uint32)
+    counts = np.ascontiguousarray(counts, np.uint32)
+    rows = len(indptr) - 1
+    qa, qp = _names(query_names)
+    da, dp = _names(db_names)
+    dense = [None if a is None else np.ascontiguousarray(a, dt)
+             for a, dt in ((observed_bins, np.float64), (p_value, np.float64), (llr, np.float64), (flags, np.uint8))]
+    args = [rows, num_sources, qp, dp, _ptr(indptr), _ptr(indices), _ptr(counts)] + [_ptr(a) for a in dense]
+    n = C.c_uint64()
+    check(load().rgl_format_stats_json(*args, None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value + 1)
+    check(load().rgl_format_stats_json(*args, buf, n.value, C.byref(n)))
+    return buf.raw[:n.value].decode()
+
+
+def intervals_json(pairs, query_names, db_names, shard_names):
+    """The reference's IntervalsOutput JSON (rgl_format_intervals_json) of a uint32[n, 8] pair array in
+    rgl_pair layout."""
+    pairs = np.ascontiguousarray(pairs, np.uint32).reshape(-1, 8)
+    qa, qp = _names(query_names)
+    da, dp = _names(db_names)
+    sa, sp = _names(shard_names)
+    args = [_ptr(pairs), len(pairs), len(query_names), len(db_names), len(shard_names), qp, dp, sp]
+    n = C.c_uint64()
+    check(load().rgl_format_intervals_json(*args, None, 0, C.byref(n)))
+    buf = C.create_string_buffer(n.value + 1)
+    check(load().rgl_format_intervals_json(*args, buf, n.value, C.byref(n)))
+    return buf.raw[:n.value].decode()
+
+
+def dense_to_csr_device(ctx, d_counts, num_rows, num_sources, d_bp=None):
+    """K9 on the device (rgl_dense_to_csr_device) for device pointers; returns host numpy arrays
+    (indptr uint64[rows+1], indices uint32[nnz], values uint32[nnz], bp uint64[nnz] or None)."""
+    import torch
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    indptr = torch.empty(num_rows + 1, dtype=torch.int64, device=dev)
+    nnz = C.c_uint64()
+    check(load().rgl_dense_to_csr_device(ctx._h, num_rows, num_sources, C.c_void_p(d_counts),
+                                         C.c_void_p(d_bp) if d_bp else None, C.c_void_p(indptr.data_ptr()), None,
+                                         None, None, 0, C.byref(nnz)))
+    n = max(nnz.value, 1)
+    ind = torch.empty(n, dtype=torch.int32, device=dev)
+    val = torch.empty(n, dtype=torch.int32, device=dev)
+    bpv = torch.empty(n, dtype=torch.int64, device=dev) if d_bp else None
+    check(load().rgl_dense_to_csr_device(ctx._h, num_rows, num_sources, C.c_void_p(d_counts),
+                                         C.c_void_p(d_bp) if d_bp else None, C.c_void_p(indptr.data_ptr()),
+                                         C.c_void_p(ind.data_ptr()), C.c_void_p(val.data_ptr()),
+                                         C.c_void_p(bpv.data_ptr()) if d_bp else None, nnz.value, C.byref(nnz)))
+    k = nnz.value
+    return (indptr.cpu().numpy().view(np.uint64), ind[:k].cpu().numpy().view(np.uint32),
+            val[:k].cpu().numpy().view(np.uint32), None if bpv is None else bpv[:k].cpu().numpy().view(np.uint64))

@@ -308,6 +308,199 @@ __global__ void k_window_moments(uint32_t G, const uint64_t* __restrict__ ls, ui
     if (var_out) var_out[i] = var;
 }
 
+// ---- the compensated-FP32 path (K5-K7 with float-float arithmetic) ------------------------------
+// Every value is an unevaluated sum hi + lo of two floats (|lo| <= ulp(hi) / 2), about 48 bits of
+// significand, kept by the error-free transformations two-sum (Knuth) and two-product (one FMA)
+// as in Dekker's double-length arithmetic (T. J. Dekker, "A floating-point technique for extending
+// the available precision", Numer. Math. 18, 1971; Y. Hida, X. S. Li, D. H. Bailey, "Algorithms for
+// quad-double precision floating point arithmetic", ARITH 2001, for the add / mul sequences).  The
+// centred signal is scaled by a power of two per chromosome so that it is O(1) (no denormal lo
+// parts), the FFT, the power spectrum and the prefix sums run in float-float, and FP64 appears only
+// when the per-L results are combined (k_window_moments: the final reduction and the variance
+// subtraction).
+struct FF {
+    float hi, lo;
+};
+struct CFF {
+    FF re, im;
+};
+__device__ __forceinline__ FF ff_two_sum(float a, float b) {
+    const float s = __fadd_rn(a, b);
+    const float bb = __fsub_rn(s, a);
+    const float e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
+    return FF{s, e};
+}
+__device__ __forceinline__ FF ff_quick(float a, float b) {  // |a| >= |b|
+    const float s = __fadd_rn(a, b);
+    return FF{s, __fsub_rn(b, __fsub_rn(s, a))};
+}
+__device__ __forceinline__ FF ff_add(FF a, FF b) {
+    FF s = ff_two_sum(a.hi, b.hi);
+    const FF t = ff_two_sum(a.lo, b.lo);
+    s.lo = __fadd_rn(s.lo, t.hi);
+    s = ff_quick(s.hi, s.lo);
+    s.lo = __fadd_rn(s.lo, t.lo);
+    return ff_quick(s.hi, s.lo);
+}
+__device__ __forceinline__ FF ff_neg(FF a) { return FF{-a.hi, -a.lo}; }
+__device__ __forceinline__ FF ff_sub(FF a, FF b) { return ff_add(a, ff_neg(b)); }
+__device__ __forceinline__ FF ff_mul(FF a, FF b) {
+    const float p = __fmul_rn(a.hi, b.hi);
+    float e = __fmaf_rn(a.hi, b.hi, -p);
+    e = __fmaf_rn(a.hi, b.lo, e);
+    e = __fmaf_rn(a.lo, b.hi, e);
+    return ff_quick(p, e);
+}
+__device__ __forceinline__ FF ff_from_double_exact(uint64_t t) {  // an integer below 2^48, exactly
+    const float hi = (float)(t & ~0xFFFFFFull);                    // the top bits (exact in a float)
+    return ff_two_sum(hi, (float)(t & 0xFFFFFFull));
+}
+__device__ __forceinline__ CFF cff_add(CFF a, CFF b) { return CFF{ff_add(a.re, b.re), ff_add(a.im, b.im)}; }
+__device__ __forceinline__ CFF cff_sub(CFF a, CFF b) { return CFF{ff_sub(a.re, b.re), ff_sub(a.im, b.im)}; }
+__device__ __forceinline__ CFF cff_mul(CFF a, CFF b) {
+    return CFF{ff_sub(ff_mul(a.re, b.re), ff_mul(a.im, b.im)), ff_add(ff_mul(a.re, b.im), ff_mul(a.im, b.re))};
+}
+struct FFAdd {
+    __device__ __forceinline__ FF operator()(const FF& a, const FF& b) const { return ff_add(a, b); }
+};
+
+__constant__ CFF c_tw16f[16];  // exp(-2 pi i k / 16) as float-float (host-computed)
+
+template <int R>
+__device__ __forceinline__ void dft_regs_ff(CFF* v) {
+#pragma unroll
+    for (int i = 0; i < R; i++) {
+        int j = 0;
+#pragma unroll
+        for (int b = 1; b < R; b <<= 1) j = (j << 1) | ((i / b) & 1);
+        if (i < j) {
+            const CFF t = v[i];
+            v[i] = v[j];
+            v[j] = t;
+        }
+    }
+#pragma unroll
+    for (int len = 2; len <= R; len <<= 1) {
+#pragma unroll
+        for (int i = 0; i < R; i += len) {
+#pragma unroll
+            for (int k = 0; k < len / 2; k++) {
+                const CFF a = v[i + k];
+                const CFF t = k == 0 ? v[i + k + len / 2] : cff_mul(v[i + k + len / 2], c_tw16f[k * (16 / len)]);
+                v[i + k] = cff_add(a, t);
+                v[i + k + len / 2] = cff_sub(a, t);
+            }
+        }
+    }
+}
+
+// One Stockham pass as k_fft_pass, in float-float.  The twiddle exp(-2 pi i t / M), t = k r M / (Ns R),
+// is the product of two table entries: wc[t >> tb] (coarse) and wf[t & (2^tb - 1)] (fine).
+template <int R>
+__global__ void __launch_bounds__(128) k_ff_fft_pass(const CFF* __restrict__ in, CFF* __restrict__ out, uint64_t M,
+                                                     uint64_t Ns, const CFF* __restrict__ wc,
+                                                     const CFF* __restrict__ wf, int tb) {
+    const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t stride = M / R;
+    if (j >= stride) return;
+    CFF v[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) v[r] = in[j + r * stride];
+    const uint64_t k = j % Ns;
+    if (Ns > 1) {
+        const uint64_t step = M / (Ns * R);  // t = k r step < M
+        const uint64_t mask = (1ull << tb) - 1;
+#pragma unroll
+        for (int r = 1; r < R; r++) {
+            const uint64_t t = k * (uint64_t)r * step;
+            const CFF w = cff_mul(wc[t >> tb], wf[t & mask]);
+            v[r] = cff_mul(v[r], w);
+        }
+    }
+    dft_regs_ff<R>(v);
+    const uint64_t base = (j / Ns) * Ns * R + k;
+#pragma unroll
+    for (int r = 0; r < R; r++) out[base + r * Ns] = v[r];
+}
+
+// u = (g - gbar) 2^-e into the zero-padded complex input (u[N] = 0 for the U scan).
+__global__ void k_ff_center(uint64_t n, uint64_t M, const float* __restrict__ g, const FF* __restrict__ gsum,
+                            float scale, CFF* __restrict__ x, FF* __restrict__ u_out) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= M) return;
+    FF u = FF{0.f, 0.f};
+    if (i < n) {
+        // gbar = gsum / n in float-float: one Newton step on the float quotient
+        const FF S = *gsum;
+        const float q = __fdiv_rn(S.hi, (float)n);
+        const FF qn = ff_mul(FF{q, 0.f}, ff_from_double_exact(n));
+        const FF r = ff_sub(S, qn);
+        const FF gbar = ff_quick(q, __fdiv_rn(r.hi, (float)n));
+        u = ff_sub(FF{g[i], 0.f}, gbar);
+        u = FF{u.hi * scale, u.lo * scale};  // exact: scale is a power of two
+    }
+    x[i] = CFF{u, FF{0.f, 0.f}};
+    if (i <= n) u_out[i] = u;
+}
+
+__global__ void k_ff_from_float(uint64_t n, const float* __restrict__ g, FF* __restrict__ out) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < n) out[i] = FF{g[i], 0.f};
+}
+
+__global__ void k_ff_power(uint64_t M, CFF* __restrict__ x) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < M) {
+        const CFF a = x[i];
+        x[i] = CFF{ff_add(ff_mul(a.re, a.re), ff_mul(a.im, a.im)), FF{0.f, 0.f}};
+    }
+}
+
+// Scan inputs of the compensated path, as k_term (A[t] = Re Y[t] / M, an exact power-of-two scale).
+__global__ void k_ff_term(uint64_t len, int term, const CFF* __restrict__ y, float inv_m, const FF* __restrict__ U,
+                          uint64_t n, FF* __restrict__ out) {
+    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (t >= len) return;
+    FF v = FF{0.f, 0.f};
+    switch (term) {
+        case T_A:
+            if (t >= 1 && t < n) v = FF{y[t].re.hi * inv_m, y[t].re.lo * inv_m};
+            break;
+        case T_MA:
+            if (t >= 1 && t < n) v = ff_mul(ff_from_double_exact(t), FF{y[t].re.hi * inv_m, y[t].re.lo * inv_m});
+            break;
+        case T_U2:
+            if (t >= 1 && t <= n) v = ff_mul(U[t], U[t]);
+            break;
+        case T_V2:
+            if (t >= 1 && t < n) {
+                const FF d = ff_sub(U[n], U[n - t]);
+                v = ff_mul(d, d);
+            }
+            break;
+        default:
+            if (t <= n) v = U[t];
+    }
+    out[t] = v;
+}
+
+// Inclusive prefix values at the requested indices, widened to double-double and scaled back by
+// the exact power of two 2^sc (the FP64 final reduction starts here).
+__global__ void k_ff_gather(uint32_t k, const uint64_t* __restrict__ at, const FF* __restrict__ pre, int sc,
+                            DD* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < k) {
+        const FF v = pre[at[i]];
+        out[i] = DD{ldexp((double)v.hi, sc), ldexp((double)v.lo, sc)};
+    }
+}
+
+// U[0] = 0, U[s] = inclusive scan of u at s - 1.
+__global__ void k_ff_shift(uint64_t n, const FF* __restrict__ incl, FF* __restrict__ U) {
+    const uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (s <= n) U[s] = s ? incl[s - 1] : FF{0.f, 0.f};
+}
+
 }  // namespace rgl
 
 using namespace rgl;
@@ -425,6 +618,164 @@ int dd_scan(MomentWs& w, uint64_t len, cudaStream_t st) {
 
 }  // namespace
 
+namespace {
+int ff_scan(MomentWs& w, uint64_t len, cudaStream_t st) {
+    // inclusive float-float scan of w.dd_in (as FF) into w.dd_out
+    FF* in = reinterpret_cast<FF*>(w.dd_in.p);
+    FF* out = reinterpret_cast<FF*>(w.dd_out.p);
+    size_t tb = 0;
+    cub::DeviceScan::InclusiveScan(nullptr, tb, in, out, FFAdd(), (int)len, st);
+    RGL_TRY(w.tmp.ensure(tb + 256));
+    tb = w.tmp.cap;
+    RGL_CUDA(cub::DeviceScan::InclusiveScan(w.tmp.p, tb, in, out, FFAdd(), (int)len, st));
+    return RGL_OK;
+}
+
+// Float-float value of a long double: hi = nearest float, lo = nearest float of the remainder.
+inline void ff_of(long double v, float* hi, float* lo) {
+    *hi = (float)v;
+    *lo = (float)(v - (long double)*hi);
+}
+
+bool g_tw16f_ready[64] = {false};
+
+// exp(-2 pi i t / M) for t = (c << tb) (coarse table) and t < 2^tb (fine table), float-float, host-made
+// in extended precision; the radix-16 constants once per device.
+int ff_twiddles(MomentWs& w, uint64_t M, int device, int* tb_out) {
+    if (device >= 0 && device < 64 && !g_tw16f_ready[device]) {
+        float h[64];
+        for (int k = 0; k < 16; k++) {
+            const long double a = -2.0L * (long double)M_PI * (long double)k / 16.0L;
+            ff_of(cosl(a), &h[4 * k], &h[4 * k + 1]);
+            ff_of(sinl(a), &h[4 * k + 2], &h[4 * k + 3]);
+        }
+        RGL_CUDA(cudaMemcpyToSymbol(c_tw16f, h, sizeof(h)));
+        g_tw16f_ready[device] = true;
+    }
+    int logm = 0;
+    while ((1ull << logm) < M) logm++;
+    const int tb = (logm + 1) / 2;
+    const uint64_t nf = 1ull << tb, nc = (M >> tb) + 1;
+    std::vector<float> h(4 * (nf + nc));
+    const long double pi2 = 2.0L * 3.141592653589793238462643383279502884L;
+    for (uint64_t t = 0; t < nf; t++) {
+        const long double a = -pi2 * (long double)t / (long double)M;
+        ff_of(cosl(a), &h[4 * t], &h[4 * t + 1]);
+        ff_of(sinl(a), &h[4 * t + 2], &h[4 * t + 3]);
+    }
+    for (uint64_t c = 0; c < nc; c++) {
+        const long double a = -pi2 * (long double)(c << tb) / (long double)M;
+        float* q = &h[4 * (nf + c)];
+        ff_of(cosl(a), &q[0], &q[1]);
+        ff_of(sinl(a), &q[2], &q[3]);
+    }
+    RGL_TRY(w.grid.ensure(h.size() * 4));
+    RGL_CUDA(cudaMemcpy(w.grid.p, h.data(), h.size() * 4, cudaMemcpyHostToDevice));
+    *tb_out = tb;
+    return RGL_OK;
+}
+
+int ff_fft_forward(MomentWs& w, uint64_t M, int tb, cudaStream_t st, CFF** result) {
+    CFF* src = reinterpret_cast<CFF*>(w.fa.p);
+    CFF* dst = reinterpret_cast<CFF*>(w.fb.p);
+    const CFF* wf = reinterpret_cast<const CFF*>(w.grid.p);
+    const CFF* wc = wf + (1ull << tb);
+    uint64_t Ns = 1;
+    int logm = 0;
+    while ((1ull << logm) < M) logm++;
+    int rem = logm;
+    while (rem > 0) {
+        const int r = rem >= 4 ? 4 : rem;
+        const uint64_t threads = M >> r;
+        const unsigned blocks = (unsigned)((threads + 127) / 128);
+        switch (r) {
+            case 4: k_ff_fft_pass<16><<<blocks, 128, 0, st>>>(src, dst, M, Ns, wc, wf, tb); break;
+            case 3: k_ff_fft_pass<8><<<blocks, 128, 0, st>>>(src, dst, M, Ns, wc, wf, tb); break;
+            case 2: k_ff_fft_pass<4><<<blocks, 128, 0, st>>>(src, dst, M, Ns, wc, wf, tb); break;
+            default: k_ff_fft_pass<2><<<blocks, 128, 0, st>>>(src, dst, M, Ns, wc, wf, tb); break;
+        }
+        Ns <<= r;
+        rem -= r;
+        std::swap(src, dst);
+    }
+    RGL_CUDA(cudaGetLastError());
+    *result = src;
+    return RGL_OK;
+}
+
+struct GMax {
+    __device__ __forceinline__ float operator()(float a, float b) const { return fmaxf(a, b); }
+};
+
+// K5-K7 of the compensated-FP32 path for the depth signal in w.g (N bins): fills outs (P0, P1, Q,
+// V, UU_L, UU_R as double-double, scaled back), *uu_total, *a0 and w.gsum (as DD) for
+// k_window_moments.
+int moments_ff(MomentWs& w, uint64_t N, uint64_t M, int device, uint32_t G, const uint64_t* d_at, DD* outs,
+               DD* uu_total, double* a0, cudaStream_t st) {
+    int tb = 0;
+    RGL_TRY(ff_twiddles(w, M, device, &tb));
+    FF* ffin = reinterpret_cast<FF*>(w.dd_in.p);
+    FF* ffout = reinterpret_cast<FF*>(w.dd_out.p);
+    FF* U = reinterpret_cast<FF*>(w.U.p);
+    // gsum in float-float, max(g) for the per-chromosome scale
+    k_ff_from_float<<<blocks_for(N), 256, 0, st>>>(N, w.g.as<float>(), ffin);
+    FF* d_gsum = reinterpret_cast<FF*>(w.gsum.p) + 4;  // beside the DD copy at w.gsum[0]
+    float* d_gmax = reinterpret_cast<float*>(w.gsum.p) + 12;
+    {
+        size_t t1 = 0, t2 = 0;
+        cub::DeviceReduce::Reduce(nullptr, t1, ffin, d_gsum, (int)N, FFAdd(), FF{0.f, 0.f}, st);
+        cub::DeviceReduce::Reduce(nullptr, t2, w.g.as<float>(), d_gmax, (int)N, GMax(), 0.0f, st);
+        RGL_TRY(w.tmp.ensure(std::max(t1, t2) + 256));
+        t1 = w.tmp.cap;
+        RGL_CUDA(cub::DeviceReduce::Reduce(w.tmp.p, t1, ffin, d_gsum, (int)N, FFAdd(), FF{0.f, 0.f}, st));
+        t2 = w.tmp.cap;
+        RGL_CUDA(cub::DeviceReduce::Reduce(w.tmp.p, t2, w.g.as<float>(), d_gmax, (int)N, GMax(), 0.0f, st));
+    }
+    FF gs;
+    float gmax = 0.f;
+    RGL_CUDA(cudaMemcpyAsync(&gs, d_gsum, sizeof(FF), cudaMemcpyDeviceToHost, st));
+    RGL_CUDA(cudaMemcpyAsync(&gmax, d_gmax, 4, cudaMemcpyDeviceToHost, st));
+    RGL_CUDA(cudaStreamSynchronize(st));
+    // the DD copy of the sum for the final reduction (exact: hi + lo of a float-float)
+    const DD gsum_dd{(double)gs.hi + (double)gs.lo, 0.0};
+    RGL_CUDA(cudaMemcpyAsync(w.gsum.p, &gsum_dd, sizeof(DD), cudaMemcpyHostToDevice, st));
+    // |u| <= max(g) (coverage is non-negative): scale u by 2^-e with 2^e >= max(g)
+    int e = 0;
+    if (gmax > 0.f) (void)std::frexp((double)gmax, &e);
+    const float scale = std::ldexp(1.0f, -e);
+    k_ff_center<<<blocks_for(M), 256, 0, st>>>(N, M, w.g.as<float>(), d_gsum, scale, reinterpret_cast<CFF*>(w.fa.p),
+                                                ffin);
+    RGL_TRY(ff_scan(w, N + 1, st));
+    k_ff_shift<<<blocks_for(N + 1), 256, 0, st>>>(N, ffout, U);
+    CFF* X = nullptr;
+    RGL_TRY(ff_fft_forward(w, M, tb, st, &X));
+    k_ff_power<<<blocks_for(M), 256, 0, st>>>(M, X);
+    if (X != reinterpret_cast<CFF*>(w.fa.p)) RGL_CUDA(cudaMemcpyAsync(w.fa.p, X, M * 16, cudaMemcpyDeviceToDevice, st));
+    CFF* Y = nullptr;
+    RGL_TRY(ff_fft_forward(w, M, tb, st, &Y));
+    const float inv_m = std::ldexp(1.0f, -(int)std::lround(std::log2((double)M)));
+    const int terms[4] = {T_A, T_MA, T_U2, T_V2};
+    for (int q = 0; q < 4; q++) {
+        k_ff_term<<<blocks_for(N + 1), 256, 0, st>>>(N + 1, terms[q], Y, inv_m, U, N, ffin);
+        RGL_TRY(ff_scan(w, N + 1, st));
+        k_ff_gather<<<blocks_for(G), 256, 0, st>>>(G, d_at, ffout, 2 * e, outs + (uint64_t)q * G);
+    }
+    k_ff_term<<<blocks_for(N + 1), 256, 0, st>>>(N + 1, T_U, Y, inv_m, U, N, ffin);
+    RGL_TRY(ff_scan(w, N + 1, st));
+    k_ff_gather<<<blocks_for(G), 256, 0, st>>>(G, d_at, ffout, e, outs + 4ull * G);
+    k_ff_gather<<<blocks_for(G), 256, 0, st>>>(G, d_at + G, ffout, e, outs + 5ull * G);
+    FF tot, y0;
+    RGL_CUDA(cudaMemcpyAsync(&tot, ffout + N, sizeof(FF), cudaMemcpyDeviceToHost, st));
+    RGL_CUDA(cudaMemcpyAsync(&y0, &Y[0].re, sizeof(FF), cudaMemcpyDeviceToHost, st));
+    RGL_CUDA(cudaStreamSynchronize(st));
+    *uu_total = DD{std::ldexp((double)tot.hi, e), std::ldexp((double)tot.lo, e)};
+    *a0 = std::ldexp(((double)y0.hi + (double)y0.lo) * (double)inv_m, 2 * e);
+    RGL_CUDA(cudaGetLastError());
+    return RGL_OK;
+}
+
+}  // namespace
+
 struct rgl_moments;  // defined in stats.cu
 namespace rgl {
 int moments_table_ptr(rgl_moments* m, uint32_t sid, uint32_t chrom, float2** ptr, uint64_t* slots, uint64_t* n_bins,
@@ -450,10 +801,12 @@ int rgl_depth_signal(int device, const rgl_interval* intervals, uint64_t n, uint
     return RGL_OK;
 }
 
-int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_interval* intervals, uint64_t n,
-                      uint32_t bin_size, double* mean_out, double* var_out) {
+int rgl_moments_build_ex(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_interval* intervals, uint64_t n,
+                         uint32_t bin_size, uint32_t precision, double* mean_out, double* var_out) {
     clear_error();
     if (!m || (n && !intervals) || bin_size == 0) return fail(RGL_ERR_INVALID_ARGUMENT, "bad arguments");
+    if (precision != RGL_MOM_FP64 && precision != RGL_MOM_FP32C)
+        return fail(RGL_ERR_INVALID_ARGUMENT, "precision must be RGL_MOM_FP64 or RGL_MOM_FP32C");
     float2* table = nullptr;
     uint64_t slots = 0, N = 0;
     int device = 0;
@@ -461,6 +814,7 @@ int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_in
     if (N * (uint64_t)bin_size > 0xFFFFFFFFull) return fail(RGL_ERR_INVALID_ARGUMENT, "n_bins * bin_size overflows u32");
     if (device < 0 || device >= 16) return fail(RGL_ERR_INVALID_ARGUMENT, "device ordinal out of range");
     if (N <= 1) return moments_mark(m, sid, chrom, 0);  // moments_from_signal returns no entries
+    if (N >= (1ull << 31)) return fail(RGL_ERR_INVALID_ARGUMENT, "at most 2^31 - 1 bins per chromosome");
     DeviceScope scope;
     RGL_TRY(scope.enter(device));
     std::lock_guard<std::mutex> lk(g_ws_mu);
@@ -468,7 +822,6 @@ int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_in
     cudaStream_t st = 0;
     RGL_TRY(upload_twiddles(device));
     RGL_TRY(depth_signal_dev(w, intervals, n, N, bin_size, st));
-    // K5: mean of g (double-double sum), centred signal, U = prefix of u
     uint64_t M = 1;
     while (M < 2 * N) M <<= 1;
     RGL_TRY(w.fa.ensure(M * 16));
@@ -477,38 +830,14 @@ int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_in
     RGL_TRY(w.dd_out.ensure((N + 2) * 16));
     RGL_TRY(w.U.ensure((N + 2) * 8));
     RGL_TRY(w.gsum.ensure(64));
-    k_to_dd<<<blocks_for(N), 256, 0, st>>>(N, w.g.as<float>(), w.dd_in.as<DD>());
-    {
-        size_t tb = 0;
-        cub::DeviceReduce::Reduce(nullptr, tb, w.dd_in.as<DD>(), w.gsum.as<DD>(), (int)N, DDAdd(), DD{0.0, 0.0}, st);
-        RGL_TRY(w.tmp.ensure(tb + 256));
-        tb = w.tmp.cap;
-        RGL_CUDA(cub::DeviceReduce::Reduce(w.tmp.p, tb, w.dd_in.as<DD>(), w.gsum.as<DD>(), (int)N, DDAdd(), DD{0.0, 0.0}, st));
-    }
-    k_center<<<blocks_for(M), 256, 0, st>>>(N, M, w.g.as<float>(), w.gsum.as<DD>(), w.fa.as<double2>(), w.dd_in.as<DD>());
-    // exclusive prefix: U[s] = sum_{k<s} u[k] for s = 0..N -> inclusive scan of u shifted by one
-    RGL_TRY(dd_scan(w, N + 1, st));  // dd_out[s] = sum_{k<=s} u[k]
-    // U[0] = 0, U[s] = dd_out[s-1]
-    {
-        RGL_CUDA(cudaMemsetAsync(w.U.p, 0, 8, st));
-        k_dd_to_double<<<blocks_for(N), 256, 0, st>>>(N, w.dd_out.as<DD>(), w.U.as<double>() + 1);
-    }
-    // K6: A[m] = Re(FFT(|FFT(u)|^2))[m] / M
-    double2* X = nullptr;
-    RGL_TRY(fft_forward(w, M, st, &X));
-    k_power<<<blocks_for(M), 256, 0, st>>>(M, X);
-    if (X != w.fa.as<double2>()) RGL_CUDA(cudaMemcpyAsync(w.fa.p, X, M * 16, cudaMemcpyDeviceToDevice, st));
-    double2* Y = nullptr;
-    RGL_TRY(fft_forward(w, M, st, &Y));
-    // K7: prefix sums at the grid points
+    // K7 gather points: the L grid of the store
     const std::vector<uint64_t> grid = moment_grid(N);
     const uint32_t G = (uint32_t)grid.size();
     if (G != slots) return fail(RGL_ERR_INVALID_ARGUMENT, "moment table size does not match the L grid");
-    std::vector<uint64_t> at_l(G), at_lm1(G), at_r(G);
+    std::vector<uint64_t> at_l(G), at_r(G);
     for (uint32_t i = 0; i < G; i++) {
-        at_l[i] = grid[i] - 1;          // inclusive prefix over t < L  -> index L-1 (terms start at t = 0)
-        at_lm1[i] = grid[i] - 1;        // sum_{t=1}^{L-1}: term 0 is zero -> inclusive index L-1
-        at_r[i] = N - grid[i];          // UU(N-L+1) = sum_{s<=N-L} U[s]
+        at_l[i] = grid[i] - 1;  // inclusive prefix over t < L (the t = 0 term of P0 / P1 is zero)
+        at_r[i] = N - grid[i];  // UU(N-L+1) = sum_{s<=N-L} U[s]
     }
     RGL_TRY(w.at.ensure(G * 8 * 3ull + 64));
     RGL_TRY(w.gl.ensure(G * 8ull + 64));
@@ -517,26 +846,55 @@ int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_in
     RGL_CUDA(cudaMemcpyAsync(d_at, at_l.data(), G * 8, cudaMemcpyHostToDevice, st));
     RGL_CUDA(cudaMemcpyAsync(d_at + G, at_r.data(), G * 8, cudaMemcpyHostToDevice, st));
     RGL_CUDA(cudaMemcpyAsync(w.gl.p, grid.data(), G * 8, cudaMemcpyHostToDevice, st));
-    DD* outs = w.outs.as<DD>();  // P0, P1, Q, V, UU_L, UU_R (G each) + UU total
-    const double inv_m = 1.0 / (double)M;
-    const int terms[4] = {T_A, T_MA, T_U2, T_V2};
-    for (int q = 0; q < 4; q++) {
-        k_term<<<blocks_for(N + 1), 256, 0, st>>>(N + 1, terms[q], Y, inv_m, w.U.as<double>(), N, w.dd_in.as<DD>());
+    DD* outs = w.outs.as<DD>();  // P0, P1, Q, V, UU_L, UU_R (G each)
+    DD uu_total{0.0, 0.0};
+    double a0 = 0.0;
+    if (precision == RGL_MOM_FP32C) {
+        RGL_TRY(moments_ff(w, N, M, device, G, d_at, outs, &uu_total, &a0, st));
+    } else {
+        // K5: mean of g (double-double sum), centred signal, U = prefix of u
+        k_to_dd<<<blocks_for(N), 256, 0, st>>>(N, w.g.as<float>(), w.dd_in.as<DD>());
+        {
+            size_t tb = 0;
+            cub::DeviceReduce::Reduce(nullptr, tb, w.dd_in.as<DD>(), w.gsum.as<DD>(), (int)N, DDAdd(), DD{0.0, 0.0}, st);
+            RGL_TRY(w.tmp.ensure(tb + 256));
+            tb = w.tmp.cap;
+            RGL_CUDA(cub::DeviceReduce::Reduce(w.tmp.p, tb, w.dd_in.as<DD>(), w.gsum.as<DD>(), (int)N, DDAdd(),
+                                               DD{0.0, 0.0}, st));
+        }
+        k_center<<<blocks_for(M), 256, 0, st>>>(N, M, w.g.as<float>(), w.gsum.as<DD>(), w.fa.as<double2>(),
+                                                 w.dd_in.as<DD>());
+        // exclusive prefix: U[s] = sum_{k<s} u[k] for s = 0..N -> inclusive scan of u shifted by one
+        RGL_TRY(dd_scan(w, N + 1, st));  // dd_out[s] = sum_{k<=s} u[k]
+        RGL_CUDA(cudaMemsetAsync(w.U.p, 0, 8, st));
+        k_dd_to_double<<<blocks_for(N), 256, 0, st>>>(N, w.dd_out.as<DD>(), w.U.as<double>() + 1);
+        // K6: A[m] = Re(FFT(|FFT(u)|^2))[m] / M
+        double2* X = nullptr;
+        RGL_TRY(fft_forward(w, M, st, &X));
+        k_power<<<blocks_for(M), 256, 0, st>>>(M, X);
+        if (X != w.fa.as<double2>()) RGL_CUDA(cudaMemcpyAsync(w.fa.p, X, M * 16, cudaMemcpyDeviceToDevice, st));
+        double2* Y = nullptr;
+        RGL_TRY(fft_forward(w, M, st, &Y));
+        // K7: prefix sums at the grid points
+        const double inv_m = 1.0 / (double)M;
+        const int terms[4] = {T_A, T_MA, T_U2, T_V2};
+        for (int q = 0; q < 4; q++) {
+            k_term<<<blocks_for(N + 1), 256, 0, st>>>(N + 1, terms[q], Y, inv_m, w.U.as<double>(), N, w.dd_in.as<DD>());
+            RGL_TRY(dd_scan(w, N + 1, st));
+            k_gather<<<blocks_for(G), 256, 0, st>>>(G, d_at, w.dd_out.as<DD>(), outs + (uint64_t)q * G);
+        }
+        k_term<<<blocks_for(N + 1), 256, 0, st>>>(N + 1, T_U, Y, inv_m, w.U.as<double>(), N, w.dd_in.as<DD>());
         RGL_TRY(dd_scan(w, N + 1, st));
-        k_gather<<<blocks_for(G), 256, 0, st>>>(G, d_at, w.dd_out.as<DD>(), outs + (uint64_t)q * G);
+        // UU(L) = sum_{s<L} U[s] = inclusive[L-1]; UU(N-L+1) = inclusive[N-L]; UU(N+1) = inclusive[N]
+        k_gather<<<blocks_for(G), 256, 0, st>>>(G, d_at, w.dd_out.as<DD>(), outs + 4ull * G);
+        k_gather<<<blocks_for(G), 256, 0, st>>>(G, d_at + G, w.dd_out.as<DD>(), outs + 5ull * G);
+        double2 a0c;
+        RGL_CUDA(cudaMemcpyAsync(&uu_total, w.dd_out.as<DD>() + N, sizeof(DD), cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaMemcpyAsync(&a0c, Y, sizeof(double2), cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaStreamSynchronize(st));
+        a0 = a0c.x * inv_m;
     }
-    k_term<<<blocks_for(N + 1), 256, 0, st>>>(N + 1, T_U, Y, inv_m, w.U.as<double>(), N, w.dd_in.as<DD>());
-    RGL_TRY(dd_scan(w, N + 1, st));
-    // UU(L) = sum_{s<L} U[s] = inclusive[L-1]; UU(N-L+1) = inclusive[N-L]; UU(N+1) = inclusive[N]
-    k_gather<<<blocks_for(G), 256, 0, st>>>(G, d_at, w.dd_out.as<DD>(), outs + 4ull * G);
-    k_gather<<<blocks_for(G), 256, 0, st>>>(G, d_at + G, w.dd_out.as<DD>(), outs + 5ull * G);
-    DD uu_total, a0pair;
-    double2 a0c;
-    RGL_CUDA(cudaMemcpyAsync(&uu_total, w.dd_out.as<DD>() + N, sizeof(DD), cudaMemcpyDeviceToHost, st));
-    RGL_CUDA(cudaMemcpyAsync(&a0c, Y, sizeof(double2), cudaMemcpyDeviceToHost, st));
-    RGL_CUDA(cudaStreamSynchronize(st));
-    (void)a0pair;
-    const double a0 = a0c.x * inv_m;
+    // the final reduction and the variance subtraction, FP64 (both paths)
     DevBuf& dm = w.mv;
     RGL_TRY(dm.ensure(G * 16ull + 64));
     double* d_mean = mean_out ? dm.as<double>() : nullptr;
@@ -549,6 +907,11 @@ int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_in
     if (var_out) RGL_CUDA(cudaMemcpyAsync(var_out, d_var, G * 8, cudaMemcpyDeviceToHost, st));
     RGL_CUDA(cudaStreamSynchronize(st));
     return moments_mark(m, sid, chrom, G);
+}
+
+int rgl_moments_build(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl_interval* intervals, uint64_t n,
+                      uint32_t bin_size, double* mean_out, double* var_out) {
+    return rgl_moments_build_ex(m, sid, chrom, intervals, n, bin_size, RGL_MOM_FP64, mean_out, var_out);
 }
 
 }  // extern "C"
