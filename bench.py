@@ -70,7 +70,9 @@ def parse():
     ap.add_argument("--serve-seconds", type=float, default=5.0,
                     help="length of the Poisson arrival trace of the serving measurement (0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=200.0)
-    ap.add_argument("--only", choices=["all", "plain", "batched", "serving"], default="all",
+    ap.add_argument("--precision-sizes", type=int, default=4,
+                    help="signal sizes of the precision part (2^19, 2^21, 2^23, 2^25 bins; 0 skips it)")
+    ap.add_argument("--only", choices=["all", "plain", "batched", "serving", "precision"], default="all",
                     help="run one part only (profiling captures)")
     return ap.parse_args()
 
@@ -201,18 +203,6 @@ def measured_peak():
             return float(json.load(f)["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
-
-
-def profiled_traffic():
-    """dram bytes per sweep launch from the committed ncu summary, when one exists."""
-    p = os.path.join(ROOT, "profiles", "k_sweep_plain.md")
-    try:
-        for ln in open(p):
-            if ln.startswith("traffic_bytes_per_launch:"):
-                return float(ln.split(":", 1)[1].strip().split()[0])
-    except Exception:
-        pass
-    return None
 
 
 # ---------------------------------------------------------------------------------------------
@@ -412,7 +402,9 @@ def run_riggle(args, rank, world, local_rank, dist):
     achieved = alg_bytes / (per_launch_ms / 1e3) / 1e9
     peak, peak_kind = measured_peak()
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": profiled_traffic(), "kernel": "k_sweep + k_pairs (sweep stage)", "peak_source": peak_kind,
+                "traffic": None, "traffic_note": "DRAM bytes per launch are measured by ncu, not in this run: the "
+                                                  "committed capture of this workload is summarised in profiles/",
+                "kernel": "k_sweep + k_pairs (sweep stage)", "peak_source": peak_kind,
                 "sweep_ms_per_launch": per_launch_ms, "algorithmic_bytes_per_launch": alg_bytes}
 
     cpu = None
@@ -661,15 +653,34 @@ def serve_trace(srv, reqs, arrivals, hp):
     return infos
 
 
-def run_serving(args, dev, idx):
+def synthetic_moments(D, cl, file_sizes, device):
+    """A moment store for every (source, chromosome) of a synthetic database, with tables of the
+    right shape and plausible values (mean = L x the source's mean coverage per bin, variance
+    over-dispersed by (1 + L / 100)): the serving and batched stats stages are timed on it.  Their
+    cost does not depend on the values; the values themselves are pinned by the p-value tests."""
+    from riggle_b200 import api
+
+    nb = (np.asarray(cl, np.uint64) + 99) // 100
+    m = api.Moments(D, nb, device=device)
+    genome = float(np.sum(cl))
+    for c in range(len(cl)):
+        L = api.moment_grid(int(nb[c])).astype(np.float64)
+        for d in range(D):
+            cov = float(file_sizes[d]) * 600.0 / genome  # mean coverage per 100 bp bin
+            mv = np.stack([L * cov, L * cov * (1.0 + L / 100.0)], 1).astype(np.float32)
+            m.set(d, c, mv)
+    return m
+
+
+def run_serving(args, dev, idx, db_desc, moments=None):
     """Serving at the configured rate, then at five times it (for a shorter trace): continuous batching
     against one query file per launch on the same arrivals."""
-    base = serve_once(args, dev, idx, args.serve_rate, args.serve_seconds, 77)
-    high = serve_once(args, dev, idx, 5 * args.serve_rate, max(1.0, args.serve_seconds / 2.5), 78)
+    base = serve_once(args, dev, idx, args.serve_rate, args.serve_seconds, 77, db_desc, moments)
+    high = serve_once(args, dev, idx, 5 * args.serve_rate, max(1.0, args.serve_seconds / 2.5), 78, db_desc, moments)
     return dict(base, high_load=high)
 
 
-def serve_once(args, dev, idx, lam, T, seed):
+def serve_once(args, dev, idx, lam, T, seed, db_desc, moments):
     import torch
 
     import riggle_b200 as rg
@@ -696,8 +707,10 @@ def serve_once(args, dev, idx, lam, T, seed):
     reqs = [[(int(sh[b]), int(off[b]), int(off[b + 1])) for b in range(k * C_, (k + 1) * C_) if off[b + 1] > off[b]]
             for k in range(nreq)]
 
+    stats_kw = {"moments": moments, "shard_chrom": np.arange(len(cl), dtype=np.uint32)} if moments else {}
+
     def measure(**kw):
-        srv = rg.Server(idx, **kw)
+        srv = rg.Server(idx, **kw, **stats_kw)
         serve_trace(srv, reqs[:32], np.zeros(32), hp.value)  # warm-up burst
         srv.reset_stats()
         infos = serve_trace(srv, reqs, arr, hp.value)
@@ -712,16 +725,86 @@ def serve_once(args, dev, idx, lam, T, seed):
                 "requests_1e5": int(len(near)),
                 "sustained_query_intervals_per_s": st["intervals"] / max(1e-9, st["last_done_s"] - st["first_submit_s"]),
                 "batches": st["batches"], "mean_batch_requests": st["mean_batch_requests"],
-                "workers": st["workers"], "failed": st["failed"]}
+                "workers": st["workers"], "failed": st["failed"], "memory_limited_batches": st["memory_limited"],
+                "refused": st["refused"], "workspace_growth_bytes": st["grown_bytes"]}
 
     batched = measure()
     plain = measure(workers=1, max_batch_requests=1)
     lib.rgl_host_free(hp)
     return {"workload": f"serving: Poisson arrivals at {lam:g}/s for {T:g} s ({nreq} query files, log-uniform "
-                        "[1e3, 1e6] intervals) against the resident 64-file x 50k database; latency = submit to "
-                        "count and overlap rows in host memory",
+                        f"[1e3, 1e6] intervals) against the resident {db_desc}; latency = submit to count, overlap "
+                        + ("and p-value rows" if moments else "rows") + " in host memory; admission by free device "
+                        "memory at batch formation",
             "offered_query_intervals_per_s": float(sizes.sum()) / T, "requests": nreq,
             "continuous_batching": batched, "plain_one_file_per_launch": plain}
+
+
+# ---------------------------------------------------------------------------------------------
+# precision: the FFT sliding-window moments at 2^20-2^26 FFT lengths, FP64 and compensated FP32
+# ---------------------------------------------------------------------------------------------
+def run_precision(args, dev):
+    """Moments of one source's coverage at 64 bp bins on synthetic chromosomes of 2^19..2^25 bins
+    (FFT lengths 2^20..2^26), interval density of a config-1 database file (50k intervals per 3.6 Gbp
+    genome; 5% broad), with the FP64 and the compensated-FP32 device paths; errors against the oracle's
+    exact (double-double, direct) window moments for L in [2^8, 2^16] and the grid's edges, and the
+    resulting ln p error of one query file's p-values (oracle compute_analytic_stats fed the device's
+    moments vs the exact ones)."""
+    import riggle_b200 as rg
+    import oracle as O
+    from riggle_b200 import api
+
+    sizes = [1 << 19, 1 << 21, 1 << 23, 1 << 25][: max(1, args.precision_sizes)]
+    out = []
+    for nb in sizes:
+        span = nb * 64
+        n = max(2000, int(round(50_000 * span / 3.6e9)))
+        iv = rg.SynthSpec(31 + nb.bit_length(), np.array([span], np.uint32), [n], broad_fraction=0.05).block(0, 0)
+        g = O.depth_signal(iv[:, 0], iv[:, 1], nb, 64)
+        grid = O.moment_grid(nb)
+        mid = np.nonzero((grid >= 256) & (grid <= 65_536))[0]
+        sel = np.unique(np.concatenate([mid[:: max(1, len(mid) // 20)], [0, 10, 99, len(grid) - 1]]))
+        t0 = time.perf_counter()
+        em, ev = O.moments_exact(g, grid[sel], threads=0)
+        oracle_s = time.perf_counter() - t0
+        q = rg.SynthSpec(77 + nb.bit_length(), np.array([span], np.uint32), [4000]).block(0, 0)
+        groups = [(0, O.query_groups(q[:, 0], q[:, 1], 64))]
+        exact_tab = np.zeros((len(grid), 2), np.float32)
+        row = {"n_bins": nb, "fft_len": 1 << (2 * nb - 1).bit_length(), "bin_size": 64, "intervals": n,
+               "grid_entries": int(len(grid)), "checked_L": int(len(sel)), "oracle_s": oracle_s}
+        for prec in ("fp64", "fp32c"):
+            m = api.Moments(1, [nb], device=dev)
+            m.build(0, 0, iv, bin_size=64, report=False, precision=prec)  # warm-up (workspace, twiddles)
+            ts = []
+            for _ in range(2):
+                t0 = time.perf_counter()
+                mean, var = m.build(0, 0, iv, bin_size=64, report=True, precision=prec)
+                ts.append(time.perf_counter() - t0)
+            scale = np.maximum(np.abs(ev), 1e-12 * em * em + 1e-300)
+            ev_rel = np.abs(var[sel] - ev) / scale
+            em_rel = np.abs(mean[sel] - em) / np.maximum(np.abs(em), 1e-300)
+            # ln p of one query file against this source: device moments vs exact ones at the checked L
+            tab = np.stack([mean, var], 1).astype(np.float32)
+            ex = tab.copy()
+            ex[sel] = np.stack([em, ev], 1).astype(np.float32)
+            lp_err = None
+            w_dev = O.analytic_stats(groups, {0: (nb, tab)}, 200.0)
+            w_ex = O.analytic_stats(groups, {0: (nb, ex)}, 200.0)
+            if w_dev and w_ex and w_dev[1] is not None and w_ex[1] is not None:
+                lp_d = O.lib().orc_log_p(w_dev[1], 1, 1.0, 1.0)
+                lp_e = O.lib().orc_log_p(w_ex[1], 1, 1.0, 1.0)
+                lp_err = abs(lp_d - lp_e) / max(abs(lp_e), 1e-300)
+            row[prec] = {"build_ms": 1e3 * min(ts), "max_rel_err_mean": float(em_rel.max()),
+                         "max_rel_err_var": float(ev_rel.max()), "ln_p_rel_err": lp_err,
+                         "within_1e-6": bool(em_rel.max() < 1e-6 and ev_rel.max() < 1e-6)}
+            m.close()
+        out.append(row)
+    return {"workload": "config 3: one source's coverage at 64 bp bins, 2^19..2^25 bins (FFT 2^20..2^26), "
+                        "config-1 interval density; errors vs the oracle's exact window moments for L in "
+                        "[2^8, 2^16] (every ~20th grid L) and the grid's edges",
+            "fp64": "FP64 Stockham FFT, double-double prefix sums",
+            "fp32c": "compensated FP32: float-float FFT / power spectrum / prefix sums, FP64 only in the final "
+                     "per-L reduction and the variance subtraction",
+            "sizes": out}
 
 
 def main():

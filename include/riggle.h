@@ -566,18 +566,33 @@ int rgl_bed_batch_free(rgl_bed_batch* batch);
 /* ------------------------------------------------------------------------------------------ */
 typedef struct rgl_server rgl_server;
 
+/* Free device memory as the server sees it when it forms a batch (bytes); the default asks the
+ * CUDA runtime (cudaMemGetInfo).  Called with the server's queue lock held, from worker threads. */
+typedef uint64_t (*rgl_free_memory_fn)(void* user);
+
 typedef struct rgl_server_opts {
     uint32_t workers;               /* batches in flight at once (default 3; fewer when HBM is short) */
     uint32_t max_batch_requests;    /* requests per batch (default 256; 1 = one query file per launch) */
     uint64_t batch_intervals;       /* intervals per batch, also the largest admissible request (default 2^23) */
-    uint64_t hbm_reserve_bytes;     /* device memory left free when sizing workers (default 4 GiB) */
+    uint64_t hbm_reserve_bytes;     /* device memory every admission leaves free (default 4 GiB) */
     uint64_t max_pending_intervals; /* host queue bound: submit refuses beyond it (default 2^28) */
     rgl_query_opts query;           /* launch shape (zeros: defaults); RGL_QF_NO_OVERLAP */
+    uint64_t initial_intervals;     /* workspace each worker reserves at creation (default min(2^21,
+                                       batch_intervals)); batches beyond it grow the workspace when
+                                       free device memory admits them */
+    rgl_free_memory_fn free_memory; /* NULL: cudaMemGetInfo */
+    void* free_memory_user;
+    rgl_moments* moments;           /* non-NULL: every request also gets its p-values (stats stage) */
+    const uint32_t* shard_chrom;    /* index shard -> moment-store chromosome (UINT32_MAX: none) */
+    uint32_t num_shard_chrom;
+    uint32_t bin_size;              /* bin of the moment store (default 100) */
 } rgl_server_opts;
 
 /* One query file.  The server copies the block tables at submit; `intervals` (page-locked for
  * asynchronous copies) must stay valid until the request completes; counts / overlap_bp (D entries
- * each, overlap_bp may be NULL) are written when it completes.  Interval sids are ignored. */
+ * each, overlap_bp may be NULL) are written when it completes, and with a moment store p_value,
+ * llr, log_p and flags (D entries each, any may be NULL; as rgl_query_pvalues writes them for one
+ * row).  Interval sids are ignored. */
 typedef struct rgl_request {
     uint32_t num_blocks;
     const uint32_t* block_shards;  /* index shard of each block */
@@ -585,6 +600,10 @@ typedef struct rgl_request {
     const rgl_interval* intervals;
     uint32_t* counts;
     uint64_t* overlap_bp;
+    double* p_value;
+    double* llr;
+    double* log_p;
+    uint8_t* flags;
 } rgl_request;
 
 typedef struct rgl_request_info {
@@ -602,10 +621,18 @@ typedef struct rgl_server_stats {
     double mean_batch_requests;
     double p50_ms, p99_ms, p999_ms, max_ms, mean_ms; /* submit -> results in host memory */
     double first_submit_s, last_done_s;
-    double worker_bytes;        /* device memory reserved per worker */
+    double worker_bytes;        /* device memory of the first worker at creation */
+    uint64_t memory_limited;    /* batches closed early because free device memory admitted no more */
+    uint64_t refused;           /* requests failed with RGL_ERR_OOM: larger than free memory admits */
+    uint64_t grown_bytes;       /* device memory the workers' workspaces grew by after creation */
 } rgl_server_stats;
 
-/* Sizes the workers by free device memory (each reserves its workspace for batch_intervals). */
+/* Creates the workers (each with its initial workspace while free device memory allows).  A worker
+ * forms each batch from the oldest pending requests: a request joins when the batch stays within
+ * max_batch_requests and batch_intervals and the device memory the batch would add to the worker's
+ * workspace fits in the free memory (free_memory()) less hbm_reserve_bytes and less what other
+ * workers have been promised; a request that does not fit even alone is failed with RGL_ERR_OOM.
+ * The server's moment store (optional) must outlive it. */
 int rgl_server_create(rgl_index* index, const rgl_server_opts* opts, rgl_server** out);
 /* Queues one request; RGL_ERR_INVALID_ARGUMENT for a bad block table or a request larger than
  * batch_intervals, RGL_ERR_OOM when the queue is full. */

@@ -113,14 +113,21 @@ class TuneTrial(C.Structure):
                 ("sweep_ms", C.c_float)]
 
 
+FREE_MEMORY_FN = C.CFUNCTYPE(C.c_uint64, C.c_void_p)
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("workers", C.c_uint32), ("max_batch_requests", C.c_uint32), ("batch_intervals", C.c_uint64),
-                ("hbm_reserve_bytes", C.c_uint64), ("max_pending_intervals", C.c_uint64), ("query", QueryOpts)]
+                ("hbm_reserve_bytes", C.c_uint64), ("max_pending_intervals", C.c_uint64), ("query", QueryOpts),
+                ("initial_intervals", C.c_uint64), ("free_memory", FREE_MEMORY_FN), ("free_memory_user", C.c_void_p),
+                ("moments", C.c_void_p), ("shard_chrom", C.c_void_p), ("num_shard_chrom", C.c_uint32),
+                ("bin_size", C.c_uint32)]
 
 
 class Request(C.Structure):
     _fields_ = [("num_blocks", C.c_uint32), ("block_shards", C.c_void_p), ("block_offsets", C.c_void_p),
-                ("intervals", C.c_void_p), ("counts", C.c_void_p), ("overlap_bp", C.c_void_p)]
+                ("intervals", C.c_void_p), ("counts", C.c_void_p), ("overlap_bp", C.c_void_p),
+                ("p_value", C.c_void_p), ("llr", C.c_void_p), ("log_p", C.c_void_p), ("flags", C.c_void_p)]
 
 
 class RequestInfo(C.Structure):
@@ -137,7 +144,8 @@ class ServerStats(C.Structure):
                 ("batches", C.c_uint64), ("intervals", C.c_uint64), ("workers", C.c_uint32),
                 ("pending", C.c_uint32), ("mean_batch_requests", C.c_double), ("p50_ms", C.c_double),
                 ("p99_ms", C.c_double), ("p999_ms", C.c_double), ("max_ms", C.c_double), ("mean_ms", C.c_double),
-                ("first_submit_s", C.c_double), ("last_done_s", C.c_double), ("worker_bytes", C.c_double)]
+                ("first_submit_s", C.c_double), ("last_done_s", C.c_double), ("worker_bytes", C.c_double),
+                ("memory_limited", C.c_uint64), ("refused", C.c_uint64), ("grown_bytes", C.c_uint64)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -346,13 +346,21 @@ class BedBatch:
 
 class Server:
     """Request server over a resident Index (rgl_server_*): submit query files as they arrive, wait
-    for their count / overlap rows; p50/p99/p99.9 latency in stats()."""
+    for their count / overlap rows (and p-values with a moment store); p50/p99/p99.9 latency in
+    stats().  free_memory (optional): a Python callable returning the free device bytes the server
+    should assume when it forms a batch (admission tests); default: the CUDA runtime's figure."""
 
     def __init__(self, index, workers=0, max_batch_requests=0, batch_intervals=0, hbm_reserve_bytes=0,
-                 max_pending_intervals=0, counts_only=False, chunk=0, ctas_per_sm=0, pair_ratio=0):
+                 max_pending_intervals=0, counts_only=False, chunk=0, ctas_per_sm=0, pair_ratio=0,
+                 initial_intervals=0, free_memory=None, moments=None, shard_chrom=None, bin_size=0):
         self.index = index
+        self._fm = _lib.FREE_MEMORY_FN(lambda user: int(free_memory())) if free_memory else _lib.FREE_MEMORY_FN()
+        self._sc = None if shard_chrom is None else np.ascontiguousarray(shard_chrom, np.uint32)
+        self.with_stats = moments is not None
         o = _lib.ServerOpts(workers, max_batch_requests, batch_intervals, hbm_reserve_bytes, max_pending_intervals,
-                            Context._opts(chunk, ctas_per_sm, counts_only, pair_ratio))
+                            Context._opts(chunk, ctas_per_sm, counts_only, pair_ratio), initial_intervals, self._fm,
+                            None, moments._h if moments is not None else None, _ptr(self._sc),
+                            0 if self._sc is None else len(self._sc), bin_size)
         h = C.c_void_p()
         check(load().rgl_server_create(index._h, C.byref(o), C.byref(h)))
         self._h = h
@@ -379,22 +387,30 @@ class Server:
             ptr = intervals_ptr
         counts = np.zeros(D, np.uint32)
         bp = np.zeros(D, np.uint64) if with_overlap else None
-        keep += [shards, offs, counts, bp]
+        pv = None
+        if self.with_stats:
+            pv = {"p": np.ones(D), "llr": np.zeros(D), "lp": np.zeros(D), "flags": np.zeros(D, np.uint8)}
+        keep += [shards, offs, counts, bp, pv]
         req = _lib.Request(len(shards), _ptr(shards), _ptr(offs), C.c_void_p(ptr) if ptr else None, _ptr(counts),
-                           _ptr(bp))
+                           _ptr(bp), *((_ptr(pv["p"]), _ptr(pv["llr"]), _ptr(pv["lp"]), _ptr(pv["flags"]))
+                                       if pv else (None,) * 4))
         t = C.c_uint64()
         check(load().rgl_server_submit(self._h, C.byref(req), C.byref(t)))
-        self._live[t.value] = (keep, counts, bp)
+        self._live[t.value] = (keep, counts, bp, pv)
         return t.value
 
     def wait(self, ticket, timeout_ms=60_000):
-        """Returns (counts uint32[D], overlap_bp uint64[D] or None, info dict)."""
+        """Returns (counts uint32[D], overlap_bp uint64[D] or None, info dict); with a moment store
+        info["pvalues"] holds the request's p, llr, lp (ln p) and flags arrays."""
         info = _lib.RequestInfo()
         check(load().rgl_server_wait(self._h, ticket, timeout_ms, C.byref(info)))
-        _, counts, bp = self._live.pop(ticket)
+        _, counts, bp, pv = self._live.pop(ticket)
         if info.status:
             raise _lib.RiggleError(info.status, "request failed")
-        return counts, bp, info.as_dict()
+        d = info.as_dict()
+        if pv is not None:
+            d["pvalues"] = pv
+        return counts, bp, d
 
     def stats(self):
         st = _lib.ServerStats()

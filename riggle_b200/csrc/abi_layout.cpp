@@ -75,10 +75,16 @@ const FieldRec f_synth_spec[] = {RGL_F(rgl_synth_spec, seed),           RGL_F(rg
                                  RGL_F(rgl_synth_spec, sid_base)};
 const FieldRec f_server_opts[] = {RGL_F(rgl_server_opts, workers),         RGL_F(rgl_server_opts, max_batch_requests),
                                   RGL_F(rgl_server_opts, batch_intervals), RGL_F(rgl_server_opts, hbm_reserve_bytes),
-                                  RGL_F(rgl_server_opts, max_pending_intervals), RGL_F(rgl_server_opts, query)};
+                                  RGL_F(rgl_server_opts, max_pending_intervals), RGL_F(rgl_server_opts, query),
+                                  RGL_F(rgl_server_opts, initial_intervals), RGL_F(rgl_server_opts, free_memory),
+                                  RGL_F(rgl_server_opts, free_memory_user), RGL_F(rgl_server_opts, moments),
+                                  RGL_F(rgl_server_opts, shard_chrom), RGL_F(rgl_server_opts, num_shard_chrom),
+                                  RGL_F(rgl_server_opts, bin_size)};
 const FieldRec f_request[] = {RGL_F(rgl_request, num_blocks), RGL_F(rgl_request, block_shards),
                               RGL_F(rgl_request, block_offsets), RGL_F(rgl_request, intervals),
-                              RGL_F(rgl_request, counts),     RGL_F(rgl_request, overlap_bp)};
+                              RGL_F(rgl_request, counts),     RGL_F(rgl_request, overlap_bp),
+                              RGL_F(rgl_request, p_value),    RGL_F(rgl_request, llr),
+                              RGL_F(rgl_request, log_p),      RGL_F(rgl_request, flags)};
 const FieldRec f_request_info[] = {RGL_F(rgl_request_info, status),          RGL_F(rgl_request_info, batch_requests),
                                    RGL_F(rgl_request_info, batch_intervals), RGL_F(rgl_request_info, intervals),
                                    RGL_F(rgl_request_info, submit_s),        RGL_F(rgl_request_info, start_s),
@@ -90,7 +96,9 @@ const FieldRec f_server_stats[] = {RGL_F(rgl_server_stats, submitted),      RGL_
                                    RGL_F(rgl_server_stats, p50_ms),         RGL_F(rgl_server_stats, p99_ms),
                                    RGL_F(rgl_server_stats, p999_ms),        RGL_F(rgl_server_stats, max_ms),
                                    RGL_F(rgl_server_stats, mean_ms),        RGL_F(rgl_server_stats, first_submit_s),
-                                   RGL_F(rgl_server_stats, last_done_s),    RGL_F(rgl_server_stats, worker_bytes)};
+                                   RGL_F(rgl_server_stats, last_done_s),    RGL_F(rgl_server_stats, worker_bytes),
+                                   RGL_F(rgl_server_stats, memory_limited), RGL_F(rgl_server_stats, refused),
+                                   RGL_F(rgl_server_stats, grown_bytes)};
 
 const StructRec g_structs[] = {
     RGL_S(rgl_interval, f_interval),       RGL_S(rgl_layer_desc, f_layer_desc),

@@ -81,6 +81,11 @@ struct DevBuf {
     }
 };
 
+// Scratch of the batched stats stage (query length groups of a batch); one per concurrent caller.
+struct StatsScratch {
+    DevBuf key_a, key_b, len_a, len_b, ukey, agg, runs, groups, goff, tmp;
+};
+
 }  // namespace rgl
 
 struct rgl_index {
@@ -151,6 +156,9 @@ int bed_read_all(const std::vector<std::string>& paths, uint32_t sid0, uint32_t 
 // ---- query contexts, for the request server --------------------------------------------------
 cudaStream_t context_stream(rgl_context* c);
 int context_reserve_rows(rgl_context* c, uint64_t max_intervals, uint32_t max_rows, uint32_t max_blocks);
+// Device bytes that running n intervals, `rows` rows and nblk blocks would add to the context's
+// workspace (0 when it is already large enough); allocates nothing.
+int context_growth_bytes(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uint64_t* bytes);
 // One batch with rows taken from the blocks (interval sids ignored); asynchronous on the context
 // stream.  off holds nblk + 1 element offsets into d_iv.
 int enqueue_block_rows(rgl_context* c, uint32_t num_rows, uint32_t nblk, const uint32_t* shards, const uint32_t* rows,
@@ -158,6 +166,15 @@ int enqueue_block_rows(rgl_context* c, uint32_t num_rows, uint32_t nblk, const u
                        unsigned long long* d_bp);
 // Error bits of the last run, read after the stream has been synchronised.
 int context_errors(rgl_context* c);
+// The stats stage of rgl_batch_pvalues_device with caller-owned scratch (so that several workers
+// can run it at once on one moment store), asynchronous on the context stream unless out_groups.
+int batch_pvalues_enqueue(rgl_context* ctx, rgl_moments* m, StatsScratch* sc, const rgl_batch* b,
+                          const uint32_t* shard_chrom, uint32_t num_shards, uint32_t bin_size, const uint32_t* d_counts,
+                          const uint64_t* d_overlap_bp, double* d_p, double* d_llr, double* d_log_p, uint8_t* d_flags,
+                          uint64_t* out_groups);
+// Builds the moment store's shared device tables once (thread-safe).
+int moments_prepare(rgl_moments* m);
+void stats_scratch_release(StatsScratch* sc);
 uint32_t context_last_launches(rgl_context* c);
 
 }  // namespace rgl

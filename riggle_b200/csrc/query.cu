@@ -1261,61 +1261,73 @@ constexpr uint64_t kPdlMaxIntervals = 1ull << 21;
 // Query intervals per pipeline run: the rank tables (up to 10 entries per interval) use 31-bit offsets.
 constexpr uint64_t kMaxRunIntervals = 200000000ull;
 
-int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
+// Sizes every workspace buffer for a run of n query intervals, `rows` output rows and nblk input
+// blocks.  With plan != nullptr nothing is allocated: *plan receives the bytes that growing the
+// buffers would add (a buffer grows by freeing and reallocating it at the larger size).
+int size_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uint64_t* plan) {
     rgl_index* idx = c->idx;
     if (n > kMaxRunIntervals) return fail(RGL_ERR_INVALID_ARGUMENT, "at most 200,000,000 query intervals per run");
     const uint64_t ns = std::max<uint32_t>(idx->num_slots, 1);
     const uint64_t tot = n * ns;
-    RGL_TRY(c->iv.ensure(n * sizeof(rgl_interval) + 16));
-    RGL_TRY(c->blk_off.ensure((nblk + 1) * 8ull));
-    RGL_TRY(c->blk_shard.ensure((nblk + 1) * 4ull));
-    RGL_TRY(c->key_a.ensure(n * 8 + 8));
-    RGL_TRY(c->key_b.ensure(n * 8 + 8));
-    RGL_TRY(c->val_a.ensure(n * 4 + 4));
-    RGL_TRY(c->val_b.ensure(n * 4 + 4));
-    RGL_TRY(c->ekey_a.ensure(n * 8 + 8));
-    RGL_TRY(c->ekey_b.ensure(n * 8 + 8));
-    RGL_TRY(c->starts.ensure(n * 4 + 4));
-    RGL_TRY(c->ends.ensure(n * 4 + 4));
-    RGL_TRY(c->seg.ensure(n * 4 + 4));
-    RGL_TRY(c->segflag.ensure(n * 4 + 4));
-    RGL_TRY(c->segnum.ensure(n * 4 + 4));
-    RGL_TRY(c->seg_begin.ensure(n * 4 + 4));
-    RGL_TRY(c->seg_need.ensure(n * 8 + 8));
-    RGL_TRY(c->ps_in.ensure(n * 8 + 16));
-    RGL_TRY(c->pe_in.ensure(n * 8 + 16));
-    RGL_TRY(c->ps.ensure(n * 8 + 16));
-    RGL_TRY(c->pe.ensure(n * 8 + 16));
-    RGL_TRY(c->lo.ensure(tot * 4 + 4));
-    RGL_TRY(c->hi.ensure(tot * 4 + 4));
-    RGL_TRY(c->maxhi.ensure(tot * 4 + 4));
-    RGL_TRY(c->rflag.ensure(tot * 4 + 8));
-    RGL_TRY(c->ridx.ensure(tot * 4 + 8));
-    RGL_TRY(c->ranges.ensure(tot * sizeof(RangeDesc) + sizeof(RangeDesc)));
-    RGL_TRY(c->rlen.ensure(tot * 8 + 16));
-    RGL_TRY(c->rpos.ensure(tot * 8 + 16));
-    RGL_TRY(c->small.ensure(256));
-    RGL_TRY(c->item_r0.ensure(kItemCap * 4));
-    RGL_TRY(c->item_t0.ensure(kItemCap * 4));
-    RGL_TRY(c->cl.ensure(tot * 8 + 16));
-    RGL_TRY(c->pc.ensure(tot * 8 + 16));
-    RGL_TRY(c->method.ensure(tot + 16));
-    RGL_TRY(c->lpos.ensure(tot * 4 + 8));
-    RGL_TRY(c->tl.ensure(tot * 4 + 8));
-    RGL_TRY(c->scan_sums.ensure((std::max<uint64_t>(tot, 10 * n + 16) / kScanTile + 4) * 8));
-    RGL_TRY(c->scan_sums2.ensure((10 * n + 16) / kScanTile * 8 + 32));
-    RGL_TRY(c->plen.ensure(tot * 8 + 16));
-    RGL_TRY(c->ppos.ensure(tot * 8 + 16));
-    RGL_TRY(c->psegs.ensure(tot * sizeof(PairSeg) + sizeof(PairSeg)));
-    RGL_TRY(c->segtab.ensure((n + 1) * sizeof(SegTab)));
-    RGL_TRY(c->tab_len.ensure((n + 2) * 4));
-    RGL_TRY(c->tab_off.ensure((n + 2) * 4));
-    RGL_TRY(c->tab_s.ensure((10 * n + 18) * 4));
-    RGL_TRY(c->tab_e.ensure((10 * n + 18) * 4));
-    RGL_TRY(c->tab2.ensure((10 * n + 18) * 8));
-    RGL_TRY(c->tab_xs.ensure((10 * n + 16) * 4));
-    RGL_TRY(c->tab_xe.ensure((10 * n + 16) * 4));
-    RGL_TRY(c->acc.ensure(64));
+    if (plan) *plan = 0;
+    struct Sizer {
+        uint64_t* plan;
+        int ensure_in(DevBuf& b, size_t bytes) {
+            if (!plan) return b.ensure(bytes);
+            if (bytes > b.cap) *plan += bytes - b.cap;
+            return RGL_OK;
+        }
+    } z{plan};
+    RGL_TRY(z.ensure_in(c->iv, n * sizeof(rgl_interval) + 16));
+    RGL_TRY(z.ensure_in(c->blk_off, (nblk + 1) * 8ull));
+    RGL_TRY(z.ensure_in(c->blk_shard, (nblk + 1) * 4ull));
+    RGL_TRY(z.ensure_in(c->key_a, n * 8 + 8));
+    RGL_TRY(z.ensure_in(c->key_b, n * 8 + 8));
+    RGL_TRY(z.ensure_in(c->val_a, n * 4 + 4));
+    RGL_TRY(z.ensure_in(c->val_b, n * 4 + 4));
+    RGL_TRY(z.ensure_in(c->ekey_a, n * 8 + 8));
+    RGL_TRY(z.ensure_in(c->ekey_b, n * 8 + 8));
+    RGL_TRY(z.ensure_in(c->starts, n * 4 + 4));
+    RGL_TRY(z.ensure_in(c->ends, n * 4 + 4));
+    RGL_TRY(z.ensure_in(c->seg, n * 4 + 4));
+    RGL_TRY(z.ensure_in(c->segflag, n * 4 + 4));
+    RGL_TRY(z.ensure_in(c->segnum, n * 4 + 4));
+    RGL_TRY(z.ensure_in(c->seg_begin, n * 4 + 4));
+    RGL_TRY(z.ensure_in(c->seg_need, n * 8 + 8));
+    RGL_TRY(z.ensure_in(c->ps_in, n * 8 + 16));
+    RGL_TRY(z.ensure_in(c->pe_in, n * 8 + 16));
+    RGL_TRY(z.ensure_in(c->ps, n * 8 + 16));
+    RGL_TRY(z.ensure_in(c->pe, n * 8 + 16));
+    RGL_TRY(z.ensure_in(c->lo, tot * 4 + 4));
+    RGL_TRY(z.ensure_in(c->hi, tot * 4 + 4));
+    RGL_TRY(z.ensure_in(c->maxhi, tot * 4 + 4));
+    RGL_TRY(z.ensure_in(c->rflag, tot * 4 + 8));
+    RGL_TRY(z.ensure_in(c->ridx, tot * 4 + 8));
+    RGL_TRY(z.ensure_in(c->ranges, tot * sizeof(RangeDesc) + sizeof(RangeDesc)));
+    RGL_TRY(z.ensure_in(c->rlen, tot * 8 + 16));
+    RGL_TRY(z.ensure_in(c->rpos, tot * 8 + 16));
+    RGL_TRY(z.ensure_in(c->small, 256));
+    RGL_TRY(z.ensure_in(c->item_r0, kItemCap * 4));
+    RGL_TRY(z.ensure_in(c->item_t0, kItemCap * 4));
+    RGL_TRY(z.ensure_in(c->cl, tot * 8 + 16));
+    RGL_TRY(z.ensure_in(c->pc, tot * 8 + 16));
+    RGL_TRY(z.ensure_in(c->method, tot + 16));
+    RGL_TRY(z.ensure_in(c->lpos, tot * 4 + 8));
+    RGL_TRY(z.ensure_in(c->tl, tot * 4 + 8));
+    RGL_TRY(z.ensure_in(c->scan_sums, (std::max<uint64_t>(tot, 10 * n + 16) / kScanTile + 4) * 8));
+    RGL_TRY(z.ensure_in(c->scan_sums2, (10 * n + 16) / kScanTile * 8 + 32));
+    RGL_TRY(z.ensure_in(c->plen, tot * 8 + 16));
+    RGL_TRY(z.ensure_in(c->ppos, tot * 8 + 16));
+    RGL_TRY(z.ensure_in(c->psegs, tot * sizeof(PairSeg) + sizeof(PairSeg)));
+    RGL_TRY(z.ensure_in(c->segtab, (n + 1) * sizeof(SegTab)));
+    RGL_TRY(z.ensure_in(c->tab_len, (n + 2) * 4));
+    RGL_TRY(z.ensure_in(c->tab_off, (n + 2) * 4));
+    RGL_TRY(z.ensure_in(c->tab_s, (10 * n + 18) * 4));
+    RGL_TRY(z.ensure_in(c->tab_e, (10 * n + 18) * 4));
+    RGL_TRY(z.ensure_in(c->tab2, (10 * n + 18) * 8));
+    RGL_TRY(z.ensure_in(c->tab_xs, (10 * n + 16) * 4));
+    RGL_TRY(z.ensure_in(c->tab_xe, (10 * n + 16) * 4));
+    RGL_TRY(z.ensure_in(c->acc, 64));
     // CUB temporary storage: the maximum over every primitive used, at these sizes.
     size_t need = 0, b = 0;
     int nn = (int)std::max<uint64_t>(n, 1);
@@ -1345,12 +1357,13 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
     need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nt, c->stream);
     need = std::max(need, b);
-    RGL_TRY(c->cub_tmp.ensure(need + 256));
-    RGL_TRY(c->cub_tmp2.ensure(need + 256));
+    RGL_TRY(z.ensure_in(c->cub_tmp, need + 256));
+    RGL_TRY(z.ensure_in(c->cub_tmp2, need + 256));
     if (rows) {
-        RGL_TRY(c->out_counts.ensure((uint64_t)rows * idx->num_sources * 4 + 16));
-        RGL_TRY(c->out_bp.ensure((uint64_t)rows * idx->num_sources * 8 + 16));
+        RGL_TRY(z.ensure_in(c->out_counts, (uint64_t)rows * idx->num_sources * 4 + 16));
+        RGL_TRY(z.ensure_in(c->out_bp, (uint64_t)rows * idx->num_sources * 8 + 16));
     }
+    if (plan) return RGL_OK;
     c->res_n = std::max(c->res_n, n);
     c->res_rows = std::max(c->res_rows, rows);
     uint64_t sig = 1469598103934665603ull;
@@ -1363,6 +1376,10 @@ int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
         sig = (sig ^ (uint64_t)(uintptr_t)b->p ^ ((uint64_t)b->cap << 17)) * 1099511628211ull;
     c->ws_sig = sig;
     return RGL_OK;
+}
+
+int ensure_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk) {
+    return size_workspace(c, n, rows, nblk, nullptr);
 }
 
 inline unsigned grid_for(uint64_t n, unsigned block) { return (unsigned)((n + block - 1) / block); }
@@ -1973,6 +1990,10 @@ cudaStream_t context_stream(rgl_context* c) { return c->stream; }
 int context_reserve_rows(rgl_context* c, uint64_t max_intervals, uint32_t max_rows, uint32_t max_blocks) {
     RGL_CUDA(cudaSetDevice(c->idx->device));
     return ensure_workspace(c, max_intervals, max_rows, max_blocks);
+}
+
+int context_growth_bytes(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uint64_t* bytes) {
+    return size_workspace(c, n, rows, nblk, bytes);
 }
 
 // One batch whose intervals are already on the device, rows taken from the blocks (interval sids are

@@ -1,13 +1,18 @@
 // Request server: continuous batching of query files against a resident index.
 //
 // Worker threads each own a query context (its own CUDA stream and workspace), a device staging
-// buffer for the intervals of one batch and page-locked output rows.  An idle worker takes the
-// oldest pending requests that fit its capacity (intervals and rows) as one batch: one host-to-device
-// copy per request, one pipeline run with the rows taken from the blocks, one device-to-host copy of
-// the batch's count and overlap rows, then the rows are handed to their requests.  With several
-// workers, requests that arrive while a batch is on the GPU start on another stream at once, so
-// their work overlaps on the device.  Workers are admitted by free device memory at creation: each
-// reserves its full workspace up front, so a running server never allocates device memory.
+// buffer for the intervals of one batch, device and page-locked output rows and, with a moment
+// store, their own scratch for the stats stage.  An idle worker takes the oldest pending requests
+// as one batch: one host-to-device copy per request, one pipeline run with the rows taken from the
+// blocks, the p-values of the batch's rows when the server has a moment store, one device-to-host
+// copy of each output, then the rows are handed to their requests.  With several workers, requests
+// that arrive while a batch is on the GPU start on another stream at once, so their work overlaps on
+// the device.
+//
+// Admission by free device memory happens when a batch is formed: a worker starts with a modest
+// workspace and a request joins its batch only while the memory the batch would add to the worker
+// (workspace, staging and output growth, computed without allocating) fits in the free memory less
+// the reserve and less what other workers have been promised but not yet allocated.
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -40,9 +45,12 @@ struct Req {
 
 struct Worker {
     rgl_context* ctx = nullptr;
-    DevBuf stage, dc, dbp;
+    DevBuf stage, dc, dbp, dp, dllr, dlp, dfl;
+    StatsScratch sc;  // the stats stage's scratch (per worker: several batches run at once)
     uint32_t* h_counts = nullptr;
     uint64_t* h_bp = nullptr;
+    double *h_p = nullptr, *h_llr = nullptr, *h_lp = nullptr;
+    uint8_t* h_fl = nullptr;
     std::thread th;
 };
 
@@ -67,7 +75,11 @@ struct rgl_server {
     bool stop = false;
     std::vector<std::unique_ptr<Worker>> workers;
     double worker_bytes = 0;
+    uint64_t promised = 0;  // device bytes admitted batches will still allocate
+    bool with_stats = false;
+    std::vector<uint32_t> shard_chrom;
     // stats
+    uint64_t memory_limited = 0, refused = 0, grown_bytes = 0;
     uint64_t submitted = 0, completed = 0, failed = 0, batches = 0, intervals = 0, batch_req_sum = 0;
     std::vector<double> lat_ms;
     double first_submit = -1, last_done = 0;
@@ -103,21 +115,96 @@ int run_batch(rgl_server* S, Worker* W, const std::vector<Req*>& batch) {
         }
     }
     unsigned long long* d_bp = S->with_bp ? W->dbp.as<unsigned long long>() : nullptr;
+    const size_t cells = (size_t)R * S->D;
     RGL_TRY(enqueue_block_rows(c, R, (uint32_t)shards.size(), shards.data(), rows.data(), off.data(),
                                W->stage.as<rgl_interval>(), &S->o.query, W->dc.as<uint32_t>(), d_bp));
-    RGL_CUDA(cudaMemcpyAsync(W->h_counts, W->dc.p, (size_t)R * S->D * 4, cudaMemcpyDeviceToHost, st));
-    if (d_bp) RGL_CUDA(cudaMemcpyAsync(W->h_bp, W->dbp.p, (size_t)R * S->D * 8, cudaMemcpyDeviceToHost, st));
+    if (S->with_stats) {
+        // the stats stage of the batch's rows: query length groups from the staged intervals,
+        // FP64 p-values of every (row, source) cell (compute_analytic_pvalues,
+        // src/tasks/query/pvalues.rs:22-77)
+        rgl_batch b{R, (uint32_t)shards.size(), shards.data(), rows.data(), off.data(), W->stage.as<rgl_interval>()};
+        RGL_TRY(batch_pvalues_enqueue(c, S->o.moments, &W->sc, &b, S->shard_chrom.data(),
+                                      (uint32_t)S->shard_chrom.size(), S->o.bin_size, W->dc.as<uint32_t>(),
+                                      W->dbp.as<uint64_t>(), W->dp.as<double>(), W->dllr.as<double>(),
+                                      W->dlp.as<double>(), W->dfl.as<uint8_t>(), nullptr));
+    }
+    RGL_CUDA(cudaMemcpyAsync(W->h_counts, W->dc.p, cells * 4, cudaMemcpyDeviceToHost, st));
+    if (d_bp) RGL_CUDA(cudaMemcpyAsync(W->h_bp, W->dbp.p, cells * 8, cudaMemcpyDeviceToHost, st));
+    if (S->with_stats) {
+        RGL_CUDA(cudaMemcpyAsync(W->h_p, W->dp.p, cells * 8, cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaMemcpyAsync(W->h_llr, W->dllr.p, cells * 8, cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaMemcpyAsync(W->h_lp, W->dlp.p, cells * 8, cudaMemcpyDeviceToHost, st));
+        RGL_CUDA(cudaMemcpyAsync(W->h_fl, W->dfl.p, cells, cudaMemcpyDeviceToHost, st));
+    }
     RGL_CUDA(cudaStreamSynchronize(st));
     RGL_TRY(context_errors(c));
+    const size_t D = S->D;
     for (uint32_t j = 0; j < R; j++) {
         const Req* q = batch[j];
-        if (q->r.counts) std::memcpy(q->r.counts, W->h_counts + (size_t)j * S->D, S->D * 4ull);
+        if (q->r.counts) std::memcpy(q->r.counts, W->h_counts + j * D, D * 4);
         if (q->r.overlap_bp) {
-            if (d_bp) std::memcpy(q->r.overlap_bp, W->h_bp + (size_t)j * S->D, S->D * 8ull);
-            else std::memset(q->r.overlap_bp, 0, S->D * 8ull);
+            if (d_bp) std::memcpy(q->r.overlap_bp, W->h_bp + j * D, D * 8);
+            else std::memset(q->r.overlap_bp, 0, D * 8);
+        }
+        if (S->with_stats) {
+            if (q->r.p_value) std::memcpy(q->r.p_value, W->h_p + j * D, D * 8);
+            if (q->r.llr) std::memcpy(q->r.llr, W->h_llr + j * D, D * 8);
+            if (q->r.log_p) std::memcpy(q->r.log_p, W->h_lp + j * D, D * 8);
+            if (q->r.flags) std::memcpy(q->r.flags, W->h_fl + j * D, D);
         }
     }
     return RGL_OK;
+}
+
+uint64_t grow(const DevBuf& b, uint64_t bytes) { return bytes > b.cap ? bytes - b.cap : 0; }
+
+// Device bytes worker W would allocate to run a batch of n intervals in nblk blocks over R rows.
+int batch_growth(rgl_server* S, Worker* W, uint64_t n, uint32_t R, uint32_t nblk, uint64_t* bytes) {
+    uint64_t ws = 0;
+    RGL_TRY(context_growth_bytes(W->ctx, n, 0, nblk, &ws));
+    const uint64_t cells = (uint64_t)R * S->D;
+    uint64_t b = ws + grow(W->stage, n * sizeof(rgl_interval)) + grow(W->dc, cells * 4 + 16) +
+                 grow(W->dbp, cells * 8 + 16);
+    if (S->with_stats) {
+        b += grow(W->dp, cells * 8 + 16) + grow(W->dllr, cells * 8 + 16) + grow(W->dlp, cells * 8 + 16) +
+             grow(W->dfl, cells + 16);
+        // the stats stage's scratch: keys, lengths, runs and groups per interval (StatsScratch)
+        b += grow(W->sc.key_a, n * 8 + 8) + grow(W->sc.key_b, n * 8 + 8) + grow(W->sc.len_a, n * 4 + 4) +
+             grow(W->sc.len_b, n * 4 + 4) + grow(W->sc.ukey, n * 8 + 8) + grow(W->sc.agg, n * 32 + 32) +
+             grow(W->sc.groups, n * 40 + 40);
+    }
+    *bytes = b;
+    return RGL_OK;
+}
+
+// Grows the worker's device buffers for a batch (the workspace grows inside the pipeline call).
+int size_worker(rgl_server* S, Worker* W, uint64_t n, uint32_t R) {
+    const uint64_t cells = (uint64_t)R * S->D;
+    RGL_TRY(W->stage.ensure(std::max<uint64_t>(n, 1) * sizeof(rgl_interval)));
+    RGL_TRY(W->dc.ensure(cells * 4 + 16));
+    RGL_TRY(W->dbp.ensure(cells * 8 + 16));
+    if (S->with_stats) {
+        RGL_TRY(W->dp.ensure(cells * 8 + 16));
+        RGL_TRY(W->dllr.ensure(cells * 8 + 16));
+        RGL_TRY(W->dlp.ensure(cells * 8 + 16));
+        RGL_TRY(W->dfl.ensure(cells + 16));
+        const uint64_t nn = std::max<uint64_t>(n, 1);
+        RGL_TRY(W->sc.key_a.ensure(nn * 8 + 8));
+        RGL_TRY(W->sc.key_b.ensure(nn * 8 + 8));
+        RGL_TRY(W->sc.len_a.ensure(nn * 4 + 4));
+        RGL_TRY(W->sc.len_b.ensure(nn * 4 + 4));
+        RGL_TRY(W->sc.ukey.ensure(nn * 8 + 8));
+        RGL_TRY(W->sc.agg.ensure(nn * 32 + 32));
+        RGL_TRY(W->sc.groups.ensure(nn * 40 + 40));
+    }
+    return RGL_OK;
+}
+
+uint64_t free_device_memory(rgl_server* S) {
+    if (S->o.free_memory) return S->o.free_memory(S->o.free_memory_user);
+    size_t f = 0, t = 0;
+    if (cudaMemGetInfo(&f, &t) != cudaSuccess) return 0;
+    return f;
 }
 
 void complete(rgl_server* S, const std::vector<Req*>& batch, const std::vector<int>& status, uint64_t n) {
@@ -145,27 +232,69 @@ void complete(rgl_server* S, const std::vector<Req*>& batch, const std::vector<i
 
 void worker_main(rgl_server* S, Worker* W) {
     cudaSetDevice(S->device);
-    std::vector<Req*> batch;
+    std::vector<Req*> batch, refused;
     for (;;) {
-        uint64_t n = 0;
+        uint64_t n = 0, promise = 0;
         {
             std::unique_lock<std::mutex> lk(S->mu);
             S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty(); });
             if (S->pending.empty()) return;  // stop requested and the queue is drained
             batch.clear();
+            refused.clear();
+            // admission: what the device can still give this worker now
+            const uint64_t free_b = free_device_memory(S);
+            const uint64_t keep = S->o.hbm_reserve_bytes + S->promised;
+            const uint64_t avail = free_b > keep ? free_b - keep : 0;
+            uint32_t nblk = 0;
             while (!S->pending.empty() && batch.size() < S->o.max_batch_requests) {
                 Req* q = S->pending.front();
                 if (!batch.empty() && n + q->n > S->o.batch_intervals) break;
+                uint64_t need = 0;
+                const uint32_t qb = (uint32_t)q->shards.size();
+                if (batch_growth(S, W, n + q->n, (uint32_t)batch.size() + 1, nblk + qb, &need) != RGL_OK) need = ~0ull;
+                if (need > avail) {
+                    if (!batch.empty()) {
+                        S->memory_limited++;
+                        break;
+                    }
+                    // not admissible even alone: fail it rather than wait for memory no one frees
+                    S->pending.pop_front();
+                    S->pending_n -= q->n;
+                    refused.push_back(q);
+                    continue;
+                }
+                promise = need;
                 batch.push_back(q);
                 n += q->n;
+                nblk += qb;
                 S->pending.pop_front();
             }
             S->pending_n -= n;
+            S->promised += promise;
             const double t = S->now();
             for (Req* q : batch) q->t_start = t;
         }
+        if (!refused.empty()) {
+            std::lock_guard<std::mutex> lk(S->mu);
+            const double t = S->now();
+            for (Req* q : refused) {
+                q->status = RGL_ERR_OOM;
+                q->t_start = q->t_done = t;
+                q->done = true;
+                S->failed++;
+                S->refused++;
+            }
+            S->cv_done.notify_all();
+        }
+        if (batch.empty()) continue;
         std::vector<int> status(batch.size(), RGL_OK);
-        int s = run_batch(S, W, batch);
+        int s = size_worker(S, W, n, (uint32_t)batch.size());
+        if (s == RGL_OK) s = run_batch(S, W, batch);
+        {
+            std::lock_guard<std::mutex> lk(S->mu);  // the growth has happened: free memory shows it now
+            S->promised -= promise;
+            S->grown_bytes += promise;
+        }
         if (s != RGL_OK && batch.size() > 1) {
             // isolate the failing request: every request of the batch again on its own
             std::vector<Req*> one(1);
@@ -183,25 +312,29 @@ void worker_main(rgl_server* S, Worker* W) {
 
 void destroy_worker(Worker* W) {
     if (W->ctx) rgl_context_destroy(W->ctx);
-    W->stage.release();
-    W->dc.release();
-    W->dbp.release();
-    if (W->h_counts) cudaFreeHost(W->h_counts);
-    if (W->h_bp) cudaFreeHost(W->h_bp);
+    for (DevBuf* b : {&W->stage, &W->dc, &W->dbp, &W->dp, &W->dllr, &W->dlp, &W->dfl}) b->release();
+    stats_scratch_release(&W->sc);
+    for (void* h : {(void*)W->h_counts, (void*)W->h_bp, (void*)W->h_p, (void*)W->h_llr, (void*)W->h_lp, (void*)W->h_fl})
+        if (h) cudaFreeHost(h);
 }
 
 int make_worker(rgl_server* S, Worker* W) {
     RGL_TRY(rgl_context_create(S->idx, nullptr, &W->ctx));
-    const uint64_t cap = S->o.batch_intervals;
+    const uint64_t cap = S->o.initial_intervals;
     const uint32_t R = S->o.max_batch_requests;
     // blocks per batch: at most one per (request, shard) for requests built from the shard list;
     // larger block tables grow the workspace on demand
     RGL_TRY(context_reserve_rows(W->ctx, cap, 0, R * std::max<uint32_t>(S->idx->num_shards, 1)));
-    RGL_TRY(W->stage.ensure(cap * sizeof(rgl_interval)));
-    RGL_TRY(W->dc.ensure((size_t)R * S->D * 4 + 16));
-    RGL_TRY(W->dbp.ensure((size_t)R * S->D * 8 + 16));
-    RGL_CUDA(cudaMallocHost(&W->h_counts, (size_t)R * S->D * 4 + 16));
-    RGL_CUDA(cudaMallocHost(&W->h_bp, (size_t)R * S->D * 8 + 16));
+    RGL_TRY(size_worker(S, W, cap, R));
+    const size_t cells = (size_t)R * S->D + 16;
+    RGL_CUDA(cudaMallocHost(&W->h_counts, cells * 4));
+    RGL_CUDA(cudaMallocHost(&W->h_bp, cells * 8));
+    if (S->with_stats) {
+        RGL_CUDA(cudaMallocHost(&W->h_p, cells * 8));
+        RGL_CUDA(cudaMallocHost(&W->h_llr, cells * 8));
+        RGL_CUDA(cudaMallocHost(&W->h_lp, cells * 8));
+        RGL_CUDA(cudaMallocHost(&W->h_fl, cells));
+    }
     return RGL_OK;
 }
 
@@ -225,12 +358,21 @@ int rgl_server_create(rgl_index* index, const rgl_server_opts* opts, rgl_server*
     if (!S->o.hbm_reserve_bytes) S->o.hbm_reserve_bytes = 4ull << 30;
     if (!S->o.max_pending_intervals) S->o.max_pending_intervals = 1ull << 28;
     S->o.batch_intervals = std::min<uint64_t>(S->o.batch_intervals, 200000000ull);  // one pipeline run
+    if (!S->o.initial_intervals) S->o.initial_intervals = 1ull << 21;
+    S->o.initial_intervals = std::min(S->o.initial_intervals, S->o.batch_intervals);
+    if (!S->o.bin_size) S->o.bin_size = 100;
     S->with_bp = !(S->o.query.flags & RGL_QF_NO_OVERLAP);
+    if (S->o.moments) {
+        if (!S->with_bp) return fail(RGL_ERR_INVALID_ARGUMENT, "the stats stage needs the overlap (no RGL_QF_NO_OVERLAP)");
+        if (S->o.num_shard_chrom && !S->o.shard_chrom) return fail(RGL_ERR_INVALID_ARGUMENT, "null shard_chrom");
+        S->with_stats = true;
+        S->shard_chrom.assign(S->o.shard_chrom, S->o.shard_chrom + S->o.num_shard_chrom);
+        RGL_TRY(moments_prepare(S->o.moments));
+    }
     RGL_CUDA(cudaSetDevice(S->device));
-    // admission of workers by free device memory: the first worker's reservation is the unit
+    // workers while free device memory (the provider's view) covers one more initial workspace
     for (uint32_t w = 0; w < S->o.workers; w++) {
-        size_t free0 = 0, total = 0;
-        RGL_CUDA(cudaMemGetInfo(&free0, &total));
+        const uint64_t free0 = free_device_memory(S.get());
         if (w > 0 && (double)free0 < S->worker_bytes + (double)S->o.hbm_reserve_bytes) break;
         auto W = std::make_unique<Worker>();
         int s = make_worker(S.get(), W.get());
@@ -243,8 +385,7 @@ int rgl_server_create(rgl_index* index, const rgl_server_opts* opts, rgl_server*
             clear_error();
             break;
         }
-        size_t free1 = 0;
-        RGL_CUDA(cudaMemGetInfo(&free1, &total));
+        const uint64_t free1 = free_device_memory(S.get());
         if (w == 0) S->worker_bytes = (double)(free0 > free1 ? free0 - free1 : 0);
         S->workers.push_back(std::move(W));
     }
@@ -333,6 +474,9 @@ int rgl_server_get_stats(rgl_server* S, rgl_server_stats* out) {
     out->first_submit_s = S->first_submit < 0 ? 0 : S->first_submit;
     out->last_done_s = S->last_done;
     out->worker_bytes = S->worker_bytes;
+    out->memory_limited = S->memory_limited;
+    out->refused = S->refused;
+    out->grown_bytes = S->grown_bytes;
     if (!S->lat_ms.empty()) {
         std::vector<double> v(S->lat_ms);
         std::sort(v.begin(), v.end());
@@ -356,6 +500,7 @@ int rgl_server_reset_stats(rgl_server* S) {
     if (!S) return fail(RGL_ERR_INVALID_ARGUMENT, "null server");
     std::lock_guard<std::mutex> lk(S->mu);
     S->submitted = S->completed = S->failed = S->batches = S->intervals = S->batch_req_sum = 0;
+    S->memory_limited = S->refused = 0;
     S->lat_ms.clear();
     S->first_submit = -1;
     S->last_done = 0;

@@ -186,6 +186,8 @@ struct LenToAgg {
 };
 
 constexpr uint64_t kNoGroup = ~0ull;
+// the request server sizes each worker's StatsScratch with these record sizes
+static_assert(sizeof(LenAgg) == 32 && sizeof(QGroupDev) == 40, "stats scratch record sizes changed");
 
 __global__ void k_group_keys(uint64_t n, const rgl_interval* __restrict__ iv, const uint64_t* __restrict__ blk_off,
                              const uint32_t* __restrict__ blk_shard, const uint32_t* __restrict__ blk_row, uint32_t nblk,
@@ -255,8 +257,14 @@ struct rgl_moments {
     float2* d_mv = nullptr;
     uint32_t* d_len = nullptr;
     std::vector<uint32_t> len;  // host mirror of the per-(source, chromosome) table lengths
-    // batched stats: compact_index table (slot of every l_int below the largest n_bins) and scratch
-    DevBuf slot_tab, coff, key_a, key_b, len_a, len_b, ukey, agg, runs, groups, goff, tmp, nb;
+    // batched stats: compact_index table (slot of every l_int below the largest n_bins), chromosome
+    // offsets and bin counts on the device (built once, under tab_mu), and the scratch of the
+    // public entry points (a request server gives each worker its own)
+    DevBuf slot_tab, coff, nb;
+    uint64_t lmax = 1;
+    bool tables_ready = false;
+    std::mutex tab_mu;
+    StatsScratch sc;
 };
 
 namespace rgl {
@@ -375,9 +383,8 @@ int rgl_moments_destroy(rgl_moments* m) {
     clear_error();
     if (!m) return RGL_OK;
     cudaSetDevice(m->device);
-    for (DevBuf* b : {&m->slot_tab, &m->coff, &m->key_a, &m->key_b, &m->len_a, &m->len_b, &m->ukey, &m->agg,
-                      &m->runs, &m->groups, &m->goff, &m->tmp, &m->nb})
-        b->release();
+    for (DevBuf* b : {&m->slot_tab, &m->coff, &m->nb}) b->release();
+    stats_scratch_release(&m->sc);
     if (m->d_mv) cudaFree(m->d_mv);
     if (m->d_len) cudaFree(m->d_len);
     delete m;
@@ -491,11 +498,47 @@ int rgl_query_pvalues(rgl_moments* m, const rgl_pvalue_batch* b, uint32_t bin_si
 
 }  // extern "C"
 
+namespace rgl {
+
+void stats_scratch_release(StatsScratch* sc) {
+    for (DevBuf* b : {&sc->key_a, &sc->key_b, &sc->len_a, &sc->len_b, &sc->ukey, &sc->agg, &sc->runs, &sc->groups,
+                      &sc->goff, &sc->tmp})
+        b->release();
+}
+
+// The device tables the batched stats stage reads: compact_index(l) for every l below the largest
+// chromosome's n_bins (on the host with the reference's f64 ln), chromosome offsets and bin counts.
+// Built once; later calls (any thread) return at once.
+int moments_prepare(rgl_moments* m) {
+    std::lock_guard<std::mutex> lk(m->tab_mu);
+    if (m->tables_ready) return RGL_OK;
+    DeviceScope scope;
+    RGL_TRY(scope.enter(m->device));
+    const uint32_t C = m->num_chroms;
+    uint64_t lmax = 1;
+    for (uint32_t c = 0; c < C; c++) lmax = std::max(lmax, m->n_bins[c]);
+    std::vector<uint32_t> tab(lmax);
+    tab[0] = 0xFFFFFFFFu;
+    for (uint64_t l = 1; l < lmax; l++) tab[l] = (uint32_t)compact_index(l);
+    RGL_TRY(m->slot_tab.ensure(lmax * 4));
+    RGL_CUDA(cudaMemcpy(m->slot_tab.p, tab.data(), lmax * 4, cudaMemcpyHostToDevice));
+    RGL_TRY(m->coff.ensure(C * 8ull + 8));
+    RGL_CUDA(cudaMemcpy(m->coff.p, m->chrom_off.data(), C * 8ull, cudaMemcpyHostToDevice));
+    RGL_TRY(m->nb.ensure(C * 8ull + 8));
+    RGL_CUDA(cudaMemcpy(m->nb.p, m->n_bins.data(), C * 8ull, cudaMemcpyHostToDevice));
+    m->lmax = lmax;
+    m->tables_ready = true;
+    return RGL_OK;
+}
+
+}  // namespace rgl
+
 // Enqueues the query length groups of a device batch on the context stream: m->groups holds them
 // (row-major, ascending (chromosome, l_int) within a row) and d_goff[0..rows] the per-row group
 // offsets.  *empty is set when there is nothing to do (no rows or no sources).
-static int enqueue_batch_groups(rgl_context* ctx, rgl_moments* m, const rgl_batch* b, const uint32_t* shard_chrom,
-                                uint32_t num_shards, uint32_t bin_size, bool* empty, uint64_t** goff_out) {
+static int enqueue_batch_groups(rgl_context* ctx, rgl_moments* m, StatsScratch* sc, const rgl_batch* b,
+                                const uint32_t* shard_chrom, uint32_t num_shards, uint32_t bin_size, bool* empty,
+                                uint64_t** goff_out) {
     if (!ctx || !m || !b || !bin_size || (num_shards && !shard_chrom))
         return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
     *empty = false;
@@ -519,19 +562,8 @@ static int enqueue_batch_groups(rgl_context* ctx, rgl_moments* m, const rgl_batc
     cudaStream_t st = context_stream(ctx);
     // slot table: compact_index(l) on the host with the reference's f64 ln, for every l below the
     // largest chromosome's n_bins; slots past a chromosome's grid are rejected per group below
-    uint64_t lmax = 1;
-    for (uint32_t c = 0; c < C; c++) lmax = std::max(lmax, m->n_bins[c]);
-    if (m->slot_tab.cap < lmax * 4) {
-        std::vector<uint32_t> tab(lmax);
-        tab[0] = 0xFFFFFFFFu;
-        for (uint64_t l = 1; l < lmax; l++) tab[l] = (uint32_t)compact_index(l);
-        RGL_TRY(m->slot_tab.ensure(lmax * 4));
-        RGL_CUDA(cudaMemcpy(m->slot_tab.p, tab.data(), lmax * 4, cudaMemcpyHostToDevice));
-        RGL_TRY(m->coff.ensure(C * 8ull));
-        RGL_CUDA(cudaMemcpy(m->coff.p, m->chrom_off.data(), C * 8ull, cudaMemcpyHostToDevice));
-        RGL_TRY(m->nb.ensure(C * 8ull));
-        RGL_CUDA(cudaMemcpy(m->nb.p, m->n_bins.data(), C * 8ull, cudaMemcpyHostToDevice));
-    }
+    RGL_TRY(moments_prepare(m));
+    const uint64_t lmax = m->lmax;
     const uint32_t nblk = b->num_blocks;
     std::vector<uint64_t> off(nblk + 1);
     for (uint32_t i = 0; i <= nblk; i++) off[i] = b->block_offsets[i] - b->block_offsets[0];
@@ -542,16 +574,16 @@ static int enqueue_batch_groups(rgl_context* ctx, rgl_moments* m, const rgl_batc
     }
     for (uint32_t i = 0; i < num_shards; i++) tabs[2ull * nblk + i] = shard_chrom[i];
     const uint64_t nn = std::max<uint64_t>(n, 1);
-    RGL_TRY(m->key_a.ensure(nn * 8));
-    RGL_TRY(m->key_b.ensure(nn * 8));
-    RGL_TRY(m->len_a.ensure(nn * 4));
-    RGL_TRY(m->len_b.ensure(nn * 4));
-    RGL_TRY(m->ukey.ensure(nn * 8));
-    RGL_TRY(m->agg.ensure(nn * sizeof(LenAgg)));
-    RGL_TRY(m->groups.ensure(nn * sizeof(QGroupDev)));
-    RGL_TRY(m->goff.ensure((rows + 1ull) * 8 + (nblk + 1ull) * 8 + tabs.size() * 4 + 64));
-    RGL_TRY(m->runs.ensure(64));
-    uint64_t* d_goff = m->goff.as<uint64_t>();
+    RGL_TRY(sc->key_a.ensure(nn * 8));
+    RGL_TRY(sc->key_b.ensure(nn * 8));
+    RGL_TRY(sc->len_a.ensure(nn * 4));
+    RGL_TRY(sc->len_b.ensure(nn * 4));
+    RGL_TRY(sc->ukey.ensure(nn * 8));
+    RGL_TRY(sc->agg.ensure(nn * sizeof(LenAgg)));
+    RGL_TRY(sc->groups.ensure(nn * sizeof(QGroupDev)));
+    RGL_TRY(sc->goff.ensure((rows + 1ull) * 8 + (nblk + 1ull) * 8 + tabs.size() * 4 + 64));
+    RGL_TRY(sc->runs.ensure(64));
+    uint64_t* d_goff = sc->goff.as<uint64_t>();
     uint64_t* d_boff = d_goff + rows + 1;
     uint32_t* d_tabs = reinterpret_cast<uint32_t*>(d_boff + nblk + 1);
     RGL_CUDA(cudaMemcpyAsync(d_boff, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st));
@@ -564,46 +596,45 @@ static int enqueue_batch_groups(rgl_context* ctx, rgl_moments* m, const rgl_batc
     cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint64_t*)nullptr, (uint64_t*)nullptr, (uint32_t*)nullptr,
                                     (uint32_t*)nullptr, (int)nn, 0, 64, st);
     need = std::max(need, tb);
-    thrust::transform_iterator<LenToAgg, const uint32_t*, LenAgg> vin(m->len_b.as<uint32_t>(), LenToAgg());
-    cub::DeviceReduce::ReduceByKey(nullptr, tb, m->key_b.as<uint64_t>(), m->ukey.as<uint64_t>(), vin,
-                                   m->agg.as<LenAgg>(), m->runs.as<uint32_t>(), LenAggOp(), (int)nn, st);
+    thrust::transform_iterator<LenToAgg, const uint32_t*, LenAgg> vin(sc->len_b.as<uint32_t>(), LenToAgg());
+    cub::DeviceReduce::ReduceByKey(nullptr, tb, sc->key_b.as<uint64_t>(), sc->ukey.as<uint64_t>(), vin,
+                                   sc->agg.as<LenAgg>(), sc->runs.as<uint32_t>(), LenAggOp(), (int)nn, st);
     need = std::max(need, tb);
-    RGL_TRY(m->tmp.ensure(need + 256));
+    RGL_TRY(sc->tmp.ensure(need + 256));
     if (n) {
         k_group_keys<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
             n, b->d_intervals + b->block_offsets[0], d_boff, d_tabs, d_tabs + nblk, nblk + 1, d_tabs + 2ull * nblk,
-            num_shards, C, m->nb.as<uint64_t>(), (double)bin_size, m->key_a.as<uint64_t>(), m->len_a.as<uint32_t>());
-        tb = m->tmp.cap;
-        RGL_CUDA(cub::DeviceRadixSort::SortPairs(m->tmp.p, tb, m->key_a.as<uint64_t>(), m->key_b.as<uint64_t>(),
-                                                 m->len_a.as<uint32_t>(), m->len_b.as<uint32_t>(), (int)n, 0,
+            num_shards, C, m->nb.as<uint64_t>(), (double)bin_size, sc->key_a.as<uint64_t>(), sc->len_a.as<uint32_t>());
+        tb = sc->tmp.cap;
+        RGL_CUDA(cub::DeviceRadixSort::SortPairs(sc->tmp.p, tb, sc->key_a.as<uint64_t>(), sc->key_b.as<uint64_t>(),
+                                                 sc->len_a.as<uint32_t>(), sc->len_b.as<uint32_t>(), (int)n, 0,
                                                  std::min(64, 32 + segbits), st));
-        tb = m->tmp.cap;
-        RGL_CUDA(cub::DeviceReduce::ReduceByKey(m->tmp.p, tb, m->key_b.as<uint64_t>(), m->ukey.as<uint64_t>(), vin,
-                                                m->agg.as<LenAgg>(), m->runs.as<uint32_t>(), LenAggOp(), (int)n, st));
+        tb = sc->tmp.cap;
+        RGL_CUDA(cub::DeviceReduce::ReduceByKey(sc->tmp.p, tb, sc->key_b.as<uint64_t>(), sc->ukey.as<uint64_t>(), vin,
+                                                sc->agg.as<LenAgg>(), sc->runs.as<uint32_t>(), LenAggOp(), (int)n, st));
     } else {
-        RGL_CUDA(cudaMemsetAsync(m->runs.p, 0, 4, st));
+        RGL_CUDA(cudaMemsetAsync(sc->runs.p, 0, 4, st));
     }
     k_group_finish<<<(unsigned)((nn + 256) / 256), 256, 0, st>>>(
-        m->ukey.as<uint64_t>(), m->agg.as<LenAgg>(), m->runs.as<uint32_t>(), rows, C, (double)bin_size,
-        m->slot_tab.as<uint32_t>(), lmax, m->groups.as<QGroupDev>(), d_goff);
+        sc->ukey.as<uint64_t>(), sc->agg.as<LenAgg>(), sc->runs.as<uint32_t>(), rows, C, (double)bin_size,
+        m->slot_tab.as<uint32_t>(), lmax, sc->groups.as<QGroupDev>(), d_goff);
     RGL_CUDA(cudaGetLastError());
     *goff_out = d_goff;
     return RGL_OK;
 }
 
-extern "C" {
+namespace rgl {
 
-int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* m, const rgl_batch* b, const uint32_t* shard_chrom,
-                             uint32_t num_shards, uint32_t bin_size, const uint32_t* d_counts,
-                             const uint64_t* d_overlap_bp, double* d_p, double* d_llr, double* d_log_p,
-                             uint8_t* d_flags, uint64_t* out_groups) {
-    clear_error();
+int batch_pvalues_enqueue(rgl_context* ctx, rgl_moments* m, StatsScratch* sc, const rgl_batch* b,
+                          const uint32_t* shard_chrom, uint32_t num_shards, uint32_t bin_size, const uint32_t* d_counts,
+                          const uint64_t* d_overlap_bp, double* d_p, double* d_llr, double* d_log_p, uint8_t* d_flags,
+                          uint64_t* out_groups) {
     if (!ctx || !m || !b || !d_counts || !d_overlap_bp || !d_p || !d_llr || !d_flags || !bin_size ||
         (num_shards && !shard_chrom))
         return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
     bool empty = false;
     uint64_t* d_goff = nullptr;
-    RGL_TRY(enqueue_batch_groups(ctx, m, b, shard_chrom, num_shards, bin_size, &empty, &d_goff));
+    RGL_TRY(enqueue_batch_groups(ctx, m, sc, b, shard_chrom, num_shards, bin_size, &empty, &d_goff));
     if (empty) {
         if (out_groups) *out_groups = 0;
         return RGL_OK;
@@ -617,17 +648,29 @@ int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* m, const rgl_batch* 
     const uint64_t warps = std::min<uint64_t>(cells, (uint64_t)nsm * 64);
     k_pvalues<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(
         rows, D, C, d_counts, reinterpret_cast<const unsigned long long*>(d_overlap_bp), (double)bin_size, d_goff,
-        m->groups.as<QGroupDev>(), m->d_mv, m->coff.as<uint64_t>(), m->stride, m->d_len, d_p, d_llr, d_log_p, d_flags);
+        sc->groups.as<QGroupDev>(), m->d_mv, m->coff.as<uint64_t>(), m->stride, m->d_len, d_p, d_llr, d_log_p, d_flags);
     RGL_CUDA(cudaGetLastError());
     if (out_groups) {
-        uint32_t runs = 0;
         uint64_t ng = 0;
-        RGL_CUDA(cudaMemcpyAsync(&runs, m->runs.p, 4, cudaMemcpyDeviceToHost, st));
         RGL_CUDA(cudaMemcpyAsync(&ng, d_goff + rows, 8, cudaMemcpyDeviceToHost, st));
         RGL_CUDA(cudaStreamSynchronize(st));
         *out_groups = ng;
     }
     return RGL_OK;
+}
+
+}  // namespace rgl
+
+extern "C" {
+
+int rgl_batch_pvalues_device(rgl_context* ctx, rgl_moments* m, const rgl_batch* b, const uint32_t* shard_chrom,
+                             uint32_t num_shards, uint32_t bin_size, const uint32_t* d_counts,
+                             const uint64_t* d_overlap_bp, double* d_p, double* d_llr, double* d_log_p,
+                             uint8_t* d_flags, uint64_t* out_groups) {
+    clear_error();
+    if (!m) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
+    return batch_pvalues_enqueue(ctx, m, &m->sc, b, shard_chrom, num_shards, bin_size, d_counts, d_overlap_bp, d_p,
+                                 d_llr, d_log_p, d_flags, out_groups);
 }
 
 int rgl_batch_query_groups(rgl_context* ctx, rgl_moments* m, const rgl_batch* b, const uint32_t* shard_chrom,
@@ -638,7 +681,7 @@ int rgl_batch_query_groups(rgl_context* ctx, rgl_moments* m, const rgl_batch* b,
     if (!out_groups) return fail(RGL_ERR_INVALID_ARGUMENT, "null argument");
     bool empty = false;
     uint64_t* d_goff = nullptr;
-    RGL_TRY(enqueue_batch_groups(ctx, m, b, shard_chrom, num_shards, bin_size, &empty, &d_goff));
+    RGL_TRY(enqueue_batch_groups(ctx, m, &m->sc, b, shard_chrom, num_shards, bin_size, &empty, &d_goff));
     const uint32_t rows = b->num_rows;
     if (empty) {
         if (row_group_offsets) std::fill(row_group_offsets, row_group_offsets + rows + 1, 0ull);
@@ -655,7 +698,7 @@ int rgl_batch_query_groups(rgl_context* ctx, rgl_moments* m, const rgl_batch* b,
     if (!group_chrom && !group_l_int && !group_sum_scale && !group_sum_scale2 && !group_count) return RGL_OK;
     if (ng > capacity) return fail(RGL_ERR_INVALID_ARGUMENT, "group capacity too small");
     std::vector<QGroupDev> g(ng);
-    if (ng) RGL_CUDA(cudaMemcpy(g.data(), m->groups.p, ng * sizeof(QGroupDev), cudaMemcpyDeviceToHost));
+    if (ng) RGL_CUDA(cudaMemcpy(g.data(), m->sc.groups.p, ng * sizeof(QGroupDev), cudaMemcpyDeviceToHost));
     for (uint64_t k = 0; k < ng; k++) {
         if (group_chrom) group_chrom[k] = g[k].chrom;
         if (group_l_int) group_l_int[k] = (uint64_t)g[k].l_int;

@@ -166,8 +166,8 @@ def _rust_layout(structs, name, memo):
         return memo[name]
     off, align, fields = 0, 1, []
     for f, t in structs[name]:
-        if t.startswith("*"):
-            fs = fa = 8
+        if t.startswith("*") or t.startswith("Option<unsafe extern") or t.startswith("Option<extern"):
+            fs = fa = 8  # raw pointers and nullable function pointers
         elif t in _RUST_SCALARS:
             fs = fa = _RUST_SCALARS[t]
         else:
