@@ -203,6 +203,8 @@ typedef struct rgl_query_opts {
 } rgl_query_opts;
 
 #define RGL_QF_NO_OVERLAP 1u /* skip base-pair accumulation (counts only) */
+#define RGL_QF_GLOBAL_TALLY 2u /* runs over several rows tally with atomics on the outputs instead of
+                                  block-local histograms of each work item's row (for comparisons) */
 
 typedef struct rgl_query_stats {
     uint64_t query_intervals;  /* intervals in the batch (on shards present in the index) */
@@ -274,7 +276,17 @@ typedef struct rgl_batch_opts {
     rgl_query_opts query; /* launch shape of every sub-batch (zeros: tuned shape or defaults) */
     uint64_t sub_batch;   /* query intervals per sub-batch, the unit of device workspace (0: 2^25) */
     uint32_t flags;       /* RGL_BF_* */
+    uint32_t region_bits; /* work order of a sub-batch of several rows: each row's intervals on a shard
+                             are cut into 2^region_bits-bp regions of their starts and the work is
+                             laid out region by region, every row's work on a region together, so the
+                             database intervals of a region are read from L2 by all rows after the
+                             first.  0: 24 for sub-batches of more than one row; RGL_BATCH_NO_REGIONS:
+                             one segment per (shard, row); else 16..31.  Results do not depend on it;
+                             the swept count (stats) grows by the look-back windows that cross
+                             region boundaries. */
 } rgl_batch_opts;
+
+#define RGL_BATCH_NO_REGIONS 32u
 
 #define RGL_BF_GRAPH 1u /* capture the batch as one CUDA graph and replay it while the batch (its block
                            tables, buffers and launch shape) is unchanged */

@@ -90,11 +90,13 @@ class BatchDesc(C.Structure):
 
 
 class BatchOpts(C.Structure):
-    _fields_ = [("query", QueryOpts), ("sub_batch", C.c_uint64), ("flags", C.c_uint32)]
+    _fields_ = [("query", QueryOpts), ("sub_batch", C.c_uint64), ("flags", C.c_uint32), ("region_bits", C.c_uint32)]
 
 
 RGL_BF_GRAPH = 1
 RGL_BF_TUNED = 2
+RGL_BATCH_NO_REGIONS = 32
+RGL_QF_GLOBAL_TALLY = 2
 
 
 class BatchStats(C.Structure):

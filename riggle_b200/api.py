@@ -222,18 +222,22 @@ class Context:
         return out
 
     def query_batch_device(self, batch, d_counts, d_bp=None, graph=False, tuned=False, sub_batch=0, chunk=0,
-                           ctas_per_sm=0, pair_ratio=0, counts_only=False, stats=True):
+                           ctas_per_sm=0, pair_ratio=0, counts_only=False, stats=True, region_bits=0,
+                           global_tally=False):
         """Batched form over a DeviceBatch; d_counts / d_bp are device pointers (int) to num_rows x D
         uint32 / uint64.  Returns the stats dict (synchronising) or None (asynchronous)."""
         flags = (_lib.RGL_BF_GRAPH if graph else 0) | (_lib.RGL_BF_TUNED if tuned else 0)
-        o = _lib.BatchOpts(self._opts(chunk, ctas_per_sm, counts_only, pair_ratio), int(sub_batch), flags)
+        q = self._opts(chunk, ctas_per_sm, counts_only, pair_ratio)
+        if global_tally:
+            q.flags |= _lib.RGL_QF_GLOBAL_TALLY
+        o = _lib.BatchOpts(q, int(sub_batch), flags, int(region_bits))
         st = _lib.BatchStats() if stats else None
         check(load().rgl_query_batch_device(self._h, C.byref(batch.c), C.byref(o), C.c_void_p(d_counts),
                                             C.c_void_p(d_bp) if d_bp else None, C.byref(st) if stats else None))
         return st.as_dict() if stats else None
 
     def query_batch_host(self, batch, h_intervals, with_overlap=True, tuned=False, sub_batch=0, chunk=0,
-                         ctas_per_sm=0, pair_ratio=0, out=None):
+                         ctas_per_sm=0, pair_ratio=0, out=None, region_bits=0):
         """Batched form with host intervals (uint32[n,3] array or an int pointer to pinned memory);
         returns (counts uint32[R, D], overlap_bp uint64[R, D] or None, stats dict)."""
         R, D = batch.num_rows, self.index.num_sources
@@ -248,7 +252,8 @@ class Context:
         else:
             hp = C.c_void_p(int(h_intervals))
         flags = _lib.RGL_BF_TUNED if tuned else 0
-        o = _lib.BatchOpts(self._opts(chunk, ctas_per_sm, not with_overlap, pair_ratio), int(sub_batch), flags)
+        o = _lib.BatchOpts(self._opts(chunk, ctas_per_sm, not with_overlap, pair_ratio), int(sub_batch), flags,
+                           int(region_bits))
         st = _lib.BatchStats()
         check(load().rgl_query_batch_host(self._h, C.byref(batch.c), hp, C.byref(o), _ptr(counts), _ptr(bp),
                                           C.byref(st)))

@@ -54,7 +54,7 @@ const FieldRec f_batch[] = {RGL_F(rgl_batch, num_rows),   RGL_F(rgl_batch, num_b
                             RGL_F(rgl_batch, block_shards), RGL_F(rgl_batch, block_rows),
                             RGL_F(rgl_batch, block_offsets), RGL_F(rgl_batch, d_intervals)};
 const FieldRec f_batch_opts[] = {RGL_F(rgl_batch_opts, query), RGL_F(rgl_batch_opts, sub_batch),
-                                 RGL_F(rgl_batch_opts, flags)};
+                                 RGL_F(rgl_batch_opts, flags), RGL_F(rgl_batch_opts, region_bits)};
 const FieldRec f_batch_stats[] = {RGL_F(rgl_batch_stats, query_intervals), RGL_F(rgl_batch_stats, db_swept),
                                   RGL_F(rgl_batch_stats, rank_positions),  RGL_F(rgl_batch_stats, pair_candidates),
                                   RGL_F(rgl_batch_stats, ranges),          RGL_F(rgl_batch_stats, sub_batches),

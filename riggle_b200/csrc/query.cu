@@ -145,7 +145,7 @@ __device__ __forceinline__ void pp_layer2(const uint2* __restrict__ pos, const u
 // ---- 1. keys ------------------------------------------------------------------------------------
 __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, const uint64_t* __restrict__ blk_off,
                               const uint32_t* __restrict__ blk_shard, const uint32_t* __restrict__ blk_row,
-                              int row_from_block, uint32_t nblk, uint32_t rows, uint32_t row_base,
+                              int row_from_block, uint32_t nblk, uint32_t rows, uint32_t row_base, uint32_t rb,
                               uint64_t* __restrict__ key, uint32_t* __restrict__ val, uint64_t* __restrict__ ekey,
                               uint32_t* __restrict__ err) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -163,7 +163,10 @@ __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, c
     if (s >= e) bad |= ERR_BAD_INTERVAL;
     if (q >= rows || (blk_row && row != blk_row[lo])) { bad |= ERR_BAD_ROW; q = 0; }
     if (bad) atomicOr(err, bad);
-    uint64_t seg = (uint64_t)blk_shard[lo] * rows + q;
+    // segment = (shard, region, row): with regions (rb > 0) a row's intervals on a shard are cut
+    // into 2^rb-bp regions of their starts, so that the rows' work on one region lies together
+    const uint64_t nreg = rb ? (1ull << (32 - rb)) : 1ull, reg = rb ? (s >> rb) : 0u;
+    uint64_t seg = ((uint64_t)blk_shard[lo] * nreg + reg) * rows + q;
     key[i] = (seg << 32) | s;
     val[i] = e;
     ekey[i] = (seg << 32) | e;
@@ -396,7 +399,7 @@ __global__ void k_tab_interleave(const uint32_t* __restrict__ count, const uint3
 
 // ---- 4. K1 partition -----------------------------------------------------------------------------
 // lo/hi of the reference's candidate scan for (slot K, query i), layer-major arrays [K][n].
-__global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_t* __restrict__ starts,
+__global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t seg_per_shard, const uint32_t* __restrict__ starts,
                        const uint32_t* __restrict__ qend, const uint32_t* __restrict__ seg,
                        const int32_t* __restrict__ slot, const LayerDev* __restrict__ layers,
                        const uint2* __restrict__ pos, const uint32_t* __restrict__ btab,
@@ -404,7 +407,7 @@ __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t rows, const uint32_
     uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (t >= (uint64_t)n * nslots) return;
     uint32_t K = (uint32_t)(t / n), i = (uint32_t)(t % n);
-    uint32_t shard = seg[i] / rows;
+    uint32_t shard = seg[i] / seg_per_shard;
     int32_t li = slot[(uint64_t)shard * nslots + K];
     uint32_t lo = 0, hi = 0;
     if (li >= 0) {
@@ -561,7 +564,7 @@ __global__ void k_crange_flags(const uint32_t* __restrict__ Lp, uint32_t n, cons
 
 template <bool PDL>
 __global__ void k_crange_emit(const uint32_t* __restrict__ Lp, uint32_t n, uint32_t nslots, uint32_t rows,
-                              const uint32_t* __restrict__ tl, const uint32_t* __restrict__ seg,
+                              uint32_t seg_per_shard, const uint32_t* __restrict__ tl, const uint32_t* __restrict__ seg,
                               const uint32_t* __restrict__ segnum, const int32_t* __restrict__ slot,
                               const uint32_t* __restrict__ lo, const uint32_t* __restrict__ maxhi,
                               const uint32_t* __restrict__ cflag, const uint32_t* __restrict__ cridx,
@@ -579,7 +582,7 @@ __global__ void k_crange_emit(const uint32_t* __restrict__ Lp, uint32_t n, uint3
             const uint32_t sg = seg[i];
             ranges[r].db_lo = lo[t];
             ranges[r].c_first = (uint32_t)c;
-            ranges[r].layer_idx = (uint32_t)slot[(uint64_t)(sg / rows) * nslots + K];
+            ranges[r].layer_idx = (uint32_t)slot[(uint64_t)(sg / seg_per_shard) * nslots + K];
             ranges[r].qrow = sg % rows;
             ranges[r].seg = segnum[i] - 1;
             ranges[r].slot = K;
@@ -630,7 +633,7 @@ __global__ void __launch_bounds__(256) k_crange_method(const uint32_t* __restric
 // Pair work space: each live run of a pair range contributes its candidates.
 template <bool PDL>
 __global__ void k_cpair_len(const uint32_t* __restrict__ Lp, uint32_t n, uint32_t nslots, uint32_t rows,
-                            const uint32_t* __restrict__ tl, const uint32_t* __restrict__ seg,
+                            uint32_t seg_per_shard, const uint32_t* __restrict__ tl, const uint32_t* __restrict__ seg,
                             const int32_t* __restrict__ slot, const LayerDev* __restrict__ layers,
                             const uint32_t* __restrict__ lo, const uint32_t* __restrict__ hi,
                             const uint32_t* __restrict__ cflag, const uint32_t* __restrict__ cridx,
@@ -648,9 +651,9 @@ __global__ void k_cpair_len(const uint32_t* __restrict__ Lp, uint32_t n, uint32_
         uint64_t len = 0;
         if (method[r] == M_PAIR) {
             const uint32_t sg = seg[i];
-            const int32_t li = slot[(uint64_t)(sg / rows) * nslots + K];
+            const int32_t li = slot[(uint64_t)(sg / seg_per_shard) * nslots + K];
             len = hi[t] - lo[t];
-            psegs[c] = PairSeg{layers[li].off + lo[t], starts[i], qend[i], sg % rows, sg / rows};
+            psegs[c] = PairSeg{layers[li].off + lo[t], starts[i], qend[i], sg % rows, sg / seg_per_shard};
         }
         plen[c] = len;
     }
@@ -821,10 +824,10 @@ __device__ __forceinline__ uint32_t ends_in(const SweepParams& P, uint32_t lo, u
 // One DB interval d with the table entries of its start's bin (a0, a1) and its end's bin (b0, b1):
 // count(d) = #{q.start < d.end} - #{q.end <= d.start}, and for a non-zero count the overlap
 // Cov(d.end) - Cov(d.start) and the tally.
-template <bool WITH_BP>
+template <bool WITH_BP, bool MULTI>
 __device__ __forceinline__ void sweep_one(const SweepParams& P, uint32_t qrow, uint2 d, uint32_t sid, uint2 a0,
                                           uint2 a1, uint2 b0, uint2 b1, uint32_t* s_cnt,
-                                          unsigned long long* s_bp) {
+                                          unsigned long long* s_bp, uint32_t cta_row) {
     const uint32_t el_s = ends_in(P, a0.y, a1.y, d.x);
     const uint32_t sl_e = starts_in(P, b0.x, b1.x, d.y);
     const uint32_t cnt = sl_e - el_s;
@@ -844,7 +847,9 @@ __device__ __forceinline__ void sweep_one(const SweepParams& P, uint32_t qrow, u
             bpv = ce - cs;
         }
     }
-    if (P.smem_tally) {
+    // one-row runs tally in the block's histogram; several-row runs (MULTI) in the histogram of the
+    // block's current row, and only the other rows in the output matrix
+    if (MULTI ? qrow == cta_row : P.smem_tally != 0) {
         atomicAdd(&s_cnt[sid], cnt);
         if (WITH_BP) add_u64(&s_bp[sid], bpv);
     } else {
@@ -854,10 +859,116 @@ __device__ __forceinline__ void sweep_one(const SweepParams& P, uint32_t qrow, u
     }
 }
 
+// Work items of the several-row sweeps are pulled by whole blocks: block item ci is the kCtaItems
+// warp items [ci * kCtaItems, (ci + 1) * kCtaItems), one per warp.
+constexpr uint32_t kCtaItems = 8;  // warps of a 256-thread block
+
+// The row of the middle of block item ci (its warp item ci * kCtaItems + kCtaItems / 2, or the last
+// item), from the first range (RANK) or run of that warp item: the row the block's histogram serves.
+template <bool RANK>
+__device__ __forceinline__ uint32_t cta_item_row(const SweepParams& P, uint32_t ci, uint64_t items, uint32_t rcap) {
+    const uint64_t wi = min((uint64_t)ci * kCtaItems + kCtaItems / 2, items - 1);
+    const uint64_t* off = RANK ? P.rpos : P.ppos;
+    uint32_t r;
+    if (wi < P.item_cap) {
+        r = __ldg((RANK ? P.item_r0 : P.item_t0) + wi);
+    } else {
+        const uint64_t p = wi * P.chunk;
+        uint64_t lo = 0, hi = rcap;
+        while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (__ldg(off + m) <= p) lo = m; else hi = m - 1; }
+        r = (uint32_t)lo;
+    }
+    return RANK ? P.ranges[r].qrow : P.psegs[r].qrow;
+}
+
+// Adds the block's histogram to row `row` of the outputs and clears it (between two __syncthreads).
+template <bool WITH_BP>
+__device__ __forceinline__ void flush_row(const SweepParams& P, uint32_t row, uint32_t* s_cnt,
+                                          unsigned long long* s_bp) {
+    const uint64_t base = (uint64_t)row * P.D;
+    for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
+        const uint32_t c = s_cnt[k];
+        if (c) {
+            atomicAdd(&P.counts[base + k], c);
+            s_cnt[k] = 0;
+        }
+        if (WITH_BP) {
+            const unsigned long long b = s_bp[k];
+            if (b) {
+                atomicAdd(&P.bp[base + k], b);
+                s_bp[k] = 0;
+            }
+        }
+    }
+}
+
 constexpr uint32_t kUnroll = 2;      // DB intervals per lane per step of the rank sweep
 constexpr uint32_t kPairUnroll = 4;  // candidates per lane per step of the pair sweep
 
-template <bool WITH_BP>
+// One work item of the rank sweep: positions [item * chunk, (item + 1) * chunk) of the concatenated
+// rank ranges, walked by one warp.
+template <bool WITH_BP, bool MULTI>
+__device__ __forceinline__ void sweep_item(const SweepParams& P, uint32_t item, uint32_t lane, uint32_t rcap,
+                                           uint64_t total, uint32_t* s_cnt, unsigned long long* s_bp,
+                                           uint32_t cta_row) {
+    const uint64_t p0 = (uint64_t)item * P.chunk;
+    const uint64_t p1 = min(p0 + P.chunk, total);
+    uint32_t r0;
+    if (item < P.item_cap) {
+        r0 = __ldg(P.item_r0 + item);
+    } else {
+        uint64_t lo = 0, hi = rcap;
+        while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (__ldg(P.rpos + m) <= p0) lo = m; else hi = m - 1; }
+        r0 = (uint32_t)lo;
+    }
+    Cursor c;
+    cursor_load(P, c, r0);
+    for (uint64_t pb = p0 + lane; pb < p1; pb += 32 * kUnroll) {
+        const uint64_t plast = min(pb + 32 * (kUnroll - 1), p1 - 1 - ((p1 - 1 - pb) & 31));
+        cursor_seek(P, c, pb, rcap);
+        if (plast < c.rhi) {
+            // all of this lane's positions of the step lie in one range: batch the loads
+            const SegTab t = c.tab;
+            const uint64_t off = c.base - c.rlo;
+            uint2 d[kUnroll];
+            uint32_t sid[kUnroll];
+#pragma unroll
+            for (uint32_t j = 0; j < kUnroll; j++) {
+                const uint64_t pj = pb + 32 * j;
+                if (pj < p1) {
+                    d[j] = __ldg(P.pos + off + pj);
+                    sid[j] = __ldg(P.sid + off + pj);
+                } else {
+                    d[j] = make_uint2(0, 0);
+                    sid[j] = 0;
+                }
+            }
+            uint2 a0[kUnroll], a1[kUnroll], b0[kUnroll], b1[kUnroll];
+#pragma unroll
+            for (uint32_t j = 0; j < kUnroll; j++) {
+                bin_pair(P, t, d[j].x, a0[j], a1[j]);
+                bin_pair(P, t, d[j].y, b0[j], b1[j]);
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kUnroll; j++)
+                if (pb + 32 * j < p1)
+                    sweep_one<WITH_BP, MULTI>(P, c.rd.qrow, d[j], sid[j], a0[j], a1[j], b0[j], b1[j], s_cnt, s_bp, cta_row);
+        } else {
+            // the step crosses a range boundary: one position at a time
+            for (uint64_t pj = pb; pj < p1 && pj <= pb + 32 * (kUnroll - 1); pj += 32) {
+                cursor_seek(P, c, pj, rcap);
+                const uint64_t di = c.base + (pj - c.rlo);
+                const uint2 d = __ldg(P.pos + di);
+                uint2 a0, a1, b0, b1;
+                bin_pair(P, c.tab, d.x, a0, a1);
+                bin_pair(P, c.tab, d.y, b0, b1);
+                sweep_one<WITH_BP, MULTI>(P, c.rd.qrow, d, __ldg(P.sid + di), a0, a1, b0, b1, s_cnt, s_bp, cta_row);
+            }
+        }
+    }
+}
+
+template <bool WITH_BP, bool MULTI>
 __global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
@@ -873,78 +984,46 @@ __global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
         }
     }
     __syncthreads();
-    // Warps pull work items independently (no block-wide barrier inside the loop).  A step covers
-    // 32 * kUnroll consecutive positions; lane l takes positions pb + l + 32 j, so every load of the
-    // DB arrays is coalesced, and the kUnroll DB intervals of a lane and their rank-table entries
-    // are all requested before any of them is used.  count(d) = #{q.start < d.end} -
-    // #{q.end <= d.start} needs two ranks, each one rank-table read plus, rarely, a search inside
-    // one bin.
-    for (;;) {
-        uint32_t item = 0;
-        if (lane == 0) item = atomicAdd(P.queue, 1u);
-        item = __shfl_sync(0xffffffffu, item, 0);
-        const uint64_t p0 = (uint64_t)item * P.chunk;
-        if (p0 >= total) break;
-        const uint64_t p1 = min(p0 + P.chunk, total);
-        uint32_t r0;
-        if (item < P.item_cap) {
-            r0 = __ldg(P.item_r0 + item);
-        } else {
-            uint64_t lo = 0, hi = rcap;
-            while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (__ldg(P.rpos + m) <= p0) lo = m; else hi = m - 1; }
-            r0 = (uint32_t)lo;
-        }
-        Cursor c;
-        cursor_load(P, c, r0);
-        for (uint64_t pb = p0 + lane; pb < p1; pb += 32 * kUnroll) {
-            const uint64_t plast = min(pb + 32 * (kUnroll - 1), p1 - 1 - ((p1 - 1 - pb) & 31));
-            cursor_seek(P, c, pb, rcap);
-            if (plast < c.rhi) {
-                // all of this lane's positions of the step lie in one range: batch the loads
-                const SegTab t = c.tab;
-                const uint64_t off = c.base - c.rlo;
-                uint2 d[kUnroll];
-                uint32_t sid[kUnroll];
-#pragma unroll
-                for (uint32_t j = 0; j < kUnroll; j++) {
-                    const uint64_t pj = pb + 32 * j;
-                    if (pj < p1) {
-                        d[j] = __ldg(P.pos + off + pj);
-                        sid[j] = __ldg(P.sid + off + pj);
-                    } else {
-                        d[j] = make_uint2(0, 0);
-                        sid[j] = 0;
-                    }
-                }
-                uint2 a0[kUnroll], a1[kUnroll], b0[kUnroll], b1[kUnroll];
-#pragma unroll
-                for (uint32_t j = 0; j < kUnroll; j++) {
-                    bin_pair(P, t, d[j].x, a0[j], a1[j]);
-                    bin_pair(P, t, d[j].y, b0[j], b1[j]);
-                }
-#pragma unroll
-                for (uint32_t j = 0; j < kUnroll; j++)
-                    if (pb + 32 * j < p1)
-                        sweep_one<WITH_BP>(P, c.rd.qrow, d[j], sid[j], a0[j], a1[j], b0[j], b1[j], s_cnt, s_bp);
-            } else {
-                // the step crosses a range boundary: one position at a time
-                for (uint64_t pj = pb; pj < p1 && pj <= pb + 32 * (kUnroll - 1); pj += 32) {
-                    cursor_seek(P, c, pj, rcap);
-                    const uint64_t di = c.base + (pj - c.rlo);
-                    const uint2 d = __ldg(P.pos + di);
-                    uint2 a0, a1, b0, b1;
-                    bin_pair(P, c.tab, d.x, a0, a1);
-                    bin_pair(P, c.tab, d.y, b0, b1);
-                    sweep_one<WITH_BP>(P, c.rd.qrow, d, __ldg(P.sid + di), a0, a1, b0, b1, s_cnt, s_bp);
-                }
+    if constexpr (MULTI) {
+        // several rows: blocks pull kCtaItems warp items at a time; the block's histogram serves the
+        // row in the middle of its item and is added to the outputs after every item
+        __shared__ uint32_t s_ctl[2];
+        const uint64_t items = (total + P.chunk - 1) / P.chunk;
+        for (;;) {
+            if (threadIdx.x == 0) {
+                const uint32_t ci = atomicAdd(P.queue, 1u);
+                s_ctl[0] = ci;
+                if ((uint64_t)ci * kCtaItems < items) s_ctl[1] = cta_item_row<true>(P, ci, items, rcap);
             }
+            __syncthreads();
+            const uint32_t ci = s_ctl[0], row = s_ctl[1];
+            if ((uint64_t)ci * kCtaItems >= items) break;
+            const uint64_t item = (uint64_t)ci * kCtaItems + (threadIdx.x >> 5);
+            if (item < items) sweep_item<WITH_BP, true>(P, (uint32_t)item, lane, rcap, total, s_cnt, s_bp, row);
+            __syncthreads();
+            flush_row<WITH_BP>(P, row, s_cnt, s_bp);
+            __syncthreads();
         }
-    }
-    if (P.smem_tally) {
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
-            if (s_cnt[k]) atomicAdd(&P.counts[k], s_cnt[k]);
-            if (WITH_BP && s_bp[k]) atomicAdd(&P.bp[k], s_bp[k]);
+    } else {
+        // Warps pull work items independently (no block-wide barrier inside the loop).  A step covers
+        // 32 * kUnroll consecutive positions; lane l takes positions pb + l + 32 j, so every load of the
+        // DB arrays is coalesced, and the kUnroll DB intervals of a lane and their rank-table entries
+        // are all requested before any of them is used.  count(d) = #{q.start < d.end} -
+        // #{q.end <= d.start} needs two ranks, each one rank-table read plus, rarely, a search inside
+        // one bin.
+        for (;;) {
+            uint32_t item = 0;
+            if (lane == 0) item = atomicAdd(P.queue, 1u);
+            item = __shfl_sync(0xffffffffu, item, 0);
+            if ((uint64_t)item * P.chunk >= total) break;
+            sweep_item<WITH_BP, false>(P, item, lane, rcap, total, s_cnt, s_bp, 0u);
+        }
+        if (P.smem_tally) {
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
+                if (s_cnt[k]) atomicAdd(&P.counts[k], s_cnt[k]);
+                if (WITH_BP && s_bp[k]) atomicAdd(&P.bp[k], s_bp[k]);
+            }
         }
     }
 }
@@ -952,11 +1031,12 @@ __global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
 // A pair candidate d of the run with query interval [qs, qe) and Q_SID qrow: when d.end > qs it
 // adds 1 and min(ends) - max(starts) to cell (qrow, sid) — in the block's shared histograms (SMEM,
 // one query row) or in the output matrix.
-template <bool WITH_BP, bool SMEM>
+template <bool WITH_BP, bool SMEM, bool MULTI>
 __device__ __forceinline__ void pair_tally(const SweepParams& P, uint32_t qs, uint32_t qe, uint32_t qrow, uint2 d,
-                                           uint32_t sid, uint32_t* s_cnt, unsigned long long* s_bp) {
+                                           uint32_t sid, uint32_t* s_cnt, unsigned long long* s_bp,
+                                           uint32_t cta_row) {
     if (d.y <= qs) return;
-    if (SMEM) {
+    if (SMEM && (!MULTI || qrow == cta_row)) {
         atomicAdd(&s_cnt[sid], 1u);
         if (WITH_BP) add_u64_lo(&s_bp[sid], min(qe, d.y) - max(qs, d.x));
     } else {
@@ -970,12 +1050,12 @@ __device__ __forceinline__ void pair_tally(const SweepParams& P, uint32_t qs, ui
 // galloping search from t.  Kept out of line: it runs only when a step holds 32 or more run
 // boundaries (a stretch of empty runs), and inlined its registers would count against the whole
 // kernel.
-template <bool WITH_BP, bool SMEM>
+template <bool WITH_BP, bool SMEM, bool MULTI>
 __device__ __noinline__ void pairs_step_slow(const uint64_t* __restrict__ ppos, const PairSeg* __restrict__ psegs,
                                              const uint2* __restrict__ pos, const uint32_t* __restrict__ sidv,
                                              uint32_t* counts, unsigned long long* bp, uint32_t D, uint32_t t,
                                              uint32_t rcap, uint64_t pb, uint32_t span, uint32_t lane,
-                                             uint32_t* s_cnt, unsigned long long* s_bp) {
+                                             uint32_t* s_cnt, unsigned long long* s_bp, uint32_t cta_row) {
     for (uint32_t o = lane; o <= span; o += 32) {
         const uint64_t pj = pb + o;
         const uint32_t tt = range_advance(ppos, t, rcap, pj);
@@ -984,7 +1064,7 @@ __device__ __noinline__ void pairs_step_slow(const uint64_t* __restrict__ ppos, 
         const uint2 d = __ldg(pos + di);
         const uint32_t sid = __ldg(sidv + di);
         if (d.y <= q.qs) continue;
-        if (SMEM) {
+        if (SMEM && (!MULTI || q.qrow == cta_row)) {
             atomicAdd(&s_cnt[sid], 1u);
             if (WITH_BP) add_u64_lo(&s_bp[sid], min(q.qe, d.y) - max(q.qs, d.x));
         } else {
@@ -1009,8 +1089,108 @@ __device__ __noinline__ void pairs_step_slow(const uint64_t* __restrict__ ppos, 
 // candidates per run), lane l holds the boundary ppos[t + 1 + l] of the following runs: a
 // position's run is t plus the number of boundaries at or below it, counted over the few
 // boundaries inside the step, and the run descriptors come from L1.
-template <bool WITH_BP, bool SMEM>
-__global__ void __launch_bounds__(256, 8) k_pairs(SweepParams P) {
+// One work item of the pair sweep (positions [item * chunk, (item + 1) * chunk) of the concatenated
+// candidate runs), walked by one warp.
+template <bool WITH_BP, bool SMEM, bool MULTI>
+__device__ __forceinline__ void pairs_item(const SweepParams& P, uint32_t item, uint32_t lane, uint32_t rcap,
+                                           uint64_t total, uint32_t* s_cnt, unsigned long long* s_bp,
+                                           uint32_t cta_row) {
+    const uint64_t p0 = (uint64_t)item * P.chunk;
+    const uint64_t p1 = min(p0 + P.chunk, total);
+    uint32_t t;
+    if (item < P.item_cap) {
+        t = __ldg(P.item_t0 + item);
+    } else {
+        uint64_t lo = 0, hi = rcap;
+        while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (__ldg(P.ppos + m) <= p0) lo = m; else hi = m - 1; }
+        t = (uint32_t)lo;
+    }
+    uint64_t rlo = __ldg(P.ppos + t), rhi = __ldg(P.ppos + t + 1);
+    PairSeg ps = P.psegs[t];
+    for (uint64_t pb = p0; pb < p1; pb += 32 * kPairUnroll) {
+        const uint64_t pend = min(pb + 32 * kPairUnroll, p1) - 1;
+        const uint32_t span = (uint32_t)(pend - pb);
+        if (pb >= rhi) {
+            t = range_advance(P.ppos, t, rcap, pb);
+            rlo = __ldg(P.ppos + t);
+            rhi = __ldg(P.ppos + t + 1);
+            ps = P.psegs[t];
+        }
+        const uint64_t base0 = ps.base - rlo + pb;  // element of offset 0 when it lies in run t
+        if (pend < rhi) {
+            uint2 d[kPairUnroll];
+            uint32_t sid[kPairUnroll];
+#pragma unroll
+            for (uint32_t j = 0; j < kPairUnroll; j++) {
+                const uint32_t o = lane + 32 * j;
+                if (o <= span) {
+                    d[j] = __ldg(P.pos + base0 + o);
+                    sid[j] = __ldg(P.sid + base0 + o);
+                } else {
+                    d[j] = make_uint2(0, 0);  // never a hit: d.y = 0 <= qs
+                    sid[j] = 0;
+                }
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kPairUnroll; j++)
+                pair_tally<WITH_BP, SMEM, MULTI>(P, ps.qs, ps.qe, ps.qrow, d[j], sid[j], s_cnt, s_bp, cta_row);
+            continue;
+        }
+        // lane l: boundary ppos[t + 1 + l] as an offset from pb (> 0, since run t holds pb);
+        // offsets inside the step fit 32 bits
+        const uint64_t B = (uint64_t)t + 1 + lane <= rcap ? __ldg(P.ppos + t + 1 + lane) : ~0ull;
+        const uint32_t rel = B - pb < 0xffffffffull ? (uint32_t)(B - pb) : 0xffffffffu;
+        const uint32_t nb = __popc(__ballot_sync(0xffffffffu, rel <= span));
+        if (nb == 32) {
+            pairs_step_slow<WITH_BP, SMEM, MULTI>(P.ppos, P.psegs, P.pos, P.sid, P.counts, P.bp, P.D, t, rcap, pb, span,
+                                           lane, s_cnt, s_bp, cta_row);
+            continue;  // the next step starts past rhi: range_advance finds its run
+        }
+        uint32_t k[kPairUnroll];  // position lane + 32 j lies in run t + k[j]
+#pragma unroll
+        for (uint32_t j = 0; j < kPairUnroll; j++) k[j] = 0;
+        for (uint32_t i = 0; i < nb; i++) {  // rel[0..nb) are the boundaries inside the step
+            const uint32_t bv = __shfl_sync(0xffffffffu, rel, i);
+#pragma unroll
+            for (uint32_t j = 0; j < kPairUnroll; j++) k[j] += bv <= lane + 32 * j ? 1u : 0u;
+        }
+        uint2 d[kPairUnroll];
+        uint32_t sid[kPairUnroll];
+#pragma unroll
+        for (uint32_t j = 0; j < kPairUnroll; j++) {
+            // run t + k (k > 0) starts at offset rel[k - 1]; t + k < rcap since ppos[rcap] = total > pend
+            const uint32_t o = lane + 32 * j;
+            const uint32_t rb = __shfl_sync(0xffffffffu, rel, k[j] ? k[j] - 1 : 0);
+            if (o <= span) {
+                const uint64_t di = k[j] ? __ldg(&P.psegs[t + k[j]].base) + (o - rb) : base0 + o;
+                d[j] = __ldg(P.pos + di);
+                sid[j] = __ldg(P.sid + di);
+            } else {
+                d[j] = make_uint2(0, 0);
+                sid[j] = 0;
+            }
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kPairUnroll; j++) {
+            const PairSeg* q = P.psegs + t + k[j];
+            pair_tally<WITH_BP, SMEM, MULTI>(P, __ldg(&q->qs), __ldg(&q->qe),
+                                             (SMEM && !MULTI) ? 0u : __ldg(&q->qrow), d[j], sid[j], s_cnt, s_bp,
+                                             cta_row);
+        }
+        // the run of the next step's first position pend + 1, from the boundaries in hand (at
+        // least one boundary, ppos[t + 1] <= pend, lies at or below it)
+        const uint32_t kn = __popc(__ballot_sync(0xffffffffu, rel <= span + 1));
+        if (pend + 1 < p1 && kn < 32) {
+            t += kn;
+            rlo = __ldg(P.ppos + t);
+            rhi = __ldg(P.ppos + t + 1);
+            ps = P.psegs[t];
+        }
+    }
+}
+
+template <bool WITH_BP, bool SMEM, bool MULTI>
+__global__ void __launch_bounds__(256, MULTI ? 6 : 8) k_pairs(SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
     uint32_t* s_cnt = reinterpret_cast<uint32_t*>(smem + (WITH_BP ? (size_t)P.D * 8 : 0));
@@ -1023,108 +1203,39 @@ __global__ void __launch_bounds__(256, 8) k_pairs(SweepParams P) {
             if (WITH_BP) s_bp[k] = 0;
         }
     __syncthreads();
-    for (;;) {
-        uint32_t item = 0;
-        if (lane == 0) item = atomicAdd(P.queue, 1u);
-        item = __shfl_sync(0xffffffffu, item, 0);
-        const uint64_t p0 = (uint64_t)item * P.chunk;
-        if (p0 >= total) break;
-        const uint64_t p1 = min(p0 + P.chunk, total);
-        uint32_t t;
-        if (item < P.item_cap) {
-            t = __ldg(P.item_t0 + item);
-        } else {
-            uint64_t lo = 0, hi = rcap;
-            while (lo < hi) { uint64_t m = (lo + hi + 1) >> 1; if (__ldg(P.ppos + m) <= p0) lo = m; else hi = m - 1; }
-            t = (uint32_t)lo;
+    if constexpr (MULTI) {
+        // several rows: whole blocks pull items, the histogram serves the item's middle row (as k_sweep)
+        __shared__ uint32_t s_ctl[2];
+        const uint64_t items = (total + P.chunk - 1) / P.chunk;
+        for (;;) {
+            if (threadIdx.x == 0) {
+                const uint32_t ci = atomicAdd(P.queue, 1u);
+                s_ctl[0] = ci;
+                if ((uint64_t)ci * kCtaItems < items) s_ctl[1] = cta_item_row<false>(P, ci, items, rcap);
+            }
+            __syncthreads();
+            const uint32_t ci = s_ctl[0], row = s_ctl[1];
+            if ((uint64_t)ci * kCtaItems >= items) break;
+            const uint64_t item = (uint64_t)ci * kCtaItems + (threadIdx.x >> 5);
+            if (item < items) pairs_item<WITH_BP, true, true>(P, (uint32_t)item, lane, rcap, total, s_cnt, s_bp, row);
+            __syncthreads();
+            flush_row<WITH_BP>(P, row, s_cnt, s_bp);
+            __syncthreads();
         }
-        uint64_t rlo = __ldg(P.ppos + t), rhi = __ldg(P.ppos + t + 1);
-        PairSeg ps = P.psegs[t];
-        for (uint64_t pb = p0; pb < p1; pb += 32 * kPairUnroll) {
-            const uint64_t pend = min(pb + 32 * kPairUnroll, p1) - 1;
-            const uint32_t span = (uint32_t)(pend - pb);
-            if (pb >= rhi) {
-                t = range_advance(P.ppos, t, rcap, pb);
-                rlo = __ldg(P.ppos + t);
-                rhi = __ldg(P.ppos + t + 1);
-                ps = P.psegs[t];
-            }
-            const uint64_t base0 = ps.base - rlo + pb;  // element of offset 0 when it lies in run t
-            if (pend < rhi) {
-                uint2 d[kPairUnroll];
-                uint32_t sid[kPairUnroll];
-#pragma unroll
-                for (uint32_t j = 0; j < kPairUnroll; j++) {
-                    const uint32_t o = lane + 32 * j;
-                    if (o <= span) {
-                        d[j] = __ldg(P.pos + base0 + o);
-                        sid[j] = __ldg(P.sid + base0 + o);
-                    } else {
-                        d[j] = make_uint2(0, 0);  // never a hit: d.y = 0 <= qs
-                        sid[j] = 0;
-                    }
-                }
-#pragma unroll
-                for (uint32_t j = 0; j < kPairUnroll; j++)
-                    pair_tally<WITH_BP, SMEM>(P, ps.qs, ps.qe, ps.qrow, d[j], sid[j], s_cnt, s_bp);
-                continue;
-            }
-            // lane l: boundary ppos[t + 1 + l] as an offset from pb (> 0, since run t holds pb);
-            // offsets inside the step fit 32 bits
-            const uint64_t B = (uint64_t)t + 1 + lane <= rcap ? __ldg(P.ppos + t + 1 + lane) : ~0ull;
-            const uint32_t rel = B - pb < 0xffffffffull ? (uint32_t)(B - pb) : 0xffffffffu;
-            const uint32_t nb = __popc(__ballot_sync(0xffffffffu, rel <= span));
-            if (nb == 32) {
-                pairs_step_slow<WITH_BP, SMEM>(P.ppos, P.psegs, P.pos, P.sid, P.counts, P.bp, P.D, t, rcap, pb, span,
-                                               lane, s_cnt, s_bp);
-                continue;  // the next step starts past rhi: range_advance finds its run
-            }
-            uint32_t k[kPairUnroll];  // position lane + 32 j lies in run t + k[j]
-#pragma unroll
-            for (uint32_t j = 0; j < kPairUnroll; j++) k[j] = 0;
-            for (uint32_t i = 0; i < nb; i++) {  // rel[0..nb) are the boundaries inside the step
-                const uint32_t bv = __shfl_sync(0xffffffffu, rel, i);
-#pragma unroll
-                for (uint32_t j = 0; j < kPairUnroll; j++) k[j] += bv <= lane + 32 * j ? 1u : 0u;
-            }
-            uint2 d[kPairUnroll];
-            uint32_t sid[kPairUnroll];
-#pragma unroll
-            for (uint32_t j = 0; j < kPairUnroll; j++) {
-                // run t + k (k > 0) starts at offset rel[k - 1]; t + k < rcap since ppos[rcap] = total > pend
-                const uint32_t o = lane + 32 * j;
-                const uint32_t rb = __shfl_sync(0xffffffffu, rel, k[j] ? k[j] - 1 : 0);
-                if (o <= span) {
-                    const uint64_t di = k[j] ? __ldg(&P.psegs[t + k[j]].base) + (o - rb) : base0 + o;
-                    d[j] = __ldg(P.pos + di);
-                    sid[j] = __ldg(P.sid + di);
-                } else {
-                    d[j] = make_uint2(0, 0);
-                    sid[j] = 0;
-                }
-            }
-#pragma unroll
-            for (uint32_t j = 0; j < kPairUnroll; j++) {
-                const PairSeg* q = P.psegs + t + k[j];
-                pair_tally<WITH_BP, SMEM>(P, __ldg(&q->qs), __ldg(&q->qe), SMEM ? 0u : __ldg(&q->qrow), d[j], sid[j],
-                                          s_cnt, s_bp);
-            }
-            // the run of the next step's first position pend + 1, from the boundaries in hand (at
-            // least one boundary, ppos[t + 1] <= pend, lies at or below it)
-            const uint32_t kn = __popc(__ballot_sync(0xffffffffu, rel <= span + 1));
-            if (pend + 1 < p1 && kn < 32) {
-                t += kn;
-                rlo = __ldg(P.ppos + t);
-                rhi = __ldg(P.ppos + t + 1);
-                ps = P.psegs[t];
-            }
+    } else {
+        for (;;) {
+            uint32_t item = 0;
+            if (lane == 0) item = atomicAdd(P.queue, 1u);
+            item = __shfl_sync(0xffffffffu, item, 0);
+            if ((uint64_t)item * P.chunk >= total) break;
+            pairs_item<WITH_BP, SMEM, false>(P, item, lane, rcap, total, s_cnt, s_bp, 0u);
         }
-    }
-    if (SMEM) {
-        __syncthreads();
-        for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
-            if (s_cnt[k]) atomicAdd(&P.counts[k], s_cnt[k]);
-            if (WITH_BP && s_bp[k]) atomicAdd(&P.bp[k], s_bp[k]);
+        if (SMEM) {
+            __syncthreads();
+            for (uint32_t k = threadIdx.x; k < P.D; k += blockDim.x) {
+                if (s_cnt[k]) atomicAdd(&P.counts[k], s_cnt[k]);
+                if (WITH_BP && s_bp[k]) atomicAdd(&P.bp[k], s_bp[k]);
+            }
         }
     }
 }
@@ -1509,6 +1620,7 @@ struct PipeIn {
     const uint32_t* blk_row;  // optional: the row every interval of the block must carry
     int row_from_block = 0;   // 1: rows come from blk_row, interval sids are ignored
     int block_local = 0;      // 1: one segment per block, no segment in two blocks, blocks <= kBlockSortCap
+    uint32_t region_bits = 0; // > 0: segments are (shard, 2^region_bits-bp region of the start, row)
 };
 
 // Whether a run's blocks allow the block-local key sort: with one row, or rows taken from the
@@ -1580,10 +1692,15 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
         return RGL_OK;
     }
     // key width: segment = shard * rows + row
-    uint64_t nseg = (uint64_t)idx->num_shards * rows;
+    const uint32_t rb = in.region_bits;
+    if (rb && (rb < 16 || rb > 31)) return fail(RGL_ERR_INVALID_ARGUMENT, "region bits must be in [16, 31]");
+    const uint64_t nreg = rb ? (1ull << (32 - rb)) : 1ull;
+    uint64_t nseg = (uint64_t)idx->num_shards * nreg * rows;
     int segbits = 1;
     while (segbits < 32 && (1ull << segbits) < nseg) segbits++;
-    if (nseg >= (1ull << 32)) return fail(RGL_ERR_INVALID_ARGUMENT, "num_shards * num_rows must be < 2^32");
+    if (nseg >= (1ull << 32))
+        return fail(RGL_ERR_INVALID_ARGUMENT, "num_shards x regions x num_rows must be < 2^32");
+    const uint32_t sps = (uint32_t)(nreg * rows);  // segments per shard
 
     if (ev) RGL_CUDA(cudaEventRecord(c->ev[0], st));
     // Two streams: `st` carries the chain from the sorted starts to the sweeps, `sd` the chains that
@@ -1593,7 +1710,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     cudaStream_t sd = c->side;
     uint32_t launches = 0;
     k_expand_keys<<<grid_for(n, 256), 256, 0, st>>>(n, in.iv, in.blk_off, in.blk_shard, in.blk_row,
-                                                    in.row_from_block, in.nblk, rows, in.row_base,
+                                                    in.row_from_block, in.nblk, rows, in.row_base, rb,
                                                     c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
                                                     c->ekey_a.as<uint64_t>(), d_small);
     launches++;
@@ -1640,7 +1757,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
         RGL_TRY(stream_after(st, sd, c->ev_join));
         return fail(RGL_ERR_INVALID_ARGUMENT, "query intervals x layer slots must be < 2^31 per run");
     }
-    k_lohi<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, rows, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
+    k_lohi<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, sps, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
                                                 c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, idx->d_pos,
                                                 idx->d_btab, c->lo.as<uint32_t>(), c->hi.as<uint32_t>());
     launches++;
@@ -1670,7 +1787,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     launches++;
     launches += scan_dev(c->scan_sums.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(), Lp, tot, st, pdl);
     launches += scan_dev(c->scan_sums.as<uint64_t>(), c->cl.as<uint64_t>(), c->pc.as<uint64_t>(), Lp, tot, st, pdl);
-    (void)launch_chain(pdl, k_crange_emit<true>, k_crange_emit<false>, gc, 256, 0, st, Lp, n, ns, rows,
+    (void)launch_chain(pdl, k_crange_emit<true>, k_crange_emit<false>, gc, 256, 0, st, Lp, n, ns, rows, sps,
                      c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), c->segnum.as<uint32_t>(), idx->d_slot,
                      c->lo.as<uint32_t>(), c->maxhi.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(),
                      c->ranges.as<RangeDesc>());
@@ -1709,7 +1826,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     launches++;
     launches += 4;
     // main stream: the pair work space and the rank ranges' positions
-    (void)launch_chain(pdl, k_cpair_len<true>, k_cpair_len<false>, gc, 256, 0, st, Lp, n, ns, rows,
+    (void)launch_chain(pdl, k_cpair_len<true>, k_cpair_len<false>, gc, 256, 0, st, Lp, n, ns, rows, sps,
                      c->tl.as<uint32_t>(), c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, c->lo.as<uint32_t>(),
                      c->hi.as<uint32_t>(), c->rflag.as<uint32_t>(), c->ridx.as<uint32_t>(), c->method.as<uint8_t>(),
                      c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(), c->plen.as<uint64_t>(),
@@ -1757,7 +1874,9 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     P.D = D;
     P.chunk = L.chunk;
     size_t smem = (size_t)D * (with_bp ? 12 : 4);
-    P.smem_tally = (rows == 1 && smem <= 160 * 1024) ? 1 : 0;
+    // tally: one row in a block-wide histogram for the whole kernel (1); several rows in a histogram
+    // of each block item's row (2); else (or with RGL_QF_GLOBAL_TALLY) atomics on the outputs (0)
+    P.smem_tally = smem > 160 * 1024 ? 0 : rows == 1 ? 1 : (opts && (opts->flags & RGL_QF_GLOBAL_TALLY)) ? 0 : 2;
     if (!P.smem_tally) smem = 0;
     unsigned grid = (unsigned)(c->num_sms * L.ctas_per_sm);
     // the rank tables are joined before the sweeps; the two sweeps run one after the other on
@@ -1765,15 +1884,23 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     RGL_TRY(stream_after(st, sd, c->ev_join));
     if (ev) RGL_CUDA(cudaEventRecord(c->ev[1], st));
     if (c->timing && mode.events) RGL_TRY(timing_record(c, true));
-    if (with_bp) k_sweep<true><<<grid, 256, smem, st>>>(P);
-    else k_sweep<false><<<grid, 256, smem, st>>>(P);
-    P.queue = d_small + 2;  // the pair sweep pulls from its own counter
-    if (P.smem_tally) {
-        if (with_bp) k_pairs<true, true><<<grid, 256, smem, st>>>(P);
-        else k_pairs<false, true><<<grid, 256, smem, st>>>(P);
+    if (P.smem_tally == 2) {
+        if (with_bp) k_sweep<true, true><<<grid, 256, smem, st>>>(P);
+        else k_sweep<false, true><<<grid, 256, smem, st>>>(P);
     } else {
-        if (with_bp) k_pairs<true, false><<<grid, 256, smem, st>>>(P);
-        else k_pairs<false, false><<<grid, 256, smem, st>>>(P);
+        if (with_bp) k_sweep<true, false><<<grid, 256, smem, st>>>(P);
+        else k_sweep<false, false><<<grid, 256, smem, st>>>(P);
+    }
+    P.queue = d_small + 2;  // the pair sweep pulls from its own counter
+    if (P.smem_tally == 2) {
+        if (with_bp) k_pairs<true, true, true><<<grid, 256, smem, st>>>(P);
+        else k_pairs<false, true, true><<<grid, 256, smem, st>>>(P);
+    } else if (P.smem_tally) {
+        if (with_bp) k_pairs<true, true, false><<<grid, 256, smem, st>>>(P);
+        else k_pairs<false, true, false><<<grid, 256, smem, st>>>(P);
+    } else {
+        if (with_bp) k_pairs<true, false, false><<<grid, 256, smem, st>>>(P);
+        else k_pairs<false, false, false><<<grid, 256, smem, st>>>(P);
     }
     launches++;
     launches++;
@@ -1860,6 +1987,19 @@ struct BatchPlan {
     }
 };
 
+// Region bits of a sub-batch of `rows` rows under the batch options (0: segments per (shard, row)).
+uint32_t batch_region_bits(const rgl_batch_opts* o, uint32_t rows) {
+    const uint32_t r = o ? o->region_bits : 0u;
+    if (r == RGL_BATCH_NO_REGIONS || rows <= 1) return 0;
+    return r ? r : 24u;
+}
+
+// Region-ordered work needs the device-wide key sort (the block-local sort keeps block order).
+void set_regions(PipeIn& in, uint32_t rb) {
+    in.region_bits = rb;
+    if (rb) in.block_local = 0;
+}
+
 int plan_batch(rgl_context* c, const rgl_batch* b, uint64_t sub, BatchPlan* P) {
     const uint64_t* bo = b->block_offsets;
     for (uint32_t i = 0; i < b->num_blocks; i++) {
@@ -1925,7 +2065,7 @@ Launch batch_launch(rgl_context* c, const rgl_batch_opts* o, rgl_query_opts* q) 
 // then the error word and the stats accumulator to pinned host memory.
 int enqueue_batch(rgl_context* c, const rgl_batch* b, const BatchPlan& P, const uint64_t* d_off,
                   const uint32_t* d_sr, const rgl_query_opts* q, uint32_t* d_counts, unsigned long long* d_bp,
-                  bool events, uint32_t* launches) {
+                  bool events, uint32_t* launches, const rgl_batch_opts* o) {
     cudaStream_t st = c->stream;
     const uint32_t D = c->idx->num_sources;
     uint32_t* d_small = c->small.as<uint32_t>();
@@ -1943,6 +2083,7 @@ int enqueue_batch(rgl_context* c, const rgl_batch* b, const BatchPlan& P, const 
         PipeIn in{b->d_intervals + sb.begin, sb.n, sb.rows, sb.row_lo, sb.nblk, d_off + sb.tab_at,
                   d_sr + sb.tab_at, b->block_rows ? d_sr + P.shard.size() + sb.tab_at : nullptr};
         in.block_local = P.local(sb, b->block_rows != nullptr);
+        set_regions(in, batch_region_bits(o, sb.rows));
         RGL_TRY(run_pipeline(c, in, q, d_counts + (uint64_t)sb.row_lo * D,
                              d_bp ? d_bp + (uint64_t)sb.row_lo * D : nullptr, nullptr, m));
         nl += c->last_launches;
@@ -1973,6 +2114,7 @@ std::vector<uint64_t> batch_key(rgl_context* c, const rgl_batch* b, const rgl_ba
     k.push_back(((uint64_t)L.chunk << 32) | L.ctas_per_sm);
     k.push_back(((uint64_t)L.pair_ratio << 32) | (o ? o->query.flags : 0));
     k.push_back(o ? o->sub_batch : 0);
+    k.push_back(o ? o->region_bits : 0);
     k.push_back(c->ws_sig);
     k.push_back(b->block_rows ? 1 : 0);
     for (uint32_t i = 0; i <= b->num_blocks; i++) k.push_back(b->block_offsets[i]);
@@ -2067,10 +2209,18 @@ int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
     // path changes function attributes (graph capture included)
     if (s == RGL_OK) {
         const int mx = 160 * 1024;
-        if (cudaFuncSetAttribute(k_sweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-            cudaFuncSetAttribute(k_sweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-            cudaFuncSetAttribute(k_pairs<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-            cudaFuncSetAttribute(k_pairs<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+        if (cudaFuncSetAttribute(k_sweep<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+            cudaFuncSetAttribute(k_sweep<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+            cudaFuncSetAttribute(k_sweep<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+            cudaFuncSetAttribute(k_sweep<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+            cudaFuncSetAttribute(k_pairs<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(k_pairs<false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(k_pairs<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
+                cudaSuccess ||
+            cudaFuncSetAttribute(k_pairs<false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
+                cudaSuccess ||
             cudaFuncSetAttribute(k_block_sort<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)block_sort_smem<true>()) != cudaSuccess ||
             cudaFuncSetAttribute(k_block_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -2257,7 +2407,7 @@ int rgl_query_batch_device(rgl_context* c, const rgl_batch* b, const rgl_batch_o
         key = batch_key(c, b, o, L, d_counts, d_bp);
         RGL_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         int s = enqueue_batch(c, b, P, c->gc.t_off.as<uint64_t>(), c->gc.t_shard.as<uint32_t>(), &q, d_counts, d_bp,
-                              false, &launches);
+                              false, &launches, o);
         cudaGraph_t g = nullptr;
         cudaError_t e = cudaStreamEndCapture(st, &g);
         if (s != RGL_OK) {
@@ -2287,7 +2437,7 @@ int rgl_query_batch_device(rgl_context* c, const rgl_batch* b, const rgl_batch_o
         RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, P.off.data(), P.off.size() * 8, cudaMemcpyHostToDevice, st));
         RGL_CUDA(cudaMemcpyAsync(c->bt_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
         RGL_TRY(enqueue_batch(c, b, P, c->bt_off.as<uint64_t>(), c->bt_shard.as<uint32_t>(), &q, d_counts, d_bp, true,
-                              &launches));
+                              &launches, o));
         subs = (uint32_t)P.subs.size();
     }
     c->last_n = 0;  // the single-call stats of finish() do not apply to a batch
@@ -2368,6 +2518,7 @@ int rgl_query_batch_host(rgl_context* c, const rgl_batch* b, const rgl_interval*
         PipeIn in{stage, sb.n, sb.rows, sb.row_lo, sb.nblk, d_off + sb.tab_at, d_sr + sb.tab_at,
                   b->block_rows ? d_sr + P.shard.size() + sb.tab_at : nullptr};
         in.block_local = P.local(sb, b->block_rows != nullptr);
+        set_regions(in, batch_region_bits(o, sb.rows));
         RGL_TRY(run_pipeline(c, in, &q, d_counts + (uint64_t)sb.row_lo * D, d_bp ? d_bp + (uint64_t)sb.row_lo * D : nullptr,
                              nullptr, m));
         RGL_CUDA(cudaEventRecord(c->ev_used[slot], st));
@@ -2430,6 +2581,7 @@ int rgl_batch_autotune(rgl_context* c, const rgl_batch* b, uint64_t sub_batch, r
               c->bt_shard.as<uint32_t>() + sb.tab_at,
               b->block_rows ? c->bt_shard.as<uint32_t>() + P.shard.size() + sb.tab_at : nullptr};
     in.block_local = P.local(sb, b->block_rows != nullptr);
+    set_regions(in, batch_region_bits(nullptr, sb.rows));
     const bool was_timing = c->timing;
     *best = rgl_query_opts{};
     uint32_t nt = 0;

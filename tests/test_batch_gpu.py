@@ -386,3 +386,29 @@ def test_batch_pvalues_device_equal_host_stats_path(seed):
     ctx.close()
     m.close()
     idx.close()
+
+
+@pytest.mark.parametrize("seed", [11, 12])
+def test_work_order_and_tally_modes_agree_with_the_oracle(seed):
+    """The region work order (every row's work on a 2^k-bp region laid out together) and the
+    block-local histograms of several-row sweeps change only the order of additions: every combination
+    (regions of 64 kbp, 16 Mbp, none; shared-memory or global tallies; chunk sizes that put many rows in
+    one block item) gives the oracle's counts and base pairs bit for bit."""
+    layers, files, D, nsh = _random_batch(seed, nfiles=29)
+    oc, obp = _oracle(layers, files, D, nsh)
+    idx = rg.Index.from_layers(layers, D, [f"s{i}" for i in range(nsh)])
+    ctx = rg.Context(idx)
+    iv, shards, offs, rows = _file_major(files, nsh)
+    t, p = _dev(iv)
+    b = rg.DeviceBatch(len(files), shards, offs, p, rows)
+    swept = {}
+    for rb in (16, 24, rg._lib.RGL_BATCH_NO_REGIONS):
+        for gt in (False, True):
+            for chunk in (0, 128):
+                c, bp, st = _run(ctx, b, D, region_bits=rb, global_tally=gt, chunk=chunk, sub_batch=4000)
+                assert (c == oc).all() and (bp == obp).all(), (rb, gt, chunk)
+                swept[rb] = st["db_swept"]
+    # regions can only add look-back windows that cross region boundaries to the swept count
+    assert swept[16] >= swept[24] >= swept[rg._lib.RGL_BATCH_NO_REGIONS]
+    ctx.close()
+    idx.close()
