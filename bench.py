@@ -67,6 +67,9 @@ def parse():
     ap.add_argument("--batch-files", type=int, default=4096,
                     help="query files of the batched measurement (0 skips it)")
     ap.add_argument("--batch-steps", type=int, default=3)
+    ap.add_argument("--batch-db", choices=["both", "config1", "config2"], default="both",
+                    help="database(s) of the batched part")
+    ap.add_argument("--batch-tune", action="store_true", help="autotune the batched part against config 2 too")
     ap.add_argument("--serve-seconds", type=float, default=5.0,
                     help="length of the Poisson arrival trace of the serving measurement (0 skips it)")
     ap.add_argument("--serve-rate", type=float, default=200.0)
@@ -439,8 +442,7 @@ def run_riggle(args, rank, world, local_rank, dist):
     lib.rgl_host_free(pc)
     lib.rgl_host_free(pb)
     ctx.close()
-    idx.close()
-    return out
+    return out, (idx, db)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -458,7 +460,12 @@ def batched_workload(nfiles):
     return cl, db, q
 
 
-def run_batched(args, dev):
+def run_batched(args, dev, which, big=None):
+    """The batched form (one call over all query files, CUDA-graph replay) against the plain form (one
+    call per file) on the same 4,096 files, results compared cell by cell.  which = "config1": the
+    64-file x 50k database; "config2": the 2e9-interval database of the plain part (big = (index,
+    database spec)).  Units are the per-file candidate unions summed (the plain form's work), counted
+    by an untimed region-free batched pass, so both forms are measured in the same units."""
     import torch
 
     import riggle_b200 as rg
@@ -466,7 +473,13 @@ def run_batched(args, dev):
 
     lib = rg.load()
     cl, dbspec, qspec = batched_workload(args.batch_files)
-    idx = rg.Index.synth(dbspec, device=dev)
+    if which == "config1":
+        idx = rg.Index.synth(dbspec, device=dev)
+        db_desc = "the 64-file x 50k database (config 1)"
+    else:
+        idx, dbspec = big
+        db_desc = (f"the 1,000-file database of {int(np.sum(dbspec.file_sizes)):.3g} intervals (config 2, "
+                   "resident 24 GB)")
     D = idx.num_sources
     off, sh, rw = rg.synth_batch_layout(qspec)
     N, F = int(off[-1]), qspec.num_files
@@ -477,13 +490,18 @@ def run_batched(args, dev):
     batch = rg.DeviceBatch(F, sh, off, t_iv.data_ptr(), rw)
     dc = torch.empty((F, D), dtype=torch.int32, device=cuda)
     dbp = torch.empty((F, D), dtype=torch.int64, device=cuda)
-    t0 = time.perf_counter()
-    best, trials = ctx.autotune(batch)
-    tune_s = time.perf_counter() - t0
+    # units: the per-file unions (no region split) and the query intervals
+    st0 = ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), region_bits=_lib.RGL_BATCH_NO_REGIONS)
+    units = float(st0["db_swept"] + st0["query_intervals"])
+    tune = which == "config1" or args.batch_tune
+    best, trials, tune_s = None, [], 0.0
+    if tune:
+        t0 = time.perf_counter()
+        best, trials = ctx.autotune(batch)
+        tune_s = time.perf_counter() - t0
     # capture, then replays: the timed steps launch the cached graph
     for _ in range(2):
-        st = ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), graph=True, tuned=True)
-    units = float(st["db_swept"] + st["query_intervals"])
+        st = ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), graph=True, tuned=tune)
     stream = torch.cuda.ExternalStream(ctx.stream)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -494,7 +512,7 @@ def run_batched(args, dev):
     torch.cuda.profiler.start()  # the profiled range under `ncu --profile-from-start off`
     e0.record(stream)
     for _ in range(args.batch_steps):
-        ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), graph=True, tuned=True, stats=False)
+        ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), graph=True, tuned=tune, stats=False)
     e1.record(stream)
     torch.cuda.synchronize()
     torch.cuda.profiler.stop()
@@ -505,17 +523,23 @@ def run_batched(args, dev):
     bc = dc.cpu().numpy().view(np.uint32)
     bb = dbp.cpu().numpy().view(np.uint64)
 
-    # the stats stage (FP64 p-value matrix): moments of every (source, chromosome) of the database
-    # built on the device at index time, then query length groups and p-values of the whole batch
+    # the stats stage (FP64 p-value matrix of every (file, source) cell) on a moment store of the
+    # database: built on the device from the database's own intervals (config 1), or tables of the
+    # right shape (config 2, whose 24,000 (source, chromosome) signals are not rebuilt here)
     from riggle_b200 import api
 
     t0 = time.perf_counter()
-    mom = api.Moments(D, (np.asarray(cl, np.uint64) + 99) // 100, device=dev)
-    for f in range(dbspec.num_files):
-        for c in range(len(cl)):
-            blk = dbspec.block(f, c)
-            if len(blk):
-                mom.build(f, c, blk)
+    if which == "config1":
+        mom = api.Moments(D, (np.asarray(cl, np.uint64) + 99) // 100, device=dev)
+        for f in range(dbspec.num_files):
+            for c in range(len(cl)):
+                blk = dbspec.block(f, c)
+                if len(blk):
+                    mom.build(f, c, blk)
+        mom_kind = "built on the device from the database intervals (FP64 FFT moments)"
+    else:
+        mom = synthetic_moments(D, cl, dbspec.file_sizes, dev)
+        mom_kind = "synthetic tables of the store's shape (the stage's cost does not depend on the values)"
     moments_s = time.perf_counter() - t0
     shard_chrom = np.arange(len(cl), dtype=np.uint32)
     pv = {k: torch.empty((F, D), dtype=dt, device=cuda)
@@ -530,7 +554,7 @@ def run_batched(args, dev):
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.batch_steps):
-        ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), graph=True, tuned=True, stats=False)
+        ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), graph=True, tuned=tune, stats=False)
         stats_stage()
     e1.record(stream)
     torch.cuda.synchronize()
@@ -538,6 +562,7 @@ def run_batched(args, dev):
     ms_pv = e0.elapsed_time(e1) / args.batch_steps
     emitted = int((pv["f"] & 1).sum().item())
     min_lp = float(pv["lp"].min().item())
+    del pv
 
     # the plain form on the same files: one rgl_query_counts_device call (one pipeline) per file
     t_plain = t_iv.clone()
@@ -569,7 +594,7 @@ def run_batched(args, dev):
     exact = bool((pc.cpu().numpy().view(np.uint32) == bc).all() and (pb.cpu().numpy().view(np.uint64) == bb).all())
     if not exact:
         raise RuntimeError("batched and plain forms disagree")
-    del t_plain
+    del t_plain, pc, pb
 
     # end to end: host intervals in page-locked memory, copies overlapped with the sweep
     hp = C.c_void_p()
@@ -578,11 +603,11 @@ def run_batched(args, dev):
     hv[:] = t_iv.cpu().numpy().view(np.uint32).reshape(-1)
     hc = np.empty((F, D), np.uint32)
     hb = np.empty((F, D), np.uint64)
-    ctx.query_batch_host(batch, hp.value, tuned=True, out=(hc, hb))
+    ctx.query_batch_host(batch, hp.value, tuned=tune, out=(hc, hb))
     walls = []
     for _ in range(2):
         t0 = time.perf_counter()
-        ctx.query_batch_host(batch, hp.value, tuned=True, out=(hc, hb))
+        ctx.query_batch_host(batch, hp.value, tuned=tune, out=(hc, hb))
         walls.append(time.perf_counter() - t0)
     e2e_s = min(walls)
     if not ((hc == bc).all() and (hb == bb).all()):
@@ -594,17 +619,20 @@ def run_batched(args, dev):
     if not args.no_cpu_baseline:
         import oracle as O
 
-        sample = list(range(0, F, max(1, F // 48)))[:48]
         host = t_iv.cpu().numpy().view(np.uint32)
+        if which == "config1":
+            sample, chroms = list(range(0, F, max(1, F // 48)))[:48], list(range(C_))
+        else:  # the 2e9 database: the shortest chromosome of a few files
+            sample, chroms = list(range(0, F, max(1, F // 6)))[:6], [int(np.argmin(cl))]
         layers = {}
-        for c in range(C_):
+        for c in chroms:
             layers.update(dbspec.chrom_layers(c))
         jumps = O.jump_tables(layers)
         n_s = 0.0
         t_s = 0.0
         for f in sample:
             per = {}
-            for c in range(C_):
+            for c in chroms:
                 a = host[int(off[f * C_ + c]):int(off[f * C_ + c + 1])].copy()
                 if len(a):
                     a[:, 2] = 0
@@ -613,21 +641,40 @@ def run_batched(args, dev):
             _, _, _, ost = O.query_database(layers, per, 1, D, threads=1, mode=0, jumps=jumps)
             t_s += time.perf_counter() - t0
             n_s += ost["db_swept"] + ost["query_intervals"]
-        cpu = {"value": n_s / t_s, "unit": UNIT, "cores": 1, "kind": "port",
-               "sample": f"{len(sample)} of the {F} query files (every {max(1, F // 48)}th), all chromosomes, "
-                         "restatement of query_database/query_sweep_windowed, one thread per query file"}
+        cpu = {"value": n_s / max(t_s, 1e-9), "unit": UNIT, "cores": 1, "kind": "port",
+               "sample": f"{len(sample)} of the {F} query files, chromosomes "
+                         f"{[rg.CHROM_NAMES_24[c] for c in chroms] if len(chroms) < 24 else 'all'}, restatement "
+                         "of query_database/query_sweep_windowed, one thread per query file"}
+    peak, peak_kind = measured_peak()
+    nsub = max(1, int(st["sub_batches"]))
+    db_bytes = 12.0 * float(idx.num_intervals)
+    alg_units = 12.0 * units + 12.0 * F * D
     out = {"workload": f"batched: {F} query files, log-uniform [1e2, 1e6] intervals (10% in 1 Mbp hot spots), "
-                       "against the 64-file x 50k database, one call (graph replay, autotuned launch shape)",
+                       f"against {db_desc}, one call (graph replay, "
+                       + ("autotuned" if tune else "default") + " launch shape)",
            "value": value, "unit": UNIT, "ms_per_step": ms, "steps": args.batch_steps, "query_files": F,
-           "query_intervals": int(st["query_intervals"]), "db_swept": int(st["db_swept"]),
-           "sub_batches": st["sub_batches"], "graph_nodes": st["graph_nodes"],
-           "gpu_launches_per_step": st["kernel_launches"],
+           "query_intervals": int(st0["query_intervals"]), "db_swept_per_file_unions": int(st0["db_swept"]),
+           "db_swept_region_order": int(st["db_swept"]), "sub_batches": st["sub_batches"],
+           "graph_nodes": st["graph_nodes"], "gpu_launches_per_step": st["kernel_launches"],
            "tuned": best, "tune_trials": len(trials), "tune_s": tune_s,
            "plain": {"value": plain_value, "ms_per_step": plain_ms,
                      "form": "one rgl_query_counts_device call per query file, same files, same units"},
            "batched_vs_plain": value / plain_value, "counts_exact_vs_plain": exact,
+           "roofline": {"bound": "hbm", "peak": peak, "unit": "GB/s", "peak_source": peak_kind,
+                        "achieved_unit_bytes": alg_units / (ms / 1e3) / 1e9,
+                        "frac_unit_bytes": alg_units / (ms / 1e3) / 1e9 / peak,
+                        "unit_bytes_note": "12 B per swept database interval of each file's union, per query interval "
+                                           "and per output cell: the plain form reads these from HBM; the batched "
+                                           "form reads a region of the database once from HBM for all rows of a "
+                                           "sub-batch and from L2 for the others",
+                        "achieved_read_once": (db_bytes * nsub + 12.0 * N + 12.0 * F * D) / (ms / 1e3) / 1e9,
+                        "read_once_note": "the database read once per sub-batch (12 B x database intervals x "
+                                          f"{nsub} sub-batches) plus the queries and outputs: the HBM traffic of "
+                                          "an ideal region-ordered sweep",
+                        "traffic": None},
            "with_pvalues": {"ms_per_step": ms_pv, "value": units / (ms_pv / 1e3), "query_length_groups": ngroups,
                             "emitted_cells": emitted, "min_ln_p": min_lp, "moments_build_s": moments_s,
+                            "moments": mom_kind,
                             "stage": "query length groups + FP64 p-values of every (file, source) cell on the "
                                      "device (rgl_batch_pvalues_device) after the counts"},
            "e2e": {"value": units / e2e_s, "unit": UNIT, "ms_per_step": e2e_s * 1e3, "h2d_bytes_per_step": N * 12,
@@ -635,7 +682,10 @@ def run_batched(args, dev):
            "cpu_baseline": cpu, "clocks": clk, "l2": "the batch's 5.6 GB of query intervals exceed L2"}
     mom.close()
     ctx.close()
-    return out, idx
+    del t_iv
+    if which == "config1":
+        idx.close()
+    return out
 
 
 # ---------------------------------------------------------------------------------------------
@@ -824,35 +874,50 @@ def main():
         torch.cuda.set_device(local_rank)
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
         dist = True
+    big = None
     try:
         out = None
         if args.only in ("all", "plain"):
-            out = run_riggle(args, rank, world, local_rank, dist)
+            out, big = run_riggle(args, rank, world, local_rank, dist)
         if rank == 0 and world == 1 and args.only != "plain":
-            idx = None
-            if args.batch_files and args.only in ("all", "batched"):
-                b, idx = run_batched(args, local_rank)
-                if out is None:  # the batched measurement alone (profiling)
-                    out = {"metric": METRIC, "value": b["value"], "unit": UNIT, "n_gpus": 1,
-                           "steps": args.batch_steps, "warmup": 2, "higher_is_better": True, "scaling": "weak",
-                           "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
-                           "config": {"workload": b["workload"]}}
-                out["batched"] = b
-            if args.serve_seconds and args.only in ("all", "serving"):
-                import riggle_b200 as rg
+            import riggle_b200 as rg
 
-                if idx is None:
-                    idx = rg.Index.synth(batched_workload(0)[1], device=local_rank)
-                sv = run_serving(args, local_rank, idx)
-                if out is None:
-                    out = {"metric": METRIC, "value": sv["continuous_batching"]["p99_ms"], "unit": "ms (p99)",
-                           "n_gpus": 1, "higher_is_better": False, "config": {"workload": sv["workload"]}}
+            def stub(part, v, unit, hib):
+                return {"metric": METRIC, "value": v, "unit": unit, "n_gpus": 1, "higher_is_better": hib,
+                        "scaling": "weak", "vs_baseline": None, "dtype": "u32", "data": "synthetic (seeded)",
+                        "config": {"workload": part}}
+
+            if big is None and args.only in ("all", "batched", "serving") and (
+                    args.only != "batched" or args.batch_db != "config1"):
+                cl, db, _, _ = workload_spec("plain", args.db_intervals, args.chroms)
+                big = (rg.Index.synth(db, device=local_rank), db)
+            if args.batch_files and args.only in ("all", "batched"):
+                if args.batch_db in ("both", "config1"):
+                    b = run_batched(args, local_rank, "config1")
+                    out = out or stub(b["workload"], b["value"], UNIT, True)
+                    out["batched"] = b
+                if args.batch_db in ("both", "config2"):
+                    b = run_batched(args, local_rank, "config2", big)
+                    out = out or stub(b["workload"], b["value"], UNIT, True)
+                    out["batched_2e9"] = b
+            if args.serve_seconds and args.only in ("all", "serving"):
+                idx, db = big
+                cl = np.asarray(db.chrom_len)
+                mom = synthetic_moments(idx.num_sources, cl, db.file_sizes, local_rank)
+                db_desc = f"1,000-file database of {int(np.sum(db.file_sizes)):.3g} intervals (config 2, 24 GB)"
+                sv = run_serving(args, local_rank, idx, db_desc, mom)
+                mom.close()
+                out = out or stub(sv["workload"], sv["continuous_batching"]["p99_ms"], "ms (p99)", False)
                 out["serving"] = sv
-            if idx is not None:
-                idx.close()
+            if args.precision_sizes and args.only in ("all", "precision"):
+                pr = run_precision(args, local_rank)
+                out = out or stub(pr["workload"], None, "relative error", False)
+                out["precision"] = pr
         if rank == 0 and out is not None:
             print(json.dumps(out), flush=True)
     finally:
+        if big is not None:
+            big[0].close()
         if dist:
             import torch
 
