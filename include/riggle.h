@@ -280,10 +280,11 @@ typedef struct rgl_batch_opts {
                              are cut into 2^region_bits-bp regions of their starts and the work is
                              laid out region by region, every row's work on a region together, so the
                              database intervals of a region are read from L2 by all rows after the
-                             first.  0: 24 for sub-batches of more than one row; RGL_BATCH_NO_REGIONS:
-                             one segment per (shard, row); else 16..31.  Results do not depend on it;
-                             the swept count (stats) grows by the look-back windows that cross
-                             region boundaries. */
+                             first.  0 or RGL_BATCH_NO_REGIONS: one segment per (shard, row) (the
+                             default: measured against the 2e9-interval database the region order
+                             gained nothing, the sweeps are not limited by DRAM traffic); else
+                             16..31.  Results do not depend on it; the swept count (stats) grows by
+                             the look-back windows that cross region boundaries. */
 } rgl_batch_opts;
 
 #define RGL_BATCH_NO_REGIONS 32u

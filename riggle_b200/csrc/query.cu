@@ -866,8 +866,8 @@ constexpr uint32_t kCtaItems = 8;  // warps of a 256-thread block
 // The row of the middle of block item ci (its warp item ci * kCtaItems + kCtaItems / 2, or the last
 // item), from the first range (RANK) or run of that warp item: the row the block's histogram serves.
 template <bool RANK>
-__device__ __forceinline__ uint32_t cta_item_row(const SweepParams& P, uint32_t ci, uint64_t items, uint32_t rcap) {
-    const uint64_t wi = min((uint64_t)ci * kCtaItems + kCtaItems / 2, items - 1);
+__device__ __forceinline__ uint32_t cta_item_row(const SweepParams& P, uint64_t ci, uint64_t items, uint32_t rcap) {
+    const uint64_t wi = min(ci * kCtaItems + kCtaItems / 2, items - 1);
     const uint64_t* off = RANK ? P.rpos : P.ppos;
     uint32_t r;
     if (wi < P.item_cap) {
@@ -879,6 +879,43 @@ __device__ __forceinline__ uint32_t cta_item_row(const SweepParams& P, uint32_t 
         r = (uint32_t)lo;
     }
     return RANK ? P.ranges[r].qrow : P.psegs[r].qrow;
+}
+
+// The outer loop of the several-row sweeps.  Blocks pull block items (kCtaItems warp items) from the
+// queue one at a time, so that the blocks running at once work on neighbouring items: with the
+// region work order they read the same database region, from L2 after the first.  The block's
+// histogram serves one row at a time: before an item whose row differs from the row it holds, it is
+// added to the outputs and cleared (and once more at the end).  item_fn(warp_item, row) walks one
+// warp item; flush_fn(row) adds and clears the histogram.
+template <bool RANK, typename ItemFn, typename FlushFn>
+__device__ __forceinline__ void multi_row_loop(const SweepParams& P, uint64_t items, uint32_t rcap, ItemFn item_fn,
+                                               FlushFn flush_fn) {
+    __shared__ uint32_t s_ctl[2];
+    constexpr uint32_t kNone = 0xFFFFFFFFu;
+    uint32_t cur = kNone;  // the row the histogram holds (block-uniform)
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t ci = atomicAdd(P.queue, 1u);
+            s_ctl[0] = ci;
+            if ((uint64_t)ci * kCtaItems < items) s_ctl[1] = cta_item_row<RANK>(P, ci, items, rcap);
+        }
+        __syncthreads();
+        const uint64_t ci = s_ctl[0];
+        const uint32_t row = s_ctl[1];
+        __syncthreads();  // every thread has read s_ctl
+        if (ci * kCtaItems >= items) break;
+        if (row != cur) {
+            if (cur != kNone) {
+                flush_fn(cur);
+                __syncthreads();
+            }
+            cur = row;
+        }
+        const uint64_t item = ci * kCtaItems + (threadIdx.x >> 5);
+        if (item < items) item_fn((uint32_t)item, cur);
+        __syncthreads();  // the item is done before the histogram may be flushed
+    }
+    if (cur != kNone) flush_fn(cur);
 }
 
 // Adds the block's histogram to row `row` of the outputs and clears it (between two __syncthreads).
@@ -985,25 +1022,15 @@ __global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
     }
     __syncthreads();
     if constexpr (MULTI) {
-        // several rows: blocks pull kCtaItems warp items at a time; the block's histogram serves the
-        // row in the middle of its item and is added to the outputs after every item
-        __shared__ uint32_t s_ctl[2];
+        // several rows: blocks pull block items (kCtaItems warp items each); the block's histogram
+        // serves the row of the current item and is added to the outputs on a row change
         const uint64_t items = (total + P.chunk - 1) / P.chunk;
-        for (;;) {
-            if (threadIdx.x == 0) {
-                const uint32_t ci = atomicAdd(P.queue, 1u);
-                s_ctl[0] = ci;
-                if ((uint64_t)ci * kCtaItems < items) s_ctl[1] = cta_item_row<true>(P, ci, items, rcap);
-            }
-            __syncthreads();
-            const uint32_t ci = s_ctl[0], row = s_ctl[1];
-            if ((uint64_t)ci * kCtaItems >= items) break;
-            const uint64_t item = (uint64_t)ci * kCtaItems + (threadIdx.x >> 5);
-            if (item < items) sweep_item<WITH_BP, true>(P, (uint32_t)item, lane, rcap, total, s_cnt, s_bp, row);
-            __syncthreads();
-            flush_row<WITH_BP>(P, row, s_cnt, s_bp);
-            __syncthreads();
-        }
+        multi_row_loop<true>(
+            P, items, rcap,
+            [&](uint32_t item, uint32_t row) {
+                sweep_item<WITH_BP, true>(P, item, lane, rcap, total, s_cnt, s_bp, row);
+            },
+            [&](uint32_t row) { flush_row<WITH_BP>(P, row, s_cnt, s_bp); });
     } else {
         // Warps pull work items independently (no block-wide barrier inside the loop).  A step covers
         // 32 * kUnroll consecutive positions; lane l takes positions pb + l + 32 j, so every load of the
@@ -1031,7 +1058,7 @@ __global__ void __launch_bounds__(256, 5) k_sweep(SweepParams P) {
 // A pair candidate d of the run with query interval [qs, qe) and Q_SID qrow: when d.end > qs it
 // adds 1 and min(ends) - max(starts) to cell (qrow, sid) — in the block's shared histograms (SMEM,
 // one query row) or in the output matrix.
-template <bool WITH_BP, bool SMEM, bool MULTI>
+template <bool WITH_BP, bool SMEM, int MULTI>
 __device__ __forceinline__ void pair_tally(const SweepParams& P, uint32_t qs, uint32_t qe, uint32_t qrow, uint2 d,
                                            uint32_t sid, uint32_t* s_cnt, unsigned long long* s_bp,
                                            uint32_t cta_row) {
@@ -1050,7 +1077,7 @@ __device__ __forceinline__ void pair_tally(const SweepParams& P, uint32_t qs, ui
 // galloping search from t.  Kept out of line: it runs only when a step holds 32 or more run
 // boundaries (a stretch of empty runs), and inlined its registers would count against the whole
 // kernel.
-template <bool WITH_BP, bool SMEM, bool MULTI>
+template <bool WITH_BP, bool SMEM, int MULTI>
 __device__ __noinline__ void pairs_step_slow(const uint64_t* __restrict__ ppos, const PairSeg* __restrict__ psegs,
                                              const uint2* __restrict__ pos, const uint32_t* __restrict__ sidv,
                                              uint32_t* counts, unsigned long long* bp, uint32_t D, uint32_t t,
@@ -1091,7 +1118,7 @@ __device__ __noinline__ void pairs_step_slow(const uint64_t* __restrict__ ppos, 
 // boundaries inside the step, and the run descriptors come from L1.
 // One work item of the pair sweep (positions [item * chunk, (item + 1) * chunk) of the concatenated
 // candidate runs), walked by one warp.
-template <bool WITH_BP, bool SMEM, bool MULTI>
+template <bool WITH_BP, bool SMEM, int MULTI>
 __device__ __forceinline__ void pairs_item(const SweepParams& P, uint32_t item, uint32_t lane, uint32_t rcap,
                                            uint64_t total, uint32_t* s_cnt, unsigned long long* s_bp,
                                            uint32_t cta_row) {
@@ -1189,7 +1216,7 @@ __device__ __forceinline__ void pairs_item(const SweepParams& P, uint32_t item, 
     }
 }
 
-template <bool WITH_BP, bool SMEM, bool MULTI>
+template <bool WITH_BP, bool SMEM, int MULTI>
 __global__ void __launch_bounds__(256, MULTI ? 6 : 8) k_pairs(SweepParams P) {
     extern __shared__ __align__(16) unsigned char smem[];
     unsigned long long* s_bp = reinterpret_cast<unsigned long long*>(smem);
@@ -1204,31 +1231,21 @@ __global__ void __launch_bounds__(256, MULTI ? 6 : 8) k_pairs(SweepParams P) {
         }
     __syncthreads();
     if constexpr (MULTI) {
-        // several rows: whole blocks pull items, the histogram serves the item's middle row (as k_sweep)
-        __shared__ uint32_t s_ctl[2];
+        // several rows: block items, the histogram serves one row at a time (as k_sweep)
         const uint64_t items = (total + P.chunk - 1) / P.chunk;
-        for (;;) {
-            if (threadIdx.x == 0) {
-                const uint32_t ci = atomicAdd(P.queue, 1u);
-                s_ctl[0] = ci;
-                if ((uint64_t)ci * kCtaItems < items) s_ctl[1] = cta_item_row<false>(P, ci, items, rcap);
-            }
-            __syncthreads();
-            const uint32_t ci = s_ctl[0], row = s_ctl[1];
-            if ((uint64_t)ci * kCtaItems >= items) break;
-            const uint64_t item = (uint64_t)ci * kCtaItems + (threadIdx.x >> 5);
-            if (item < items) pairs_item<WITH_BP, true, true>(P, (uint32_t)item, lane, rcap, total, s_cnt, s_bp, row);
-            __syncthreads();
-            flush_row<WITH_BP>(P, row, s_cnt, s_bp);
-            __syncthreads();
-        }
+        multi_row_loop<false>(
+            P, items, rcap,
+            [&](uint32_t item, uint32_t row) {
+                pairs_item<WITH_BP, true, 1>(P, item, lane, rcap, total, s_cnt, s_bp, row);
+            },
+            [&](uint32_t row) { flush_row<WITH_BP>(P, row, s_cnt, s_bp); });
     } else {
         for (;;) {
             uint32_t item = 0;
             if (lane == 0) item = atomicAdd(P.queue, 1u);
             item = __shfl_sync(0xffffffffu, item, 0);
             if ((uint64_t)item * P.chunk >= total) break;
-            pairs_item<WITH_BP, SMEM, false>(P, item, lane, rcap, total, s_cnt, s_bp, 0u);
+            pairs_item<WITH_BP, SMEM, 0>(P, item, lane, rcap, total, s_cnt, s_bp, 0u);
         }
         if (SMEM) {
             __syncthreads();
@@ -1365,6 +1382,9 @@ namespace {
 
 // Work items whose first range is precomputed; items beyond it search the range list themselves.
 constexpr uint64_t kItemCap = 1ull << 22;
+
+// Default work-item size of runs with several output rows.
+constexpr uint32_t kMultiRowChunk = 8192;
 
 // Runs up to this many query intervals chain their kernels with programmatic dependent launch.
 constexpr uint64_t kPdlMaxIntervals = 1ull << 21;
@@ -1672,6 +1692,9 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     const uint32_t n = (uint32_t)in.n;
     const uint32_t rows = in.rows;
     Launch L = pick_launch(opts);
+    // several rows: the block items flush their row histogram, so larger work items pay (measured
+    // on the 2e9-interval database: 1024 -> 8192 positions, sweeps 3.45 -> 2.46 s per 4,096 files)
+    if (rows > 1 && !(opts && opts->chunk)) L.chunk = kMultiRowChunk;
     const bool with_bp = d_bp != nullptr && !(opts && (opts->flags & RGL_QF_NO_OVERLAP));
     const bool ev = mode.events && stats;
     const bool pdl = in.n <= kPdlMaxIntervals;
@@ -1877,6 +1900,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     // tally: one row in a block-wide histogram for the whole kernel (1); several rows in a histogram
     // of each block item's row (2); else (or with RGL_QF_GLOBAL_TALLY) atomics on the outputs (0)
     P.smem_tally = smem > 160 * 1024 ? 0 : rows == 1 ? 1 : (opts && (opts->flags & RGL_QF_GLOBAL_TALLY)) ? 0 : 2;
+
     if (!P.smem_tally) smem = 0;
     unsigned grid = (unsigned)(c->num_sms * L.ctas_per_sm);
     // the rank tables are joined before the sweeps; the two sweeps run one after the other on
@@ -1893,14 +1917,14 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     }
     P.queue = d_small + 2;  // the pair sweep pulls from its own counter
     if (P.smem_tally == 2) {
-        if (with_bp) k_pairs<true, true, true><<<grid, 256, smem, st>>>(P);
-        else k_pairs<false, true, true><<<grid, 256, smem, st>>>(P);
+        if (with_bp) k_pairs<true, true, 1><<<grid, 256, smem, st>>>(P);
+        else k_pairs<false, true, 1><<<grid, 256, smem, st>>>(P);
     } else if (P.smem_tally) {
-        if (with_bp) k_pairs<true, true, false><<<grid, 256, smem, st>>>(P);
-        else k_pairs<false, true, false><<<grid, 256, smem, st>>>(P);
+        if (with_bp) k_pairs<true, true, 0><<<grid, 256, smem, st>>>(P);
+        else k_pairs<false, true, 0><<<grid, 256, smem, st>>>(P);
     } else {
-        if (with_bp) k_pairs<true, false, false><<<grid, 256, smem, st>>>(P);
-        else k_pairs<false, false, false><<<grid, 256, smem, st>>>(P);
+        if (with_bp) k_pairs<true, false, 0><<<grid, 256, smem, st>>>(P);
+        else k_pairs<false, false, 0><<<grid, 256, smem, st>>>(P);
     }
     launches++;
     launches++;
@@ -1990,8 +2014,8 @@ struct BatchPlan {
 // Region bits of a sub-batch of `rows` rows under the batch options (0: segments per (shard, row)).
 uint32_t batch_region_bits(const rgl_batch_opts* o, uint32_t rows) {
     const uint32_t r = o ? o->region_bits : 0u;
-    if (r == RGL_BATCH_NO_REGIONS || rows <= 1) return 0;
-    return r ? r : 24u;
+    if (r == RGL_BATCH_NO_REGIONS || r == 0 || rows <= 1) return 0;
+    return r;
 }
 
 // Region-ordered work needs the device-wide key sort (the block-local sort keeps block order).
@@ -2213,14 +2237,15 @@ int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
             cudaFuncSetAttribute(k_sweep<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
             cudaFuncSetAttribute(k_sweep<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
             cudaFuncSetAttribute(k_sweep<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
-            cudaFuncSetAttribute(k_pairs<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
+            cudaFuncSetAttribute(k_pairs<true, true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
                 cudaSuccess ||
-            cudaFuncSetAttribute(k_pairs<false, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
+            cudaFuncSetAttribute(k_pairs<false, true, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
                 cudaSuccess ||
-            cudaFuncSetAttribute(k_pairs<true, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
+            cudaFuncSetAttribute(k_pairs<true, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
                 cudaSuccess ||
-            cudaFuncSetAttribute(k_pairs<false, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
+            cudaFuncSetAttribute(k_pairs<false, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
                 cudaSuccess ||
+
             cudaFuncSetAttribute(k_block_sort<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)block_sort_smem<true>()) != cudaSuccess ||
             cudaFuncSetAttribute(k_block_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -405,11 +405,15 @@ def test_work_order_and_tally_modes_agree_with_the_oracle(seed):
     b = rg.DeviceBatch(len(files), shards, offs, p, rows)
     swept = {}
     for rb in (16, 24, rg._lib.RGL_BATCH_NO_REGIONS):
-        for gt in (False, True):
+        for tally in ("shared", "global"):
             for chunk in (0, 128):
-                c, bp, st = _run(ctx, b, D, region_bits=rb, global_tally=gt, chunk=chunk, sub_batch=4000)
-                assert (c == oc).all() and (bp == obp).all(), (rb, gt, chunk)
+                c, bp, st = _run(ctx, b, D, region_bits=rb, global_tally=tally == "global", chunk=chunk,
+                                 sub_batch=4000)
+                assert (c == oc).all() and (bp == obp).all(), (rb, tally, chunk)
                 swept[rb] = st["db_swept"]
+    # counts only (no overlap): the 32-bit shared histogram of the row
+    c, _, _ = _run(ctx, b, D, counts_only=True, sub_batch=4000)
+    assert (c == oc).all()
     # regions can only add look-back windows that cross region boundaries to the swept count
     assert swept[16] >= swept[24] >= swept[rg._lib.RGL_BATCH_NO_REGIONS]
     ctx.close()

@@ -142,7 +142,8 @@ def test_stats_stage_alone_equals_mix_equals_oracle():
     rng = np.random.default_rng(55)
     nbins = [20_000, 20_000, 20_000]  # the shards span 2 Mbp: 100 bp bins
     m, tables = _moments_for(rng, D, nbins)
-    srv = rg.Server(idx, workers=3, moments=m, shard_chrom=[0, 1, 2])
+    # one worker: the requests submitted while it runs the first one are batched together
+    srv = rg.Server(idx, workers=1, max_batch_requests=64, moments=m, shard_chrom=[0, 1, 2])
     alone = [srv.wait(srv.submit(per)) for per in reqs]
     tickets = [srv.submit(per) for per in reqs]
     mix = [srv.wait(t) for t in tickets]
