@@ -590,9 +590,10 @@ typedef struct rgl_server_opts {
     uint64_t hbm_reserve_bytes;     /* device memory every admission leaves free (default 4 GiB) */
     uint64_t max_pending_intervals; /* host queue bound: submit refuses beyond it (default 2^28) */
     rgl_query_opts query;           /* launch shape (zeros: defaults); RGL_QF_NO_OVERLAP */
-    uint64_t initial_intervals;     /* workspace each worker reserves at creation (default min(2^21,
-                                       batch_intervals)); batches beyond it grow the workspace when
-                                       free device memory admits them */
+    uint64_t initial_intervals;     /* workspace each worker reserves at creation (default
+                                       batch_intervals: no growth while serving); batches beyond it
+                                       grow the workspace when free device memory admits them (a
+                                       growth reallocates, which synchronises the device) */
     rgl_free_memory_fn free_memory; /* NULL: cudaMemGetInfo */
     void* free_memory_user;
     rgl_moments* moments;           /* non-NULL: every request also gets its p-values (stats stage) */

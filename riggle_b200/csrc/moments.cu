@@ -281,11 +281,66 @@ __global__ void k_gather(uint32_t k, const uint64_t* __restrict__ at, const DD* 
     if (i < k) out[i] = pre[at[i]];
 }
 
+// Windows with few positions (nw = N - L + 1 small, L close to N): the window sums F_L(j) then differ
+// from one another by a small part of their size, and any formula that forms the second moment and
+// subtracts the squared mean cancels (the reference's own f64 formula loses all digits there).
+// These L are reduced directly: d_j = F_L(j) - F_L(0) = (U[j+L] - U[j]) - U[L] from the prefix sums
+// U of the centred signal (U[0] = 0), summed with d_j^2 in double-double over the nw windows, and
+// var = sum d^2 / nw - (sum d / nw)^2.  One block per such L; out[i] = var.
+__device__ __forceinline__ DD dd_mul(DD a, DD b) {
+    const double p = a.hi * b.hi;
+    double e = fma(a.hi, b.hi, -p);
+    e = fma(a.hi, b.lo, e);
+    e = fma(a.lo, b.hi, e);
+    return dd_two_sum(p, e);
+}
+__device__ __forceinline__ DD dd_div_d(DD a, double b) {
+    const double q = a.hi / b;
+    const DD r = dd_add(a, dd_neg(dd_mul_d(DD{q, 0.0}, b)));
+    return dd_two_sum(q, (r.hi + r.lo) / b);
+}
+template <typename UT>
+__device__ __forceinline__ DD u_at(const UT* U, uint64_t i);
+template <>
+__device__ __forceinline__ DD u_at<double>(const double* U, uint64_t i) { return DD{U[i], 0.0}; }
+template <typename UT>
+__global__ void __launch_bounds__(256) k_direct_var(const uint32_t* __restrict__ which, const uint64_t* __restrict__ ls,
+                                                    uint64_t n, const UT* __restrict__ U, double uscale,
+                                                    double* __restrict__ out) {
+    const uint32_t i = which[blockIdx.x];
+    const uint64_t L = ls[i], nw = n - L + 1;
+    const DD uL = u_at<UT>(U, L);
+    DD s1{0.0, 0.0}, s2{0.0, 0.0};
+    for (uint64_t j = threadIdx.x; j < nw; j += blockDim.x) {
+        const DD d = dd_add(dd_add(u_at<UT>(U, j + L), dd_neg(u_at<UT>(U, j))), dd_neg(uL));
+        s1 = dd_add(s1, d);
+        s2 = dd_add(s2, dd_mul(d, d));
+    }
+    __shared__ DD r1[256], r2[256];
+    r1[threadIdx.x] = s1;
+    r2[threadIdx.x] = s2;
+    __syncthreads();
+    for (uint32_t k = blockDim.x / 2; k > 0; k >>= 1) {
+        if (threadIdx.x < k) {
+            r1[threadIdx.x] = dd_add(r1[threadIdx.x], r1[threadIdx.x + k]);
+            r2[threadIdx.x] = dd_add(r2[threadIdx.x], r2[threadIdx.x + k]);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        const DD m1 = dd_div_d(r1[0], (double)nw), m2 = dd_div_d(r2[0], (double)nw);
+        const DD v = dd_add(m2, dd_neg(dd_mul(m1, m1)));
+        const double var = (v.hi + v.lo) * uscale * uscale;
+        out[i] = var > 0.0 ? var : 0.0;
+    }
+}
+
 __global__ void k_window_moments(uint32_t G, const uint64_t* __restrict__ ls, uint64_t n,
                                  const DD* __restrict__ gsum, double a0, const DD* __restrict__ P0,
                                  const DD* __restrict__ P1, const DD* __restrict__ Q, const DD* __restrict__ V,
                                  const DD* __restrict__ UU_L, const DD* __restrict__ UU_R, DD uu_total,
-                                 float2* __restrict__ out, double* __restrict__ mean_out, double* __restrict__ var_out) {
+                                 float2* __restrict__ out, double* __restrict__ mean_out, double* __restrict__ var_out,
+                                 const double* __restrict__ direct_var) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= G) return;
     const uint64_t L = ls[i];
@@ -303,6 +358,7 @@ __global__ void k_window_moments(uint32_t G, const uint64_t* __restrict__ ls, ui
     const double mean = (double)L * gbar + fbar;
     double var = (s2.hi + s2.lo) / nw - fbar * fbar;
     if (!(var > 0.0)) var = 0.0;
+    if (direct_var && direct_var[i] >= 0.0) var = direct_var[i];  // few windows: reduced directly
     out[i] = make_float2((float)mean, (float)var);
     if (mean_out) mean_out[i] = mean;
     if (var_out) var_out[i] = var;
@@ -363,6 +419,10 @@ __device__ __forceinline__ CFF cff_mul(CFF a, CFF b) {
 struct FFAdd {
     __device__ __forceinline__ FF operator()(const FF& a, const FF& b) const { return ff_add(a, b); }
 };
+template <>
+__device__ __forceinline__ DD u_at<FF>(const FF* U, uint64_t i) {
+    return dd_two_sum((double)U[i].hi, (double)U[i].lo);
+}
 
 __constant__ CFF c_tw16f[16];  // exp(-2 pi i k / 16) as float-float (host-computed)
 
@@ -509,7 +569,7 @@ using namespace rgl;
 namespace {
 struct MomentWs {
     DevBuf iv, key_a, key_b, val_a, val_b, g, totals, nz, idx, cum, cnt, fa, fb, U, dd_in, dd_out, at, gl, outs, tmp,
-        gsum, grid, mv;
+        gsum, grid, mv, dv;
 };
 std::mutex g_ws_mu;
 MomentWs g_ws[16];  // one workspace per device ordinal
@@ -711,7 +771,7 @@ struct GMax {
 // V, UU_L, UU_R as double-double, scaled back), *uu_total, *a0 and w.gsum (as DD) for
 // k_window_moments.
 int moments_ff(MomentWs& w, uint64_t N, uint64_t M, int device, uint32_t G, const uint64_t* d_at, DD* outs,
-               DD* uu_total, double* a0, cudaStream_t st) {
+               DD* uu_total, double* a0, int* scale_exp, cudaStream_t st) {
     int tb = 0;
     RGL_TRY(ff_twiddles(w, M, device, &tb));
     FF* ffin = reinterpret_cast<FF*>(w.dd_in.p);
@@ -743,6 +803,7 @@ int moments_ff(MomentWs& w, uint64_t N, uint64_t M, int device, uint32_t G, cons
     int e = 0;
     if (gmax > 0.f) (void)std::frexp((double)gmax, &e);
     const float scale = std::ldexp(1.0f, -e);
+    *scale_exp = e;
     k_ff_center<<<blocks_for(M), 256, 0, st>>>(N, M, w.g.as<float>(), d_gsum, scale, reinterpret_cast<CFF*>(w.fa.p),
                                                 ffin);
     RGL_TRY(ff_scan(w, N + 1, st));
@@ -849,8 +910,9 @@ int rgl_moments_build_ex(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl
     DD* outs = w.outs.as<DD>();  // P0, P1, Q, V, UU_L, UU_R (G each)
     DD uu_total{0.0, 0.0};
     double a0 = 0.0;
+    int ff_exp = 0;
     if (precision == RGL_MOM_FP32C) {
-        RGL_TRY(moments_ff(w, N, M, device, G, d_at, outs, &uu_total, &a0, st));
+        RGL_TRY(moments_ff(w, N, M, device, G, d_at, outs, &uu_total, &a0, &ff_exp, st));
     } else {
         // K5: mean of g (double-double sum), centred signal, U = prefix of u
         k_to_dd<<<blocks_for(N), 256, 0, st>>>(N, w.g.as<float>(), w.dd_in.as<DD>());
@@ -899,9 +961,27 @@ int rgl_moments_build_ex(rgl_moments* m, uint32_t sid, uint32_t chrom, const rgl
     RGL_TRY(dm.ensure(G * 16ull + 64));
     double* d_mean = mean_out ? dm.as<double>() : nullptr;
     double* d_var = var_out ? dm.as<double>() + G : nullptr;
+    // windows with few positions: the variance reduced directly from the prefix sums (k_direct_var)
+    const uint64_t few = std::max<uint64_t>(65536, N / 32);
+    std::vector<uint32_t> direct;
+    for (uint32_t i = 0; i < G; i++)
+        if (N - grid[i] + 1 <= few) direct.push_back(i);
+    RGL_TRY(w.dv.ensure(G * 8ull + 64));
+    RGL_CUDA(cudaMemsetAsync(w.dv.p, 0xFF, G * 8ull, st));  // NaN: not reduced directly
+    if (!direct.empty()) {
+        uint32_t* d_which = reinterpret_cast<uint32_t*>(d_at + 2ull * G);
+        RGL_CUDA(cudaMemcpyAsync(d_which, direct.data(), direct.size() * 4, cudaMemcpyHostToDevice, st));
+        if (precision == RGL_MOM_FP32C)
+            k_direct_var<FF><<<(unsigned)direct.size(), 256, 0, st>>>(
+                d_which, w.gl.as<uint64_t>(), N, reinterpret_cast<const FF*>(w.U.p), std::ldexp(1.0, ff_exp),
+                w.dv.as<double>());
+        else
+            k_direct_var<double><<<(unsigned)direct.size(), 256, 0, st>>>(d_which, w.gl.as<uint64_t>(), N,
+                                                                           w.U.as<double>(), 1.0, w.dv.as<double>());
+    }
     k_window_moments<<<blocks_for(G), 256, 0, st>>>(G, w.gl.as<uint64_t>(), N, w.gsum.as<DD>(), a0, outs, outs + G,
                                                     outs + 2ull * G, outs + 3ull * G, outs + 4ull * G, outs + 5ull * G,
-                                                    uu_total, table, d_mean, d_var);
+                                                    uu_total, table, d_mean, d_var, w.dv.as<double>());
     RGL_CUDA(cudaGetLastError());
     if (mean_out) RGL_CUDA(cudaMemcpyAsync(mean_out, d_mean, G * 8, cudaMemcpyDeviceToHost, st));
     if (var_out) RGL_CUDA(cudaMemcpyAsync(var_out, d_var, G * 8, cudaMemcpyDeviceToHost, st));

@@ -358,7 +358,9 @@ int rgl_server_create(rgl_index* index, const rgl_server_opts* opts, rgl_server*
     if (!S->o.hbm_reserve_bytes) S->o.hbm_reserve_bytes = 4ull << 30;
     if (!S->o.max_pending_intervals) S->o.max_pending_intervals = 1ull << 28;
     S->o.batch_intervals = std::min<uint64_t>(S->o.batch_intervals, 200000000ull);  // one pipeline run
-    if (!S->o.initial_intervals) S->o.initial_intervals = 1ull << 21;
+    // by default a worker reserves its whole workspace at creation: growing one later frees and
+    // reallocates device buffers, which synchronises the device and stalls every other worker
+    if (!S->o.initial_intervals) S->o.initial_intervals = S->o.batch_intervals;
     S->o.initial_intervals = std::min(S->o.initial_intervals, S->o.batch_intervals);
     if (!S->o.bin_size) S->o.bin_size = 100;
     S->with_bp = !(S->o.query.flags & RGL_QF_NO_OVERLAP);
