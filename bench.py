@@ -552,12 +552,14 @@ def run_batched(args, dev, which, big=None):
 
     ngroups = stats_stage(True)
     torch.cuda.synchronize()
+    torch.cuda.profiler.start()  # a second profiled range: counts plus the stats stage
     e0.record(stream)
     for _ in range(args.batch_steps):
         ctx.query_batch_device(batch, dc.data_ptr(), dbp.data_ptr(), graph=True, tuned=tune, stats=False)
         stats_stage()
     e1.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
     ctx.check()
     ms_pv = e0.elapsed_time(e1) / args.batch_steps
     emitted = int((pv["f"] & 1).sum().item())
