@@ -646,6 +646,10 @@ typedef struct rgl_server_stats {
  * max_batch_requests and batch_intervals and the device memory the batch would add to the worker's
  * workspace fits in the free memory (free_memory()) less hbm_reserve_bytes and less what other
  * workers have been promised; a request that does not fit even alone is failed with RGL_ERR_OOM.
+ * free_memory() is called only for a batch that would grow the worker's buffers (a batch within
+ * them needs no admission), and without the server's lock held, so a slow query (cudaMemGetInfo
+ * can take tens of milliseconds on a busy node) delays neither submissions nor other workers.
+ * Workers wait for their batches with blocking (not spinning) synchronisation.
  * The server's moment store (optional) must outlive it. */
 int rgl_server_create(rgl_index* index, const rgl_server_opts* opts, rgl_server** out);
 /* Queues one request; RGL_ERR_INVALID_ARGUMENT for a bad block table or a request larger than

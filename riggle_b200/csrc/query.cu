@@ -6,8 +6,10 @@
 //   1. k_expand_keys: each query interval becomes key (segment << 32 | start), value end, and a
 //      second key (segment << 32 | end); segment = shard * rows + Q_SID.  Invalid intervals
 //      (start >= end, sid >= rows) raise an error bit.
-//   2. radix sort both key sets (the reference sorts by (sid, start), mod.rs:202; ends are sorted
-//      too, which the rank formulation below needs).
+//   2. sort both key sets (the reference sorts by (sid, start), mod.rs:202; ends are sorted too,
+//      which the rank formulation below needs): block by block when every input block is one
+//      segment (tiles sorted in shared memory, then merge passes; ordered blocks copied through),
+//      else a device-wide radix sort.
 //   3. exclusive u64 prefix sums of the sorted starts and sorted ends (PS, PE).
 //   4. K1 partition: for every (layer slot K, query i) the candidate range of the reference's scan,
 //      [pp(start - max_K), pp(end)) with pp = partition point of the layer's starts
@@ -147,7 +149,8 @@ __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, c
                               const uint32_t* __restrict__ blk_shard, const uint32_t* __restrict__ blk_row,
                               int row_from_block, uint32_t nblk, uint32_t rows, uint32_t row_base, uint32_t rb,
                               uint64_t* __restrict__ key, uint32_t* __restrict__ val, uint64_t* __restrict__ ekey,
-                              uint32_t* __restrict__ err) {
+                              uint32_t* __restrict__ err, uint32_t* __restrict__ unsorted,
+                              const uint64_t* __restrict__ sdst, const uint32_t* __restrict__ sidx) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t lo = 0, hi = nblk;  // block b with blk_off[b] <= i < blk_off[b+1]
@@ -156,6 +159,15 @@ __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, c
         if (blk_off[m] <= i) lo = m; else hi = m;
     }
     const uint32_t* w = reinterpret_cast<const uint32_t*>(iv) + 3ull * i;
+    // the block-local sort: block b's keys at sdst[b] + their place in the block (segment-order
+    // layout) or in place; order flags of the block's rank k in that layout: starts (ends) out of
+    // order -> unsorted[k] (unsorted[nblk + k]) = 1
+    const uint64_t o = sdst ? sdst[lo] + (i - blk_off[lo]) : (uint64_t)i;
+    if (unsorted && i > blk_off[lo]) {
+        const uint32_t k = sidx ? sidx[lo] : lo;
+        if (w[0] < w[-3]) unsorted[k] = 1u;
+        if (w[1] < w[-2]) unsorted[nblk + k] = 1u;
+    }
     // the row is the interval's sid, or with row_from_block its block's row (sid ignored)
     const uint32_t row = row_from_block ? blk_row[lo] : w[2];
     uint32_t s = w[0], e = w[1], q = row - row_base;  // rows below row_base wrap to >= rows
@@ -167,21 +179,95 @@ __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, c
     // into 2^rb-bp regions of their starts, so that the rows' work on one region lies together
     const uint64_t nreg = rb ? (1ull << (32 - rb)) : 1ull, reg = rb ? (s >> rb) : 0u;
     uint64_t seg = ((uint64_t)blk_shard[lo] * nreg + reg) * rows + q;
-    key[i] = (seg << 32) | s;
-    val[i] = e;
-    ekey[i] = (seg << 32) | e;
+    key[o] = (seg << 32) | s;
+    val[o] = e;
+    ekey[o] = (seg << 32) | e;
 }
 
-// ---- 2/3. unpack sorted keys ---------------------------------------------------------------------
-// Block-local sort of the query keys, for runs in which every input block holds one segment
-// ((shard, row)) and no two blocks share one: the segment-major order of the device-wide radix
-// sort is then the blocks' own order, each block sorted by position.  One thread block per input
-// block of at most kBlockSortCap intervals: with VALUES the start keys with their ends as values
-// (key_a / val_a -> key_b / val_b), else the end keys alone (ekey_a -> ekey_b).  A block that is
-// already in order (the usual case for sorted BED input) is copied through; otherwise a shared-memory
-// radix sort over the bits the block's positions use.  Both forms are stable, like the radix sort.
-constexpr int kBsThreads = 1024, kBsItems = 16;
+// ---- 2. block-local key sort ---------------------------------------------------------------------
+// For runs in which every input block holds one segment ((shard, row)) and no two blocks share one,
+// the segment-major order of a device-wide sort is the blocks' own order with each block sorted by
+// position, so the keys are sorted block by block, at any block size:
+//   * k_expand_keys marks a block whose starts (ends) are not in order (the usual sorted BED input
+//     has its starts in order; its ends are in order unless an interval contains the next one);
+//   * k_sort_plan lays the blocks out as tiles of kBlockSortCap intervals and, for blocks of more
+//     than one tile, merge chunks of kMergeChunk output positions;
+//   * k_tile_sort copies a tile of an ordered block to its place, or sorts it in shared memory (a
+//     radix sort over the bits its positions use; a tile already in order is copied through);
+//   * merge passes q = 1, 2, ... combine sorted runs of kBlockSortCap << (q - 1) pairwise until each
+//     block is one run: every CTA takes kMergeChunk outputs of one run pair, finds where they start
+//     in both runs by a merge-path search, and merges them in shared memory.
+// Every step is stable (equal positions keep their input order), like the radix sort it replaces.
+// A block that needs p merge passes has its tiles written where p ping-pong passes end in the
+// output buffer (in place into the input buffer when p is odd), so blocks of different sizes share
+// the passes and all finish in the output.
+constexpr int kBsThreads = 256, kBsItems = 16;
 constexpr uint64_t kBlockSortCap = (uint64_t)kBsThreads * kBsItems;
+constexpr int kMergeThreads = 256, kMergeItems = 8;
+constexpr uint32_t kMergeChunk = (uint32_t)(kMergeThreads * kMergeItems);
+static_assert(kBlockSortCap % kMergeChunk == 0, "a merge chunk lies inside one run pair");
+
+__host__ __device__ inline uint32_t sort_tiles(uint64_t cnt) {
+    return (uint32_t)((cnt + kBlockSortCap - 1) / kBlockSortCap);
+}
+__host__ __device__ inline uint32_t sort_passes(uint64_t cnt) {
+    const uint32_t t = sort_tiles(cnt);
+    uint32_t p = 0;
+    while ((1u << p) < t) p++;
+    return p;
+}
+__host__ __device__ inline uint32_t merge_chunks(uint64_t cnt) {
+    return cnt > kBlockSortCap ? (uint32_t)((cnt + kMergeChunk - 1) / kMergeChunk) : 0u;
+}
+
+// The block b with pre[b] <= x < pre[b + 1] (pre: nblk + 1 non-decreasing prefix counts, x < pre[nblk]).
+__device__ inline uint32_t find_block(const uint32_t* __restrict__ pre, uint32_t nblk, uint32_t x) {
+    uint32_t lo = 0, hi = nblk;
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (__ldg(pre + m) <= x) lo = m; else hi = m;
+    }
+    return lo;
+}
+
+// Exclusive prefix counts of the blocks' tiles and merge chunks, by one thread block: each thread
+// sums a contiguous stretch of blocks, a block scan of the stretch totals gives each stretch its
+// offset, and the stretch is written.
+__global__ void __launch_bounds__(1024) k_sort_plan(uint32_t nblk, const uint64_t* __restrict__ blk_off,
+                                                    uint32_t* __restrict__ tile_pre, uint32_t* __restrict__ chunk_pre) {
+    __shared__ uint32_t pt[1024], pc[1024];
+    const uint32_t t = threadIdx.x;
+    const uint32_t per = (nblk + 1023) / 1024;
+    const uint32_t a = min(t * per, nblk), b = min(a + per, nblk);
+    uint32_t st = 0, sc = 0;
+    for (uint32_t i = a; i < b; i++) {
+        const uint64_t cnt = blk_off[i + 1] - blk_off[i];
+        st += sort_tiles(cnt);
+        sc += merge_chunks(cnt);
+    }
+    pt[t] = st;
+    pc[t] = sc;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scan of the totals
+        const uint32_t vt = t >= off ? pt[t - off] : 0u, vc = t >= off ? pc[t - off] : 0u;
+        __syncthreads();
+        pt[t] += vt;
+        pc[t] += vc;
+        __syncthreads();
+    }
+    uint32_t rt = t ? pt[t - 1] : 0u, rc = t ? pc[t - 1] : 0u;
+    for (uint32_t i = a; i < b; i++) {
+        tile_pre[i] = rt;
+        chunk_pre[i] = rc;
+        const uint64_t cnt = blk_off[i + 1] - blk_off[i];
+        rt += sort_tiles(cnt);
+        rc += merge_chunks(cnt);
+    }
+    if (t == 1023) {
+        tile_pre[nblk] = pt[1023];
+        chunk_pre[nblk] = pc[1023];
+    }
+}
 
 template <bool VALUES>
 struct BlockSortTypes {
@@ -192,17 +278,29 @@ struct BlockSortTypes {
     };
 };
 
+// One tile per thread block (grid: an upper bound of the tiles; CTAs past the last tile return).
+// With VALUES the start keys with their ends as values (key_a / val_a), else the end keys alone.
+// unsorted[b] != 0: block b is not in order.  Output: `out` when the block is in order or needs
+// an even number of merge passes, else in place (`in`).
 template <bool VALUES>
-__global__ void __launch_bounds__(kBsThreads, 1) k_block_sort(const uint64_t* __restrict__ blk_off,
-                                                             const uint64_t* __restrict__ kin,
-                                                             const uint32_t* __restrict__ vin,
-                                                             uint64_t* __restrict__ kout, uint32_t* __restrict__ vout) {
+__global__ void __launch_bounds__(kBsThreads) k_tile_sort(uint32_t nblk, const uint64_t* __restrict__ blk_off,
+                                                            const uint32_t* __restrict__ tile_pre,
+                                                            const uint32_t* __restrict__ unsorted, uint64_t* kin,
+                                                            uint32_t* vin, uint64_t* __restrict__ kout,
+                                                            uint32_t* __restrict__ vout) {
     using T = BlockSortTypes<VALUES>;
     extern __shared__ __align__(16) unsigned char bs_smem[];
     typename T::Smem& sm = *reinterpret_cast<typename T::Smem*>(bs_smem);
-    const uint64_t base = blk_off[blockIdx.x];
-    const uint32_t cnt = (uint32_t)(blk_off[blockIdx.x + 1] - base);
-    if (cnt == 0) return;
+    const uint32_t tile = blockIdx.x;
+    if (tile >= __ldg(tile_pre + nblk)) return;
+    const uint32_t blk = find_block(tile_pre, nblk, tile);
+    const uint64_t bbeg = blk_off[blk], bcnt = blk_off[blk + 1] - bbeg;
+    const uint64_t base = bbeg + (uint64_t)(tile - tile_pre[blk]) * kBlockSortCap;
+    const uint64_t rest = bbeg + bcnt - base;
+    const uint32_t cnt = (uint32_t)(rest < kBlockSortCap ? rest : kBlockSortCap);
+    const bool ordered = unsorted[blk] == 0u;
+    uint64_t* ko = (ordered || !(sort_passes(bcnt) & 1u)) ? kout : kin;
+    uint32_t* vo = (ordered || !(sort_passes(bcnt) & 1u)) ? vout : vin;
     const uint64_t hi = kin[base] & 0xFFFFFFFF00000000ull;  // the block's segment, in the high word
     uint32_t k[kBsItems], v[kBsItems];
     uint32_t any = 0;
@@ -215,14 +313,16 @@ __global__ void __launch_bounds__(kBsThreads, 1) k_block_sort(const uint64_t* __
         any |= i < cnt ? k[j] : 0u;
         if (j) ok = ok && k[j - 1] <= k[j];
     }
-    __shared__ uint32_t s_bits;  // bitwise OR of the block's keys
+    __shared__ uint32_t s_bits;  // bitwise OR of the tile's keys
     sm.last[threadIdx.x] = k[kBsItems - 1];
     if (threadIdx.x == 0) s_bits = 0;
     __syncthreads();
     if (threadIdx.x) ok = ok && sm.last[threadIdx.x - 1] <= k[0];
     any = __reduce_or_sync(0xffffffffu, any);
     if ((threadIdx.x & 31u) == 0) atomicOr(&s_bits, any);
-    const bool sorted = __syncthreads_and(ok);  // also orders the atomicOr before the read below
+    // also orders every read of the tile before the in-place writes below, and the atomicOr
+    // before the read of s_bits
+    const bool sorted = __syncthreads_and(ok);
     const uint32_t bits = s_bits;
     if (!sorted) {
         const int end_bit = bits ? 32 - __clz(bits) : 1;
@@ -235,14 +335,95 @@ __global__ void __launch_bounds__(kBsThreads, 1) k_block_sort(const uint64_t* __
     for (int j = 0; j < kBsItems; j++) {
         const uint32_t i = threadIdx.x * kBsItems + j;
         if (i < cnt) {
-            kout[base + i] = hi | k[j];
-            if (VALUES) vout[base + i] = v[j];
+            ko[base + i] = hi | k[j];
+            if (VALUES) vo[base + i] = v[j];
         }
     }
 }
 
 template <bool VALUES>
 constexpr size_t block_sort_smem() { return sizeof(typename BlockSortTypes<VALUES>::Smem); }
+
+// Merge-path split of output diagonal d of runs a (na keys) and b (nb keys): the number of the d
+// first outputs that come from a, ties going to a (stability).
+template <class K>
+__device__ inline uint32_t merge_split(const K* a, uint32_t na, const K* b, uint32_t nb, uint32_t d) {
+    uint32_t lo = d > nb ? d - nb : 0u, hi = min(d, na);
+    while (lo < hi) {
+        const uint32_t m = (lo + hi) >> 1;
+        if ((uint32_t)a[m] <= (uint32_t)b[d - 1 - m]) lo = m + 1; else hi = m;
+    }
+    return lo;
+}
+
+// Merge pass q (1-based) of the block sort: one CTA per merge chunk (grid: an upper bound of the
+// chunks; CTAs past the last chunk, of ordered blocks or of blocks needing fewer passes return).
+// A block needing p passes reads buffer A at pass q when p - q + 1 is odd, else B, and writes the
+// other one.
+template <bool VALUES>
+__global__ void __launch_bounds__(kMergeThreads) k_merge_pass(uint32_t q, uint32_t nblk,
+                                                              const uint64_t* __restrict__ blk_off,
+                                                              const uint32_t* __restrict__ chunk_pre,
+                                                              const uint32_t* __restrict__ unsorted, uint64_t* ka,
+                                                              uint32_t* va, uint64_t* kb, uint32_t* vb) {
+    __shared__ uint32_t sk[kMergeChunk], sv[VALUES ? kMergeChunk : 1];
+    __shared__ uint32_t ok[kMergeChunk], ov[VALUES ? kMergeChunk : 1];
+    __shared__ uint32_t s_split[2];
+    const uint32_t chunk = blockIdx.x;
+    if (chunk >= __ldg(chunk_pre + nblk)) return;
+    const uint32_t blk = find_block(chunk_pre, nblk, chunk);
+    if (unsorted[blk] == 0u) return;
+    const uint64_t bbeg = blk_off[blk];
+    const uint32_t cnt = (uint32_t)(blk_off[blk + 1] - bbeg);
+    const uint32_t p = sort_passes(cnt);
+    if (p < q) return;
+    const bool from_a = ((p - q + 1) & 1u) != 0u;
+    const uint64_t* ks = (from_a ? ka : kb) + bbeg;
+    const uint32_t* vs = (from_a ? va : vb) + bbeg;
+    uint64_t* kd = (from_a ? kb : ka) + bbeg;
+    uint32_t* vd = (from_a ? vb : va) + bbeg;
+    const uint32_t o0 = (chunk - chunk_pre[blk]) * kMergeChunk, o1 = min(o0 + kMergeChunk, cnt);
+    const uint32_t L = (uint32_t)kBlockSortCap << (q - 1);  // run length of this pass
+    const uint32_t pa = (uint32_t)(((uint64_t)o0 / (2ull * L)) * 2ull * L);  // start of the run pair
+    const uint32_t na = min(L, cnt - pa), nb = cnt - pa > L ? min(L, cnt - pa - L) : 0u;
+    const uint32_t d0 = o0 - pa, d1 = o1 - pa;
+    const uint64_t hi = ks[0] & 0xFFFFFFFF00000000ull;
+    if (nb == 0) {  // a lone run: copy
+        for (uint32_t x = o0 + threadIdx.x; x < o1; x += kMergeThreads) {
+            kd[x] = ks[x];
+            if (VALUES) vd[x] = vs[x];
+        }
+        return;
+    }
+    const uint64_t* A = ks + pa;
+    const uint64_t* B = ks + pa + L;
+    if (threadIdx.x < 2) s_split[threadIdx.x] = merge_split(A, na, B, nb, threadIdx.x ? d1 : d0);
+    __syncthreads();
+    const uint32_t i0 = s_split[0], i1 = s_split[1];
+    const uint32_t j0 = d0 - i0, j1 = d1 - i1;
+    const uint32_t ca = i1 - i0, cb = j1 - j0, tot = ca + cb;
+    for (uint32_t x = threadIdx.x; x < tot; x += kMergeThreads) {
+        const bool in_a = x < ca;
+        const uint32_t src = in_a ? pa + i0 + x : pa + L + j0 + (x - ca);
+        sk[x] = (uint32_t)ks[src];
+        if (VALUES) sv[x] = vs[src];
+    }
+    __syncthreads();
+    // each thread merges kMergeItems outputs from its own split of the staged windows
+    const uint32_t dd = min((uint32_t)threadIdx.x * kMergeItems, tot);
+    uint32_t ia = merge_split(sk, ca, sk + ca, cb, dd), ib = dd - ia;
+    for (uint32_t m = 0; m < (uint32_t)kMergeItems && dd + m < tot; m++) {
+        const bool take_a = ib >= cb || (ia < ca && sk[ia] <= sk[ca + ib]);
+        const uint32_t from = take_a ? ia++ : ca + ib++;
+        ok[dd + m] = sk[from];
+        if (VALUES) ov[dd + m] = sv[from];
+    }
+    __syncthreads();
+    for (uint32_t x = threadIdx.x; x < tot; x += kMergeThreads) {
+        kd[o0 + x] = hi | ok[x];
+        if (VALUES) vd[o0 + x] = ov[x];
+    }
+}
 
 // The sorted start keys into starts, segment ids, segment-start flags and the starts' prefix-sum
 // input (entry n = 0); the sorted end keys into ends and the ends' prefix-sum input.
@@ -1346,6 +1527,8 @@ struct rgl_context {
     DevBuf segtab, tab_len, tab_off, tab_s, tab_e, tab_xs, tab_xe, tab2;
     DevBuf cl, pc, method, plen, ppos, psegs, item_t0, seg_need, lpos, tl, scan_sums;
     DevBuf cub_tmp2, scan_sums2;  // the side stream's own scratch
+    DevBuf sortplan;  // block-local sort: order flags, tile and merge-chunk prefix counts
+    DevBuf sort_tab, sort_rank;  // its segment-order layout, for the single-call entry points
     DevBuf item_hits, item_base, pairs;  // intervals mode
     DevBuf bt_off, bt_shard, acc;  // batched form: sub-batch block tables (offsets; shards then rows), stats
     uint32_t* h_small = nullptr;  // pinned mirror of `small`
@@ -1366,8 +1549,10 @@ struct rgl_context {
     bool has_tuned = false;       // rgl_batch_autotune result
     rgl_query_opts tuned{};
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    uint64_t res_n = 0;
-    uint32_t res_rows = 0;
+    uint64_t res_n = 0;           // the workspace covers runs of res_n intervals, res_rows rows and
+    uint32_t res_rows = 0;        // res_blk blocks (every buffer's size depends on one of the three)
+    uint32_t res_blk = 0;
+    bool ws_ready = false;        // res_* describe the workspace (set by the first full sizing)
     // sweep-kernel timing on the launch stream (rgl_context_set_timing)
     bool timing = false;
     std::vector<cudaEvent_t> tev;  // pairs (start, end)
@@ -1401,6 +1586,7 @@ int size_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uin
     const uint64_t ns = std::max<uint32_t>(idx->num_slots, 1);
     const uint64_t tot = n * ns;
     if (plan) *plan = 0;
+    if (c->ws_ready && n <= c->res_n && rows <= c->res_rows && nblk <= c->res_blk) return RGL_OK;  // nothing grows
     struct Sizer {
         uint64_t* plan;
         int ensure_in(DevBuf& b, size_t bytes) {
@@ -1412,6 +1598,7 @@ int size_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uin
     RGL_TRY(z.ensure_in(c->iv, n * sizeof(rgl_interval) + 16));
     RGL_TRY(z.ensure_in(c->blk_off, (nblk + 1) * 8ull));
     RGL_TRY(z.ensure_in(c->blk_shard, (nblk + 1) * 4ull));
+    RGL_TRY(z.ensure_in(c->sortplan, (4ull * nblk + 4) * 4));
     RGL_TRY(z.ensure_in(c->key_a, n * 8 + 8));
     RGL_TRY(z.ensure_in(c->key_b, n * 8 + 8));
     RGL_TRY(z.ensure_in(c->val_a, n * 4 + 4));
@@ -1497,13 +1684,15 @@ int size_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uin
     if (plan) return RGL_OK;
     c->res_n = std::max(c->res_n, n);
     c->res_rows = std::max(c->res_rows, rows);
+    c->res_blk = std::max(c->res_blk, nblk);
+    c->ws_ready = true;
     uint64_t sig = 1469598103934665603ull;
     for (DevBuf* b : {&c->iv, &c->key_a, &c->key_b, &c->val_a, &c->val_b, &c->ekey_a, &c->ekey_b, &c->starts,
                       &c->ends, &c->seg, &c->segflag, &c->segnum, &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps,
                       &c->pe, &c->lo, &c->hi, &c->maxhi, &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos,
                       &c->cub_tmp, &c->small, &c->item_r0, &c->item_t0, &c->segtab, &c->tab_len, &c->tab_off,
                       &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->tab2, &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs,
-                      &c->seg_need, &c->acc, &c->cub_tmp2, &c->scan_sums2})
+                      &c->seg_need, &c->acc, &c->cub_tmp2, &c->scan_sums2, &c->sortplan})
         sig = (sig ^ (uint64_t)(uintptr_t)b->p ^ ((uint64_t)b->cap << 17)) * 1099511628211ull;
     c->ws_sig = sig;
     return RGL_OK;
@@ -1631,6 +1820,20 @@ int stream_after(cudaStream_t to, cudaStream_t from, cudaEvent_t e) {
 
 // Input of one pipeline run: n intervals at `iv` (device), block b = [blk_off[b], blk_off[b+1]) on
 // shard blk_shard[b] (both tables on the device), rows [row_base, row_base + rows) of the output.
+// Shape of a run's block-local key sort, from the host's block offsets.
+struct LocalSort {
+    uint64_t max_block = 0;  // the largest block: sets the number of merge passes
+    uint64_t tiles = 0;      // tiles of kBlockSortCap intervals over all blocks
+    uint64_t chunks = 0;     // merge chunks of the blocks of more than one tile
+    // When the blocks are not in segment order (file-major blocks of several rows), the sorted keys
+    // are laid out segment by segment, as a device-wide sort would lay them out, so that the sweeps
+    // take every row's work on one chromosome together: block b's keys go to [dst[b], dst[b] +
+    // cnt_b), its rank in segment order is idx[b], and soff (nblk + 1) are the offsets of the blocks
+    // in that order.  Empty: the blocks are in segment order already.
+    std::vector<uint64_t> soff, dst;
+    std::vector<uint32_t> idx;
+};
+
 struct PipeIn {
     const rgl_interval* iv;
     uint64_t n;
@@ -1639,25 +1842,71 @@ struct PipeIn {
     const uint32_t* blk_shard;
     const uint32_t* blk_row;  // optional: the row every interval of the block must carry
     int row_from_block = 0;   // 1: rows come from blk_row, interval sids are ignored
-    int block_local = 0;      // 1: one segment per block, no segment in two blocks, blocks <= kBlockSortCap
+    int block_local = 0;      // 1: one segment per block, no segment in two blocks (block-local key sort)
+    LocalSort ls;             // with block_local: the sort's tile and merge-chunk counts
+    // with block_local and a segment-order layout: device copies of ls.soff, ls.dst, ls.idx
+    const uint64_t* sort_off = nullptr;
+    const uint64_t* sort_dst = nullptr;
+    const uint32_t* sort_idx = nullptr;
     uint32_t region_bits = 0; // > 0: segments are (shard, 2^region_bits-bp region of the start, row)
 };
 
 // Whether a run's blocks allow the block-local key sort: with one row, or rows taken from the
-// blocks, every block is one segment; they must be distinct and each at most kBlockSortCap
-// intervals.  off: nblk + 1 host offsets; row: the blocks' rows (null: row 0 of one row).
+// blocks, every block is one segment, and they must be distinct.  off: nblk + 1 host offsets; row:
+// the blocks' rows (null: row 0 of one row).  *ls receives the shape of the sort.
 bool blocks_local(uint32_t nblk, const uint64_t* off, const uint32_t* shard, const uint32_t* row, uint32_t rows,
-                  uint32_t row_base) {
+                  uint32_t row_base, LocalSort* ls) {
+    *ls = LocalSort();
     if (!row && rows != 1) return false;
-    std::vector<uint64_t> segs;
+    std::vector<std::pair<uint64_t, uint32_t>> segs;  // (segment, block) of the non-empty blocks
     segs.reserve(nblk);
+    LocalSort t;
+    bool ordered = true;
     for (uint32_t b = 0; b < nblk; b++) {
         const uint64_t cnt = off[b + 1] - off[b];
-        if (cnt > kBlockSortCap) return false;
-        if (cnt) segs.push_back((uint64_t)shard[b] * rows + (row ? row[b] - row_base : 0u));
+        t.max_block = std::max(t.max_block, cnt);
+        t.tiles += sort_tiles(cnt);
+        t.chunks += merge_chunks(cnt);
+        const uint64_t sg = (uint64_t)shard[b] * rows + (row ? row[b] - row_base : 0u);
+        if (cnt) {
+            if (!segs.empty() && sg < segs.back().first) ordered = false;
+            segs.push_back({sg, b});
+        }
     }
-    std::sort(segs.begin(), segs.end());
-    return std::adjacent_find(segs.begin(), segs.end()) == segs.end();
+    std::vector<std::pair<uint64_t, uint32_t>> sorted(segs);
+    std::stable_sort(sorted.begin(), sorted.end(),
+                     [](const std::pair<uint64_t, uint32_t>& a, const std::pair<uint64_t, uint32_t>& b) {
+                         return a.first < b.first;
+                     });
+    for (size_t k = 1; k < sorted.size(); k++)
+        if (sorted[k].first == sorted[k - 1].first) return false;  // a segment in two blocks
+    if (!ordered) {
+        // empty blocks keep their place in the order (rank) and take no room
+        std::vector<uint32_t> order;
+        order.reserve(nblk);
+        size_t k = 0;
+        for (uint32_t b = 0; b < nblk; b++)
+            if (off[b + 1] == off[b]) order.push_back(b);
+        std::vector<uint32_t> empties(order);
+        order.clear();
+        for (const auto& e : sorted) order.push_back(e.second);
+        order.insert(order.end(), empties.begin(), empties.end());
+        t.soff.assign(nblk + 1, 0);
+        t.dst.assign(nblk + 1, 0);
+        t.idx.assign(nblk + 1, 0);
+        uint64_t at = 0;
+        for (k = 0; k < order.size(); k++) {
+            const uint32_t b = order[k];
+            t.soff[k] = at;
+            t.dst[b] = at;
+            t.idx[b] = (uint32_t)k;
+            at += off[b + 1] - off[b];
+        }
+        t.soff[nblk] = at;
+        t.dst[nblk] = at;
+    }
+    *ls = std::move(t);
+    return true;
 }
 
 // What a run does besides the sweep: the single-call entry points zero their rows, reset the error
@@ -1732,20 +1981,65 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     // sweeps.
     cudaStream_t sd = c->side;
     uint32_t launches = 0;
+    // block-local sort with a segment-order layout: callers that did not upload its tables (the
+    // single-call entry points, never inside a graph capture) have them uploaded here
+    const uint64_t* sort_off = in.sort_off;
+    const uint64_t* sort_dst = in.sort_dst;
+    const uint32_t* sort_idx = in.sort_idx;
+    if (in.block_local && !in.ls.dst.empty() && !sort_dst) {
+        const uint64_t nb1 = (uint64_t)in.nblk + 1;
+        RGL_TRY(c->sort_tab.ensure(2 * nb1 * 8));
+        RGL_TRY(c->sort_rank.ensure(nb1 * 4));
+        RGL_CUDA(cudaMemcpyAsync(c->sort_tab.p, in.ls.soff.data(), nb1 * 8, cudaMemcpyHostToDevice, st));
+        RGL_CUDA(cudaMemcpyAsync(c->sort_tab.as<uint64_t>() + nb1, in.ls.dst.data(), nb1 * 8, cudaMemcpyHostToDevice,
+                                 st));
+        RGL_CUDA(cudaMemcpyAsync(c->sort_rank.p, in.ls.idx.data(), nb1 * 4, cudaMemcpyHostToDevice, st));
+        sort_off = c->sort_tab.as<uint64_t>();
+        sort_dst = sort_off + nb1;
+        sort_idx = c->sort_rank.as<uint32_t>();
+    }
+    // block-local sort: per-block order flags ([0, nblk) starts, [nblk, 2 nblk) ends), then the
+    // tile and merge-chunk prefix counts
+    uint32_t* d_unsorted = c->sortplan.as<uint32_t>();
+    uint32_t* d_tile_pre = d_unsorted + 2ull * in.nblk;
+    uint32_t* d_chunk_pre = d_tile_pre + in.nblk + 1;
+    if (in.block_local) RGL_CUDA(cudaMemsetAsync(d_unsorted, 0, 2ull * in.nblk * 4, st));
     k_expand_keys<<<grid_for(n, 256), 256, 0, st>>>(n, in.iv, in.blk_off, in.blk_shard, in.blk_row,
                                                     in.row_from_block, in.nblk, rows, in.row_base, rb,
                                                     c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
-                                                    c->ekey_a.as<uint64_t>(), d_small);
+                                                    c->ekey_a.as<uint64_t>(), d_small,
+                                                    in.block_local ? d_unsorted : nullptr,
+                                                    in.block_local ? sort_dst : nullptr,
+                                                    in.block_local ? sort_idx : nullptr);
     launches++;
+    // the sort's view of the blocks: their offsets in the layout the keys were written in
+    const uint64_t* soff = sort_dst ? sort_off : in.blk_off;
+    if (in.block_local) {
+        k_sort_plan<<<1, 1024, 0, st>>>(in.nblk, soff, d_tile_pre, d_chunk_pre);
+        launches++;
+    }
     RGL_TRY(stream_after(sd, st, c->ev_fork));
     size_t tb = c->cub_tmp2.cap;
     if (in.block_local) {
-        k_block_sort<false><<<in.nblk, kBsThreads, block_sort_smem<false>(), sd>>>(
-            in.blk_off, c->ekey_a.as<uint64_t>(), nullptr, c->ekey_b.as<uint64_t>(), nullptr);
-        k_block_sort<true><<<in.nblk, kBsThreads, block_sort_smem<true>(), st>>>(
-            in.blk_off, c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(), c->key_b.as<uint64_t>(),
-            c->val_b.as<uint32_t>());
+        const unsigned tiles = (unsigned)std::max<uint64_t>(in.ls.tiles, 1);
+        const unsigned chunks = (unsigned)std::max<uint64_t>(in.ls.chunks, 1);
+        const uint32_t passes = sort_passes(in.ls.max_block);
+        k_tile_sort<false><<<tiles, kBsThreads, block_sort_smem<false>(), sd>>>(
+            in.nblk, soff, d_tile_pre, d_unsorted + in.nblk, c->ekey_a.as<uint64_t>(), nullptr,
+            c->ekey_b.as<uint64_t>(), nullptr);
+        k_tile_sort<true><<<tiles, kBsThreads, block_sort_smem<true>(), st>>>(
+            in.nblk, soff, d_tile_pre, d_unsorted, c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
+            c->key_b.as<uint64_t>(), c->val_b.as<uint32_t>());
         launches += 2;
+        for (uint32_t q = 1; q <= passes; q++) {
+            k_merge_pass<false><<<chunks, kMergeThreads, 0, sd>>>(q, in.nblk, soff, d_chunk_pre,
+                                                                  d_unsorted + in.nblk, c->ekey_a.as<uint64_t>(),
+                                                                  nullptr, c->ekey_b.as<uint64_t>(), nullptr);
+            k_merge_pass<true><<<chunks, kMergeThreads, 0, st>>>(q, in.nblk, soff, d_chunk_pre, d_unsorted,
+                                                                 c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
+                                                                 c->key_b.as<uint64_t>(), c->val_b.as<uint32_t>());
+            launches += 2;
+        }
     } else {
         RGL_CUDA(cub::DeviceRadixSort::SortKeys(c->cub_tmp2.p, tb, c->ekey_a.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
                                                 (int)n, 0, 32 + segbits, sd));
@@ -2000,14 +2294,56 @@ struct BatchPlan {
     std::vector<uint32_t> row;   // per sub-batch: nblk block rows (same layout; unused without block_rows)
     uint64_t max_n = 0;
     uint32_t max_rows = 0, max_blk = 0;
-    bool local(const SubBatch& sb, bool block_rows) const {  // block-local key sort allowed
-        return blocks_local(sb.nblk, &off[sb.tab_at], &shard[sb.tab_at], block_rows ? &row[sb.tab_at] : nullptr,
-                            sb.rows, sb.row_lo);
+    // per sub-batch: whether the block-local key sort applies, and its shape
+    std::vector<char> local;
+    std::vector<LocalSort> ls;
+    // the sorts' segment-order layouts, in the offsets' (soff, sdst) and shards' (sidx) layouts
+    std::vector<uint64_t> soff, sdst;
+    std::vector<uint32_t> sidx;
+    void prepare(bool block_rows) {
+        local.assign(subs.size(), 0);
+        ls.assign(subs.size(), LocalSort());
+        soff = off;
+        sdst = off;
+        sidx.assign(shard.size(), 0);
+        for (size_t k = 0; k < subs.size(); k++) {
+            const SubBatch& sb = subs[k];
+            local[k] = blocks_local(sb.nblk, &off[sb.tab_at], &shard[sb.tab_at],
+                                    block_rows ? &row[sb.tab_at] : nullptr, sb.rows, sb.row_lo, &ls[k]);
+            if (!local[k] || ls[k].dst.empty()) continue;
+            std::copy(ls[k].soff.begin(), ls[k].soff.end(), soff.begin() + sb.tab_at);
+            std::copy(ls[k].dst.begin(), ls[k].dst.end(), sdst.begin() + sb.tab_at);
+            std::copy(ls[k].idx.begin(), ls[k].idx.end(), sidx.begin() + sb.tab_at);
+        }
     }
-    std::vector<uint32_t> shard_rows() const {  // the device table: shards, then rows
+    std::vector<uint64_t> off_table() const {  // the device table: offsets, then soff, then sdst
+        std::vector<uint64_t> v(off);
+        v.insert(v.end(), soff.begin(), soff.end());
+        v.insert(v.end(), sdst.begin(), sdst.end());
+        return v;
+    }
+    std::vector<uint32_t> shard_rows() const {  // the device table: shards, then rows, then sidx
         std::vector<uint32_t> v(shard);
         v.insert(v.end(), row.begin(), row.end());
+        v.insert(v.end(), sidx.begin(), sidx.end());
         return v;
+    }
+    // The pipeline input of sub-batch k over intervals iv, with the device tables d_off / d_sr.
+    PipeIn pipe_in(size_t k, const rgl_interval* iv, const uint64_t* d_off, const uint32_t* d_sr,
+                   bool block_rows) const {
+        const SubBatch& sb = subs[k];
+        PipeIn in{iv, sb.n, sb.rows, sb.row_lo, sb.nblk, d_off + sb.tab_at, d_sr + sb.tab_at,
+                  block_rows ? d_sr + shard.size() + sb.tab_at : nullptr};
+        in.block_local = local[k];
+        in.ls.max_block = ls[k].max_block;  // the layout goes by the device tables below
+        in.ls.tiles = ls[k].tiles;
+        in.ls.chunks = ls[k].chunks;
+        if (local[k] && !ls[k].dst.empty()) {
+            in.sort_off = d_off + off.size() + sb.tab_at;
+            in.sort_dst = d_off + 2 * off.size() + sb.tab_at;
+            in.sort_idx = d_sr + 2 * shard.size() + sb.tab_at;
+        }
+        return in;
     }
 };
 
@@ -2072,6 +2408,7 @@ int plan_batch(rgl_context* c, const rgl_batch* b, uint64_t sub, BatchPlan* P) {
         }
     }
     close();
+    P->prepare(b->block_rows != nullptr);
     return RGL_OK;
 }
 
@@ -2103,10 +2440,9 @@ int enqueue_batch(rgl_context* c, const rgl_batch* b, const BatchPlan& P, const 
     m.events = events;
     m.acc = c->acc.as<unsigned long long>();
     uint32_t nl = 0;
-    for (const SubBatch& sb : P.subs) {
-        PipeIn in{b->d_intervals + sb.begin, sb.n, sb.rows, sb.row_lo, sb.nblk, d_off + sb.tab_at,
-                  d_sr + sb.tab_at, b->block_rows ? d_sr + P.shard.size() + sb.tab_at : nullptr};
-        in.block_local = P.local(sb, b->block_rows != nullptr);
+    for (size_t k = 0; k < P.subs.size(); k++) {
+        const SubBatch& sb = P.subs[k];
+        PipeIn in = P.pipe_in(k, b->d_intervals + sb.begin, d_off, d_sr, b->block_rows != nullptr);
         set_regions(in, batch_region_bits(o, sb.rows));
         RGL_TRY(run_pipeline(c, in, q, d_counts + (uint64_t)sb.row_lo * D,
                              d_bp ? d_bp + (uint64_t)sb.row_lo * D : nullptr, nullptr, m));
@@ -2177,21 +2513,38 @@ int enqueue_block_rows(rgl_context* c, uint32_t num_rows, uint32_t nblk, const u
     RGL_TRY(ensure_workspace(c, n, 0, nblk));
     std::vector<uint64_t> rel(nblk + 1);
     for (uint32_t i = 0; i <= nblk; i++) rel[i] = off[i] - off[0];
-    std::vector<uint32_t> sr(2ull * nblk + 2, 0);
+    // device tables: offsets then the sort's segment-order offsets and destinations; shards, rows,
+    // then the blocks' ranks in segment order
+    LocalSort ls;
+    const bool local = blocks_local(nblk, rel.data(), shards, rows, num_rows, 0, &ls);
+    const bool perm = local && !ls.dst.empty();
+    std::vector<uint64_t> ot(rel);
+    if (perm) {
+        ot.insert(ot.end(), ls.soff.begin(), ls.soff.end());
+        ot.insert(ot.end(), ls.dst.begin(), ls.dst.end());
+    }
+    std::vector<uint32_t> sr(3ull * nblk + 3, 0);
     for (uint32_t i = 0; i < nblk; i++) {
         sr[i] = shards[i];
         sr[nblk + 1 + i] = rows[i];
+        if (perm) sr[2 * (nblk + 1) + i] = ls.idx[i];
     }
-    RGL_TRY(c->bt_off.ensure(rel.size() * 8 + 8));
+    RGL_TRY(c->bt_off.ensure(ot.size() * 8 + 8));
     RGL_TRY(c->bt_shard.ensure(sr.size() * 4 + 4));
-    RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, rel.data(), rel.size() * 8, cudaMemcpyHostToDevice, st));
+    RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, ot.data(), ot.size() * 8, cudaMemcpyHostToDevice, st));
     RGL_CUDA(cudaMemcpyAsync(c->bt_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
     // the interval copies and table uploads above are ordered before the pipeline on this stream
     RGL_CUDA(cudaMemsetAsync(d_counts, 0, (size_t)num_rows * D * 4, st));
     if (d_bp) RGL_CUDA(cudaMemsetAsync(d_bp, 0, (size_t)num_rows * D * 8, st));
     PipeIn in{d_iv + off[0], n, num_rows, 0, nblk, c->bt_off.as<uint64_t>(), c->bt_shard.as<uint32_t>(),
               c->bt_shard.as<uint32_t>() + nblk + 1, 1};
-    in.block_local = blocks_local(nblk, rel.data(), shards, rows, num_rows, 0);
+    in.block_local = local;
+    if (perm) {
+        in.sort_off = c->bt_off.as<uint64_t>() + (nblk + 1);
+        in.sort_dst = c->bt_off.as<uint64_t>() + 2 * (nblk + 1);
+        in.sort_idx = c->bt_shard.as<uint32_t>() + 2 * (nblk + 1);
+    }
+    in.ls = std::move(ls);
     PipeMode m;
     m.zero_out = false;
     // the table uploads read pageable vectors that die here: an asynchronous copy from pageable
@@ -2246,9 +2599,9 @@ int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
             cudaFuncSetAttribute(k_pairs<false, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
                 cudaSuccess ||
 
-            cudaFuncSetAttribute(k_block_sort<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_tile_sort<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)block_sort_smem<true>()) != cudaSuccess ||
-            cudaFuncSetAttribute(k_block_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            cudaFuncSetAttribute(k_tile_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)block_sort_smem<false>()) != cudaSuccess)
             s = fail(RGL_ERR_DEVICE, "cudaFuncSetAttribute");
     }
@@ -2279,7 +2632,7 @@ int rgl_context_destroy(rgl_context* c) {
                       &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->tab2,
                       &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs, &c->item_t0,
                       &c->seg_need, &c->item_hits, &c->item_base, &c->pairs, &c->bt_off, &c->bt_shard, &c->acc, &c->gc.t_off, &c->gc.t_shard,
-                      &c->cub_tmp2, &c->scan_sums2};
+                      &c->cub_tmp2, &c->scan_sums2, &c->sortplan, &c->sort_tab, &c->sort_rank};
     if (c->gc.exec) cudaGraphExecDestroy(c->gc.exec);
     if (c->gc.graph) cudaGraphDestroy(c->gc.graph);
     if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
@@ -2343,7 +2696,7 @@ int rgl_query_counts_device(rgl_context* c, uint32_t num_rows, uint32_t num_shar
     }
     PipeIn in{c->iv.as<rgl_interval>(), n, num_rows, 0, num_shards, c->blk_off.as<uint64_t>(),
               c->blk_shard.as<uint32_t>(), nullptr};
-    in.block_local = blocks_local(num_shards, off.data(), shard_ids, nullptr, num_rows, 0);
+    in.block_local = blocks_local(num_shards, off.data(), shard_ids, nullptr, num_rows, 0, &in.ls);
     RGL_TRY(run_pipeline(c, in, opts, d_counts, reinterpret_cast<unsigned long long*>(d_overlap_bp), stats));
     if (!stats) return RGL_OK;
     RGL_CUDA(cudaStreamSynchronize(c->stream));
@@ -2377,7 +2730,7 @@ int rgl_query_counts(rgl_context* c, const rgl_query_batch* b, const rgl_query_o
     }
     PipeIn in{c->iv.as<rgl_interval>(), n, rows, 0, (uint32_t)blocks.size(), c->blk_off.as<uint64_t>(),
               c->blk_shard.as<uint32_t>(), nullptr};
-    in.block_local = blocks_local((uint32_t)blocks.size(), off.data(), ids.data(), nullptr, rows, 0);
+    in.block_local = blocks_local((uint32_t)blocks.size(), off.data(), ids.data(), nullptr, rows, 0, &in.ls);
     RGL_TRY(run_pipeline(c, in, opts, c->out_counts.as<uint32_t>(),
                          overlap_bp ? c->out_bp.as<unsigned long long>() : nullptr, stats));
     if (cells) {
@@ -2423,10 +2776,11 @@ int rgl_query_batch_device(rgl_context* c, const rgl_batch* b, const rgl_batch_o
     } else if (graph) {
         RGL_CUDA(cudaStreamSynchronize(st));  // the previous graph may still read its tables
         graph_drop(c);
-        RGL_TRY(c->gc.t_off.ensure(P.off.size() * 8 + 8));
+        const std::vector<uint64_t> ot = P.off_table();
+        RGL_TRY(c->gc.t_off.ensure(ot.size() * 8 + 8));
         const std::vector<uint32_t> sr = P.shard_rows();
         RGL_TRY(c->gc.t_shard.ensure(sr.size() * 4 + 4));
-        RGL_CUDA(cudaMemcpy(c->gc.t_off.p, P.off.data(), P.off.size() * 8, cudaMemcpyHostToDevice));
+        RGL_CUDA(cudaMemcpy(c->gc.t_off.p, ot.data(), ot.size() * 8, cudaMemcpyHostToDevice));
         RGL_CUDA(cudaMemcpy(c->gc.t_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice));
         // the key is taken after the workspace is sized, so that a later reallocation invalidates it
         key = batch_key(c, b, o, L, d_counts, d_bp);
@@ -2456,10 +2810,11 @@ int rgl_query_batch_device(rgl_context* c, const rgl_batch* b, const rgl_batch_o
         c->gc.subs = subs = (uint32_t)P.subs.size();
         RGL_CUDA(cudaGraphLaunch(x, st));
     } else {
-        RGL_TRY(c->bt_off.ensure(P.off.size() * 8 + 8));
+        const std::vector<uint64_t> ot = P.off_table();
+        RGL_TRY(c->bt_off.ensure(ot.size() * 8 + 8));
         const std::vector<uint32_t> sr = P.shard_rows();
         RGL_TRY(c->bt_shard.ensure(sr.size() * 4 + 4));
-        RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, P.off.data(), P.off.size() * 8, cudaMemcpyHostToDevice, st));
+        RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, ot.data(), ot.size() * 8, cudaMemcpyHostToDevice, st));
         RGL_CUDA(cudaMemcpyAsync(c->bt_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
         RGL_TRY(enqueue_batch(c, b, P, c->bt_off.as<uint64_t>(), c->bt_shard.as<uint32_t>(), &q, d_counts, d_bp, true,
                               &launches, o));
@@ -2512,10 +2867,11 @@ int rgl_query_batch_host(rgl_context* c, const rgl_batch* b, const rgl_interval*
     if (!c->copy_stream) RGL_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
     cudaStream_t st = c->stream, cs = c->copy_stream;
     const std::vector<uint32_t> sr = P.shard_rows();
-    RGL_TRY(c->bt_off.ensure(P.off.size() * 8 + 8));
+    const std::vector<uint64_t> ot = P.off_table();
+    RGL_TRY(c->bt_off.ensure(ot.size() * 8 + 8));
     RGL_TRY(c->bt_shard.ensure(sr.size() * 4 + 4));
     if (stats) RGL_CUDA(cudaEventRecord(c->ev[0], st));
-    RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, P.off.data(), P.off.size() * 8, cudaMemcpyHostToDevice, st));
+    RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, ot.data(), ot.size() * 8, cudaMemcpyHostToDevice, st));
     RGL_CUDA(cudaMemcpyAsync(c->bt_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
     uint32_t* d_counts = c->out_counts.as<uint32_t>();
     unsigned long long* d_bp = want_bp ? c->out_bp.as<unsigned long long>() : nullptr;
@@ -2540,9 +2896,7 @@ int rgl_query_batch_host(rgl_context* c, const rgl_batch* b, const rgl_interval*
         RGL_CUDA(cudaMemcpyAsync(stage, h_intervals + sb.begin, sb.n * sizeof(rgl_interval), cudaMemcpyHostToDevice, cs));
         RGL_CUDA(cudaEventRecord(c->ev_copied[slot], cs));
         RGL_CUDA(cudaStreamWaitEvent(st, c->ev_copied[slot], 0));
-        PipeIn in{stage, sb.n, sb.rows, sb.row_lo, sb.nblk, d_off + sb.tab_at, d_sr + sb.tab_at,
-                  b->block_rows ? d_sr + P.shard.size() + sb.tab_at : nullptr};
-        in.block_local = P.local(sb, b->block_rows != nullptr);
+        PipeIn in = P.pipe_in(k, stage, d_off, d_sr, b->block_rows != nullptr);
         set_regions(in, batch_region_bits(o, sb.rows));
         RGL_TRY(run_pipeline(c, in, &q, d_counts + (uint64_t)sb.row_lo * D, d_bp ? d_bp + (uint64_t)sb.row_lo * D : nullptr,
                              nullptr, m));
@@ -2597,15 +2951,14 @@ int rgl_batch_autotune(rgl_context* c, const rgl_batch* b, uint64_t sub_batch, r
     const SubBatch sb = P.subs[big];
     RGL_TRY(ensure_workspace(c, sb.n, sb.rows, sb.nblk));
     cudaStream_t st = c->stream;
-    RGL_TRY(c->bt_off.ensure(P.off.size() * 8 + 8));
+    const std::vector<uint64_t> ot = P.off_table();
+    RGL_TRY(c->bt_off.ensure(ot.size() * 8 + 8));
     const std::vector<uint32_t> sr = P.shard_rows();
     RGL_TRY(c->bt_shard.ensure(sr.size() * 4 + 4));
-    RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, P.off.data(), P.off.size() * 8, cudaMemcpyHostToDevice, st));
+    RGL_CUDA(cudaMemcpyAsync(c->bt_off.p, ot.data(), ot.size() * 8, cudaMemcpyHostToDevice, st));
     RGL_CUDA(cudaMemcpyAsync(c->bt_shard.p, sr.data(), sr.size() * 4, cudaMemcpyHostToDevice, st));
-    PipeIn in{b->d_intervals + sb.begin, sb.n, sb.rows, sb.row_lo, sb.nblk, c->bt_off.as<uint64_t>() + sb.tab_at,
-              c->bt_shard.as<uint32_t>() + sb.tab_at,
-              b->block_rows ? c->bt_shard.as<uint32_t>() + P.shard.size() + sb.tab_at : nullptr};
-    in.block_local = P.local(sb, b->block_rows != nullptr);
+    PipeIn in = P.pipe_in(big, b->d_intervals + sb.begin, c->bt_off.as<uint64_t>(), c->bt_shard.as<uint32_t>(),
+                          b->block_rows != nullptr);
     set_regions(in, batch_region_bits(nullptr, sb.rows));
     const bool was_timing = c->timing;
     *best = rgl_query_opts{};
@@ -2702,6 +3055,7 @@ int rgl_query_pairs(rgl_context* c, const rgl_query_batch* b, uint64_t capacity,
     q.pair_ratio = 0xFFFFFFFFu;
     PipeIn in{c->iv.as<rgl_interval>(), n, b->num_rows, 0, (uint32_t)blocks.size(), c->blk_off.as<uint64_t>(),
               c->blk_shard.as<uint32_t>(), nullptr};
+    in.block_local = blocks_local((uint32_t)blocks.size(), off.data(), ids.data(), nullptr, b->num_rows, 0, &in.ls);
     PipeMode m;
     m.zero_out = false;
     m.no_sweep = true;

@@ -51,6 +51,9 @@ struct Worker {
     uint64_t* h_bp = nullptr;
     double *h_p = nullptr, *h_llr = nullptr, *h_lp = nullptr;
     uint8_t* h_fl = nullptr;
+    // the end of a batch, waited on with a blocking (not spinning) synchronisation: several workers
+    // spinning on their streams would take host cores from the callers and from each other
+    cudaEvent_t done = nullptr;
     std::thread th;
 };
 
@@ -136,7 +139,8 @@ int run_batch(rgl_server* S, Worker* W, const std::vector<Req*>& batch) {
         RGL_CUDA(cudaMemcpyAsync(W->h_lp, W->dlp.p, cells * 8, cudaMemcpyDeviceToHost, st));
         RGL_CUDA(cudaMemcpyAsync(W->h_fl, W->dfl.p, cells, cudaMemcpyDeviceToHost, st));
     }
-    RGL_CUDA(cudaStreamSynchronize(st));
+    RGL_CUDA(cudaEventRecord(W->done, st));
+    RGL_CUDA(cudaEventSynchronize(W->done));
     RGL_TRY(context_errors(c));
     const size_t D = S->D;
     for (uint32_t j = 0; j < R; j++) {
@@ -230,6 +234,23 @@ void complete(rgl_server* S, const std::vector<Req*>& batch, const std::vector<i
     }
 }
 
+// Whether the batch the worker would form now (the oldest pending requests within
+// max_batch_requests and batch_intervals) needs any device memory beyond what the worker holds;
+// called with the server's lock held.  Growth is monotonic in the batch, so the whole tentative
+// batch answers for each of its prefixes.
+bool formation_grows(rgl_server* S, Worker* W) {
+    uint64_t n = 0;
+    uint32_t R = 0, nblk = 0;
+    for (Req* q : S->pending) {
+        if (R >= S->o.max_batch_requests || (R && n + q->n > S->o.batch_intervals)) break;
+        n += q->n;
+        nblk += (uint32_t)q->shards.size();
+        R++;
+    }
+    uint64_t need = 0;
+    return batch_growth(S, W, n, R, nblk, &need) != RGL_OK || need > 0;
+}
+
 void worker_main(rgl_server* S, Worker* W) {
     cudaSetDevice(S->device);
     std::vector<Req*> batch, refused;
@@ -237,14 +258,25 @@ void worker_main(rgl_server* S, Worker* W) {
         uint64_t n = 0, promise = 0;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty(); });
-            if (S->pending.empty()) return;  // stop requested and the queue is drained
+            // admission needs the free device memory only when the batch would grow this worker's
+            // buffers; the query (which can take milliseconds) runs without the lock, so that
+            // submissions and the other workers do not wait on it
+            uint64_t free_b = 0;
+            bool have_free = false;
+            for (;;) {
+                S->cv_work.wait(lk, [&] { return S->stop || !S->pending.empty(); });
+                if (S->pending.empty()) return;  // stop requested and the queue is drained
+                if (have_free || !formation_grows(S, W)) break;
+                lk.unlock();
+                free_b = free_device_memory(S);
+                have_free = true;
+                lk.lock();
+            }
             batch.clear();
             refused.clear();
-            // admission: what the device can still give this worker now
-            const uint64_t free_b = free_device_memory(S);
+            // what the device can still give this worker now (unbounded when nothing grows)
             const uint64_t keep = S->o.hbm_reserve_bytes + S->promised;
-            const uint64_t avail = free_b > keep ? free_b - keep : 0;
+            const uint64_t avail = !have_free ? ~0ull : free_b > keep ? free_b - keep : 0;
             uint32_t nblk = 0;
             while (!S->pending.empty() && batch.size() < S->o.max_batch_requests) {
                 Req* q = S->pending.front();
@@ -252,6 +284,7 @@ void worker_main(rgl_server* S, Worker* W) {
                 uint64_t need = 0;
                 const uint32_t qb = (uint32_t)q->shards.size();
                 if (batch_growth(S, W, n + q->n, (uint32_t)batch.size() + 1, nblk + qb, &need) != RGL_OK) need = ~0ull;
+                if (need > 0 && !have_free) break;  // requests queued since the check: next round
                 if (need > avail) {
                     if (!batch.empty()) {
                         S->memory_limited++;
@@ -312,6 +345,7 @@ void worker_main(rgl_server* S, Worker* W) {
 
 void destroy_worker(Worker* W) {
     if (W->ctx) rgl_context_destroy(W->ctx);
+    if (W->done) cudaEventDestroy(W->done);
     for (DevBuf* b : {&W->stage, &W->dc, &W->dbp, &W->dp, &W->dllr, &W->dlp, &W->dfl}) b->release();
     stats_scratch_release(&W->sc);
     for (void* h : {(void*)W->h_counts, (void*)W->h_bp, (void*)W->h_p, (void*)W->h_llr, (void*)W->h_lp, (void*)W->h_fl})
@@ -320,6 +354,7 @@ void destroy_worker(Worker* W) {
 
 int make_worker(rgl_server* S, Worker* W) {
     RGL_TRY(rgl_context_create(S->idx, nullptr, &W->ctx));
+    RGL_CUDA(cudaEventCreateWithFlags(&W->done, cudaEventBlockingSync | cudaEventDisableTiming));
     const uint64_t cap = S->o.initial_intervals;
     const uint32_t R = S->o.max_batch_requests;
     // blocks per batch: at most one per (request, shard) for requests built from the shard list;

@@ -171,10 +171,12 @@ def test_config1_parity_with_oracle():
 
 
 def test_block_local_sort_equals_radix_sort():
-    """With one row and one block per chromosome of at most 16,384 query intervals, the keys are
-    sorted block by block in shared memory (copied through when a block is already in order);
-    otherwise by the device-wide radix sort.  Both must give the oracle's counts and overlaps, on
-    unsorted blocks, an already sorted block, a block at the cap and one just above it."""
+    """With one row and one block per chromosome, the keys are sorted block by block: tiles of
+    4,096 intervals in shared memory (copied through when a block is already in order), then merge
+    passes for larger blocks; with a chromosome in two blocks, by the device-wide radix sort.  Both
+    must give the oracle's counts and overlaps: unsorted blocks, sorted ones (starts in order, ends
+    not), blocks of 1 to 35 tiles (0 to 6 merge passes, blocks of different pass counts in one run),
+    equal starts and whole duplicates."""
     rng = np.random.default_rng(11)
     D = 23
     blocks = [(sh, helpers.random_db(rng, 30000, 2_000_000, D)) for sh in range(2)]
@@ -188,40 +190,17 @@ def test_block_local_sort_equals_radix_sort():
 
     idx = rg.Index.from_layers(layers, D, ["s0", "s1"])
     ctx = rg.Context(idx)
-    for n0, n1, presorted in ((5000, 700, False), (16384, 3000, True), (16384, 16385, False)):
+    cases = ((5000, 700, False, False), (16384, 3000, True, False), (16384, 16385, False, False),
+             (40000, 16385, False, True), (70001, 33000, True, False), (140000, 50000, False, True))
+    for n0, n1, sort0, sort1 in cases:
         q0, q1 = queries(blocks[0][1], n0), queries(blocks[1][1], n1)
-        if presorted:
+        if sort0:
             q0 = q0[np.lexsort((q0[:, 1], q0[:, 0]))]
+        if sort1:
+            q1 = q1[np.lexsort((q1[:, 1], q1[:, 0]))]
         oc, _, obp, _ = O.query_database(layers, {0: q0.copy(), 1: q1.copy()}, 1, D, threads=4)
         local = ctx.query_counts({"s0": q0, "s1": q1}, 1)  # one block per chromosome
         k = n0 // 3
         split = ctx.query_counts({"s0": q0[:k], 0: q0[k:], "s1": q1}, 1)  # chromosome 0 in two blocks
         for c, bp, _ in (local, split):
-            assert (c == oc).all() and (bp == obp).all(), (n0, n1, presorted)
-    ctx.close()
-    idx.close()
-
-
-def test_blocks_adjacent_in_host_memory():
-    """Chromosome blocks that are consecutive slices of one host buffer travel in one copy; the
-    result equals that of separately allocated blocks (and the oracle's)."""
-    rng = np.random.default_rng(12)
-    D, nsh = 17, 4
-    blocks = [(sh, helpers.random_db(rng, 8000, 2_000_000, D)) for sh in range(nsh)]
-    layers = rg.bucket_layers(blocks)
-    parts = [helpers.queries_touching(rng, b, 900, 2) for _, b in blocks]
-    buf = np.concatenate(parts)
-    views, at = {}, 0
-    for sh, p in enumerate(parts):
-        views[f"s{sh}"] = buf[at:at + len(p)]  # views into one buffer, back to back
-        at += len(p)
-    oc, _, obp, _ = O.query_database(layers, {sh: p.copy() for sh, p in enumerate(parts)}, 2, D, threads=4)
-    idx = rg.Index.from_layers(layers, D, [f"s{i}" for i in range(nsh)])
-    ctx = rg.Context(idx)
-    a = ctx.query_counts(views, 2)
-    b = ctx.query_counts({f"s{sh}": p.copy() for sh, p in enumerate(parts)}, 2)
-    rev = ctx.query_counts({k: views[k] for k in reversed(list(views))}, 2)  # adjacent, but in reverse order
-    for c, bp, _ in (a, b, rev):
-        assert (c == oc).all() and (bp == obp).all()
-    ctx.close()
-    idx.close()
+            assert (c == oc).all() and (bp == obp).all(), (n0, n1, sort0, sort1)
