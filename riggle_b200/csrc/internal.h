@@ -84,6 +84,7 @@ struct DevBuf {
 // Scratch of the batched stats stage (query length groups of a batch); one per concurrent caller.
 struct StatsScratch {
     DevBuf key_a, key_b, len_a, len_b, ukey, agg, runs, groups, goff, tmp;
+    DevBuf plan;  // block-local form: the sort's plan and order flags, run-head counts per tile
 };
 
 }  // namespace rgl

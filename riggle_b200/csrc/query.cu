@@ -36,6 +36,7 @@
 #include <cstring>
 #include <type_traits>
 
+#include "block_sort.cuh"
 #include "internal.h"
 
 namespace rgl {
@@ -182,247 +183,6 @@ __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, c
     key[o] = (seg << 32) | s;
     val[o] = e;
     ekey[o] = (seg << 32) | e;
-}
-
-// ---- 2. block-local key sort ---------------------------------------------------------------------
-// For runs in which every input block holds one segment ((shard, row)) and no two blocks share one,
-// the segment-major order of a device-wide sort is the blocks' own order with each block sorted by
-// position, so the keys are sorted block by block, at any block size:
-//   * k_expand_keys marks a block whose starts (ends) are not in order (the usual sorted BED input
-//     has its starts in order; its ends are in order unless an interval contains the next one);
-//   * k_sort_plan lays the blocks out as tiles of kBlockSortCap intervals and, for blocks of more
-//     than one tile, merge chunks of kMergeChunk output positions;
-//   * k_tile_sort copies a tile of an ordered block to its place, or sorts it in shared memory (a
-//     radix sort over the bits its positions use; a tile already in order is copied through);
-//   * merge passes q = 1, 2, ... combine sorted runs of kBlockSortCap << (q - 1) pairwise until each
-//     block is one run: every CTA takes kMergeChunk outputs of one run pair, finds where they start
-//     in both runs by a merge-path search, and merges them in shared memory.
-// Every step is stable (equal positions keep their input order), like the radix sort it replaces.
-// A block that needs p merge passes has its tiles written where p ping-pong passes end in the
-// output buffer (in place into the input buffer when p is odd), so blocks of different sizes share
-// the passes and all finish in the output.
-constexpr int kBsThreads = 256, kBsItems = 16;
-constexpr uint64_t kBlockSortCap = (uint64_t)kBsThreads * kBsItems;
-constexpr int kMergeThreads = 256, kMergeItems = 8;
-constexpr uint32_t kMergeChunk = (uint32_t)(kMergeThreads * kMergeItems);
-static_assert(kBlockSortCap % kMergeChunk == 0, "a merge chunk lies inside one run pair");
-
-__host__ __device__ inline uint32_t sort_tiles(uint64_t cnt) {
-    return (uint32_t)((cnt + kBlockSortCap - 1) / kBlockSortCap);
-}
-__host__ __device__ inline uint32_t sort_passes(uint64_t cnt) {
-    const uint32_t t = sort_tiles(cnt);
-    uint32_t p = 0;
-    while ((1u << p) < t) p++;
-    return p;
-}
-__host__ __device__ inline uint32_t merge_chunks(uint64_t cnt) {
-    return cnt > kBlockSortCap ? (uint32_t)((cnt + kMergeChunk - 1) / kMergeChunk) : 0u;
-}
-
-// The block b with pre[b] <= x < pre[b + 1] (pre: nblk + 1 non-decreasing prefix counts, x < pre[nblk]).
-__device__ inline uint32_t find_block(const uint32_t* __restrict__ pre, uint32_t nblk, uint32_t x) {
-    uint32_t lo = 0, hi = nblk;
-    while (hi - lo > 1) {
-        const uint32_t m = (lo + hi) >> 1;
-        if (__ldg(pre + m) <= x) lo = m; else hi = m;
-    }
-    return lo;
-}
-
-// Exclusive prefix counts of the blocks' tiles and merge chunks, by one thread block: each thread
-// sums a contiguous stretch of blocks, a block scan of the stretch totals gives each stretch its
-// offset, and the stretch is written.
-__global__ void __launch_bounds__(1024) k_sort_plan(uint32_t nblk, const uint64_t* __restrict__ blk_off,
-                                                    uint32_t* __restrict__ tile_pre, uint32_t* __restrict__ chunk_pre) {
-    __shared__ uint32_t pt[1024], pc[1024];
-    const uint32_t t = threadIdx.x;
-    const uint32_t per = (nblk + 1023) / 1024;
-    const uint32_t a = min(t * per, nblk), b = min(a + per, nblk);
-    uint32_t st = 0, sc = 0;
-    for (uint32_t i = a; i < b; i++) {
-        const uint64_t cnt = blk_off[i + 1] - blk_off[i];
-        st += sort_tiles(cnt);
-        sc += merge_chunks(cnt);
-    }
-    pt[t] = st;
-    pc[t] = sc;
-    __syncthreads();
-    for (uint32_t off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scan of the totals
-        const uint32_t vt = t >= off ? pt[t - off] : 0u, vc = t >= off ? pc[t - off] : 0u;
-        __syncthreads();
-        pt[t] += vt;
-        pc[t] += vc;
-        __syncthreads();
-    }
-    uint32_t rt = t ? pt[t - 1] : 0u, rc = t ? pc[t - 1] : 0u;
-    for (uint32_t i = a; i < b; i++) {
-        tile_pre[i] = rt;
-        chunk_pre[i] = rc;
-        const uint64_t cnt = blk_off[i + 1] - blk_off[i];
-        rt += sort_tiles(cnt);
-        rc += merge_chunks(cnt);
-    }
-    if (t == 1023) {
-        tile_pre[nblk] = pt[1023];
-        chunk_pre[nblk] = pc[1023];
-    }
-}
-
-template <bool VALUES>
-struct BlockSortTypes {
-    using Sort = cub::BlockRadixSort<uint32_t, kBsThreads, kBsItems, typename std::conditional<VALUES, uint32_t, cub::NullType>::type>;
-    union Smem {
-        typename Sort::TempStorage sort;
-        uint32_t last[kBsThreads];
-    };
-};
-
-// One tile per thread block (grid: an upper bound of the tiles; CTAs past the last tile return).
-// With VALUES the start keys with their ends as values (key_a / val_a), else the end keys alone.
-// unsorted[b] != 0: block b is not in order.  Output: `out` when the block is in order or needs
-// an even number of merge passes, else in place (`in`).
-template <bool VALUES>
-__global__ void __launch_bounds__(kBsThreads) k_tile_sort(uint32_t nblk, const uint64_t* __restrict__ blk_off,
-                                                            const uint32_t* __restrict__ tile_pre,
-                                                            const uint32_t* __restrict__ unsorted, uint64_t* kin,
-                                                            uint32_t* vin, uint64_t* __restrict__ kout,
-                                                            uint32_t* __restrict__ vout) {
-    using T = BlockSortTypes<VALUES>;
-    extern __shared__ __align__(16) unsigned char bs_smem[];
-    typename T::Smem& sm = *reinterpret_cast<typename T::Smem*>(bs_smem);
-    const uint32_t tile = blockIdx.x;
-    if (tile >= __ldg(tile_pre + nblk)) return;
-    const uint32_t blk = find_block(tile_pre, nblk, tile);
-    const uint64_t bbeg = blk_off[blk], bcnt = blk_off[blk + 1] - bbeg;
-    const uint64_t base = bbeg + (uint64_t)(tile - tile_pre[blk]) * kBlockSortCap;
-    const uint64_t rest = bbeg + bcnt - base;
-    const uint32_t cnt = (uint32_t)(rest < kBlockSortCap ? rest : kBlockSortCap);
-    const bool ordered = unsorted[blk] == 0u;
-    uint64_t* ko = (ordered || !(sort_passes(bcnt) & 1u)) ? kout : kin;
-    uint32_t* vo = (ordered || !(sort_passes(bcnt) & 1u)) ? vout : vin;
-    const uint64_t hi = kin[base] & 0xFFFFFFFF00000000ull;  // the block's segment, in the high word
-    uint32_t k[kBsItems], v[kBsItems];
-    uint32_t any = 0;
-    bool ok = true;
-#pragma unroll
-    for (int j = 0; j < kBsItems; j++) {
-        const uint32_t i = threadIdx.x * kBsItems + j;  // blocked: thread t holds [16 t, 16 t + 16)
-        k[j] = i < cnt ? (uint32_t)kin[base + i] : 0xFFFFFFFFu;  // padding sorts last
-        v[j] = (VALUES && i < cnt) ? vin[base + i] : 0u;
-        any |= i < cnt ? k[j] : 0u;
-        if (j) ok = ok && k[j - 1] <= k[j];
-    }
-    __shared__ uint32_t s_bits;  // bitwise OR of the tile's keys
-    sm.last[threadIdx.x] = k[kBsItems - 1];
-    if (threadIdx.x == 0) s_bits = 0;
-    __syncthreads();
-    if (threadIdx.x) ok = ok && sm.last[threadIdx.x - 1] <= k[0];
-    any = __reduce_or_sync(0xffffffffu, any);
-    if ((threadIdx.x & 31u) == 0) atomicOr(&s_bits, any);
-    // also orders every read of the tile before the in-place writes below, and the atomicOr
-    // before the read of s_bits
-    const bool sorted = __syncthreads_and(ok);
-    const uint32_t bits = s_bits;
-    if (!sorted) {
-        const int end_bit = bits ? 32 - __clz(bits) : 1;
-        if constexpr (VALUES)
-            typename T::Sort(sm.sort).Sort(k, v, 0, end_bit);
-        else
-            typename T::Sort(sm.sort).Sort(k, 0, end_bit);
-    }
-#pragma unroll
-    for (int j = 0; j < kBsItems; j++) {
-        const uint32_t i = threadIdx.x * kBsItems + j;
-        if (i < cnt) {
-            ko[base + i] = hi | k[j];
-            if (VALUES) vo[base + i] = v[j];
-        }
-    }
-}
-
-template <bool VALUES>
-constexpr size_t block_sort_smem() { return sizeof(typename BlockSortTypes<VALUES>::Smem); }
-
-// Merge-path split of output diagonal d of runs a (na keys) and b (nb keys): the number of the d
-// first outputs that come from a, ties going to a (stability).
-template <class K>
-__device__ inline uint32_t merge_split(const K* a, uint32_t na, const K* b, uint32_t nb, uint32_t d) {
-    uint32_t lo = d > nb ? d - nb : 0u, hi = min(d, na);
-    while (lo < hi) {
-        const uint32_t m = (lo + hi) >> 1;
-        if ((uint32_t)a[m] <= (uint32_t)b[d - 1 - m]) lo = m + 1; else hi = m;
-    }
-    return lo;
-}
-
-// Merge pass q (1-based) of the block sort: one CTA per merge chunk (grid: an upper bound of the
-// chunks; CTAs past the last chunk, of ordered blocks or of blocks needing fewer passes return).
-// A block needing p passes reads buffer A at pass q when p - q + 1 is odd, else B, and writes the
-// other one.
-template <bool VALUES>
-__global__ void __launch_bounds__(kMergeThreads) k_merge_pass(uint32_t q, uint32_t nblk,
-                                                              const uint64_t* __restrict__ blk_off,
-                                                              const uint32_t* __restrict__ chunk_pre,
-                                                              const uint32_t* __restrict__ unsorted, uint64_t* ka,
-                                                              uint32_t* va, uint64_t* kb, uint32_t* vb) {
-    __shared__ uint32_t sk[kMergeChunk], sv[VALUES ? kMergeChunk : 1];
-    __shared__ uint32_t ok[kMergeChunk], ov[VALUES ? kMergeChunk : 1];
-    __shared__ uint32_t s_split[2];
-    const uint32_t chunk = blockIdx.x;
-    if (chunk >= __ldg(chunk_pre + nblk)) return;
-    const uint32_t blk = find_block(chunk_pre, nblk, chunk);
-    if (unsorted[blk] == 0u) return;
-    const uint64_t bbeg = blk_off[blk];
-    const uint32_t cnt = (uint32_t)(blk_off[blk + 1] - bbeg);
-    const uint32_t p = sort_passes(cnt);
-    if (p < q) return;
-    const bool from_a = ((p - q + 1) & 1u) != 0u;
-    const uint64_t* ks = (from_a ? ka : kb) + bbeg;
-    const uint32_t* vs = (from_a ? va : vb) + bbeg;
-    uint64_t* kd = (from_a ? kb : ka) + bbeg;
-    uint32_t* vd = (from_a ? vb : va) + bbeg;
-    const uint32_t o0 = (chunk - chunk_pre[blk]) * kMergeChunk, o1 = min(o0 + kMergeChunk, cnt);
-    const uint32_t L = (uint32_t)kBlockSortCap << (q - 1);  // run length of this pass
-    const uint32_t pa = (uint32_t)(((uint64_t)o0 / (2ull * L)) * 2ull * L);  // start of the run pair
-    const uint32_t na = min(L, cnt - pa), nb = cnt - pa > L ? min(L, cnt - pa - L) : 0u;
-    const uint32_t d0 = o0 - pa, d1 = o1 - pa;
-    const uint64_t hi = ks[0] & 0xFFFFFFFF00000000ull;
-    if (nb == 0) {  // a lone run: copy
-        for (uint32_t x = o0 + threadIdx.x; x < o1; x += kMergeThreads) {
-            kd[x] = ks[x];
-            if (VALUES) vd[x] = vs[x];
-        }
-        return;
-    }
-    const uint64_t* A = ks + pa;
-    const uint64_t* B = ks + pa + L;
-    if (threadIdx.x < 2) s_split[threadIdx.x] = merge_split(A, na, B, nb, threadIdx.x ? d1 : d0);
-    __syncthreads();
-    const uint32_t i0 = s_split[0], i1 = s_split[1];
-    const uint32_t j0 = d0 - i0, j1 = d1 - i1;
-    const uint32_t ca = i1 - i0, cb = j1 - j0, tot = ca + cb;
-    for (uint32_t x = threadIdx.x; x < tot; x += kMergeThreads) {
-        const bool in_a = x < ca;
-        const uint32_t src = in_a ? pa + i0 + x : pa + L + j0 + (x - ca);
-        sk[x] = (uint32_t)ks[src];
-        if (VALUES) sv[x] = vs[src];
-    }
-    __syncthreads();
-    // each thread merges kMergeItems outputs from its own split of the staged windows
-    const uint32_t dd = min((uint32_t)threadIdx.x * kMergeItems, tot);
-    uint32_t ia = merge_split(sk, ca, sk + ca, cb, dd), ib = dd - ia;
-    for (uint32_t m = 0; m < (uint32_t)kMergeItems && dd + m < tot; m++) {
-        const bool take_a = ib >= cb || (ia < ca && sk[ia] <= sk[ca + ib]);
-        const uint32_t from = take_a ? ia++ : ca + ib++;
-        ok[dd + m] = sk[from];
-        if (VALUES) ov[dd + m] = sv[from];
-    }
-    __syncthreads();
-    for (uint32_t x = threadIdx.x; x < tot; x += kMergeThreads) {
-        kd[o0 + x] = hi | ok[x];
-        if (VALUES) vd[o0 + x] = ov[x];
-    }
 }
 
 // The sorted start keys into starts, segment ids, segment-start flags and the starts' prefix-sum
@@ -2014,32 +1774,19 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     launches++;
     // the sort's view of the blocks: their offsets in the layout the keys were written in
     const uint64_t* soff = sort_dst ? sort_off : in.blk_off;
-    if (in.block_local) {
-        k_sort_plan<<<1, 1024, 0, st>>>(in.nblk, soff, d_tile_pre, d_chunk_pre);
-        launches++;
-    }
+    const uint32_t passes = in.block_local ? sort_passes(in.ls.max_block) : 0u;
+    if (in.block_local)  // the plan (before the fork), then the end keys here and the start keys there
+        launches += block_sort_enqueue(in.nblk, soff, 0, 0, 0, d_tile_pre, d_chunk_pre, nullptr, nullptr, nullptr,
+                                       nullptr, nullptr, st, true);
     RGL_TRY(stream_after(sd, st, c->ev_fork));
     size_t tb = c->cub_tmp2.cap;
     if (in.block_local) {
-        const unsigned tiles = (unsigned)std::max<uint64_t>(in.ls.tiles, 1);
-        const unsigned chunks = (unsigned)std::max<uint64_t>(in.ls.chunks, 1);
-        const uint32_t passes = sort_passes(in.ls.max_block);
-        k_tile_sort<false><<<tiles, kBsThreads, block_sort_smem<false>(), sd>>>(
-            in.nblk, soff, d_tile_pre, d_unsorted + in.nblk, c->ekey_a.as<uint64_t>(), nullptr,
-            c->ekey_b.as<uint64_t>(), nullptr);
-        k_tile_sort<true><<<tiles, kBsThreads, block_sort_smem<true>(), st>>>(
-            in.nblk, soff, d_tile_pre, d_unsorted, c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
-            c->key_b.as<uint64_t>(), c->val_b.as<uint32_t>());
-        launches += 2;
-        for (uint32_t q = 1; q <= passes; q++) {
-            k_merge_pass<false><<<chunks, kMergeThreads, 0, sd>>>(q, in.nblk, soff, d_chunk_pre,
-                                                                  d_unsorted + in.nblk, c->ekey_a.as<uint64_t>(),
-                                                                  nullptr, c->ekey_b.as<uint64_t>(), nullptr);
-            k_merge_pass<true><<<chunks, kMergeThreads, 0, st>>>(q, in.nblk, soff, d_chunk_pre, d_unsorted,
-                                                                 c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
-                                                                 c->key_b.as<uint64_t>(), c->val_b.as<uint32_t>());
-            launches += 2;
-        }
+        launches += block_sort_enqueue(in.nblk, soff, in.ls.tiles, in.ls.chunks, passes, d_tile_pre, d_chunk_pre,
+                                       d_unsorted + in.nblk, c->ekey_a.as<uint64_t>(), nullptr,
+                                       c->ekey_b.as<uint64_t>(), nullptr, sd, false);
+        launches += block_sort_enqueue(in.nblk, soff, in.ls.tiles, in.ls.chunks, passes, d_tile_pre, d_chunk_pre,
+                                       d_unsorted, c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
+                                       c->key_b.as<uint64_t>(), c->val_b.as<uint32_t>(), st, false);
     } else {
         RGL_CUDA(cub::DeviceRadixSort::SortKeys(c->cub_tmp2.p, tb, c->ekey_a.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
                                                 (int)n, 0, 32 + segbits, sd));
@@ -2597,12 +2344,7 @@ int rgl_context_create(rgl_index* index, void* stream, rgl_context** out) {
             cudaFuncSetAttribute(k_pairs<true, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
                 cudaSuccess ||
             cudaFuncSetAttribute(k_pairs<false, true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) !=
-                cudaSuccess ||
-
-            cudaFuncSetAttribute(k_tile_sort<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)block_sort_smem<true>()) != cudaSuccess ||
-            cudaFuncSetAttribute(k_tile_sort<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)block_sort_smem<false>()) != cudaSuccess)
+                cudaSuccess)
             s = fail(RGL_ERR_DEVICE, "cudaFuncSetAttribute");
     }
     for (int i = 0; i < 4 && s == RGL_OK; i++)

@@ -23,6 +23,7 @@
 #include <thread>
 #include <unordered_map>
 
+#include "block_sort.cuh"
 #include "internal.h"
 
 namespace rgl {
@@ -162,6 +163,12 @@ int run_batch(rgl_server* S, Worker* W, const std::vector<Req*>& batch) {
 
 uint64_t grow(const DevBuf& b, uint64_t bytes) { return bytes > b.cap ? bytes - b.cap : 0; }
 
+// The stats stage's plan scratch for n intervals in nblk blocks (its tiles are at most
+// n / kBlockSortCap + nblk): sort plan, order flags and run-head counts (StatsScratch::plan).
+uint64_t stats_plan_bytes(uint64_t n, uint32_t nblk) {
+    return (3ull * nblk + 2 * (n / kBlockSortCap + nblk) + 8) * 4;
+}
+
 // Device bytes worker W would allocate to run a batch of n intervals in nblk blocks over R rows.
 int batch_growth(rgl_server* S, Worker* W, uint64_t n, uint32_t R, uint32_t nblk, uint64_t* bytes) {
     uint64_t ws = 0;
@@ -175,14 +182,14 @@ int batch_growth(rgl_server* S, Worker* W, uint64_t n, uint32_t R, uint32_t nblk
         // the stats stage's scratch: keys, lengths, runs and groups per interval (StatsScratch)
         b += grow(W->sc.key_a, n * 8 + 8) + grow(W->sc.key_b, n * 8 + 8) + grow(W->sc.len_a, n * 4 + 4) +
              grow(W->sc.len_b, n * 4 + 4) + grow(W->sc.ukey, n * 8 + 8) + grow(W->sc.agg, n * 32 + 32) +
-             grow(W->sc.groups, n * 40 + 40);
+             grow(W->sc.groups, n * 40 + 40) + grow(W->sc.plan, stats_plan_bytes(n, nblk));
     }
     *bytes = b;
     return RGL_OK;
 }
 
 // Grows the worker's device buffers for a batch (the workspace grows inside the pipeline call).
-int size_worker(rgl_server* S, Worker* W, uint64_t n, uint32_t R) {
+int size_worker(rgl_server* S, Worker* W, uint64_t n, uint32_t R, uint32_t nblk) {
     const uint64_t cells = (uint64_t)R * S->D;
     RGL_TRY(W->stage.ensure(std::max<uint64_t>(n, 1) * sizeof(rgl_interval)));
     RGL_TRY(W->dc.ensure(cells * 4 + 16));
@@ -200,6 +207,7 @@ int size_worker(rgl_server* S, Worker* W, uint64_t n, uint32_t R) {
         RGL_TRY(W->sc.ukey.ensure(nn * 8 + 8));
         RGL_TRY(W->sc.agg.ensure(nn * 32 + 32));
         RGL_TRY(W->sc.groups.ensure(nn * 40 + 40));
+        RGL_TRY(W->sc.plan.ensure(stats_plan_bytes(nn, nblk)));
     }
     return RGL_OK;
 }
@@ -256,6 +264,7 @@ void worker_main(rgl_server* S, Worker* W) {
     std::vector<Req*> batch, refused;
     for (;;) {
         uint64_t n = 0, promise = 0;
+        uint32_t nblk = 0;
         {
             std::unique_lock<std::mutex> lk(S->mu);
             // admission needs the free device memory only when the batch would grow this worker's
@@ -277,7 +286,6 @@ void worker_main(rgl_server* S, Worker* W) {
             // what the device can still give this worker now (unbounded when nothing grows)
             const uint64_t keep = S->o.hbm_reserve_bytes + S->promised;
             const uint64_t avail = !have_free ? ~0ull : free_b > keep ? free_b - keep : 0;
-            uint32_t nblk = 0;
             while (!S->pending.empty() && batch.size() < S->o.max_batch_requests) {
                 Req* q = S->pending.front();
                 if (!batch.empty() && n + q->n > S->o.batch_intervals) break;
@@ -321,7 +329,7 @@ void worker_main(rgl_server* S, Worker* W) {
         }
         if (batch.empty()) continue;
         std::vector<int> status(batch.size(), RGL_OK);
-        int s = size_worker(S, W, n, (uint32_t)batch.size());
+        int s = size_worker(S, W, n, (uint32_t)batch.size(), nblk);
         if (s == RGL_OK) s = run_batch(S, W, batch);
         {
             std::lock_guard<std::mutex> lk(S->mu);  // the growth has happened: free memory shows it now
@@ -360,7 +368,7 @@ int make_worker(rgl_server* S, Worker* W) {
     // blocks per batch: at most one per (request, shard) for requests built from the shard list;
     // larger block tables grow the workspace on demand
     RGL_TRY(context_reserve_rows(W->ctx, cap, 0, R * std::max<uint32_t>(S->idx->num_shards, 1)));
-    RGL_TRY(size_worker(S, W, cap, R));
+    RGL_TRY(size_worker(S, W, cap, R, R * std::max<uint32_t>(S->idx->num_shards, 1)));
     const size_t cells = (size_t)R * S->D + 16;
     RGL_CUDA(cudaMallocHost(&W->h_counts, cells * 4));
     RGL_CUDA(cudaMallocHost(&W->h_bp, cells * 8));

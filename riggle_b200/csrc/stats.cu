@@ -18,6 +18,7 @@
 #include <cmath>
 #include <cstring>
 
+#include "block_sort.cuh"
 #include "internal.h"
 
 namespace rgl {
@@ -186,13 +187,14 @@ struct LenToAgg {
 };
 
 constexpr uint64_t kNoGroup = ~0ull;
+constexpr uint32_t kNoLen = 0xFFFFFFFFu;  // block-local keys: the low word of an interval in no group
 // the request server sizes each worker's StatsScratch with these record sizes
 static_assert(sizeof(LenAgg) == 32 && sizeof(QGroupDev) == 40, "stats scratch record sizes changed");
 
 __global__ void k_group_keys(uint64_t n, const rgl_interval* __restrict__ iv, const uint64_t* __restrict__ blk_off,
                              const uint32_t* __restrict__ blk_shard, const uint32_t* __restrict__ blk_row, uint32_t nblk,
                              const uint32_t* __restrict__ shard_chrom, uint32_t nshards, uint32_t C,
-                             const uint64_t* __restrict__ n_bins, double bin, uint64_t* __restrict__ key,
+                             const uint64_t* __restrict__ n_bins, double bin, int local, uint64_t* __restrict__ key,
                              uint32_t* __restrict__ len_out) {
     const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (j >= n) return;
@@ -213,8 +215,146 @@ __global__ void k_group_keys(uint64_t n, const rgl_interval* __restrict__ iv, co
         // groups with l_int >= n_bins never meet a moment (src/io/momentstore.rs:66-79)
         if (li < n_bins[c]) k = (((uint64_t)blk_row[lo] * C + c) << 32) | li;
     }
+    // block-local form: every key of a block carries the block's (row, chromosome) in its high word
+    // (all ones without a chromosome), an interval that joins no group kNoLen in its low word
+    if (local && k == kNoGroup)
+        k = ((c < C ? (uint64_t)blk_row[lo] * C + c : 0xFFFFFFFFull) << 32) | kNoLen;
     key[j] = k;
     len_out[j] = len;
+}
+
+// ---- the groups of block-sorted keys ------------------------------------------------------------
+// After the block-local sort every block's keys are in ascending l_int order, and the blocks come in
+// ascending (row, chromosome) order: the groups are the runs of equal keys, in order.  Run heads
+// are counted per tile of the sort (k_run_count), the counts scanned (k_scan_small), heads and tails
+// placed (k_run_emit) and each run summed by one warp (k_run_agg), with the exact integer sums of
+// the device-wide form.
+constexpr int kRunThreads = 256;
+
+__device__ inline uint32_t tile_block(const uint32_t* __restrict__ pre, uint32_t nblk, uint32_t x) {
+    uint32_t lo = 0, hi = nblk;  // pre[lo] <= x < pre[lo + 1]
+    while (hi - lo > 1) {
+        const uint32_t m = (lo + hi) >> 1;
+        if (__ldg(pre + m) <= x) lo = m; else hi = m;
+    }
+    return lo;
+}
+
+// Whether sorted element g (block [bbeg, bend)) starts a run / ends a run of a usable key.
+__device__ inline bool run_head(const uint64_t* __restrict__ key, uint64_t bbeg, uint64_t g) {
+    const uint64_t k = key[g];
+    return (uint32_t)k != kNoLen && (g == bbeg || key[g - 1] != k);
+}
+__device__ inline bool run_tail(const uint64_t* __restrict__ key, uint64_t bend, uint64_t g) {
+    const uint64_t k = key[g];
+    return (uint32_t)k != kNoLen && (g + 1 == bend || key[g + 1] != k);
+}
+
+// tile_heads[t] = run heads among the elements of tile t (tiles of kBlockSortCap per block).
+__global__ void __launch_bounds__(kRunThreads) k_run_count(uint32_t nblk, const uint64_t* __restrict__ blk_off,
+                                                           const uint32_t* __restrict__ tile_pre,
+                                                           const uint64_t* __restrict__ key,
+                                                           uint32_t* __restrict__ tile_heads) {
+    const uint32_t t = blockIdx.x;
+    if (t >= __ldg(tile_pre + nblk)) return;
+    const uint32_t b = tile_block(tile_pre, nblk, t);
+    const uint64_t bbeg = blk_off[b], bend = blk_off[b + 1];
+    const uint64_t base = bbeg + (uint64_t)(t - tile_pre[b]) * kBlockSortCap;
+    const uint32_t cnt = (uint32_t)min((uint64_t)kBlockSortCap, bend - base);
+    uint32_t total = 0;
+    for (uint32_t i0 = 0; i0 < cnt; i0 += kRunThreads) {
+        const uint32_t i = i0 + threadIdx.x;
+        total += __syncthreads_count(i < cnt && run_head(key, bbeg, base + i));
+    }
+    if (threadIdx.x == 0) tile_heads[t] = total;
+}
+
+// out[0..n] = exclusive prefix sums of in[0..n) (out[n] = the total), by one thread block.
+__global__ void __launch_bounds__(1024) k_scan_small(uint32_t n, const uint32_t* __restrict__ in,
+                                                     uint32_t* __restrict__ out) {
+    __shared__ uint32_t part[1024];
+    const uint32_t t = threadIdx.x;
+    const uint32_t per = (n + 1023) / 1024;
+    const uint32_t a = min(t * per, n), b = min(a + per, n);
+    uint32_t s = 0;
+    for (uint32_t i = a; i < b; i++) s += in[i];
+    part[t] = s;
+    __syncthreads();
+    for (uint32_t off = 1; off < 1024; off <<= 1) {  // Hillis-Steele inclusive scan of the totals
+        const uint32_t v = t >= off ? part[t - off] : 0u;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    uint32_t run = t ? part[t - 1] : 0u;
+    for (uint32_t i = a; i < b; i++) {
+        out[i] = run;
+        run += in[i];
+    }
+    if (t == 1023) out[n] = part[1023];
+}
+
+// Run g: ukey[g] its key, bounds[2 g], bounds[2 g + 1] its first and one-past-last element.
+__global__ void __launch_bounds__(kRunThreads) k_run_emit(uint32_t nblk, const uint64_t* __restrict__ blk_off,
+                                                          const uint32_t* __restrict__ tile_pre,
+                                                          const uint32_t* __restrict__ tile_off,
+                                                          const uint64_t* __restrict__ key,
+                                                          uint64_t* __restrict__ ukey, uint32_t* __restrict__ bounds) {
+    using Scan = cub::BlockScan<uint32_t, kRunThreads>;
+    __shared__ typename Scan::TempStorage tmp;
+    const uint32_t t = blockIdx.x;
+    if (t >= __ldg(tile_pre + nblk)) return;
+    const uint32_t b = tile_block(tile_pre, nblk, t);
+    const uint64_t bbeg = blk_off[b], bend = blk_off[b + 1];
+    const uint64_t base = bbeg + (uint64_t)(t - tile_pre[b]) * kBlockSortCap;
+    const uint32_t cnt = (uint32_t)min((uint64_t)kBlockSortCap, bend - base);
+    uint32_t at = tile_off[t];  // runs started before this 256-element step
+    for (uint32_t i0 = 0; i0 < cnt; i0 += kRunThreads) {
+        const uint32_t i = i0 + threadIdx.x;
+        const uint64_t g = base + i;
+        const bool head = i < cnt && run_head(key, bbeg, g);
+        const bool tail = i < cnt && run_tail(key, bend, g);
+        uint32_t excl, step;
+        Scan(tmp).ExclusiveSum(head ? 1u : 0u, excl, step);
+        if (head) {
+            ukey[at + excl] = key[g];
+            bounds[2ull * (at + excl)] = (uint32_t)g;
+        }
+        // the run a tail closes: the last head at or before it
+        if (tail) bounds[2ull * (at + excl + (head ? 1u : 0u) - 1u) + 1] = (uint32_t)(g + 1);
+        at += step;
+        __syncthreads();  // tmp is reused by the next step's scan
+    }
+}
+
+// One warp per run (grid-stride): count, sum of lengths and 128-bit sum of squared lengths.
+__global__ void __launch_bounds__(kRunThreads) k_run_agg(const uint32_t* __restrict__ num_runs,
+                                                         const uint32_t* __restrict__ bounds,
+                                                         const uint32_t* __restrict__ len, LenAgg* __restrict__ agg) {
+    const uint32_t runs = *num_runs;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint64_t warps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t g = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; g < runs; g += warps) {
+        const uint32_t a = bounds[2 * g], e = bounds[2 * g + 1];
+        unsigned long long c = 0, s1 = 0, lo = 0, hi = 0;
+        for (uint32_t j = a + lane; j < e; j += 32) {
+            const unsigned long long l = len[j], q = l * l;
+            c++;
+            s1 += l;
+            lo += q;
+            hi += lo < q ? 1ull : 0ull;
+        }
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            c += __shfl_down_sync(0xffffffffu, c, o);
+            s1 += __shfl_down_sync(0xffffffffu, s1, o);
+            const unsigned long long plo = __shfl_down_sync(0xffffffffu, lo, o);
+            const unsigned long long phi = __shfl_down_sync(0xffffffffu, hi, o);
+            lo += plo;
+            hi += phi + (lo < plo ? 1ull : 0ull);
+        }
+        if (lane == 0) agg[g] = LenAgg{c, s1, lo, hi};
+    }
 }
 
 // One thread per group: FP64 sums, the host-made slot table, and the per-row group offsets.
@@ -502,7 +642,7 @@ namespace rgl {
 
 void stats_scratch_release(StatsScratch* sc) {
     for (DevBuf* b : {&sc->key_a, &sc->key_b, &sc->len_a, &sc->len_b, &sc->ukey, &sc->agg, &sc->runs, &sc->groups,
-                      &sc->goff, &sc->tmp})
+                      &sc->goff, &sc->tmp, &sc->plan})
         b->release();
 }
 
@@ -573,6 +713,25 @@ static int enqueue_batch_groups(rgl_context* ctx, rgl_moments* m, StatsScratch* 
         tabs[nblk + i] = b->block_rows[i];
     }
     for (uint32_t i = 0; i < num_shards; i++) tabs[2ull * nblk + i] = shard_chrom[i];
+    // block-local form: every non-empty block with a chromosome holds one (row, chromosome), in
+    // ascending order, so sorting within the blocks orders the whole batch
+    bool local = true;
+    uint64_t tiles = 0, chunks = 0, max_block = 0, prev = 0;
+    bool any = false;
+    for (uint32_t i = 0; i < nblk && local; i++) {
+        const uint64_t cnt = off[i + 1] - off[i];
+        tiles += sort_tiles(cnt);
+        chunks += merge_chunks(cnt);
+        max_block = std::max(max_block, cnt);
+        const uint32_t sh = b->block_shards[i];
+        const uint32_t c = sh < num_shards ? shard_chrom[sh] : 0xFFFFFFFFu;
+        if (!cnt || c >= C) continue;
+        const uint64_t rc = (uint64_t)b->block_rows[i] * C + c;
+        if (any && rc <= prev) local = false;
+        prev = rc;
+        any = true;
+    }
+    if ((uint64_t)rows * C >= 0xFFFFFFFFull) local = false;  // all ones marks blocks without a chromosome
     const uint64_t nn = std::max<uint64_t>(n, 1);
     RGL_TRY(sc->key_a.ensure(nn * 8));
     RGL_TRY(sc->key_b.ensure(nn * 8));
@@ -583,35 +742,71 @@ static int enqueue_batch_groups(rgl_context* ctx, rgl_moments* m, StatsScratch* 
     RGL_TRY(sc->groups.ensure(nn * sizeof(QGroupDev)));
     RGL_TRY(sc->goff.ensure((rows + 1ull) * 8 + (nblk + 1ull) * 8 + tabs.size() * 4 + 64));
     RGL_TRY(sc->runs.ensure(64));
+    if (local) RGL_TRY(sc->plan.ensure((3ull * nblk + 2 * tiles + 8) * 4));
     uint64_t* d_goff = sc->goff.as<uint64_t>();
     uint64_t* d_boff = d_goff + rows + 1;
     uint32_t* d_tabs = reinterpret_cast<uint32_t*>(d_boff + nblk + 1);
     RGL_CUDA(cudaMemcpyAsync(d_boff, off.data(), off.size() * 8, cudaMemcpyHostToDevice, st));
     RGL_CUDA(cudaMemcpyAsync(d_tabs, tabs.data(), tabs.size() * 4, cudaMemcpyHostToDevice, st));
-    // 2^segbits > rows * C: every valid key's high part is below all ones, so kNoGroup (all bits
-    // set) sorts strictly after every valid key within the sorted 32 + segbits bits
-    int segbits = 1;
-    while (segbits < 32 && (1ull << segbits) <= (uint64_t)rows * C) segbits++;
-    size_t need = 0, tb = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint64_t*)nullptr, (uint64_t*)nullptr, (uint32_t*)nullptr,
-                                    (uint32_t*)nullptr, (int)nn, 0, 64, st);
-    need = std::max(need, tb);
     thrust::transform_iterator<LenToAgg, const uint32_t*, LenAgg> vin(sc->len_b.as<uint32_t>(), LenToAgg());
-    cub::DeviceReduce::ReduceByKey(nullptr, tb, sc->key_b.as<uint64_t>(), sc->ukey.as<uint64_t>(), vin,
-                                   sc->agg.as<LenAgg>(), sc->runs.as<uint32_t>(), LenAggOp(), (int)nn, st);
-    need = std::max(need, tb);
-    RGL_TRY(sc->tmp.ensure(need + 256));
+    int segbits = 1;
+    if (!local) {
+        // 2^segbits > rows * C: every valid key's high part is below all ones, so kNoGroup (all bits
+        // set) sorts strictly after every valid key within the sorted 32 + segbits bits
+        while (segbits < 32 && (1ull << segbits) <= (uint64_t)rows * C) segbits++;
+        size_t need = 0, tb = 0;
+        cub::DeviceRadixSort::SortPairs(nullptr, tb, (uint64_t*)nullptr, (uint64_t*)nullptr, (uint32_t*)nullptr,
+                                        (uint32_t*)nullptr, (int)nn, 0, 64, st);
+        need = std::max(need, tb);
+        cub::DeviceReduce::ReduceByKey(nullptr, tb, sc->key_b.as<uint64_t>(), sc->ukey.as<uint64_t>(), vin,
+                                       sc->agg.as<LenAgg>(), sc->runs.as<uint32_t>(), LenAggOp(), (int)nn, st);
+        need = std::max(need, tb);
+        RGL_TRY(sc->tmp.ensure(need + 256));
+    }
     if (n) {
         k_group_keys<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(
             n, b->d_intervals + b->block_offsets[0], d_boff, d_tabs, d_tabs + nblk, nblk + 1, d_tabs + 2ull * nblk,
-            num_shards, C, m->nb.as<uint64_t>(), (double)bin_size, sc->key_a.as<uint64_t>(), sc->len_a.as<uint32_t>());
-        tb = sc->tmp.cap;
-        RGL_CUDA(cub::DeviceRadixSort::SortPairs(sc->tmp.p, tb, sc->key_a.as<uint64_t>(), sc->key_b.as<uint64_t>(),
-                                                 sc->len_a.as<uint32_t>(), sc->len_b.as<uint32_t>(), (int)n, 0,
-                                                 std::min(64, 32 + segbits), st));
-        tb = sc->tmp.cap;
-        RGL_CUDA(cub::DeviceReduce::ReduceByKey(sc->tmp.p, tb, sc->key_b.as<uint64_t>(), sc->ukey.as<uint64_t>(), vin,
-                                                sc->agg.as<LenAgg>(), sc->runs.as<uint32_t>(), LenAggOp(), (int)n, st));
+            num_shards, C, m->nb.as<uint64_t>(), (double)bin_size, local ? 1 : 0, sc->key_a.as<uint64_t>(),
+            sc->len_a.as<uint32_t>());
+        if (local) {
+            // sort every block by l_int (every block counts as out of order: lengths come in any order),
+            // then the runs of equal keys
+            uint32_t* tile_pre = sc->plan.as<uint32_t>();
+            uint32_t* chunk_pre = tile_pre + nblk + 1;
+            uint32_t* unsorted = chunk_pre + nblk + 1;
+            uint32_t* tile_heads = unsorted + nblk;
+            uint32_t* tile_off = tile_heads + tiles + 1;
+            RGL_CUDA(cudaMemsetAsync(unsorted, 0x01, nblk * 4ull, st));
+            block_sort_enqueue(nblk, d_boff, tiles, chunks, sort_passes(max_block), tile_pre, chunk_pre, unsorted,
+                               sc->key_a.as<uint64_t>(), sc->len_a.as<uint32_t>(), sc->key_b.as<uint64_t>(),
+                               sc->len_b.as<uint32_t>(), st, true);
+            if (tiles) {
+                k_run_count<<<(unsigned)tiles, kRunThreads, 0, st>>>(nblk, d_boff, tile_pre, sc->key_b.as<uint64_t>(),
+                                                                    tile_heads);
+                k_scan_small<<<1, 1024, 0, st>>>((uint32_t)tiles, tile_heads, tile_off);
+                // run bounds in the sort's scratch keys (free once the blocks are sorted)
+                uint32_t* bounds = reinterpret_cast<uint32_t*>(sc->key_a.p);
+                k_run_emit<<<(unsigned)tiles, kRunThreads, 0, st>>>(nblk, d_boff, tile_pre, tile_off,
+                                                                   sc->key_b.as<uint64_t>(), sc->ukey.as<uint64_t>(),
+                                                                   bounds);
+                int nsm = 148;
+                cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, m->device);
+                k_run_agg<<<(unsigned)nsm * 8, kRunThreads, 0, st>>>(tile_off + tiles, bounds,
+                                                                     sc->len_b.as<uint32_t>(), sc->agg.as<LenAgg>());
+                RGL_CUDA(cudaMemcpyAsync(sc->runs.p, tile_off + tiles, 4, cudaMemcpyDeviceToDevice, st));
+            } else {
+                RGL_CUDA(cudaMemsetAsync(sc->runs.p, 0, 4, st));
+            }
+        } else {
+            size_t tb = sc->tmp.cap;
+            RGL_CUDA(cub::DeviceRadixSort::SortPairs(sc->tmp.p, tb, sc->key_a.as<uint64_t>(), sc->key_b.as<uint64_t>(),
+                                                     sc->len_a.as<uint32_t>(), sc->len_b.as<uint32_t>(), (int)n, 0,
+                                                     std::min(64, 32 + segbits), st));
+            tb = sc->tmp.cap;
+            RGL_CUDA(cub::DeviceReduce::ReduceByKey(sc->tmp.p, tb, sc->key_b.as<uint64_t>(), sc->ukey.as<uint64_t>(),
+                                                    vin, sc->agg.as<LenAgg>(), sc->runs.as<uint32_t>(), LenAggOp(),
+                                                    (int)n, st));
+        }
     } else {
         RGL_CUDA(cudaMemsetAsync(sc->runs.p, 0, 4, st));
     }
