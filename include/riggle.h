@@ -649,7 +649,7 @@ typedef struct rgl_server_stats {
  * free_memory() is called only for a batch that would grow the worker's buffers (a batch within
  * them needs no admission), and without the server's lock held, so a slow query (cudaMemGetInfo
  * can take tens of milliseconds on a busy node) delays neither submissions nor other workers.
- * Workers wait for their batches with blocking (not spinning) synchronisation.
+ * Workers wait for their batches by polling with yields (a blocking synchronisation after 100 ms).
  * The server's moment store (optional) must outlive it. */
 int rgl_server_create(rgl_index* index, const rgl_server_opts* opts, rgl_server** out);
 /* Queues one request; RGL_ERR_INVALID_ARGUMENT for a bad block table or a request larger than

@@ -1359,6 +1359,10 @@ int size_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uin
     RGL_TRY(z.ensure_in(c->blk_off, (nblk + 1) * 8ull));
     RGL_TRY(z.ensure_in(c->blk_shard, (nblk + 1) * 4ull));
     RGL_TRY(z.ensure_in(c->sortplan, (4ull * nblk + 4) * 4));
+    // the block tables of a run with rows taken from the blocks (offsets, the sort's segment-order
+    // offsets and destinations; shards, rows, ranks), sized here so that no run reallocates them
+    RGL_TRY(z.ensure_in(c->bt_off, 3ull * (nblk + 1) * 8 + 8));
+    RGL_TRY(z.ensure_in(c->bt_shard, 3ull * (nblk + 1) * 4 + 4));
     RGL_TRY(z.ensure_in(c->key_a, n * 8 + 8));
     RGL_TRY(z.ensure_in(c->key_b, n * 8 + 8));
     RGL_TRY(z.ensure_in(c->val_a, n * 4 + 4));

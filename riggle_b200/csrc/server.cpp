@@ -52,8 +52,8 @@ struct Worker {
     uint64_t* h_bp = nullptr;
     double *h_p = nullptr, *h_llr = nullptr, *h_lp = nullptr;
     uint8_t* h_fl = nullptr;
-    // the end of a batch, waited on with a blocking (not spinning) synchronisation: several workers
-    // spinning on their streams would take host cores from the callers and from each other
+    // the end of a batch: polled with yields, so that waiting workers leave their cores to the
+    // callers and to each other, then waited on with a blocking synchronisation
     cudaEvent_t done = nullptr;
     std::thread th;
 };
@@ -141,7 +141,19 @@ int run_batch(rgl_server* S, Worker* W, const std::vector<Req*>& batch) {
         RGL_CUDA(cudaMemcpyAsync(W->h_fl, W->dfl.p, cells, cudaMemcpyDeviceToHost, st));
     }
     RGL_CUDA(cudaEventRecord(W->done, st));
-    RGL_CUDA(cudaEventSynchronize(W->done));
+    // wait by polling with yields (a blocking synchronisation's wake-up took up to ~30 ms on busy
+    // hosts); a batch still running after 100 ms is waited for with the blocking call
+    const auto w0 = std::chrono::steady_clock::now();
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(W->done);
+        if (q == cudaSuccess) break;
+        if (q != cudaErrorNotReady) RGL_CUDA(q);
+        if (std::chrono::steady_clock::now() - w0 > std::chrono::milliseconds(100)) {
+            RGL_CUDA(cudaEventSynchronize(W->done));
+            break;
+        }
+        std::this_thread::yield();
+    }
     RGL_TRY(context_errors(c));
     const size_t D = S->D;
     for (uint32_t j = 0; j < R; j++) {
@@ -169,6 +181,11 @@ uint64_t stats_plan_bytes(uint64_t n, uint32_t nblk) {
     return (3ull * nblk + 2 * (n / kBlockSortCap + nblk) + 8) * 4;
 }
 
+// The stats stage's group offsets and block tables (StatsScratch::goff) for R rows and nblk blocks.
+uint64_t stats_goff_bytes(rgl_server* S, uint32_t R, uint32_t nblk) {
+    return (R + 1ull) * 8 + (nblk + 1ull) * 8 + (2ull * nblk + S->shard_chrom.size() + 1) * 4 + 64;
+}
+
 // Device bytes worker W would allocate to run a batch of n intervals in nblk blocks over R rows.
 int batch_growth(rgl_server* S, Worker* W, uint64_t n, uint32_t R, uint32_t nblk, uint64_t* bytes) {
     uint64_t ws = 0;
@@ -182,7 +199,8 @@ int batch_growth(rgl_server* S, Worker* W, uint64_t n, uint32_t R, uint32_t nblk
         // the stats stage's scratch: keys, lengths, runs and groups per interval (StatsScratch)
         b += grow(W->sc.key_a, n * 8 + 8) + grow(W->sc.key_b, n * 8 + 8) + grow(W->sc.len_a, n * 4 + 4) +
              grow(W->sc.len_b, n * 4 + 4) + grow(W->sc.ukey, n * 8 + 8) + grow(W->sc.agg, n * 32 + 32) +
-             grow(W->sc.groups, n * 40 + 40) + grow(W->sc.plan, stats_plan_bytes(n, nblk));
+             grow(W->sc.groups, n * 40 + 40) + grow(W->sc.plan, stats_plan_bytes(n, nblk)) +
+             grow(W->sc.goff, stats_goff_bytes(S, R, nblk)) + grow(W->sc.runs, 64);
     }
     *bytes = b;
     return RGL_OK;
@@ -208,6 +226,8 @@ int size_worker(rgl_server* S, Worker* W, uint64_t n, uint32_t R, uint32_t nblk)
         RGL_TRY(W->sc.agg.ensure(nn * 32 + 32));
         RGL_TRY(W->sc.groups.ensure(nn * 40 + 40));
         RGL_TRY(W->sc.plan.ensure(stats_plan_bytes(nn, nblk)));
+        RGL_TRY(W->sc.goff.ensure(stats_goff_bytes(S, R, nblk)));
+        RGL_TRY(W->sc.runs.ensure(64));
     }
     return RGL_OK;
 }
