@@ -66,16 +66,42 @@ struct BlockSortTypes {
     };
 };
 
+// The tiles of ordered blocks, copied to the output (one tile per thread block, coalesced; the
+// tiles of other blocks return at once).  Few registers, so the copy runs at full occupancy instead
+// of in the sort's register-heavy blocks.
+template <bool VALUES>
+__global__ void __launch_bounds__(kBsThreads) k_tile_copy(uint32_t nblk, const uint64_t* __restrict__ blk_off,
+                                                            const uint32_t* __restrict__ tile_pre,
+                                                            const uint32_t* __restrict__ unsorted,
+                                                            const uint64_t* __restrict__ kin,
+                                                            const uint32_t* __restrict__ vin, uint64_t* __restrict__ kout,
+                                                            uint32_t* __restrict__ vout) {
+    const uint32_t tile = blockIdx.x;
+    if (tile >= __ldg(tile_pre + nblk)) return;
+    const uint32_t blk = find_block(tile_pre, nblk, tile);
+    if (unsorted[blk] != 0u) return;
+    const uint64_t bbeg = blk_off[blk], bend = blk_off[blk + 1];
+    const uint64_t base = bbeg + (uint64_t)(tile - tile_pre[blk]) * kBlockSortCap;
+    const uint64_t rest = bend - base;
+    const uint32_t cnt = (uint32_t)(rest < kBlockSortCap ? rest : kBlockSortCap);
+#pragma unroll 4
+    for (uint32_t i = threadIdx.x; i < cnt; i += kBsThreads) {
+        kout[base + i] = kin[base + i];
+        if (VALUES) vout[base + i] = vin[base + i];
+    }
+}
+
 // One tile per thread block (grid: an upper bound of the tiles; CTAs past the last tile return).
 // With VALUES the start keys with their ends as values (key_a / val_a), else the end keys alone.
-// unsorted[b] != 0: block b is not in order.  Output: `out` when the block is in order or needs
-// an even number of merge passes, else in place (`in`).
+// unsorted[b] != 0: block b is not in order (only such blocks are sorted here).  Output: `out` when
+// the block needs an even number of merge passes, else in place (`in`); *maxp: the most merge
+// passes any of these blocks needs.
 template <bool VALUES>
 __global__ void __launch_bounds__(kBsThreads) k_tile_sort(uint32_t nblk, const uint64_t* __restrict__ blk_off,
                                                             const uint32_t* __restrict__ tile_pre,
                                                             const uint32_t* __restrict__ unsorted, uint64_t* kin,
                                                             uint32_t* vin, uint64_t* __restrict__ kout,
-                                                            uint32_t* __restrict__ vout) {
+                                                            uint32_t* __restrict__ vout, uint32_t* __restrict__ maxp) {
     using T = BlockSortTypes<VALUES>;
     extern __shared__ __align__(16) unsigned char bs_smem[];
     typename T::Smem& sm = *reinterpret_cast<typename T::Smem*>(bs_smem);
@@ -86,9 +112,11 @@ __global__ void __launch_bounds__(kBsThreads) k_tile_sort(uint32_t nblk, const u
     const uint64_t base = bbeg + (uint64_t)(tile - tile_pre[blk]) * kBlockSortCap;
     const uint64_t rest = bbeg + bcnt - base;
     const uint32_t cnt = (uint32_t)(rest < kBlockSortCap ? rest : kBlockSortCap);
-    const bool ordered = unsorted[blk] == 0u;
-    uint64_t* ko = (ordered || !(sort_passes(bcnt) & 1u)) ? kout : kin;
-    uint32_t* vo = (ordered || !(sort_passes(bcnt) & 1u)) ? vout : vin;
+    if (unsorted[blk] == 0u) return;  // an ordered block is copied by k_tile_copy
+    const uint32_t passes = sort_passes(bcnt);
+    if (threadIdx.x == 0 && tile == tile_pre[blk] && passes) atomicMax(maxp, passes);
+    uint64_t* ko = (passes & 1u) ? kin : kout;
+    uint32_t* vo = (passes & 1u) ? vin : vout;
     const uint64_t hi = kin[base] & 0xFFFFFFFF00000000ull;  // the block's segment, in the high word
     uint32_t k[kBsItems], v[kBsItems];
     uint32_t any = 0;
@@ -153,10 +181,12 @@ __global__ void __launch_bounds__(kMergeThreads) k_merge_pass(uint32_t q, uint32
                                                               const uint64_t* __restrict__ blk_off,
                                                               const uint32_t* __restrict__ chunk_pre,
                                                               const uint32_t* __restrict__ unsorted, uint64_t* ka,
-                                                              uint32_t* va, uint64_t* kb, uint32_t* vb) {
+                                                              uint32_t* va, uint64_t* kb, uint32_t* vb,
+                                                              const uint32_t* __restrict__ maxp) {
     __shared__ uint32_t sk[kMergeChunk], sv[VALUES ? kMergeChunk : 1];
     __shared__ uint32_t ok[kMergeChunk], ov[VALUES ? kMergeChunk : 1];
     __shared__ uint32_t s_split[2];
+    if (q > *maxp) return;  // no block out of order needs this pass
     const uint32_t chunk = blockIdx.x;
     if (chunk >= __ldg(chunk_pre + nblk)) return;
     const uint32_t blk = find_block(chunk_pre, nblk, chunk);
@@ -219,19 +249,21 @@ static_assert(block_sort_smem<true>() <= 48 * 1024 && block_sort_smem<false>() <
 template <bool VALUES>
 uint32_t enqueue_t(uint32_t nblk, const uint64_t* off, uint64_t tiles, uint64_t chunks, uint32_t passes,
                    uint32_t* tile_pre, uint32_t* chunk_pre, const uint32_t* unsorted, uint64_t* ka, uint32_t* va,
-                   uint64_t* kb, uint32_t* vb, cudaStream_t st, bool plan) {
+                   uint64_t* kb, uint32_t* vb, uint32_t* maxp, cudaStream_t st, bool plan) {
     uint32_t launches = 0;
     if (plan) {
         k_sort_plan<<<1, 1024, 0, st>>>(nblk, off, tile_pre, chunk_pre);
         launches++;
     }
     if (!tiles) return launches;
+    cudaMemsetAsync(maxp, 0, 4, st);
+    k_tile_copy<VALUES><<<(unsigned)tiles, kBsThreads, 0, st>>>(nblk, off, tile_pre, unsorted, ka, va, kb, vb);
     k_tile_sort<VALUES><<<(unsigned)tiles, kBsThreads, block_sort_smem<VALUES>(), st>>>(nblk, off, tile_pre, unsorted,
-                                                                                      ka, va, kb, vb);
-    launches++;
+                                                                                      ka, va, kb, vb, maxp);
+    launches += 2;
     for (uint32_t q = 1; q <= passes && chunks; q++) {
         k_merge_pass<VALUES><<<(unsigned)chunks, kMergeThreads, 0, st>>>(q, nblk, off, chunk_pre, unsorted, ka, va, kb,
-                                                                       vb);
+                                                                       vb, maxp);
         launches++;
     }
     return launches;
@@ -241,10 +273,11 @@ uint32_t enqueue_t(uint32_t nblk, const uint64_t* off, uint64_t tiles, uint64_t 
 
 uint32_t block_sort_enqueue(uint32_t nblk, const uint64_t* off, uint64_t tiles, uint64_t chunks, uint32_t passes,
                             uint32_t* tile_pre, uint32_t* chunk_pre, const uint32_t* unsorted, uint64_t* ka,
-                            uint32_t* va, uint64_t* kb, uint32_t* vb, cudaStream_t st, bool plan) {
-    return va ? enqueue_t<true>(nblk, off, tiles, chunks, passes, tile_pre, chunk_pre, unsorted, ka, va, kb, vb, st, plan)
+                            uint32_t* va, uint64_t* kb, uint32_t* vb, uint32_t* maxp, cudaStream_t st, bool plan) {
+    return va ? enqueue_t<true>(nblk, off, tiles, chunks, passes, tile_pre, chunk_pre, unsorted, ka, va, kb, vb, maxp,
+                                st, plan)
               : enqueue_t<false>(nblk, off, tiles, chunks, passes, tile_pre, chunk_pre, unsorted, ka, nullptr, kb,
-                                 nullptr, st, plan);
+                                 nullptr, maxp, st, plan);
 }
 
 }  // namespace rgl

@@ -48,9 +48,11 @@ __host__ __device__ inline uint32_t merge_chunks(uint64_t cnt) {
 // tiles, then `passes` merge passes.  off: nblk + 1 block offsets; unsorted[b] != 0 marks block b
 // as not in order; tiles / chunks / passes: the host's counts for these blocks (sort_tiles,
 // merge_chunks, sort_passes of the largest block).  (ka, va) is the input and scratch, (kb, vb) the
-// output; va and vb null: keys alone.  Returns the number of kernels launched.
+// output; va and vb null: keys alone.  maxp: one device word of scratch (the most merge passes an
+// out-of-order block needs; passes beyond it return at once), its own for each concurrent sort.
+// Returns the number of kernels launched.
 uint32_t block_sort_enqueue(uint32_t nblk, const uint64_t* off, uint64_t tiles, uint64_t chunks, uint32_t passes,
                             uint32_t* tile_pre, uint32_t* chunk_pre, const uint32_t* unsorted, uint64_t* ka,
-                            uint32_t* va, uint64_t* kb, uint32_t* vb, cudaStream_t st, bool plan);
+                            uint32_t* va, uint64_t* kb, uint32_t* vb, uint32_t* maxp, cudaStream_t st, bool plan);
 
 }  // namespace rgl

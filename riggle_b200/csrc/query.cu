@@ -345,9 +345,10 @@ __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t seg_per_shard, cons
                        const int32_t* __restrict__ slot, const LayerDev* __restrict__ layers,
                        const uint2* __restrict__ pos, const uint32_t* __restrict__ btab,
                        uint32_t* __restrict__ lo_out, uint32_t* __restrict__ hi_out) {
-    uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (t >= (uint64_t)n * nslots) return;
-    uint32_t K = (uint32_t)(t / n), i = (uint32_t)(t % n);
+    // grid: x over the queries, y over the layer slots (no 64-bit division per thread)
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, K = blockIdx.y;
+    if (i >= n) return;
+    const uint64_t t = (uint64_t)K * n + i;
     uint32_t shard = seg[i] / seg_per_shard;
     int32_t li = slot[(uint64_t)shard * nslots + K];
     uint32_t lo = 0, hi = 0;
@@ -1287,7 +1288,7 @@ struct rgl_context {
     DevBuf segtab, tab_len, tab_off, tab_s, tab_e, tab_xs, tab_xe, tab2;
     DevBuf cl, pc, method, plen, ppos, psegs, item_t0, seg_need, lpos, tl, scan_sums;
     DevBuf cub_tmp2, scan_sums2;  // the side stream's own scratch
-    DevBuf sortplan;  // block-local sort: order flags, tile and merge-chunk prefix counts
+    DevBuf sortplan;  // block-local sort: order flags, tile and merge-chunk prefix counts, two pass words
     DevBuf sort_tab, sort_rank;  // its segment-order layout, for the single-call entry points
     DevBuf item_hits, item_base, pairs;  // intervals mode
     DevBuf bt_off, bt_shard, acc;  // batched form: sub-batch block tables (offsets; shards then rows), stats
@@ -1358,7 +1359,7 @@ int size_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uin
     RGL_TRY(z.ensure_in(c->iv, n * sizeof(rgl_interval) + 16));
     RGL_TRY(z.ensure_in(c->blk_off, (nblk + 1) * 8ull));
     RGL_TRY(z.ensure_in(c->blk_shard, (nblk + 1) * 4ull));
-    RGL_TRY(z.ensure_in(c->sortplan, (4ull * nblk + 4) * 4));
+    RGL_TRY(z.ensure_in(c->sortplan, (4ull * nblk + 8) * 4));
     // the block tables of a run with rows taken from the blocks (offsets, the sort's segment-order
     // offsets and destinations; shards, rows, ranks), sized here so that no run reallocates them
     RGL_TRY(z.ensure_in(c->bt_off, 3ull * (nblk + 1) * 8 + 8));
@@ -1582,8 +1583,6 @@ int stream_after(cudaStream_t to, cudaStream_t from, cudaEvent_t e) {
     return RGL_OK;
 }
 
-// Input of one pipeline run: n intervals at `iv` (device), block b = [blk_off[b], blk_off[b+1]) on
-// shard blk_shard[b] (both tables on the device), rows [row_base, row_base + rows) of the output.
 // Shape of a run's block-local key sort, from the host's block offsets.
 struct LocalSort {
     uint64_t max_block = 0;  // the largest block: sets the number of merge passes
@@ -1598,6 +1597,8 @@ struct LocalSort {
     std::vector<uint32_t> idx;
 };
 
+// Input of one pipeline run: n intervals at `iv` (device), block b = [blk_off[b], blk_off[b+1]) on
+// shard blk_shard[b] (both tables on the device), rows [row_base, row_base + rows) of the output.
 struct PipeIn {
     const rgl_interval* iv;
     uint64_t n;
@@ -1781,16 +1782,17 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     const uint32_t passes = in.block_local ? sort_passes(in.ls.max_block) : 0u;
     if (in.block_local)  // the plan (before the fork), then the end keys here and the start keys there
         launches += block_sort_enqueue(in.nblk, soff, 0, 0, 0, d_tile_pre, d_chunk_pre, nullptr, nullptr, nullptr,
-                                       nullptr, nullptr, st, true);
+                                       nullptr, nullptr, nullptr, st, true);
     RGL_TRY(stream_after(sd, st, c->ev_fork));
     size_t tb = c->cub_tmp2.cap;
     if (in.block_local) {
         launches += block_sort_enqueue(in.nblk, soff, in.ls.tiles, in.ls.chunks, passes, d_tile_pre, d_chunk_pre,
                                        d_unsorted + in.nblk, c->ekey_a.as<uint64_t>(), nullptr,
-                                       c->ekey_b.as<uint64_t>(), nullptr, sd, false);
+                                       c->ekey_b.as<uint64_t>(), nullptr, d_chunk_pre + in.nblk + 2, sd, false);
         launches += block_sort_enqueue(in.nblk, soff, in.ls.tiles, in.ls.chunks, passes, d_tile_pre, d_chunk_pre,
                                        d_unsorted, c->key_a.as<uint64_t>(), c->val_a.as<uint32_t>(),
-                                       c->key_b.as<uint64_t>(), c->val_b.as<uint32_t>(), st, false);
+                                       c->key_b.as<uint64_t>(), c->val_b.as<uint32_t>(), d_chunk_pre + in.nblk + 1, st,
+                                       false);
     } else {
         RGL_CUDA(cub::DeviceRadixSort::SortKeys(c->cub_tmp2.p, tb, c->ekey_a.as<uint64_t>(), c->ekey_b.as<uint64_t>(),
                                                 (int)n, 0, 32 + segbits, sd));
@@ -1825,7 +1827,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
         RGL_TRY(stream_after(st, sd, c->ev_join));
         return fail(RGL_ERR_INVALID_ARGUMENT, "query intervals x layer slots must be < 2^31 per run");
     }
-    k_lohi<<<grid_for(tot, 256), 256, 0, st>>>(n, ns, sps, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
+    k_lohi<<<dim3(grid_for(n, 256), ns), 256, 0, st>>>(n, ns, sps, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
                                                 c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, idx->d_pos,
                                                 idx->d_btab, c->lo.as<uint32_t>(), c->hi.as<uint32_t>());
     launches++;

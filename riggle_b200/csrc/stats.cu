@@ -779,7 +779,7 @@ static int enqueue_batch_groups(rgl_context* ctx, rgl_moments* m, StatsScratch* 
             RGL_CUDA(cudaMemsetAsync(unsorted, 0x01, nblk * 4ull, st));
             block_sort_enqueue(nblk, d_boff, tiles, chunks, sort_passes(max_block), tile_pre, chunk_pre, unsorted,
                                sc->key_a.as<uint64_t>(), sc->len_a.as<uint32_t>(), sc->key_b.as<uint64_t>(),
-                               sc->len_b.as<uint32_t>(), st, true);
+                               sc->len_b.as<uint32_t>(), tile_off + tiles + 1, st, true);
             if (tiles) {
                 k_run_count<<<(unsigned)tiles, kRunThreads, 0, st>>>(nblk, d_boff, tile_pre, sc->key_b.as<uint64_t>(),
                                                                     tile_heads);
