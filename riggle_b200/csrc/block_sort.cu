@@ -1,7 +1,6 @@
 // The block-local sort's kernels (its shape and launcher are declared in block_sort.cuh).
 #include <cub/block/block_radix_sort.cuh>
 
-#include <algorithm>
 #include <type_traits>
 
 #include "block_sort.cuh"
@@ -92,9 +91,9 @@ __global__ void __launch_bounds__(kBsThreads) k_tile_copy(uint32_t nblk, const u
     }
 }
 
-// The tiles of out-of-order blocks, grid-stride over all tiles.  With VALUES the start keys with
-// their ends as values (key_a / val_a), else the end keys alone.  unsorted[b] != 0: block b is not
-// in order (only such blocks are sorted here).  Output: `out` when
+// One tile per thread block (grid: an upper bound of the tiles; CTAs past the last tile return).
+// With VALUES the start keys with their ends as values (key_a / val_a), else the end keys alone.
+// unsorted[b] != 0: block b is not in order (only such blocks are sorted here).  Output: `out` when
 // the block needs an even number of merge passes, else in place (`in`); *maxp: the most merge
 // passes any of these blocks needs.
 template <bool VALUES>
@@ -106,58 +105,55 @@ __global__ void __launch_bounds__(kBsThreads) k_tile_sort(uint32_t nblk, const u
     using T = BlockSortTypes<VALUES>;
     extern __shared__ __align__(16) unsigned char bs_smem[];
     typename T::Smem& sm = *reinterpret_cast<typename T::Smem*>(bs_smem);
+    const uint32_t tile = blockIdx.x;
+    if (tile >= __ldg(tile_pre + nblk)) return;
+    const uint32_t blk = find_block(tile_pre, nblk, tile);
+    const uint64_t bbeg = blk_off[blk], bcnt = blk_off[blk + 1] - bbeg;
+    const uint64_t base = bbeg + (uint64_t)(tile - tile_pre[blk]) * kBlockSortCap;
+    const uint64_t rest = bbeg + bcnt - base;
+    const uint32_t cnt = (uint32_t)(rest < kBlockSortCap ? rest : kBlockSortCap);
+    if (unsorted[blk] == 0u) return;  // an ordered block is copied by k_tile_copy
+    const uint32_t passes = sort_passes(bcnt);
+    if (threadIdx.x == 0 && tile == tile_pre[blk] && passes) atomicMax(maxp, passes);
+    uint64_t* ko = (passes & 1u) ? kin : kout;
+    uint32_t* vo = (passes & 1u) ? vin : vout;
+    const uint64_t hi = kin[base] & 0xFFFFFFFF00000000ull;  // the block's segment, in the high word
+    uint32_t k[kBsItems], v[kBsItems];
+    uint32_t any = 0;
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < kBsItems; j++) {
+        const uint32_t i = threadIdx.x * kBsItems + j;  // blocked: thread t holds [16 t, 16 t + 16)
+        k[j] = i < cnt ? (uint32_t)kin[base + i] : 0xFFFFFFFFu;  // padding sorts last
+        v[j] = (VALUES && i < cnt) ? vin[base + i] : 0u;
+        any |= i < cnt ? k[j] : 0u;
+        if (j) ok = ok && k[j - 1] <= k[j];
+    }
     __shared__ uint32_t s_bits;  // bitwise OR of the tile's keys
-    const uint32_t ntiles = __ldg(tile_pre + nblk);
-    // grid-stride over the tiles: the tiles of ordered blocks cost a check, not a block launch
-    for (uint32_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        const uint32_t blk = find_block(tile_pre, nblk, tile);
-        if (unsorted[blk] == 0u) continue;  // an ordered block is copied by k_tile_copy
-        const uint64_t bbeg = blk_off[blk], bcnt = blk_off[blk + 1] - bbeg;
-        const uint64_t base = bbeg + (uint64_t)(tile - tile_pre[blk]) * kBlockSortCap;
-        const uint64_t rest = bbeg + bcnt - base;
-        const uint32_t cnt = (uint32_t)(rest < kBlockSortCap ? rest : kBlockSortCap);
-        const uint32_t passes = sort_passes(bcnt);
-        if (threadIdx.x == 0 && tile == tile_pre[blk] && passes) atomicMax(maxp, passes);
-        uint64_t* ko = (passes & 1u) ? kin : kout;
-        uint32_t* vo = (passes & 1u) ? vin : vout;
-        const uint64_t hi = kin[base] & 0xFFFFFFFF00000000ull;  // the block's segment, in the high word
-        uint32_t k[kBsItems], v[kBsItems];
-        uint32_t any = 0;
-        bool ok = true;
+    sm.last[threadIdx.x] = k[kBsItems - 1];
+    if (threadIdx.x == 0) s_bits = 0;
+    __syncthreads();
+    if (threadIdx.x) ok = ok && sm.last[threadIdx.x - 1] <= k[0];
+    any = __reduce_or_sync(0xffffffffu, any);
+    if ((threadIdx.x & 31u) == 0) atomicOr(&s_bits, any);
+    // also orders every read of the tile before the in-place writes below, and the atomicOr
+    // before the read of s_bits
+    const bool sorted = __syncthreads_and(ok);
+    const uint32_t bits = s_bits;
+    if (!sorted) {
+        const int end_bit = bits ? 32 - __clz(bits) : 1;
+        if constexpr (VALUES)
+            typename T::Sort(sm.sort).Sort(k, v, 0, end_bit);
+        else
+            typename T::Sort(sm.sort).Sort(k, 0, end_bit);
+    }
 #pragma unroll
-        for (int j = 0; j < kBsItems; j++) {
-            const uint32_t i = threadIdx.x * kBsItems + j;  // blocked: thread t holds [16 t, 16 t + 16)
-            k[j] = i < cnt ? (uint32_t)kin[base + i] : 0xFFFFFFFFu;  // padding sorts last
-            v[j] = (VALUES && i < cnt) ? vin[base + i] : 0u;
-            any |= i < cnt ? k[j] : 0u;
-            if (j) ok = ok && k[j - 1] <= k[j];
+    for (int j = 0; j < kBsItems; j++) {
+        const uint32_t i = threadIdx.x * kBsItems + j;
+        if (i < cnt) {
+            ko[base + i] = hi | k[j];
+            if (VALUES) vo[base + i] = v[j];
         }
-        sm.last[threadIdx.x] = k[kBsItems - 1];
-        if (threadIdx.x == 0) s_bits = 0;
-        __syncthreads();
-        if (threadIdx.x) ok = ok && sm.last[threadIdx.x - 1] <= k[0];
-        any = __reduce_or_sync(0xffffffffu, any);
-        if ((threadIdx.x & 31u) == 0) atomicOr(&s_bits, any);
-        // also orders every read of the tile before the in-place writes below, and the atomicOr
-        // before the read of s_bits
-        const bool sorted = __syncthreads_and(ok);
-        const uint32_t bits = s_bits;
-        if (!sorted) {
-            const int end_bit = bits ? 32 - __clz(bits) : 1;
-            if constexpr (VALUES)
-                typename T::Sort(sm.sort).Sort(k, v, 0, end_bit);
-            else
-                typename T::Sort(sm.sort).Sort(k, 0, end_bit);
-        }
-#pragma unroll
-        for (int j = 0; j < kBsItems; j++) {
-            const uint32_t i = threadIdx.x * kBsItems + j;
-            if (i < cnt) {
-                ko[base + i] = hi | k[j];
-                if (VALUES) vo[base + i] = v[j];
-            }
-        }
-        __syncthreads();  // shared memory and s_bits are reused by the next tile
     }
 }
 
@@ -262,12 +258,8 @@ uint32_t enqueue_t(uint32_t nblk, const uint64_t* off, uint64_t tiles, uint64_t 
     if (!tiles) return launches;
     cudaMemsetAsync(maxp, 0, 4, st);
     k_tile_copy<VALUES><<<(unsigned)tiles, kBsThreads, 0, st>>>(nblk, off, tile_pre, unsorted, ka, va, kb, vb);
-    int dev = 0, nsm = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    const unsigned sort_grid = (unsigned)std::min<uint64_t>(tiles, (uint64_t)nsm * 4);
-    k_tile_sort<VALUES><<<sort_grid, kBsThreads, block_sort_smem<VALUES>(), st>>>(nblk, off, tile_pre, unsorted, ka, va,
-                                                                                kb, vb, maxp);
+    k_tile_sort<VALUES><<<(unsigned)tiles, kBsThreads, block_sort_smem<VALUES>(), st>>>(nblk, off, tile_pre, unsorted,
+                                                                                      ka, va, kb, vb, maxp);
     launches += 2;
     for (uint32_t q = 1; q <= passes && chunks; q++) {
         k_merge_pass<VALUES><<<(unsigned)chunks, kMergeThreads, 0, st>>>(q, nblk, off, chunk_pre, unsorted, ka, va, kb,
