@@ -344,7 +344,7 @@ __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t seg_per_shard, cons
                        const uint32_t* __restrict__ qend, const uint32_t* __restrict__ seg,
                        const int32_t* __restrict__ slot, const LayerDev* __restrict__ layers,
                        const uint2* __restrict__ pos, const uint32_t* __restrict__ btab,
-                       uint32_t* __restrict__ lo_out, uint32_t* __restrict__ hi_out) {
+                       uint32_t* __restrict__ lo_out, uint32_t* __restrict__ hi_out, uint32_t* __restrict__ live) {
     // grid: x over the queries, y over the layer slots (no 64-bit division per thread)
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, K = blockIdx.y;
     if (i >= n) return;
@@ -363,6 +363,9 @@ __global__ void k_lohi(uint32_t n, uint32_t nslots, uint32_t seg_per_shard, cons
     }
     lo_out[t] = lo;
     hi_out[t] = hi;
+    // the live-run flags of the compaction below (entry n * nslots: the scan's closing zero)
+    live[t] = hi > lo ? 1u : 0u;
+    if (t == 0) live[(uint64_t)n * nslots] = 0u;
 }
 
 // ---- scans whose length is a device count ------------------------------------------------------
@@ -460,12 +463,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const Tin* __restri
 // An entry (K, i) whose run [lo, hi) is empty takes part in nothing: with starts sorted, lo is
 // non-decreasing within a (K, segment) row, so an empty run's hi (= its lo) never exceeds a later
 // entry's lo and can neither merge nor split ranges.  The live entries are compacted (tl[c] = t,
-// c < L) and everything after this works on them.
-__global__ void k_live(uint64_t tot, const uint32_t* __restrict__ lo, const uint32_t* __restrict__ hi,
-                       uint32_t* __restrict__ flag) {
-    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (t <= tot) flag[t] = (t < tot && hi[t] > lo[t]) ? 1u : 0u;
-}
+// c < L) and everything after this works on them.  k_lohi writes the live flags with lo and hi.
 
 template <bool PDL>
 __global__ void k_compact(uint64_t tot, const uint32_t* __restrict__ lpos, uint32_t* __restrict__ tl,
@@ -1829,7 +1827,8 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     }
     k_lohi<<<dim3(grid_for(n, 256), ns), 256, 0, st>>>(n, ns, sps, c->starts.as<uint32_t>(), c->val_b.as<uint32_t>(),
                                                 c->seg.as<uint32_t>(), idx->d_slot, idx->d_layers, idx->d_pos,
-                                                idx->d_btab, c->lo.as<uint32_t>(), c->hi.as<uint32_t>());
+                                                idx->d_btab, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
+                                                c->rflag.as<uint32_t>());
     launches++;
     {  // running max of hi along every (slot, segment) row: one scan keyed by (slot, segment)
         RowKeyIter keys(thrust::counting_iterator<uint32_t>(0), RowKey{c->segnum.as<uint32_t>(), n});
@@ -1838,9 +1837,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                                      c->maxhi.as<uint32_t>(), MaxOp(), (int)tot, cub::Equality(),
                                                      st));
     }
-    // live runs: compaction of the (K, query) entries with a non-empty candidate run
-    k_live<<<grid_for(tot + 1, 256), 256, 0, st>>>(tot, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
-                                                   c->rflag.as<uint32_t>());
+    // live runs: compaction of the (K, query) entries with a non-empty candidate run (flags from k_lohi)
     tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->rflag.as<uint32_t>(), c->lpos.as<uint32_t>(),
                                            (int)(tot + 1), st));
@@ -1848,7 +1845,7 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     uint32_t* Rp = d_small + 9;  // ranges R
     (void)launch_chain(pdl, k_compact<true>, k_compact<false>, grid_for(tot + 1, 256), 256, 0, st, tot,
                      c->lpos.as<uint32_t>(), c->tl.as<uint32_t>(), Lp);
-    launches += 2;
+    launches++;
     // ranges over the live runs, their candidate counts and methods
     const unsigned gc = (unsigned)std::min<uint64_t>(grid_for(tot, 256), (uint64_t)c->num_sms * 32);
     (void)launch_chain(pdl, k_crange_flags<true>, k_crange_flags<false>, gc, 256, 0, st, Lp, n, c->tl.as<uint32_t>(),
