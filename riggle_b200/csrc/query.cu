@@ -152,13 +152,22 @@ __global__ void k_expand_keys(uint32_t n, const rgl_interval* __restrict__ iv, c
                               uint64_t* __restrict__ key, uint32_t* __restrict__ val, uint64_t* __restrict__ ekey,
                               uint32_t* __restrict__ err, uint32_t* __restrict__ unsorted,
                               const uint64_t* __restrict__ sdst, const uint32_t* __restrict__ sidx) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    uint32_t lo = 0, hi = nblk;  // block b with blk_off[b] <= i < blk_off[b+1]
-    while (hi - lo > 1) {
-        uint32_t m = (lo + hi) >> 1;
-        if (blk_off[m] <= i) lo = m; else hi = m;
+    // block b with blk_off[b] <= i < blk_off[b+1]: one search per thread block, for its first
+    // element, then a short walk (256 consecutive elements span few blocks)
+    __shared__ uint32_t s_b0;
+    const uint32_t i0 = blockIdx.x * blockDim.x, i = i0 + threadIdx.x;
+    if (threadIdx.x == 0) {
+        uint32_t lo = 0, hi = nblk;
+        while (hi - lo > 1) {
+            const uint32_t m = (lo + hi) >> 1;
+            if (blk_off[m] <= i0) lo = m; else hi = m;
+        }
+        s_b0 = lo;
     }
+    __syncthreads();
+    if (i >= n) return;
+    uint32_t lo = s_b0;
+    while (lo + 1 < nblk && blk_off[lo + 1] <= i) lo++;
     const uint32_t* w = reinterpret_cast<const uint32_t*>(iv) + 3ull * i;
     // the block-local sort: block b's keys at sdst[b] + their place in the block (segment-order
     // layout) or in place; order flags of the block's rank k in that layout: starts (ends) out of
@@ -463,19 +472,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const Tin* __restri
 // An entry (K, i) whose run [lo, hi) is empty takes part in nothing: with starts sorted, lo is
 // non-decreasing within a (K, segment) row, so an empty run's hi (= its lo) never exceeds a later
 // entry's lo and can neither merge nor split ranges.  The live entries are compacted (tl[c] = t,
-// c < L) and everything after this works on them.  k_lohi writes the live flags with lo and hi.
+// c < L, by a flagged selection) and everything after this works on them.  k_lohi writes the live
+// flags with lo and hi.
 
-template <bool PDL>
-__global__ void k_compact(uint64_t tot, const uint32_t* __restrict__ lpos, uint32_t* __restrict__ tl,
-                          uint32_t* __restrict__ L_out) {
-    if constexpr (PDL) {
-        pdl_wait();
-        pdl_release();
-    }
-    const uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (t < tot && lpos[t + 1] != lpos[t]) tl[lpos[t]] = (uint32_t)t;
-    if (t == tot) *L_out = lpos[tot];
-}
 
 // Range starts among the live runs: the first live run of a (K, segment) row, or one whose lo is
 // past the running maximum of hi (maxhi over the row, which empty runs never raise past a later
@@ -1284,7 +1283,7 @@ struct rgl_context {
     DevBuf starts, ends, seg, segflag, segnum, seg_begin, ps_in, pe_in, ps, pe;
     DevBuf lo, hi, maxhi, rflag, ridx, ranges, rlen, rpos, cub_tmp, small, out_counts, out_bp, item_r0;
     DevBuf segtab, tab_len, tab_off, tab_s, tab_e, tab_xs, tab_xe, tab2;
-    DevBuf cl, pc, method, plen, ppos, psegs, item_t0, seg_need, lpos, tl, scan_sums;
+    DevBuf cl, pc, method, plen, ppos, psegs, item_t0, seg_need, tl, scan_sums;
     DevBuf cub_tmp2, scan_sums2;  // the side stream's own scratch
     DevBuf sortplan;  // block-local sort: order flags, tile and merge-chunk prefix counts, two pass words
     DevBuf sort_tab, sort_rank;  // its segment-order layout, for the single-call entry points
@@ -1393,7 +1392,6 @@ int size_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uin
     RGL_TRY(z.ensure_in(c->cl, tot * 8 + 16));
     RGL_TRY(z.ensure_in(c->pc, tot * 8 + 16));
     RGL_TRY(z.ensure_in(c->method, tot + 16));
-    RGL_TRY(z.ensure_in(c->lpos, tot * 4 + 8));
     RGL_TRY(z.ensure_in(c->tl, tot * 4 + 8));
     RGL_TRY(z.ensure_in(c->scan_sums, (std::max<uint64_t>(tot, 10 * n + 16) / kScanTile + 4) * 8));
     RGL_TRY(z.ensure_in(c->scan_sums2, (10 * n + 16) / kScanTile * 8 + 32));
@@ -1432,6 +1430,9 @@ int size_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uin
     need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, nt, c->stream);
     need = std::max(need, b);
+    cub::DeviceSelect::Flagged(nullptr, b, thrust::counting_iterator<uint32_t>(0), (const uint32_t*)nullptr,
+                               (uint32_t*)nullptr, (uint32_t*)nullptr, nt, c->stream);
+    need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, nn + 1, c->stream);
     need = std::max(need, b);
     cub::DeviceReduce::Sum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nt, c->stream);
@@ -1454,7 +1455,7 @@ int size_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uin
                       &c->ends, &c->seg, &c->segflag, &c->segnum, &c->seg_begin, &c->ps_in, &c->pe_in, &c->ps,
                       &c->pe, &c->lo, &c->hi, &c->maxhi, &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos,
                       &c->cub_tmp, &c->small, &c->item_r0, &c->item_t0, &c->segtab, &c->tab_len, &c->tab_off,
-                      &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->tab2, &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs,
+                      &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->tab2, &c->cl, &c->pc, &c->method, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs,
                       &c->seg_need, &c->acc, &c->cub_tmp2, &c->scan_sums2, &c->sortplan})
         sig = (sig ^ (uint64_t)(uintptr_t)b->p ^ ((uint64_t)b->cap << 17)) * 1099511628211ull;
     c->ws_sig = sig;
@@ -1837,15 +1838,13 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                                      c->maxhi.as<uint32_t>(), MaxOp(), (int)tot, cub::Equality(),
                                                      st));
     }
-    // live runs: compaction of the (K, query) entries with a non-empty candidate run (flags from k_lohi)
-    tb = c->cub_tmp.cap;
-    RGL_CUDA(cub::DeviceScan::ExclusiveSum(c->cub_tmp.p, tb, c->rflag.as<uint32_t>(), c->lpos.as<uint32_t>(),
-                                           (int)(tot + 1), st));
+    // live runs: compaction of the (K, query) entries with a non-empty candidate run (flags from
+    // k_lohi) in one pass: tl[c] = t of the c-th live entry, *Lp = their number
     uint32_t* Lp = d_small + 8;  // live runs L
     uint32_t* Rp = d_small + 9;  // ranges R
-    (void)launch_chain(pdl, k_compact<true>, k_compact<false>, grid_for(tot + 1, 256), 256, 0, st, tot,
-                     c->lpos.as<uint32_t>(), c->tl.as<uint32_t>(), Lp);
-    launches++;
+    tb = c->cub_tmp.cap;
+    RGL_CUDA(cub::DeviceSelect::Flagged(c->cub_tmp.p, tb, thrust::counting_iterator<uint32_t>(0),
+                                        c->rflag.as<uint32_t>(), c->tl.as<uint32_t>(), Lp, (int)tot, st));
     // ranges over the live runs, their candidate counts and methods
     const unsigned gc = (unsigned)std::min<uint64_t>(grid_for(tot, 256), (uint64_t)c->num_sms * 32);
     (void)launch_chain(pdl, k_crange_flags<true>, k_crange_flags<false>, gc, 256, 0, st, Lp, n, c->tl.as<uint32_t>(),
@@ -2375,7 +2374,7 @@ int rgl_context_destroy(rgl_context* c) {
                       &c->rflag, &c->ridx, &c->ranges, &c->rlen, &c->rpos, &c->cub_tmp, &c->small,
                       &c->out_counts, &c->out_bp, &c->item_r0,
                       &c->segtab, &c->tab_len, &c->tab_off, &c->tab_s, &c->tab_e, &c->tab_xs, &c->tab_xe, &c->tab2,
-                      &c->cl, &c->pc, &c->method, &c->lpos, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs, &c->item_t0,
+                      &c->cl, &c->pc, &c->method, &c->tl, &c->scan_sums, &c->plen, &c->ppos, &c->psegs, &c->item_t0,
                       &c->seg_need, &c->item_hits, &c->item_base, &c->pairs, &c->bt_off, &c->bt_shard, &c->acc, &c->gc.t_off, &c->gc.t_shard,
                       &c->cub_tmp2, &c->scan_sums2, &c->sortplan, &c->sort_tab, &c->sort_rank};
     if (c->gc.exec) cudaGraphExecDestroy(c->gc.exec);

@@ -196,13 +196,22 @@ __global__ void k_group_keys(uint64_t n, const rgl_interval* __restrict__ iv, co
                              const uint32_t* __restrict__ shard_chrom, uint32_t nshards, uint32_t C,
                              const uint64_t* __restrict__ n_bins, double bin, int local, uint64_t* __restrict__ key,
                              uint32_t* __restrict__ len_out) {
-    const uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    uint32_t lo = 0, hi = nblk;  // last block with blk_off[b] <= j
-    while (hi - lo > 1) {
-        const uint32_t m = (lo + hi) >> 1;
-        if (blk_off[m] <= j) lo = m; else hi = m;
+    // last block with blk_off[b] <= j: one search per thread block, for its first element, then a
+    // short walk (256 consecutive intervals span few blocks)
+    __shared__ uint32_t s_b0;
+    const uint64_t j0 = blockIdx.x * (uint64_t)blockDim.x, j = j0 + threadIdx.x;
+    if (threadIdx.x == 0) {
+        uint32_t lo = 0, hi = nblk;
+        while (hi - lo > 1) {
+            const uint32_t m = (lo + hi) >> 1;
+            if (blk_off[m] <= j0) lo = m; else hi = m;
+        }
+        s_b0 = lo;
     }
+    __syncthreads();
+    if (j >= n) return;
+    uint32_t lo = s_b0;
+    while (lo + 1 < nblk && blk_off[lo + 1] <= j) lo++;
     const rgl_interval v = iv[j];
     const uint32_t sh = blk_shard[lo];
     const uint32_t c = sh < nshards ? shard_chrom[sh] : 0xFFFFFFFFu;
