@@ -101,3 +101,43 @@ def test_device_batch_groups_match_the_oracle():
             want = O.query_groups(blocks[b][:, 0], blocks[b][:, 1])
             assert_groups_close(per.pop(c), want, int(n_bins[c]))
         assert not per  # no group on a chromosome the file has no intervals on
+
+
+@pytest.mark.gpu
+def test_device_groups_block_local_and_device_wide_forms_agree():
+    """With every (file, chromosome) block in ascending order the length keys are sorted within the
+    blocks (block-local form); with a file's chromosomes in descending order the batch takes the
+    device-wide sort and reduce-by-key.  Both sum exact integers, so the groups must be identical."""
+    import torch
+
+    rng = np.random.default_rng(12)
+    cl = np.array([46_709_983, 50_818_468, 20_000_000], np.uint32)
+    n_bins = (cl.astype(np.uint64) + 99) // 100
+    idx = rg.Index.synth(rg.SynthSpec(3, cl, [2000] * 4))
+    ctx = rg.Context(idx)
+    mom = api.Moments(4, n_bins)
+    per_file = {}
+    for f, n in enumerate([9000, 300, 60_000]):
+        for c in range(len(cl)):
+            iv = intervals(rng, lengths_case(rng, "mixed", n), span=int(cl[c]))
+            iv[:, 2] = f
+            per_file[(f, c)] = iv
+
+    def groups(order):
+        blocks = [per_file[k] for k in order]
+        off = np.zeros(len(blocks) + 1, np.uint64)
+        off[1:] = np.cumsum([len(b) for b in blocks])
+        d_iv = torch.from_numpy(np.concatenate(blocks).view(np.int32)).cuda()
+        batch = rg.DeviceBatch(3, [k[1] for k in order], off, d_iv.data_ptr(), [k[0] for k in order])
+        return mom.batch_query_groups(ctx, batch, np.arange(len(cl), dtype=np.uint32))
+
+    ascending = [(f, c) for f in range(3) for c in range(3)]
+    descending = [(f, c) for f in range(3) for c in reversed(range(3))]
+    a, d = groups(ascending), groups(descending)
+    assert len(a) == len(d) == 3
+    for f in range(3):
+        ga, gd = dict(a[f]), dict(d[f])
+        assert sorted(ga) == sorted(gd)
+        for c in ga:
+            for x, y in zip(ga[c], gd[c]):
+                assert np.array_equal(x, y), (f, c)
