@@ -30,7 +30,6 @@
 //      one row, else with global atomics.
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
-#include <thrust/iterator/transform_iterator.h>
 
 #include <algorithm>
 #include <cstring>
@@ -67,22 +66,6 @@ struct SegTab {
     uint32_t shift, nbins;
     uint32_t off;       // first entry of the segment's tables (nbins + 1 entries each)
     uint32_t pad;
-};
-
-// Key of entry t = K * n + i of the [K][n] arrays: (K, segment of query i).
-struct RowKey {
-    const uint32_t* segnum;
-    uint32_t n;
-    __host__ __device__ __forceinline__ uint64_t operator()(uint32_t t) const {
-        return ((uint64_t)(t / n) << 32) | segnum[t % n];
-    }
-};
-
-// (slot, segment) key of every (slot, query) entry, as an iterator over the entries.
-using RowKeyIter = thrust::transform_iterator<RowKey, thrust::counting_iterator<uint32_t>>;
-
-struct MaxOp {
-    __device__ __forceinline__ uint32_t operator()(uint32_t a, uint32_t b) const { return a > b ? a : b; }
 };
 
 enum : uint32_t { ERR_BAD_INTERVAL = 1u, ERR_BAD_ROW = 2u };
@@ -468,6 +451,114 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const Tin* __restri
     }
 }
 
+// ---- running maximum of hi over the live runs of each (slot, segment) row -----------------------
+// maxc[c] = max of hi over the live entries of entry c's row up to c.  Empty entries never raise the
+// running maximum past a later entry's lo (see 4b), so the maximum over live entries alone decides
+// every range exactly as the maximum over all entries would.  A segmented scan over the L live
+// entries (a device count): per-tile summaries (head seen, maximum since the last head), one block
+// scanning them into each tile's carry, per-tile block scans with the carry.
+struct SegMax {
+    uint32_t f, v;  // f: the span holds a row start; v: maximum since the span's last row start
+};
+struct SegMaxOp {
+    __device__ __forceinline__ SegMax operator()(const SegMax& a, const SegMax& b) const {
+        return SegMax{a.f | b.f, b.f ? b.v : max(a.v, b.v)};
+    }
+};
+
+// Live entry c as a scan item: its hi and whether it starts a (slot, segment) row.
+__device__ __forceinline__ SegMax segmax_item(uint64_t c, const uint32_t* __restrict__ tl, uint32_t n,
+                                              const uint32_t* __restrict__ segnum, const uint32_t* __restrict__ hi) {
+    const uint32_t t = tl[c];
+    bool head = c == 0;
+    if (!head) {
+        const uint32_t tp = tl[c - 1];
+        head = (tp / n != t / n) || (segnum[tp % n] != segnum[t % n]);
+    }
+    return SegMax{head ? 1u : 0u, hi[t]};
+}
+
+template <bool PDL>
+__global__ void __launch_bounds__(kScanThreads) k_segmax_reduce(const uint32_t* __restrict__ Lp, uint32_t n,
+                                                                const uint32_t* __restrict__ tl,
+                                                                const uint32_t* __restrict__ segnum,
+                                                                const uint32_t* __restrict__ hi,
+                                                                unsigned long long* __restrict__ tile_sums) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
+    const uint32_t L = *Lp;
+    using BS = cub::BlockScan<SegMax, kScanThreads>;
+    __shared__ typename BS::TempStorage tmp;
+    for (uint64_t tile = blockIdx.x; tile * kScanTile < L; tile += gridDim.x) {
+        const uint64_t base = tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+        SegMax v[kScanItems];
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++)
+            v[k] = base + k < L ? segmax_item(base + k, tl, n, segnum, hi) : SegMax{0u, 0u};
+        SegMax agg;
+        BS(tmp).InclusiveScan(v, v, SegMaxOp(), agg);
+        if (threadIdx.x == 0) tile_sums[tile] = ((unsigned long long)agg.f << 32) | agg.v;
+        __syncthreads();  // tmp is reused by the next tile
+    }
+}
+
+// tile_sums[t] <- the running maximum carried into tile t (the value before its first row start).
+template <bool PDL>
+__global__ void __launch_bounds__(1024) k_segmax_tops(const uint32_t* __restrict__ Lp,
+                                                      unsigned long long* __restrict__ tile_sums) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
+    const uint32_t L = *Lp;
+    const uint32_t nt = (uint32_t)((L + kScanTile - 1) / kScanTile);
+    using BS = cub::BlockScan<SegMax, 1024>;
+    __shared__ typename BS::TempStorage tmp;
+    SegMax run{0u, 0u};
+    for (uint32_t b0 = 0; b0 < nt; b0 += 1024) {
+        const uint32_t b = b0 + threadIdx.x;
+        const unsigned long long w = b < nt ? tile_sums[b] : 0ull;
+        SegMax v{(uint32_t)(w >> 32), (uint32_t)w}, ex, agg;
+        BS(tmp).ExclusiveScan(v, ex, SegMax{0u, 0u}, SegMaxOp(), agg);
+        const SegMax carry = threadIdx.x ? SegMaxOp()(run, ex) : run;
+        __syncthreads();  // every thread has read its summary before any is overwritten
+        if (b < nt) tile_sums[b] = carry.v;
+        run = SegMaxOp()(run, agg);
+        __syncthreads();
+    }
+}
+
+template <bool PDL>
+__global__ void __launch_bounds__(kScanThreads) k_segmax_apply(const uint32_t* __restrict__ Lp, uint32_t n,
+                                                               const uint32_t* __restrict__ tl,
+                                                               const uint32_t* __restrict__ segnum,
+                                                               const uint32_t* __restrict__ hi,
+                                                               const unsigned long long* __restrict__ carry,
+                                                               uint32_t* __restrict__ maxc) {
+    if constexpr (PDL) {
+        pdl_wait();
+        pdl_release();
+    }
+    const uint32_t L = *Lp;
+    using BS = cub::BlockScan<SegMax, kScanThreads>;
+    __shared__ typename BS::TempStorage tmp;
+    for (uint64_t tile = blockIdx.x; tile * kScanTile < L; tile += gridDim.x) {
+        const uint64_t base = tile * kScanTile + (uint64_t)threadIdx.x * kScanItems;
+        SegMax v[kScanItems];
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++)
+            v[k] = base + k < L ? segmax_item(base + k, tl, n, segnum, hi) : SegMax{0u, 0u};
+        if (threadIdx.x == 0 && !v[0].f) v[0].v = max(v[0].v, (uint32_t)carry[tile]);
+        BS(tmp).InclusiveScan(v, v, SegMaxOp());
+#pragma unroll
+        for (int k = 0; k < kScanItems; k++)
+            if (base + k < L) maxc[base + k] = v[k].v;
+        __syncthreads();  // tmp is reused by the next tile
+    }
+}
+
 // ---- 4b. live candidate runs -------------------------------------------------------------------
 // An entry (K, i) whose run [lo, hi) is empty takes part in nothing: with starts sorted, lo is
 // non-decreasing within a (K, segment) row, so an empty run's hi (= its lo) never exceeds a later
@@ -475,10 +566,9 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(const Tin* __restri
 // c < L, by a flagged selection) and everything after this works on them.  k_lohi writes the live
 // flags with lo and hi.
 
-
 // Range starts among the live runs: the first live run of a (K, segment) row, or one whose lo is
-// past the running maximum of hi (maxhi over the row, which empty runs never raise past a later
-// lo); cl = the run's candidate count.
+// past the running maximum of hi over the row's earlier live runs (maxhi[c - 1]); cl = the run's
+// candidate count.
 template <bool PDL>
 __global__ void k_crange_flags(const uint32_t* __restrict__ Lp, uint32_t n, const uint32_t* __restrict__ tl,
                                const uint32_t* __restrict__ segnum, const uint32_t* __restrict__ lo,
@@ -494,7 +584,7 @@ __global__ void k_crange_flags(const uint32_t* __restrict__ Lp, uint32_t n, cons
         bool start = c == 0;
         if (!start) {
             const uint32_t tp = tl[c - 1];
-            start = (tp / n != t / n) || (segnum[tp % n] != segnum[t % n]) || (lo[t] >= maxhi[t - 1]);
+            start = (tp / n != t / n) || (segnum[tp % n] != segnum[t % n]) || (lo[t] >= maxhi[c - 1]);
         }
         cflag[c] = start ? 1u : 0u;
         ccl[c] = (uint64_t)(hi[t] - lo[t]);
@@ -528,7 +618,7 @@ __global__ void k_crange_emit(const uint32_t* __restrict__ Lp, uint32_t n, uint3
         }
         if (c + 1 == L || cflag[c + 1]) {
             ranges[r].c_last = (uint32_t)c;
-            ranges[r].db_hi = maxhi[t];
+            ranges[r].db_hi = maxhi[c];
         }
     }
 }
@@ -1422,12 +1512,6 @@ int size_workspace(rgl_context* c, uint64_t n, uint32_t rows, uint32_t nblk, uin
     need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint64_t*)nullptr, (uint64_t*)nullptr, nn + 1, c->stream);
     need = std::max(need, b);
-    {
-        RowKeyIter keys(thrust::counting_iterator<uint32_t>(0), RowKey{nullptr, 1});
-        cub::DeviceScan::InclusiveScanByKey(nullptr, b, keys, (uint32_t*)nullptr, (uint32_t*)nullptr, MaxOp(), nt,
-                                            cub::Equality(), c->stream);
-    }
-    need = std::max(need, b);
     cub::DeviceScan::ExclusiveSum(nullptr, b, (uint32_t*)nullptr, (uint32_t*)nullptr, nt, c->stream);
     need = std::max(need, b);
     cub::DeviceSelect::Flagged(nullptr, b, thrust::counting_iterator<uint32_t>(0), (const uint32_t*)nullptr,
@@ -1831,13 +1915,6 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
                                                 idx->d_btab, c->lo.as<uint32_t>(), c->hi.as<uint32_t>(),
                                                 c->rflag.as<uint32_t>());
     launches++;
-    {  // running max of hi along every (slot, segment) row: one scan keyed by (slot, segment)
-        RowKeyIter keys(thrust::counting_iterator<uint32_t>(0), RowKey{c->segnum.as<uint32_t>(), n});
-        tb = c->cub_tmp.cap;
-        RGL_CUDA(cub::DeviceScan::InclusiveScanByKey(c->cub_tmp.p, tb, keys, c->hi.as<uint32_t>(),
-                                                     c->maxhi.as<uint32_t>(), MaxOp(), (int)tot, cub::Equality(),
-                                                     st));
-    }
     // live runs: compaction of the (K, query) entries with a non-empty candidate run (flags from
     // k_lohi) in one pass: tl[c] = t of the c-th live entry, *Lp = their number
     uint32_t* Lp = d_small + 8;  // live runs L
@@ -1845,6 +1922,17 @@ int run_pipeline(rgl_context* c, const PipeIn& in, const rgl_query_opts* opts, u
     tb = c->cub_tmp.cap;
     RGL_CUDA(cub::DeviceSelect::Flagged(c->cub_tmp.p, tb, thrust::counting_iterator<uint32_t>(0),
                                         c->rflag.as<uint32_t>(), c->tl.as<uint32_t>(), Lp, (int)tot, st));
+    {  // running max of hi along every (slot, segment) row, over the live runs: maxhi[c]
+        unsigned long long* sums = c->scan_sums.as<unsigned long long>();
+        const unsigned g = (unsigned)std::min<uint64_t>(tot / kScanTile + 1, 148ull * 8);
+        (void)launch_chain(pdl, k_segmax_reduce<true>, k_segmax_reduce<false>, g, kScanThreads, 0, st, Lp, n,
+                           c->tl.as<uint32_t>(), c->segnum.as<uint32_t>(), c->hi.as<uint32_t>(), sums);
+        (void)launch_chain(pdl, k_segmax_tops<true>, k_segmax_tops<false>, 1, 1024, 0, st, Lp, sums);
+        (void)launch_chain(pdl, k_segmax_apply<true>, k_segmax_apply<false>, g, kScanThreads, 0, st, Lp, n,
+                           c->tl.as<uint32_t>(), c->segnum.as<uint32_t>(), c->hi.as<uint32_t>(), sums,
+                           c->maxhi.as<uint32_t>());
+        launches += 3;
+    }
     // ranges over the live runs, their candidate counts and methods
     const unsigned gc = (unsigned)std::min<uint64_t>(grid_for(tot, 256), (uint64_t)c->num_sms * 32);
     (void)launch_chain(pdl, k_crange_flags<true>, k_crange_flags<false>, gc, 256, 0, st, Lp, n, c->tl.as<uint32_t>(),
