@@ -10,13 +10,18 @@ One JSON line with three parts:
     query file of 1e5 intervals per step (a different seeded file every step).  A step is one pass of
     the hot path: sort the query file, partition the candidate ranges, sweep and tally the 1 x 1000
     count vector and overlap base pairs.  Carries roofline, cpu_baseline, e2e and clocks.
-  "batched": 4,096 query files (log-uniform [1e2, 1e6] intervals, 10% in 1 Mbp hot spots) against
-    the 64-file x 50k database in one call (CUDA graph replay, autotuned launch shape), next to the
-    plain form on the same files (one call per file), with the results compared cell by cell.
+  "batched" / "batched_2e9": 4,096 query files (log-uniform [1e2, 1e6] intervals, 10% in 1 Mbp hot
+    spots, sorted by start within each chromosome) against the 64-file x 50k database and against
+    the 2e9-interval database, in one call (CUDA graph replay; autotuned launch shape against the
+    small database), next to the plain form on the same files (one call per file), with the results
+    compared cell by cell; the same files in generation order beside; the stats stage (FP64 p-value
+    of every cell) and the host-input form.
   "serving": Poisson arrivals at 200 query files/s (log-uniform [1e3, 1e6] intervals) against the
-    resident 64-file database through the request server: p50/p99/p99.9 latency and sustained rate,
-    continuous batching vs one query file per launch; "high_load" repeats it at 1,000 files/s, where
-    one file per launch can no longer keep up.
+    resident 2e9-interval database through the request server, with p-values: p50/p99/p99.9 latency
+    and sustained rate, continuous batching vs one query file per launch; "high_load" repeats it at
+    twice the rate and "overload" at four times, beyond what one file per launch sustains.
+  "precision": FFT sliding-window moments at 2^20..2^26 FFT points in FP64 and compensated FP32,
+    errors against the oracle's exact moments.
 
 "intervals swept" = query intervals + database intervals in the union of the reference's candidate
 ranges [q.start - layer_max_K, q.end) over all (shard, layer), per query file (computed by the
@@ -767,12 +772,13 @@ def synthetic_moments(D, cl, file_sizes, device):
 
 
 def run_serving(args, dev, idx, db_desc, moments=None):
-    """Serving at the configured rate, then at twice it (a shorter trace, near the plain form's
-    capacity against the 2e9-interval database): continuous batching against one query file per
-    launch on the same arrivals."""
+    """Serving at the configured rate, at twice it and at four times it (shorter traces; four times
+    is beyond what one file per launch sustains against the 2e9-interval database): continuous
+    batching against one query file per launch on the same arrivals."""
     base = serve_once(args, dev, idx, args.serve_rate, args.serve_seconds, 77, db_desc, moments)
     high = serve_once(args, dev, idx, 2 * args.serve_rate, max(1.0, args.serve_seconds / 2.5), 78, db_desc, moments)
-    return dict(base, high_load=high)
+    over = serve_once(args, dev, idx, 4 * args.serve_rate, max(1.0, args.serve_seconds / 4), 79, db_desc, moments)
+    return dict(base, high_load=high, overload=over)
 
 
 def serve_once(args, dev, idx, lam, T, seed, db_desc, moments):
