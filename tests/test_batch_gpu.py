@@ -418,3 +418,43 @@ def test_work_order_and_tally_modes_agree_with_the_oracle(seed):
     assert swept[16] >= swept[24] >= swept[rg._lib.RGL_BATCH_NO_REGIONS]
     ctx.close()
     idx.close()
+
+
+def test_batch_blocks_in_any_order_and_of_many_tiles():
+    """Blocks handed over in a shuffled order (rows and shards interleaved), some of them several
+    sort tiles long, some already sorted by start: the block-local key sort lays the keys out in
+    segment order and must give the oracle's counts and overlaps, in one sub-batch and in several."""
+    rng = np.random.default_rng(21)
+    D, nsh = 19, 3
+    dbs = [(sh, helpers.random_db(rng, int(rng.integers(5000, 20000)), 3_000_000, D)) for sh in range(nsh)]
+    layers = rg.bucket_layers(dbs)
+    files = []
+    for f in range(9):
+        per = {}
+        for sh, b in dbs:
+            n = int(rng.choice([0, 50, 4096, 4097, 9000, 20000]))
+            if n == 0:
+                continue
+            q = np.concatenate([helpers.queries_touching(rng, b, n // 2, 1), helpers.random_db(rng, n - n // 2, 3_000_000, 1)])
+            if rng.random() < 0.5:
+                q = q[np.lexsort((q[:, 1], q[:, 0]))]
+            q[:, 2] = f
+            per[sh] = q
+        files.append(per)
+    oc, obp = _oracle(layers, files, D, nsh)
+    idx = rg.Index.from_layers(layers, D, [f"s{i}" for i in range(nsh)])
+    ctx = rg.Context(idx)
+    keys = [(f, sh) for f, per in enumerate(files) for sh in per]
+    order = [keys[k] for k in rng.permutation(len(keys))]
+    parts = [files[f][sh] for f, sh in order]
+    offs = np.zeros(len(parts) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(a) for a in parts])
+    iv = np.concatenate(parts)
+    t, p = _dev(iv)
+    b = rg.DeviceBatch(len(files), np.array([sh for _, sh in order], np.uint32), offs, p,
+                       np.array([f for f, _ in order], np.uint32))
+    for sub in (0, 30011):
+        c, bp, _ = _run(ctx, b, D, sub_batch=sub)
+        assert (c == oc).all() and (bp == obp).all(), sub
+    ctx.close()
+    idx.close()
